@@ -1,0 +1,223 @@
+// tp_apply.cu -- matrix-free operator apply and the standalone multi-column CSR apply.
+//
+// Matrix-free (replaces gpu/ceed_operators.py CeedDiffusionMassOp / DiffMassBilinear,
+// :87-108, 247-353): one thread per cell gathers its 4 vertex coordinates with
+// 32-byte loads, recomputes J, det J and the cofactor rows c_k = (J^-1 row k) det J in
+// FP64, and applies, for every column s,
+//     y_i += scale (c_i . w) + react M_e u,    w = sum_k (u_k - u_0) c_k
+// with scale = De/(6|det J|) (exact P1 stiffness) or 4 De/det^2 (legacy: the reference
+// QFunction drops wdetJ), and consistent (|det|/120 (1+d_ij)) or lumped (|det|/24) mass.
+// Contributions land with hardware atomics (FP32 columns as one 16-byte vector atomic),
+// so the result's last bits depend on arrival order, as in the reference.
+#include "tp_ops.cuh"
+
+namespace tp {
+
+template <typename T, int LD>
+__global__ void __launch_bounds__(256) k_matfree(
+    int64_t n, const int4* __restrict__ cells, const double4* __restrict__ X,
+    const double* __restrict__ De, const double* __restrict__ alpha, double4 dsc, double4 shf,
+    double inv_dt, int S, int lumped, int legacy, const T* __restrict__ x, T* __restrict__ y) {
+  const double dscale[4] = {dsc.x, dsc.y, dsc.z, dsc.w};
+  const double shift[4] = {shf.x, shf.y, shf.z, shf.w};
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    const int4 v = cells[c];
+    const double4 x0 = ldg_d4(X + v.x), x1 = ldg_d4(X + v.y), x2 = ldg_d4(X + v.z),
+                  x3 = ldg_d4(X + v.w);
+    const double e[3][3] = {{x1.x - x0.x, x1.y - x0.y, x1.z - x0.z},
+                            {x2.x - x0.x, x2.y - x0.y, x2.z - x0.z},
+                            {x3.x - x0.x, x3.y - x0.y, x3.z - x0.z}};
+    double cr[3][3];  // cr[k] = row k of adj(J): e2 x e3, e3 x e1, e1 x e2
+    cr[0][0] = e[1][1] * e[2][2] - e[1][2] * e[2][1];
+    cr[0][1] = e[1][2] * e[2][0] - e[1][0] * e[2][2];
+    cr[0][2] = e[1][0] * e[2][1] - e[1][1] * e[2][0];
+    cr[1][0] = e[2][1] * e[0][2] - e[2][2] * e[0][1];
+    cr[1][1] = e[2][2] * e[0][0] - e[2][0] * e[0][2];
+    cr[1][2] = e[2][0] * e[0][1] - e[2][1] * e[0][0];
+    cr[2][0] = e[0][1] * e[1][2] - e[0][2] * e[1][1];
+    cr[2][1] = e[0][2] * e[1][0] - e[0][0] * e[1][2];
+    cr[2][2] = e[0][0] * e[1][1] - e[0][1] * e[1][0];
+    const double det = e[0][0] * cr[0][0] + e[0][1] * cr[0][1] + e[0][2] * cr[0][2];
+    const double adet = fabs(det);
+    const double De_c = De[c];
+    const double kbase = legacy ? 4.0 * De_c / (det * det) : De_c / (6.0 * adet);
+    const double mbase = lumped ? adet / 24.0 : adet / 120.0;
+    const double al = alpha ? alpha[c] : 0.0;
+    T c_[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+      for (int b = 0; b < 3; b++) c_[a][b] = (T)cr[a][b];
+    T xv[4][LD];
+    ldv<T, LD>(x, v.x, xv[0]);
+    ldv<T, LD>(x, v.y, xv[1]);
+    ldv<T, LD>(x, v.z, xv[2]);
+    ldv<T, LD>(x, v.w, xv[3]);
+    T out[4][LD];
+#pragma unroll
+    for (int s = 0; s < LD; s++) {
+      if (s >= S) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) out[i][s] = T(0);
+        continue;
+      }
+      const T ks = (T)(kbase * dscale[s]);
+      const T ms = (T)(mbase * (inv_dt + al + shift[s]));
+      const T d1 = xv[1][s] - xv[0][s], d2 = xv[2][s] - xv[0][s], d3 = xv[3][s] - xv[0][s];
+      T w[3];
+#pragma unroll
+      for (int b = 0; b < 3; b++) w[b] = d1 * c_[0][b] + d2 * c_[1][b] + d3 * c_[2][b];
+      T yk[4];
+#pragma unroll
+      for (int i = 1; i < 4; i++)
+        yk[i] = ks * (c_[i - 1][0] * w[0] + c_[i - 1][1] * w[1] + c_[i - 1][2] * w[2]);
+      yk[0] = -(yk[1] + yk[2] + yk[3]);
+      if (lumped) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) out[i][s] = yk[i] + ms * xv[i][s];
+      } else {
+        const T su = xv[0][s] + xv[1][s] + xv[2][s] + xv[3][s];
+#pragma unroll
+        for (int i = 0; i < 4; i++) out[i][s] = yk[i] + ms * (su + xv[i][s]);
+      }
+    }
+    const int vid[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      T* dst = y + (int64_t)vid[i] * LD;
+      if constexpr (sizeof(T) == 4 && LD == 4) {
+        atomicAdd(reinterpret_cast<float4*>(dst),
+                  make_float4(out[i][0], out[i][1], out[i][2], out[i][3]));
+      } else {
+#pragma unroll
+        for (int s = 0; s < LD; s++)
+          if (s < S) atomicAdd(dst + s, out[i][s]);
+      }
+    }
+  }
+}
+
+template <typename T, int LD, int G>
+__global__ void __launch_bounds__(256) k_csr_apply(int64_t n, CsrView<T> A,
+                                                   const T* __restrict__ x, T* __restrict__ y) {
+  const int gl = threadIdx.x % G;
+  const int64_t rpb = blockDim.x / G;
+  for (int64_t base = blockIdx.x * rpb; base < n; base += (int64_t)gridDim.x * rpb) {
+    const int64_t row = base + threadIdx.x / G;
+    const int64_t rr = row < n ? row : n - 1;
+    T out[LD];
+    csr_row<T, LD, G, true>(A, rr, gl, x, out);
+    if (row < n && gl == 0) stv<T, LD>(y, row, out);
+  }
+}
+
+template <typename T>
+static int launch_matfree(const tp_mesh* m, int S, int ld, const double* De, const double* al,
+                          double4 dsc, double4 shf, double inv_dt, int lumped, int legacy,
+                          const void* x, void* y, cudaStream_t st) {
+  const int grid = grid_for(m->n_cells, 256, sm_count() * 8);
+  const int4* cells = reinterpret_cast<const int4*>(m->cells);
+  const double4* X = reinterpret_cast<const double4*>(m->coords4);
+  const T* xx = static_cast<const T*>(x);
+  T* yy = static_cast<T*>(y);
+  switch (ld) {
+    case 1:
+      k_matfree<T, 1><<<grid, 256, 0, st>>>(m->n_cells, cells, X, De, al, dsc, shf, inv_dt, S,
+                                            lumped, legacy, xx, yy);
+      break;
+    case 2:
+      k_matfree<T, 2><<<grid, 256, 0, st>>>(m->n_cells, cells, X, De, al, dsc, shf, inv_dt, S,
+                                            lumped, legacy, xx, yy);
+      break;
+    case 4:
+      k_matfree<T, 4><<<grid, 256, 0, st>>>(m->n_cells, cells, X, De, al, dsc, shf, inv_dt, S,
+                                            lumped, legacy, xx, yy);
+      break;
+    default:
+      set_error("ld must be 1, 2 or 4");
+      return TP_ERR_ARG;
+  }
+  TP_LAUNCH_CHECK();
+  return TP_OK;
+}
+
+template <typename T>
+static CsrView<T> make_view(const tp_csr_op* op, bool fp32) {
+  CsrView<T> v;
+  v.indptr = op->indptr;
+  v.indices = op->indices;
+  if constexpr (sizeof(T) == 4) {
+    v.K = op->K32;
+    v.M = op->M32;
+    v.diag = op->diag32;
+  } else {
+    v.K = op->K64;
+    v.M = op->M64;
+    v.diag = op->diag64;
+  }
+  (void)fp32;
+  v.bc = op->bc_mask;
+  for (int s = 0; s < 4; s++) {
+    v.dscale[s] = s < op->S ? op->dscale[s] : 0.0;
+    v.cscale[s] = s < op->S ? op->cscale[s] : 0.0;
+  }
+  return v;
+}
+
+template <typename T, int LD>
+static void launch_csr(const tp_csr_op* op, const void* x, void* y, cudaStream_t st) {
+  constexpr int G = 4;
+  const int64_t n = op->n_rows;
+  const int grid = grid_for(n * G, 256, sm_count() * 8);
+  k_csr_apply<T, LD, G><<<grid, 256, 0, st>>>(n, make_view<T>(op, sizeof(T) == 4),
+                                              static_cast<const T*>(x), static_cast<T*>(y));
+}
+
+}  // namespace tp
+
+using namespace tp;
+
+extern "C" int tp_matfree_apply(const tp_mesh* m, int S, int ld, int fp32, const double* De_cell,
+                                const double* alpha_cell, const double* diff_scale,
+                                const double* shift, double inv_dt, int lumped, int legacy,
+                                const void* x, void* y, void* stream) {
+  TP_REQUIRE(m && m->cells && m->coords4 && De_cell && x && y, "null pointer");
+  TP_REQUIRE(S >= 1 && S <= TP_MAX_COLS && (ld == 1 || ld == 2 || ld == 4) && ld >= S,
+             "bad S/ld");
+  cudaStream_t st = as_stream(stream);
+  const size_t esz = fp32 ? 4 : 8;
+  TP_CUDA_TRY(cudaMemsetAsync(y, 0, esz * ld * (size_t)m->n_verts, st));
+  if (m->n_cells == 0) return TP_OK;
+  double d[4] = {1, 1, 1, 1}, s[4] = {0, 0, 0, 0};
+  for (int i = 0; i < S; i++) {
+    if (diff_scale) d[i] = diff_scale[i];
+    if (shift) s[i] = shift[i];
+  }
+  const double4 dsc = make_double4(d[0], d[1], d[2], d[3]);
+  const double4 shf = make_double4(s[0], s[1], s[2], s[3]);
+  if (fp32)
+    return launch_matfree<float>(m, S, ld, De_cell, alpha_cell, dsc, shf, inv_dt, lumped, legacy,
+                                 x, y, st);
+  return launch_matfree<double>(m, S, ld, De_cell, alpha_cell, dsc, shf, inv_dt, lumped, legacy,
+                                x, y, st);
+}
+
+extern "C" int tp_csr_apply(const tp_csr_op* op, int fp32, const void* x, void* y, void* stream) {
+  TP_REQUIRE(op && op->indptr && op->indices && x && y, "null pointer");
+  TP_REQUIRE(fp32 ? (op->K32 != nullptr) : (op->K64 != nullptr), "operator values missing");
+  TP_REQUIRE(op->ld == 1 || op->ld == 2 || op->ld == 4, "ld must be 1, 2 or 4");
+  if (op->n_rows == 0) return TP_OK;
+  cudaStream_t st = as_stream(stream);
+  if (fp32) {
+    if (op->ld == 1) launch_csr<float, 1>(op, x, y, st);
+    else if (op->ld == 2) launch_csr<float, 2>(op, x, y, st);
+    else launch_csr<float, 4>(op, x, y, st);
+  } else {
+    if (op->ld == 1) launch_csr<double, 1>(op, x, y, st);
+    else if (op->ld == 2) launch_csr<double, 2>(op, x, y, st);
+    else launch_csr<double, 4>(op, x, y, st);
+  }
+  TP_LAUNCH_CHECK();
+  return TP_OK;
+}

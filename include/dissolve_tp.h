@@ -1,0 +1,278 @@
+/*
+ * dissolve_tp.h -- C ABI of the B200 P1-tetrahedral reaction-diffusion transport path.
+ *
+ * Plain C: every pointer is device memory owned by the caller unless marked (host),
+ * sizes are int64_t, `stream` is a cudaStream_t passed as void* (NULL = legacy
+ * default stream).  Every entry point returns TP_OK or a TP_ERR_* code;
+ * tp_last_error() gives the detail text of the last failure on the calling thread.
+ * Functions marked [sync] synchronise `stream` before returning (they validate
+ * input on the device and report through the return code); all others only
+ * enqueue work on `stream`.
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   gpu/gpu_assembler.py   GPUSparseAssembler and its five NVRTC kernels
+ *   gpu/ceed_operators.py  CeedDiffusionMassOp (libCEED matrix-free operator)
+ *   numerics/solvers.py    _solve_gpu_asm's PETSc KSP solve
+ *   dissolve.py            per-species coefficient builders (CuPy elementwise)
+ * The Python module dissolve_tp (dissolve-2.0_b200/) binds these through ctypes and
+ * keeps the reference's Python call signatures on top.
+ */
+#ifndef DISSOLVE_TP_H
+#define DISSOLVE_TP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define TP_API __attribute__((visibility("default")))
+#else
+#define TP_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status codes */
+#define TP_OK 0
+#define TP_ERR_ARG 1          /* invalid argument (null pointer, size, option)        */
+#define TP_ERR_CUDA 2         /* CUDA runtime error                                   */
+#define TP_ERR_INDEX 3        /* a vertex or dof id outside [0, n_verts)              */
+#define TP_ERR_DEGENERATE 4   /* a cell with det J == 0 or non-finite coordinates     */
+#define TP_ERR_CAPACITY 5     /* a CSR row or vertex degree beyond the kernel limits  */
+#define TP_ERR_NOT_CONVERGED 6 /* Krylov solve stopped at max_it                      */
+#define TP_ERR_BREAKDOWN 7    /* p.Ap <= 0: operator not SPD on the free dofs         */
+#define TP_ERR_NONFINITE 8    /* NaN/Inf in a Krylov scalar                           */
+
+/* assembly modes for tp_assemble_csr */
+#define TP_ASM_FULL 0   /* De K + (inv_dt + alpha) M  (gpu_assembler.py:60-139)      */
+#define TP_ASM_STIFF 1  /* De K only (shared stiffness for multi-species operators) */
+#define TP_ASM_MASS 2   /* M only, coefficient 1 (consistent or lumped)             */
+
+#define TP_MAX_COLS 4   /* right-hand sides per multi-column operator/solve          */
+
+TP_API int tp_version(void);
+TP_API const char* tp_status_string(int status);
+TP_API const char* tp_last_error(void);
+TP_API int tp_device_sm_count(void);
+
+/* ------------------------------------------------------------------ mesh on device */
+/* Device-resident mesh: the state GPUSparseAssembler keeps between calls
+ * (gpu_assembler.py:323-326, 350-367).  Built once by the setup calls below. */
+typedef struct tp_mesh {
+  int64_t n_cells;
+  int64_t n_verts;
+  int64_t nnz;
+  int32_t max_row_len;        /* longest CSR row (<= 255)                            */
+  int32_t max_degree;         /* most cells sharing one vertex                       */
+  const int32_t* cells;       /* (n_cells, 4) vertex ids = P1 dofs                   */
+  const double* coords4;      /* (n_verts, 4) x, y, z, 0 (32-byte rows)              */
+  const double* geo;          /* (n_cells, 8) G00 G01 G02 G11 G12 G22 |detJ| 0       */
+  const int32_t* v2c_ptr;     /* (n_verts + 1) incidence offsets                     */
+  const int32_t* v2c;         /* (4 n_cells) cell*4 + local index, ascending cell    */
+  const uint32_t* v2c_slots;  /* (4 n_cells) row-local CSR slot of the cell's 4 vertices,
+                                 byte j = slot of vertex j in the incidence row      */
+  const int32_t* indptr;      /* (n_verts + 1) CSR row offsets                       */
+  const int32_t* indices;     /* (nnz) sorted column ids                             */
+} tp_mesh;
+
+/* [sync] Per-cell geometry of gpu_assembler.py:380-393: J = [x1-x0 | x2-x0 | x3-x0],
+ * detJ = |det J|, G = J^-1 J^-T and J^-T, all row-major, plus the compact 64-byte record
+ * `geo` and the padded coordinate copy `coords4` the kernels read.  detJ, Gflat, JinvT
+ * and coords4 may be NULL.  flags_dev: 1 int32 of device scratch.
+ * Returns TP_ERR_INDEX / TP_ERR_DEGENERATE on bad cells. */
+TP_API int tp_cell_geometry(int64_t n_cells, int64_t n_verts, const int32_t* cells,
+                     const double* coords, double* coords4, double* geo, double* detJ,
+                     double* Gflat, double* JinvT, int32_t* flags_dev, void* stream);
+
+/* [sync] Compact record from the reference-layout arrays (detJ (n), Gflat (n, 9)), so the
+ * assembly can run on geometry computed elsewhere (gpu_assembler.py:380-386 numpy). */
+TP_API int tp_pack_geometry(int64_t n_cells, const double* detJ, const double* Gflat, double* geo,
+                     void* stream);
+
+/* bytes of device scratch the setup calls below need */
+TP_API size_t tp_setup_scratch_bytes(int64_t n_cells, int64_t n_verts);
+
+/* [sync] Vertex -> cell incidence (ascending cell id per vertex).  Replaces the
+ * per-row Python sets of gpu_assembler.py:396-400. */
+TP_API int tp_incidence(int64_t n_cells, int64_t n_verts, const int32_t* cells, int32_t* v2c_ptr,
+                 int32_t* v2c, void* scratch, int32_t* max_degree_out /* host */,
+                 void* stream);
+
+/* [sync] CSR sparsity of gpu_assembler.py:396-410: row r = sorted set of every vertex
+ * sharing a cell with r, r included.  Call once with indices == NULL (fills indptr,
+ * returns nnz), then with indices allocated to nnz. */
+TP_API int tp_pattern(int64_t n_cells, int64_t n_verts, const int32_t* cells, const int32_t* v2c_ptr,
+               const int32_t* v2c, int32_t max_degree, int32_t* indptr, int32_t* indices,
+               void* scratch, int64_t* nnz_out /* host */,
+               int32_t* max_row_len_out /* host */, void* stream);
+
+/* gpu_assembler.py:419-438: scatter_map[c*16 + i*4 + j] = CSR position of
+ * (cells[c,i], cells[c,j]). */
+TP_API int tp_scatter_map(int64_t n_cells, const int32_t* cells, const int32_t* indptr,
+                   const int32_t* indices, int32_t* scatter_map, void* stream);
+
+/* [sync] Row-local slots of every incidence entry (no reference counterpart: this is
+ * the element-to-nonzero map the atomics-free row assembly reads instead of the
+ * reference's scatter_map + atomicAdd). */
+TP_API int tp_incidence_slots(const tp_mesh* m, uint32_t* slots, int32_t* flags_dev, void* stream);
+
+/* ------------------------------------------------------------------ per-step kernels */
+/* gpu_assembler.py:452-470 (_to_cell_avg, per-vertex branch): mean of 4 vertex values */
+TP_API int tp_cell_average(int64_t n_cells, const int32_t* cells, const double* vert_vals,
+                    double* cell_vals, void* stream);
+
+/* [sync] mask[v] = 1 for v in bc_dofs, 0 elsewhere (mask is cleared first).
+ * TP_ERR_INDEX if a dof is outside [0, n_verts). */
+TP_API int tp_bc_mask(int64_t n_bc, const int32_t* bc_dofs, int64_t n_verts, uint8_t* mask,
+               int32_t* flags_dev, void* stream);
+
+/* gpu_assembler.py:60-139 (+ :147-165 when bc_mask != NULL) without atomics: each CSR
+ * row sums its incident cells in ascending cell order, in the reference's operation
+ * order, so the result equals the reference kernel run in cell order.  mode TP_ASM_*;
+ * De_cell per cell; alpha_cell per cell or NULL (0).  out64 / out32: either may be NULL. */
+TP_API int tp_assemble_csr(const tp_mesh* m, const double* De_cell, const double* alpha_cell,
+                    double inv_dt, int lumped, int mode, const uint8_t* bc_mask,
+                    double* out64, float* out32, void* stream);
+
+/* gpu_assembler.py:147-165 on its own: rows of bc_dofs become identity rows (ids outside
+ * [0, n_rows) are skipped) */
+TP_API int tp_dirichlet_rows(int64_t n_bc, const int32_t* bc_dofs, int64_t n_rows,
+                             const int32_t* indptr, const int32_t* indices, double* data,
+                             void* stream);
+
+/* Lumped-mass diagonal per column: diag[v, s] = sum_{c at v} (shift[s] + alpha[c, s])
+ * |detJ_c|/24; alpha (n_cells, ld) or NULL; shift (host, S).  diag64/diag32 (n_verts, ld),
+ * either may be NULL; bc rows (bc_mask != 0) get 1. */
+TP_API int tp_lumped_diag(const tp_mesh* m, int S, int ld, const double* alpha, const double* shift,
+                   const uint8_t* bc_mask, double* diag64, float* diag32, void* stream);
+
+/* gpu_assembler.py:176-221 + :228-239 for S columns (interleaved, leading dim ld):
+ * b = M (inv_dt u_old + f) lumped or consistent, then b[bc_dofs, s] = bc_value[s]
+ * (host array of S values; bc_dofs may be NULL).  f may be NULL (zero source). */
+TP_API int tp_assemble_rhs(const tp_mesh* m, int S, int ld, const double* u_old, const double* f,
+                    double inv_dt, int lumped, int64_t n_bc, const int32_t* bc_dofs,
+                    const double* bc_value, double* b, void* stream);
+
+/* gpu_assembler.py:251-304, 646-673: volume-weighted vertex average of the cellwise
+ * gradient.  JinvT (n_cells, 9) as the reference stores it, or NULL to recompute J^-T
+ * from coords4.  grad (n_verts, 3). */
+TP_API int tp_nodal_gradient(const tp_mesh* m, const double* JinvT, const double* u, double* grad,
+                      void* stream);
+
+/* gpu_assembler.py:605-644: integral of the smoothed Heaviside H_eps(phi) with the
+ * 4-point degree-2 rule.  out_dev: 1 double (device). scratch >= tp_setup_scratch_bytes. */
+TP_API int tp_scaffold_volume(const tp_mesh* m, const double* phi, double eps, double* out_dev,
+                       void* scratch, void* stream);
+
+/* dissolve.py:866-875: alpha_O2 = delta_eps(phi) |grad phi| k_orr (per vertex) */
+TP_API int tp_o2_alpha(int64_t n, const double* phi, const double* normgradphi, double eps,
+                double k_orr, double* alpha, void* stream);
+
+/* dissolve.py:923-936: f_OH = [phi <= 0] kd F Cl^2 + orr_factor delta_eps |grad phi| k_orr O2 */
+TP_API int tp_oh_source(int64_t n, const double* phi, const double* normgradphi, const double* F,
+                 const double* Cl, const double* O2, double eps, double kd, double k_orr,
+                 double orr_factor, double* f, void* stream);
+
+/* y = a x + b y (n doubles): numerics/solvers.py:278-279 under-relaxation */
+TP_API int tp_axpby(int64_t n, double a, const double* x, double b, double* y, void* stream);
+
+/* ------------------------------------------------------------------ operators */
+/* gpu/ceed_operators.py:87-108, 247-353 as intended, on S interleaved columns:
+ * y[:, s] = sum_e [diff_scale[s] De_e K_e + (inv_dt + alpha_e + shift[s]) M_e] x_e[:, s]
+ * recomputing the P1 gradients of every cell from coords4 in FP64.  legacy != 0 weights
+ * the stiffness by 4 (the reference QFunction omits wdetJ, :101-104) instead of |detJ|/6.
+ * fp32 != 0: x, y float (geometry still FP64).  diff_scale/shift: host, S values, or NULL.
+ * y is overwritten. */
+TP_API int tp_matfree_apply(const tp_mesh* m, int S, int ld, int fp32, const double* De_cell,
+                     const double* alpha_cell, const double* diff_scale, const double* shift,
+                     double inv_dt, int lumped, int legacy, const void* x, void* y,
+                     void* stream);
+
+/* Multi-column CSR operator: y[:, s] = dscale[s] (K x)[:, s] + cscale[s] (M x)[:, s]
+ * + diag[:, s] .* x[:, s], with K and M sharing the CSR pattern (M may be NULL).
+ * val32/val64 hold the same matrix in FP32/FP64 (inner and outer operator of the
+ * mixed-precision solve).  Rows with bc_mask != 0 are identity rows. */
+typedef struct tp_csr_op {
+  int64_t n_rows;
+  int32_t S;            /* columns in use, 1..4                                 */
+  int32_t ld;           /* interleave stride: 1, 2 or 4                         */
+  const int32_t* indptr;
+  const int32_t* indices;
+  const double* K64;    /* (nnz) */
+  const float* K32;     /* (nnz) or NULL when the solve is FP64 only            */
+  const double* M64;    /* (nnz) or NULL */
+  const float* M32;
+  const double* diag64; /* (n_rows, ld) or NULL */
+  const float* diag32;
+  const uint8_t* bc_mask; /* (n_rows) or NULL */
+  double dscale[TP_MAX_COLS];
+  double cscale[TP_MAX_COLS];
+  /* independent systems solved together (block-diagonal union), rows contiguous:
+     sys_row_ptr (n_systems + 1, host); n_systems = 1 for a single mesh */
+  int32_t n_systems;
+  const int64_t* sys_row_ptr;
+} tp_csr_op;
+
+/* y = A x with the FP64 (fp32 = 0) or FP32 (fp32 = 1) values of op */
+TP_API int tp_csr_apply(const tp_csr_op* op, int fp32, const void* x, void* y, void* stream);
+
+/* ------------------------------------------------------------------ Krylov solve */
+/* Jacobi-preconditioned CG on every (system, column) lane at once, captured in a CUDA
+ * graph whose device-side while loop runs until every lane converges or max_it.
+ * Replaces KSP(gmres, restart 50) + PC(bjacobi) of numerics/solvers.py:322-335, 369 on
+ * the symmetric free block (Dirichlet rows are identity rows; the preconditioner is zero
+ * there).  Stopping rule per lane: ||b - A x||_2 <= rtol ||b||_2 in FP64.
+ * inner_fp32 = 1: the iteration (operator, vectors) runs in FP32 and FP64 reliable
+ * updates (x += x_inner, r = b - A x recomputed with the FP64 operator) happen whenever
+ * the FP32 residual falls below `delta` times its value at the last update, or below the
+ * tolerance; convergence is only ever declared on the FP64 residual.  Dot products and
+ * norms accumulate in FP64 in both modes. */
+typedef struct tp_cg_config {
+  int32_t max_it;
+  int32_t inner_fp32;
+  double delta;          /* reliable-update ratio (FP32 inner); <= 0 -> 0.1         */
+  int32_t group;         /* threads per CSR row: 1, 2, 4, 8 (autotuned)             */
+  int32_t block;         /* threads per block: 128 or 256                           */
+  int32_t rows_per_tile; /* rows per reduction tile (multiple of block/group)        */
+  int32_t use_graph_loop;/* 1: conditional-node while loop; 0: host loop            */
+} tp_cg_config;
+
+typedef struct tp_cg_result {
+  int32_t status;        /* TP_OK if every lane converged                            */
+  int32_t iterations;    /* iterations of the longest lane                           */
+  int32_t n_reliable;    /* FP64 residual recomputations                             */
+  int32_t n_lanes;
+} tp_cg_result;
+
+typedef struct tp_cg_handle tp_cg_handle;
+
+/* bytes of device workspace a handle needs */
+TP_API size_t tp_cg_workspace_bytes(const tp_csr_op* op, const tp_cg_config* cfg);
+
+/* Build a solver for fixed buffers: b (n_rows, ld) FP64 right-hand sides, x (n_rows, ld)
+ * FP64 initial guess in / solution out, rtol (n_systems * S lanes, device doubles,
+ * lane = system * S + column).  The op arrays, b, x, rtol and workspace must stay valid
+ * and unmoved for the handle's lifetime; their contents may change between runs. */
+TP_API int tp_cg_create(const tp_csr_op* op, const tp_cg_config* cfg, const double* b, double* x,
+                 const double* rtol, void* workspace, size_t workspace_bytes, void* stream,
+                 tp_cg_handle** out);
+
+/* enqueue one solve (recomputes the Jacobi diagonal from the current values) */
+TP_API int tp_cg_run(tp_cg_handle* h, void* stream);
+
+/* [sync] summary of the last run, plus per-lane arrays (host, n_lanes each, any NULL) */
+TP_API int tp_cg_result_get(tp_cg_handle* h, tp_cg_result* res, int32_t* lane_iters,
+                     int32_t* lane_status, double* lane_rnorm, double* lane_bnorm,
+                     void* stream);
+
+TP_API int tp_cg_destroy(tp_cg_handle* h);
+
+/* time `reps` launches of one inner SpMV+dot with the given config (autotuner support);
+ * returns milliseconds per launch through *ms (host). [sync] */
+TP_API int tp_cg_time_spmv(tp_cg_handle* h, int reps, float* ms, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DISSOLVE_TP_H */

@@ -5,7 +5,7 @@ The reference keeps its kernels as CUDA C string literals in gpu/gpu_assembler.p
 `_RHS_BC_KERNEL_SRC` :228-239, `_GRAD_KERNEL_SRC` :251-304) and compiles them at
 import with CuPy NVRTC.  This recipe reads those literals with `ast` from the
 mounted reference (never copying them into the repository), writes them under
-oracle/_ref/ and builds two libraries from them:
+a temporary directory and builds two libraries from them into oracle/_ref/:
 
   libref_kernels_cpu.so  the kernels compiled by g++ through cuda_cpu_shim.h, each
                          wrapped in `ref_cpu_<name>(grid, block, args...)`, which
@@ -87,13 +87,12 @@ def _wrapper(name, params, gpu: bool) -> str:
             f"    }}\n}}\n")
 
 
-def write_sources() -> tuple[str, str, list]:
-    os.makedirs(OUT, exist_ok=True)
+def write_sources(workdir: str) -> tuple[str, str, list]:
     srcs = extract_sources()
     body = "\n".join(srcs[k] for k in KERNEL_VARS)
     kernels = parse_kernels(body)
-    cpu = os.path.join(OUT, "ref_kernels_cpu.cpp")
-    gpu = os.path.join(OUT, "ref_kernels_gpu.cu")
+    cpu = os.path.join(workdir, "ref_kernels_cpu.cpp")
+    gpu = os.path.join(workdir, "ref_kernels_gpu.cu")
     with open(cpu, "w") as f:
         f.write('#include "cuda_cpu_shim.h"\n')
         f.write(body)
@@ -110,7 +109,16 @@ def write_sources() -> tuple[str, str, list]:
 
 
 def build(verbose: bool = False, gpu: bool = True) -> dict:
-    cpu_src, gpu_src, kernels = write_sources()
+    """Compile in a temporary directory; only the two libraries land in oracle/_ref/."""
+    import tempfile
+
+    os.makedirs(OUT, exist_ok=True)
+    with tempfile.TemporaryDirectory(prefix="ref_recipe_") as work:
+        return _build_in(work, verbose, gpu)
+
+
+def _build_in(work: str, verbose: bool, gpu: bool) -> dict:
+    cpu_src, gpu_src, kernels = write_sources(work)
     outs = {}
     cpu_so = os.path.join(OUT, "libref_kernels_cpu.so")
     cmd = ["g++", "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-I", HERE,
