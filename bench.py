@@ -1,0 +1,398 @@
+"""Benchmark: 3-species backward-Euler steps/s at 1.57M P1 tets, rtol 1e-8.
+
+Workload (the three-species multi-RHS case): [0,1]^3 with 64^3 cells Kuhn-split
+(1,572,864 tets, 274,625 vertices), interior vertices jittered +-0.2h (seed 0);
+per-cell diffusivity D_s exp(0.3 xi), xi ~ N(0,1) (seed 1), D_s = (1.0, 1.0, 2.6)
+for O2 / Cl- / OH-, reaction k_s = (0.5, 0.0, 0.2), dt = 0.02, u_prev ~ U(0,1) per
+vertex and species (seed 2), lumped mass, no Dirichlet rows.  One step = assemble the
+operator, assemble the 3 right-hand sides, form the initial guess and solve all three
+species to ||b - A x|| <= 1e-8 ||b||.  Synthetic inputs with the configuration's
+shapes and distributions; nothing is read from disk.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` is the batched, FP32-inner / FP64-refined form with the learned (or, if no
+predictor is trained, previous-step) initial guess, inputs resident on the device;
+`e2e` is the same step through the host-buffer API (H2D of u_prev, D2H of u_new inside
+the timed region).  `forms` reports the plain FP64 GPU form (species one at a time,
+full FP64 CSR assembly + FP64 Jacobi-PCG) on the same steps.  Between timed steps a
+512 MiB buffer is written to flush the 126 MB L2.  N > 1 runs N independent replicas
+(one mesh per GPU, no collective on the data path; weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+for _p in (REPO, os.path.join(REPO, "dissolve-2.0_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "3-species BE steps/s at 1.57M P1 tets, rtol 1e-8: mixed+learned vs plain FP64"
+N_SIDE, JITTER = 64, 0.2
+D_S, K_S, DT, RTOL = (1.0, 1.0, 2.6), (0.5, 0.0, 0.2), 0.02, 1e-8
+WORKLOAD = ("3-species backward-Euler step, 64^3 Kuhn cube (1,572,864 P1 tets, 274,625 "
+            "vertices), jitter 0.2h, De = D_s exp(0.3 xi), rtol 1e-8")
+
+
+def make_inputs(n_side=N_SIDE):
+    from dissolve_tp.mesh import kuhn_cube
+    m = kuhn_cube(n_side, JITTER, seed=0)
+    xi = np.random.default_rng(1).standard_normal(m.n_cells)
+    coef = np.exp(0.3 * xi)
+    u0 = np.random.default_rng(2).uniform(0.0, 1.0, (m.n_verts, 3))
+    return m, coef, u0
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+        return False
+
+    def summary(self):
+        mhz, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                mhz.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+# ------------------------------------------------------------------ timing helpers
+def timed_steps(step_fn, steps, flush, torch):
+    """Per-step CUDA-event timing on the current stream, L2 flushed before each step."""
+    ms = []
+    for _ in range(steps):
+        flush()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        step_fn()
+        e1.record()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return ms
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    from dissolve_tp.transport import BatchedTransport, PlainTransport
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    m, coef, u0 = make_inputs()
+    flush_buf = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def flush():
+        flush_buf.zero_()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- mixed + batched (+ learned) form
+    fast = BatchedTransport(m, coef, D_S, K_S, DT, rtol=RTOL, inner_fp32=True, guess="previous")
+    learned = False
+    if args.guess == "learned":
+        from dissolve_tp import mlp as mlpmod
+        learned = mlpmod.attach_trained_predictor(fast, m, coef, u0, D_S, K_S, DT,
+                                                  train_steps=args.train_steps)
+    fast.set_state(u0)
+    results = []
+    for _ in range(args.warmup):
+        fast.step(sync=True)
+    torch.cuda.synchronize()
+    barrier()
+    launches = 0
+    with ClockSampler(local_rank) as clk:
+        torch.cuda.synchronize()
+        barrier()
+        step_ms = []
+        for _ in range(args.steps):
+            flush()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.nvtx.range_push("timed_step")
+            e0.record()
+            fast.step(sync=False)
+            e1.record()
+            torch.cuda.nvtx.range_pop()
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            r = fast.solver.result()
+            results.append(r)
+            launches += fast.launches_per_step(r)
+        torch.cuda.synchronize()
+        barrier()
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * args.steps / (total_ms / 1e3)
+    conv = all(r["converged"] for r in results)
+    iters = [int(r["iterations"]) for r in results]
+
+    # ---- roofline of the dominant kernel (inner SpMV + dot, FP32, 3 columns)
+    spmv_ms = fast.solver.time_spmv(50)
+    nnz, nv = fast.dm.nnz, fast.dm.n_verts
+    spmv_bytes = nnz * (4 + 4) + (nv + 1) * 4 + nv * 16 * 3
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = spmv_bytes / (spmv_ms * 1e-3) / 1e9
+
+    # ---- e2e through the host-buffer API
+    e2e = None
+    if args.e2e:
+        fast.set_state(u0)
+        u_host = torch.from_numpy(np.ascontiguousarray(u0)).pin_memory()
+        out_host = torch.empty_like(u_host).pin_memory()
+        for _ in range(max(1, args.warmup)):
+            fast.step_host(u_host, out_host)
+        torch.cuda.synchronize()
+        e_ms = []
+        for _ in range(args.steps):
+            flush()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fast.step_host(u_host, out_host)
+            e1.record()
+            e1.synchronize()
+            e_ms.append(e0.elapsed_time(e1))
+            u_host.copy_(out_host)
+        tot = sum(e_ms)
+        if world > 1:
+            t = torch.tensor([tot], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            tot = float(t.item())
+        e2e = {"value": world * args.steps / (tot / 1e3), "unit": "steps/s",
+               "h2d_bytes_per_step": int(u_host.numel() * 8),
+               "d2h_bytes_per_step": int(out_host.numel() * 8)}
+
+    # ---- the plain FP64 GPU form on the same steps
+    forms = {}
+    if args.forms:
+        plain = PlainTransport(m, coef, D_S, K_S, DT, rtol=RTOL)
+        plain.set_state(u0)
+        for _ in range(args.warmup):
+            plain.step(sync=True)
+        p_ms, p_it = [], []
+        for _ in range(args.steps):
+            flush()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            plain.step(sync=False)
+            e1.record()
+            e1.synchronize()
+            p_ms.append(e0.elapsed_time(e1))
+            p_it.append([int(r["iterations"]) for r in (s.result() for s in plain.solvers)])
+        # the same steps in the batched form with FP64 inner iterations
+        b64 = BatchedTransport(m, coef, D_S, K_S, DT, rtol=RTOL, inner_fp32=False,
+                               guess="previous")
+        b64.set_state(u0)
+        for _ in range(args.warmup):
+            b64.step(sync=True)
+        q_ms = timed_steps(lambda: b64.step(sync=False), args.steps, flush, torch)
+        # agreement of the fast form with the plain FP64 form after W+K steps
+        up = plain.state()
+        fast.set_state(u0)
+        for _ in range(args.warmup + args.steps):
+            fast.step(sync=True)
+        uf = fast.state()
+        rel = float(np.linalg.norm(uf - up) / np.linalg.norm(up))
+        forms = {
+            "plain_fp64": {"steps_per_s": args.steps / (sum(p_ms) / 1e3),
+                           "ms_per_step": sum(p_ms) / args.steps,
+                           "iterations_per_species": p_it[-1]},
+            "batched_fp64": {"steps_per_s": args.steps / (sum(q_ms) / 1e3),
+                             "ms_per_step": sum(q_ms) / args.steps},
+            "fast_vs_plain_speedup": (args.steps / (total_ms / 1e3 / world)) /
+                                     (args.steps / (sum(p_ms) / 1e3)),
+            "fast_vs_plain_rel_l2": rel,
+        }
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32-inner/f64-refined", "data": "synthetic (seeded, config shapes)",
+        "config": {"workload": WORKLOAD, "n_tets": m.n_cells, "n_verts": m.n_verts,
+                   "nnz": nnz, "species": 3, "form": "batched 3-column CG, FP32 inner + "
+                   "FP64 reliable updates, " + ("learned" if learned else "previous-step")
+                   + " initial guess", "mass": "lumped", "l2": "flushed (512 MiB write) "
+                   "before every timed step", "parallelism": f"replicas x{world}",
+                   "cg_launch": fast.cg_config},
+        "converged": conv, "cg_iterations": iters,
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "kernel": "k_b1 (FP32 3-column CSR SpMV + FP64 dot)",
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None,
+                     "algorithmic_bytes": spmv_bytes, "launch_us": spmv_ms * 1e3,
+                     "note": "in-loop launches: operator and vectors are L2-resident at "
+                             "this size, so frac can exceed HBM-bound 1.0"},
+        "clocks": clk.summary(),
+        "e2e": e2e,
+        "forms": forms,
+    }
+    if rank == 0 and world == 1 and args.cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(m, coef, u0, sample_steps=args.cpu_sample_steps)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ CPU legs
+def cpu_step_runner(m, coef, u0):
+    """The reference CPU path restated (oracle): per species FP64 assembly in cell
+    order + RHS + GMRES(50) right-preconditioned by block-Jacobi ILU(0), one block per
+    host thread, from the previous step, to ||b - A x|| <= rtol ||b||."""
+    from oracle import oracle as orc
+    nt = orc.num_threads()
+    detJ, G, JT = orc.geometry(m.coords, m.cells)
+    ip, ix, sm = orc.csr_pattern(m.cells, m.n_verts)
+    state = {"U": np.array(u0, dtype=np.float64), "iters": []}
+    alphas = [np.full(m.n_cells, k) for k in K_S]
+
+    def step():
+        its = []
+        for s in range(3):
+            A = orc.assemble(detJ, G, D_S[s] * coef, alphas[s], 1.0 / DT, 1, sm, ix.size)
+            b = orc.assemble_rhs(m.cells, detJ, state["U"][:, s], None, 1.0 / DT, 1)
+            x, it, st, _ = orc.gmres_bjacobi(ip, ix, A, b, state["U"][:, s], RTOL, nblocks=nt)
+            state["U"][:, s] = x
+            its.append(it)
+        state["iters"].append(its)
+
+    return step, nt, state
+
+
+def cpu_baseline(m, coef, u0, sample_steps=3):
+    step, nt, state = cpu_step_runner(m, coef, u0)
+    t = time.perf_counter()
+    for _ in range(sample_steps):
+        step()
+    dt = time.perf_counter() - t
+    return {"value": sample_steps / dt, "unit": "steps/s", "cores": nt, "kind": "port",
+            "sample": f"{sample_steps} full 3-species steps from u_prev ~ U(0,1) "
+                      f"(GMRES iterations per species {state['iters'][-1]})"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    m, coef, u0 = make_inputs()
+    step, nt, state = cpu_step_runner(m, coef, u0)
+    for _ in range(args.warmup):
+        step()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = time.perf_counter() - t
+    v = args.steps / dt
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded, config shapes)",
+            "config": {"workload": WORKLOAD, "n_tets": m.n_cells, "n_verts": m.n_verts,
+                       "parallelism": "host threads"},
+            "cpu_baseline": {"value": v, "unit": "steps/s", "cores": nt, "kind": "port",
+                             "sample": f"{args.steps} full 3-species steps after {args.warmup} "
+                                       f"warm-up steps; GMRES(50) + block-Jacobi ILU(0), "
+                                       f"{nt} blocks"},
+            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "gmres_iterations": state["iters"][-1]}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--guess", default="previous", choices=["learned", "previous"])
+    ap.add_argument("--train-steps", type=int, default=12)
+    ap.add_argument("--no-forms", dest="forms", action="store_false")
+    ap.add_argument("--no-e2e", dest="e2e", action="store_false")
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--cpu-sample-steps", type=int, default=3)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

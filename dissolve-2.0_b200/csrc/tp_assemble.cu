@@ -384,9 +384,48 @@ __global__ void k_axpby(int64_t n, double a, const double* __restrict__ x, doubl
     y[i] = a * x[i] + b * y[i];
 }
 
+// (n, S) contiguous <-> (n, ld) interleaved with zero padding
+__global__ void k_pack(int64_t n, int S, int ld, const double* __restrict__ src,
+                       double* __restrict__ dst) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n * ld;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = i / ld;
+    const int s = (int)(i - r * ld);
+    dst[i] = (s < S) ? src[r * S + s] : 0.0;
+  }
+}
+
+__global__ void k_unpack(int64_t n, int S, int ld, const double* __restrict__ src,
+                         double* __restrict__ dst) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n * S;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = i / S;
+    const int s = (int)(i - r * S);
+    dst[i] = src[r * ld + s];
+  }
+}
+
 }  // namespace tp
 
 using namespace tp;
+
+extern "C" int tp_pack_columns(int64_t n, int S, int ld, const double* src, double* dst,
+                               void* stream) {
+  TP_REQUIRE(src && dst && S >= 1 && ld >= S, "bad argument");
+  if (n == 0) return TP_OK;
+  k_pack<<<grid_for(n * ld, 256, 65535), 256, 0, as_stream(stream)>>>(n, S, ld, src, dst);
+  TP_LAUNCH_CHECK();
+  return TP_OK;
+}
+
+extern "C" int tp_unpack_columns(int64_t n, int S, int ld, const double* src, double* dst,
+                                 void* stream) {
+  TP_REQUIRE(src && dst && S >= 1 && ld >= S, "bad argument");
+  if (n == 0) return TP_OK;
+  k_unpack<<<grid_for(n * S, 256, 65535), 256, 0, as_stream(stream)>>>(n, S, ld, src, dst);
+  TP_LAUNCH_CHECK();
+  return TP_OK;
+}
 
 static bool mesh_ok(const tp_mesh* m) {
   return m && m->cells && m->geo && m->v2c_ptr && m->v2c && m->indptr;

@@ -98,6 +98,8 @@ SIGNATURES = {
     "tp_oh_source": (ctypes.c_int, [_c_i64, _vp, _vp, _vp, _vp, _vp, _c_dbl, _c_dbl, _c_dbl,
                                     _c_dbl, _vp, _vp]),
     "tp_axpby": (ctypes.c_int, [_c_i64, _c_dbl, _vp, _c_dbl, _vp, _vp]),
+    "tp_pack_columns": (ctypes.c_int, [_c_i64, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
+    "tp_unpack_columns": (ctypes.c_int, [_c_i64, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
     "tp_matfree_apply": (ctypes.c_int, [_P(TpMesh), ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
                                         _vp, _P(_c_dbl), _P(_c_dbl), _c_dbl, ctypes.c_int,
                                         ctypes.c_int, _vp, _vp, _vp]),

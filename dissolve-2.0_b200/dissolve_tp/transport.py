@@ -1,0 +1,233 @@
+"""Backward-Euler reaction-diffusion step for several species on one mesh.
+
+Per species s the step solves  [(1/dt + k_s + alpha_s) M + D_s K_xi] u^{n+1} = M (u^n/dt + f_s)
+(physics/weak_forms.py:85-143; dissolve.py:780-954 calls solve_transport once per
+species), with K_xi the stiffness of the per-cell diffusivity factor shared by all
+species (De_s = D_s * coef_cell) and M the lumped (default, gpu_assembler.py:37) mass.
+
+Two forms:
+
+  PlainTransport     the reference's flow, one species at a time: full FP64 assembly of
+                     each species' matrix into CSR (GPUSparseAssembler.assemble), FP64
+                     RHS, FP64 Jacobi-PCG from the previous step -- the plain FP64 form.
+  BatchedTransport   all species in one solve: the shared stiffness is assembled once
+                     per step (FP64 and FP32 values), the mass/reaction terms become a
+                     per-column diagonal, the RHS is one interleaved (V, 4) array and one
+                     CG runs every species as a lane -- FP64, or FP32 inner iterations
+                     with FP64 reliable updates.  The initial guess is the previous step
+                     or a learned prediction (dissolve_tp.mlp).
+"""
+from __future__ import annotations
+
+import ctypes
+import time
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import call
+from .assembler import GPUSparseAssembler
+from .autotune import tune_cg
+from .device import ptr, stream_handle, to_device
+from .krylov import CGSolver, CsrOperator
+
+
+class PlainTransport:
+    """The plain FP64 GPU form: per species assemble + RHS + FP64 Jacobi-PCG."""
+
+    def __init__(self, mesh, coef_cell, D, k, dt, rtol=1e-8, max_it=5000, lumped=True,
+                 bc=None, cg=None):
+        from . import assembler as A
+
+        self.S = len(D)
+        self.D, self.k, self.dt = list(D), list(k), float(dt)
+        self.inv_dt = 1.0 / self.dt
+        self._lumped_prev = A.LUMP_MASS
+        self.lumped = bool(lumped)
+        self.asm = [GPUSparseAssembler(mesh)]
+        for _ in range(1, self.S):
+            self.asm.append(GPUSparseAssembler(ref_asm=self.asm[0]))
+        dev = self.asm[0].device
+        self.device = dev
+        nc = self.asm[0].n_cells
+        self.coef = to_device(coef_cell, torch.float64, dev)
+        self.De = [self.coef * float(d) for d in self.D]
+        self.alpha = [torch.full((nc,), float(kk), dtype=torch.float64, device=dev)
+                      for kk in self.k]
+        self.bc = bc or [None] * self.S
+        cg = cg or {}
+        self.solvers = []
+        for s in range(self.S):
+            mask = self.asm[0]._dm.bc_mask(self.bc[s][0]) if self.bc[s] is not None else None
+            op = CsrOperator(self.asm[s].d_indptr, self.asm[s].d_indices, self.asm[s].d_data,
+                             bc_mask=mask)
+            self.solvers.append(CGSolver(op, rtol=rtol, max_it=max_it, **cg))
+        nv = self.asm[0].n_dofs
+        self.U = [torch.zeros(nv, dtype=torch.float64, device=dev) for _ in range(self.S)]
+
+    def set_state(self, U):
+        U = np.asarray(U) if not isinstance(U, torch.Tensor) else U.cpu().numpy()
+        for s in range(self.S):
+            self.U[s].copy_(torch.from_numpy(np.ascontiguousarray(U[:, s], dtype=np.float64)))
+
+    def state(self) -> np.ndarray:
+        return np.stack([u.cpu().numpy() for u in self.U], axis=1)
+
+    def step(self, sync=True):
+        from . import assembler as A
+
+        A.LUMP_MASS = 1 if self.lumped else 0
+        try:
+            for s in range(self.S):
+                asm, sol = self.asm[s], self.solvers[s]
+                bc = self.bc[s]
+                asm.assemble(self.De[s], self.inv_dt, alpha=self.alpha[s],
+                             bc_dofs=None if bc is None else bc[0])
+                b = asm.assemble_rhs(self.U[s], self.inv_dt,
+                                     bc_dofs=None if bc is None else bc[0],
+                                     bc_value=0.0 if bc is None else bc[1])
+                sol.b.view(-1).copy_(b)
+                sol.x.view(-1).copy_(self.U[s])
+                sol.run()
+                self.U[s].copy_(sol.x.view(-1))
+        finally:
+            A.LUMP_MASS = self._lumped_prev
+        if not sync:
+            return None
+        return [sol.result() for sol in self.solvers]
+
+    def step_host(self, u_host: torch.Tensor, out_host: torch.Tensor):
+        """End-to-end step through host buffers: (S, V) float64 pinned in -> out."""
+        for s in range(self.S):
+            self.U[s].copy_(u_host[s], non_blocking=True)
+        self.step(sync=False)
+        for s in range(self.S):
+            out_host[s].copy_(self.U[s], non_blocking=True)
+
+
+class BatchedTransport:
+    """All species in one multi-column solve (shared stiffness, per-column diagonal)."""
+
+    def __init__(self, mesh, coef_cell, D, k, dt, rtol=1e-8, max_it=5000, lumped=True,
+                 inner_fp32=True, delta=0.1, guess="previous", bc_dofs=None, bc_values=None,
+                 alpha_cells=None, autotune=True, cg=None, asm=None):
+        if not lumped:
+            raise ValueError("the batched form splits the operator into a shared stiffness "
+                             "and a per-column lumped diagonal; use PlainTransport for "
+                             "consistent mass")
+        self.S = len(D)
+        if not 1 <= self.S <= 4:
+            raise ValueError("1 to 4 species per batched solve")
+        self.ld = {1: 1, 2: 2, 3: 4, 4: 4}[self.S]
+        self.D, self.k, self.dt = list(D), list(k), float(dt)
+        self.inv_dt = 1.0 / self.dt
+        self.asm = asm if asm is not None else GPUSparseAssembler(mesh)
+        dm = self.asm._dm
+        self.dm = dm
+        dev = self.asm.device
+        self.device = dev
+        n, nnz = dm.n_verts, dm.nnz
+        self.coef = to_device(coef_cell, torch.float64, dev)
+        self.K64 = torch.empty(nnz, dtype=torch.float64, device=dev)
+        self.K32 = torch.empty(nnz, dtype=torch.float32, device=dev) if inner_fp32 else None
+        self.D64 = torch.empty((n, self.ld), dtype=torch.float64, device=dev)
+        self.D32 = (torch.empty((n, self.ld), dtype=torch.float32, device=dev)
+                    if inner_fp32 else None)
+        self.alpha = None
+        if alpha_cells is not None:
+            self.alpha = torch.zeros((dm.n_cells, self.ld), dtype=torch.float64, device=dev)
+            self.alpha[:, : self.S] = to_device(alpha_cells, torch.float64, dev)
+        self.bc_mask = dm.bc_mask(bc_dofs) if bc_dofs is not None else None
+        self.bc_dofs = to_device(bc_dofs, torch.int32, dev) if bc_dofs is not None else None
+        self.bc_values = (ctypes.c_double * 4)(*(list(bc_values or [0.0] * self.S) +
+                                                 [0.0] * (4 - self.S)))
+        self.op = CsrOperator(dm.indptr, dm.indices, self.K64, K32=self.K32, diag64=self.D64,
+                              diag32=self.D32, bc_mask=self.bc_mask, dscale=self.D, S=self.S,
+                              ld=self.ld)
+        cg = dict(cg or {})
+        if autotune and not {"group", "block", "rows_per_tile"} & set(cg):
+            self.assemble_operator()
+            cg.update(tune_cg(self.op, inner_fp32=inner_fp32))
+        self.cg_config = cg
+        self.solver = CGSolver(self.op, rtol=rtol, max_it=max_it, inner_fp32=inner_fp32,
+                               delta=delta, **cg)
+        self.U = torch.zeros((n, self.ld), dtype=torch.float64, device=dev)
+        self.U_prev = torch.zeros_like(self.U)
+        self.guess = guess
+        self.predictor = None
+        self.steps_done = 0
+
+    # -- per-step pieces -------------------------------------------------------------
+    def assemble_operator(self):
+        st = stream_handle()
+        call("tp_assemble_csr", ctypes.byref(self.dm.tpm), ptr(self.coef), None, 0.0, 1,
+             _lib.TP_ASM_STIFF, None, ptr(self.K64), ptr(self.K32), st)
+        shift = (ctypes.c_double * 4)(*([self.inv_dt + kk for kk in self.k] +
+                                        [0.0] * (4 - self.S)))
+        call("tp_lumped_diag", ctypes.byref(self.dm.tpm), self.S, self.ld, ptr(self.alpha),
+             shift, ptr(self.bc_mask), ptr(self.D64), ptr(self.D32), st)
+
+    def assemble_rhs(self):
+        n_bc = 0 if self.bc_dofs is None else int(self.bc_dofs.numel())
+        call("tp_assemble_rhs", ctypes.byref(self.dm.tpm), self.S, self.ld, ptr(self.U), None,
+             self.inv_dt, 1, n_bc, ptr(self.bc_dofs), self.bc_values, ptr(self.solver.b),
+             stream_handle())
+
+    def initial_guess(self):
+        x = self.solver.x
+        if self.guess == "learned" and self.predictor is not None and self.steps_done > 0:
+            self.predictor.predict_into(self, x)
+        elif self.guess == "extrapolate" and self.steps_done > 0:
+            x.copy_(self.U)  # x = 2 u^n - u^{n-1}
+            call("tp_axpby", x.numel(), -1.0, ptr(self.U_prev), 2.0, ptr(x), stream_handle())
+        else:
+            x.copy_(self.U)
+
+    def set_state(self, U, U_prev=None):
+        u = to_device(U, torch.float64, self.device).reshape(-1, self.S)
+        self.U.zero_()
+        self.U[:, : self.S] = u
+        self.U_prev.copy_(self.U if U_prev is None else self._pad(U_prev))
+        self.steps_done = 0 if U_prev is None else 1
+
+    def _pad(self, U):
+        out = torch.zeros_like(self.U)
+        out[:, : self.S] = to_device(U, torch.float64, self.device).reshape(-1, self.S)
+        return out
+
+    def step(self, sync=True):
+        self.assemble_operator()
+        self.assemble_rhs()
+        self.initial_guess()
+        self.solver.run()
+        self.U_prev.copy_(self.U)
+        self.U.copy_(self.solver.x)
+        self.steps_done += 1
+        return self.solver.result() if sync else None
+
+    def state(self) -> np.ndarray:
+        return self.U[:, : self.S].cpu().numpy()
+
+    def launches_per_step(self, res: dict) -> int:
+        """Kernels of this library one step launched: stiffness assembly, lumped diagonal,
+        RHS, the guess, and the solve graph's I1, I2, F1, F2 plus B1, B2, B4 per iteration
+        and RU1, RU2 per reliable update."""
+        guess = 1 if (self.guess != "previous" and self.steps_done > 1) else 0
+        if self.guess == "learned" and self.predictor is not None:
+            guess = self.predictor.launches
+        return 3 + guess + 4 + 3 * int(res["iterations"]) + 2 * int(res["n_reliable"])
+
+    def step_host(self, u_host: torch.Tensor, out_host: torch.Tensor):
+        """End-to-end step through host buffers: (V, S) float64 pinned in -> out (V, S).
+        One H2D copy into a staging array, packing to the interleaved state on the
+        device, the step, unpacking and one D2H copy."""
+        n = self.U.shape[0]
+        if getattr(self, "_stage", None) is None:
+            self._stage = torch.empty((n, self.S), dtype=torch.float64, device=self.device)
+        st = stream_handle()
+        self._stage.copy_(u_host, non_blocking=True)
+        call("tp_pack_columns", n, self.S, self.ld, ptr(self._stage), ptr(self.U), st)
+        self.step(sync=False)
+        call("tp_unpack_columns", n, self.S, self.ld, ptr(self.U), ptr(self._stage), st)
+        out_host.copy_(self._stage, non_blocking=True)

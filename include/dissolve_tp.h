@@ -177,6 +177,13 @@ TP_API int tp_oh_source(int64_t n, const double* phi, const double* normgradphi,
 /* y = a x + b y (n doubles): numerics/solvers.py:278-279 under-relaxation */
 TP_API int tp_axpby(int64_t n, double a, const double* x, double b, double* y, void* stream);
 
+/* (n, S) row-major columns -> (n, ld) interleaved, padding columns zero, and back.
+ * Plumbing for host arrays of S species (no reference counterpart). */
+TP_API int tp_pack_columns(int64_t n, int S, int ld, const double* src, double* dst,
+                           void* stream);
+TP_API int tp_unpack_columns(int64_t n, int S, int ld, const double* src, double* dst,
+                             void* stream);
+
 /* ------------------------------------------------------------------ operators */
 /* gpu/ceed_operators.py:87-108, 247-353 as intended, on S interleaved columns:
  * y[:, s] = sum_e [diff_scale[s] De_e K_e + (inv_dt + alpha_e + shift[s]) M_e] x_e[:, s]
