@@ -138,7 +138,9 @@ def run_ours(args, rank, world, local_rank):
             dist.barrier()
 
     # ---- mixed + batched (+ learned) form
-    fast = BatchedTransport(m, coef, D_S, K_S, DT, rtol=RTOL, inner_fp32=True, guess="previous")
+    cg_extra = {"use_graph_loop": not args.host_loop}
+    fast = BatchedTransport(m, coef, D_S, K_S, DT, rtol=RTOL, inner_fp32=True, guess="previous",
+                            cg=cg_extra)
     learned = False
     if args.guess == "learned":
         from dissolve_tp import mlp as mlpmod
@@ -365,6 +367,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--guess", default="previous", choices=["learned", "previous"])
     ap.add_argument("--train-steps", type=int, default=12)
+    ap.add_argument("--host-loop", action="store_true",
+                    help="iterate the CG from the host (plain graphs, one per iteration) "
+                         "instead of the device-side while loop; for profilers that cannot "
+                         "see kernels inside conditional graphs")
     ap.add_argument("--no-forms", dest="forms", action="store_false")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")

@@ -75,34 +75,53 @@ __global__ void __launch_bounds__(128) k_assemble_rows(
   for (int s = 0; s < len; s++) acc[s * B + tid] = 0.0;
   const bool is_bc = valid && bc_mask && bc_mask[r];
   if (valid && !is_bc) {
-    const int kend = v2c_ptr[r + 1];
-    for (int k = v2c_ptr[r]; k < kend; k++) {
-      const int32_t e = __ldg(v2c + k);
-      const int64_t c = e >> 2;
-      const int li = e & 3;
-      const uint32_t sl = __ldg(slots + k);
-      const GeoRec g = load_geo(geo, c);
-      double G[3][3], S[3];
-      unpack_G(g, G, S);
-      const double kscale = (MODE == TP_ASM_MASS)
-                                ? 0.0
-                                : __ddiv_rn(__dmul_rn(g.dJ, __ldg(De + c)), 6.0);
-      const double react =
-          (MODE == TP_ASM_FULL) ? __dadd_rn(inv_dt, alpha ? __ldg(alpha + c) : 0.0) : 1.0;
+    // incident cells in ascending order, fetched PF at a time so their loads overlap;
+    // accumulation stays in cell order
+    constexpr int PF = 4;
+    const int kbeg = v2c_ptr[r], kend = v2c_ptr[r + 1];
+    for (int k0 = kbeg; k0 < kend; k0 += PF) {
+      int32_t ev[PF];
+      uint32_t sv[PF];
 #pragma unroll
-      for (int j = 0; j < 4; j++) {
-        double a = 0.0;
-        if (MODE != TP_ASM_MASS) a = __dmul_rn(kref(li, j, G, S), kscale);
-        if (MODE != TP_ASM_STIFF) {
-          double M;
-          if (lumped)
-            M = (li == j) ? __ddiv_rn(__dmul_rn(g.dJ, 5.0), 120.0) : 0.0;
-          else
-            M = __ddiv_rn(__dmul_rn(g.dJ, (li == j) ? 2.0 : 1.0), 120.0);
-          a = (MODE == TP_ASM_FULL) ? __dadd_rn(a, __dmul_rn(react, M)) : M;
+      for (int u = 0; u < PF; u++) {
+        const bool ok = k0 + u < kend;
+        ev[u] = ok ? __ldg(v2c + k0 + u) : 0;
+        sv[u] = ok ? __ldg(slots + k0 + u) : 0u;
+      }
+      GeoRec gv[PF];
+      double dev[PF], alv[PF];
+#pragma unroll
+      for (int u = 0; u < PF; u++) {
+        const int64_t c = ev[u] >> 2;
+        gv[u] = load_geo(geo, c);
+        dev[u] = (MODE == TP_ASM_MASS) ? 0.0 : __ldg(De + c);
+        alv[u] = (MODE == TP_ASM_FULL && alpha) ? __ldg(alpha + c) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < PF; u++) {
+        if (k0 + u >= kend) break;
+        const int li = ev[u] & 3;
+        const GeoRec& g = gv[u];
+        double G[3][3], S[3];
+        unpack_G(g, G, S);
+        const double kscale = (MODE == TP_ASM_MASS) ? 0.0
+                                                    : __ddiv_rn(__dmul_rn(g.dJ, dev[u]), 6.0);
+        const double react = (MODE == TP_ASM_FULL) ? __dadd_rn(inv_dt, alv[u]) : 1.0;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          double a = 0.0;
+          if (MODE != TP_ASM_MASS) a = __dmul_rn(kref(li, j, G, S), kscale);
+          if (MODE != TP_ASM_STIFF) {
+            double M;
+            if (lumped)
+              M = (li == j) ? __ddiv_rn(__dmul_rn(g.dJ, 5.0), 120.0) : 0.0;
+            else
+              M = __ddiv_rn(__dmul_rn(g.dJ, (li == j) ? 2.0 : 1.0), 120.0);
+            a = (MODE == TP_ASM_FULL) ? __dadd_rn(a, __dmul_rn(react, M)) : M;
+          }
+          const int slot = (sv[u] >> (8 * j)) & 0xff;
+          if (slot < len) acc[slot * B + tid] = __dadd_rn(acc[slot * B + tid], a);
         }
-        const int slot = (sl >> (8 * j)) & 0xff;
-        if (slot < len) acc[slot * B + tid] = __dadd_rn(acc[slot * B + tid], a);
       }
     }
   }
@@ -172,13 +191,23 @@ __global__ void k_lumped_diag(int64_t nv, int S, int ld, const int32_t* __restri
     const double sh[4] = {shift.x, shift.y, shift.z, shift.w};
     const bool is_bc = bc_mask && bc_mask[r];
     if (!is_bc) {
-      for (int k = v2c_ptr[r]; k < v2c_ptr[r + 1]; k++) {
-        const int64_t c = v2c[k] >> 2;
-        const double dJ = geo[8 * c + 6];
-        const double Ld = __dmul_rn(__ddiv_rn(dJ, 120.0), 5.0);
-        for (int s = 0; s < S; s++) {
-          const double w = __dadd_rn(sh[s], alpha ? alpha[c * ld + s] : 0.0);
-          acc[s] = __dadd_rn(acc[s], __dmul_rn(w, Ld));
+      constexpr int PF = 8;
+      const int kbeg = v2c_ptr[r], kend = v2c_ptr[r + 1];
+      for (int k0 = kbeg; k0 < kend; k0 += PF) {
+        int64_t cv[PF];
+        double dJ[PF];
+#pragma unroll
+        for (int u = 0; u < PF; u++) cv[u] = (k0 + u < kend) ? (v2c[k0 + u] >> 2) : 0;
+#pragma unroll
+        for (int u = 0; u < PF; u++) dJ[u] = geo[8 * cv[u] + 6];
+#pragma unroll
+        for (int u = 0; u < PF; u++) {
+          if (k0 + u >= kend) break;
+          const double Ld = __dmul_rn(__ddiv_rn(dJ[u], 120.0), 5.0);
+          for (int s = 0; s < S; s++) {
+            const double w = __dadd_rn(sh[s], alpha ? alpha[cv[u] * ld + s] : 0.0);
+            acc[s] = __dadd_rn(acc[s], __dmul_rn(w, Ld));
+          }
         }
       }
     }
@@ -205,31 +234,42 @@ __global__ void k_rhs_rows(int64_t nv, int S, int ld, const int32_t* __restrict_
       ur[s] = u[r * ld + s];
       fr[s] = f ? f[r * ld + s] : 0.0;
     }
-    for (int k = v2c_ptr[r]; k < v2c_ptr[r + 1]; k++) {
-      const int32_t e = v2c[k];
-      const int64_t c = e >> 2;
-      const double dJ = geo[8 * c + 6];
-      const double base = __ddiv_rn(dJ, 120.0);
-      if (lumped) {
-        const double Ld = __dmul_rn(base, 5.0);
-        for (int s = 0; s < S; s++)
-          acc[s] = __dadd_rn(acc[s], __dmul_rn(Ld, __dadd_rn(__dmul_rn(inv_dt, ur[s]), fr[s])));
-      } else {
-        const int4 cv = reinterpret_cast<const int4*>(cells)[c];
-        const double mdt = __dmul_rn(base, inv_dt);
-        for (int s = 0; s < S; s++) {
-          const double su = __dadd_rn(
-              __dadd_rn(__dadd_rn(u[(int64_t)cv.x * ld + s], u[(int64_t)cv.y * ld + s]),
-                        u[(int64_t)cv.z * ld + s]),
-              u[(int64_t)cv.w * ld + s]);
-          double sf = 0.0;
-          if (f)
-            sf = __dadd_rn(
-                __dadd_rn(__dadd_rn(f[(int64_t)cv.x * ld + s], f[(int64_t)cv.y * ld + s]),
-                          f[(int64_t)cv.z * ld + s]),
-                f[(int64_t)cv.w * ld + s]);
-          acc[s] = __dadd_rn(acc[s], __dadd_rn(__dmul_rn(mdt, __dadd_rn(su, ur[s])),
-                                               __dmul_rn(base, __dadd_rn(sf, fr[s]))));
+    constexpr int PF = 8;
+    const int kbeg = v2c_ptr[r], kend = v2c_ptr[r + 1];
+    for (int k0 = kbeg; k0 < kend; k0 += PF) {
+      int64_t cvv[PF];
+      double dJv[PF];
+#pragma unroll
+      for (int q = 0; q < PF; q++) cvv[q] = (k0 + q < kend) ? (v2c[k0 + q] >> 2) : 0;
+#pragma unroll
+      for (int q = 0; q < PF; q++) dJv[q] = geo[8 * cvv[q] + 6];
+#pragma unroll
+      for (int q = 0; q < PF; q++) {
+        if (k0 + q >= kend) break;
+        const int64_t c = cvv[q];
+        const double base = __ddiv_rn(dJv[q], 120.0);
+        if (lumped) {
+          const double Ld = __dmul_rn(base, 5.0);
+          for (int s = 0; s < S; s++)
+            acc[s] = __dadd_rn(acc[s],
+                               __dmul_rn(Ld, __dadd_rn(__dmul_rn(inv_dt, ur[s]), fr[s])));
+        } else {
+          const int4 cv = reinterpret_cast<const int4*>(cells)[c];
+          const double mdt = __dmul_rn(base, inv_dt);
+          for (int s = 0; s < S; s++) {
+            const double su = __dadd_rn(
+                __dadd_rn(__dadd_rn(u[(int64_t)cv.x * ld + s], u[(int64_t)cv.y * ld + s]),
+                          u[(int64_t)cv.z * ld + s]),
+                u[(int64_t)cv.w * ld + s]);
+            double sf = 0.0;
+            if (f)
+              sf = __dadd_rn(
+                  __dadd_rn(__dadd_rn(f[(int64_t)cv.x * ld + s], f[(int64_t)cv.y * ld + s]),
+                            f[(int64_t)cv.z * ld + s]),
+                  f[(int64_t)cv.w * ld + s]);
+            acc[s] = __dadd_rn(acc[s], __dadd_rn(__dmul_rn(mdt, __dadd_rn(su, ur[s])),
+                                                 __dmul_rn(base, __dadd_rn(sf, fr[s]))));
+          }
         }
       }
     }

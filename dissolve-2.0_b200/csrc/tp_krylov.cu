@@ -42,22 +42,30 @@ struct Lanes {
 };
 
 struct Glob {
-  int32_t iter, max_it, any_trigger, n_reliable, n_active, cont, pad0, pad1;
+  int32_t iter, max_it, n_trigger, n_reliable, n_active, cont, timing, pad1;
   uint32_t ticket[8];
   double delta2;
 };
 
 constexpr int PQ = 12;  // partial slots per tile: 3 quantities x 4 columns
+constexpr int CHUNK = 32;  // tiles per first-level reduction chunk
+enum Kind { K_I2 = 0, K_B1 = 1, K_B2 = 2, K_RU2 = 3, K_F2 = 4, N_KINDS = 5 };
 
 template <typename VT>
 struct Args {
   int64_t n;
-  int S, ld, NL, nsys, ntiles, use_cond;
+  int S, ld, NL, nsys, ntiles;
   CsrView<VT> Ain;
   CsrView<double> A64;
   const int64_t* tile_row0;
   const int32_t* tile_sys;
   const int32_t* sys_tile_ptr;
+  const int32_t* tile_chunk;     // ntiles
+  const int32_t* chunk_tile_ptr; // nchunks + 1
+  const int32_t* sys_chunk_ptr;  // nsys + 1
+  int nchunks;
+  double* chunk_part;            // nchunks * PQ
+  uint32_t* chunk_ticket;        // N_KINDS * nchunks
   VT *p, *q, *r, *z, *xi, *dinv;
   double* x;
   const double* b;
@@ -65,6 +73,8 @@ struct Args {
   double* part;
   Lanes L;
   int32_t* sys_active;
+  int32_t* sys_trig;
+  uint32_t* sys_ticket;  // N_KINDS * nsys
   Glob* g;
   cudaGraphConditionalHandle h_while, h_if;
 };
@@ -91,56 +101,78 @@ __device__ __forceinline__ void block_sum_vec(double v[NV], double* sh /* 32*NV 
   __syncthreads();
 }
 
-// returns true in every thread of the block that finished last
-__device__ __forceinline__ bool last_block(uint32_t* ticket) {
+// Called by every thread after thread 0 wrote tile t's partials (slots 0..PQ-1).
+// Two-level, fixed-order reduction: the block completing the last tile of a chunk sums
+// the chunk's tiles in order into chunk_part; the block completing the last chunk of a
+// system returns true (in every thread) and then calls reduce_system.
+template <typename VT>
+__device__ __forceinline__ bool finish_tile(const Args<VT>& a, int t, int sys, int kind) {
+  __shared__ int s_flag;
+  const int c = a.tile_chunk[t];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const uint32_t ntl = (uint32_t)(a.chunk_tile_ptr[c + 1] - a.chunk_tile_ptr[c]);
+    const uint32_t k = atomicAdd(&a.chunk_ticket[kind * a.nchunks + c], 1u);
+    s_flag = (k == ntl - 1);
+    if (s_flag) a.chunk_ticket[kind * a.nchunks + c] = 0u;
+  }
+  __syncthreads();
+  if (!s_flag) return false;
+  __threadfence();
+  if (threadIdx.x < PQ) {
+    const int t0 = a.chunk_tile_ptr[c], t1 = a.chunk_tile_ptr[c + 1];
+    double v = 0.0;
+#pragma unroll 8
+    for (int u = t0; u < t1; u++) v += __ldcg(a.part + (int64_t)u * PQ + threadIdx.x);
+    a.chunk_part[(int64_t)c * PQ + threadIdx.x] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const uint32_t nch = (uint32_t)(a.sys_chunk_ptr[sys + 1] - a.sys_chunk_ptr[sys]);
+    const uint32_t k = atomicAdd(&a.sys_ticket[kind * a.nsys + sys], 1u);
+    s_flag = (k == nch - 1);
+    if (s_flag) a.sys_ticket[kind * a.nsys + sys] = 0u;
+  }
+  __syncthreads();
+  const bool last = s_flag;
+  if (last) __threadfence();
+  return last;
+}
+
+// true in every thread of the block that finished last in the grid
+__device__ __forceinline__ bool global_last(uint32_t* ticket) {
   __shared__ int s_last;
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
     const uint32_t t = atomicAdd(ticket, 1u);
     s_last = (t == gridDim.x - 1);
+    if (s_last) *ticket = 0u;
   }
   __syncthreads();
-  if (s_last) __threadfence();
-  return s_last;
+  const bool last = s_last;
+  if (last) __threadfence();
+  return last;
 }
 
-// Sum NQ partial quantities per lane over the lane's tiles (warp per lane, fixed order)
-// and hand them to `fn(lane, sums)` in lane 0 of the warp.
-template <int NQ, typename VT, typename F>
-__device__ __forceinline__ void for_each_lane(const Args<VT>& a, F fn) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int l = w; l < a.NL; l += nw) {
-    const int sys = l / a.S, s = l % a.S;
-    const int t0 = a.sys_tile_ptr[sys], t1 = a.sys_tile_ptr[sys + 1];
-    double sums[NQ];
-#pragma unroll
-    for (int k = 0; k < NQ; k++) sums[k] = 0.0;
-    for (int t = t0 + lane; t < t1; t += 32) {
-#pragma unroll
-      for (int k = 0; k < NQ; k++) sums[k] += __ldcg(a.part + (int64_t)t * PQ + k * 4 + s);
-    }
-#pragma unroll
-    for (int k = 0; k < NQ; k++) sums[k] = warp_sum(sums[k]);
-    if (lane == 0) fn(l, sums);
-  }
-}
-
-// recount active lanes and refresh per-system activity (last block only)
-template <typename VT>
-__device__ __forceinline__ void refresh_activity(const Args<VT>& a) {
-  __syncthreads();
-  __shared__ int s_cnt;
-  if (threadIdx.x == 0) s_cnt = 0;
-  __syncthreads();
-  for (int m = threadIdx.x; m < a.nsys; m += blockDim.x) {
-    int act = 0;
-    for (int s = 0; s < a.S; s++) act += a.L.active[m * a.S + s];
-    a.sys_active[m] = act > 0;
-    if (act) atomicAdd(&s_cnt, act);
+// Fixed-order sum of the system's chunk partials: NQ quantities x 4 columns, result in
+// tot (valid in thread 0).
+template <int NQ, typename VT>
+__device__ __forceinline__ void reduce_system(const Args<VT>& a, int sys, double tot[NQ * 4]) {
+  __shared__ double s_tot[PQ];
+  if (threadIdx.x < NQ * 4) {
+    const int c0 = a.sys_chunk_ptr[sys], c1 = a.sys_chunk_ptr[sys + 1];
+    double v = 0.0;
+#pragma unroll 8
+    for (int c = c0; c < c1; c++) v += __ldcg(a.chunk_part + (int64_t)c * PQ + threadIdx.x);
+    s_tot[threadIdx.x] = v;
   }
   __syncthreads();
-  if (threadIdx.x == 0) a.g->n_active = s_cnt;
+#pragma unroll
+  for (int k = 0; k < NQ * 4; k++) tot[k] = s_tot[k];
+  __syncthreads();
 }
 
 template <typename VT, int LD>
@@ -150,10 +182,31 @@ __device__ __forceinline__ void lane_vals(const double* arr, const Args<VT>& a, 
   for (int s = 0; s < LD; s++) out[s] = (s < a.S) ? arr[sys * a.S + s] : 0.0;
 }
 
+template <typename VT>
+__device__ __forceinline__ void set_inactive(const Args<VT>& a, int l, int status, int it) {
+  a.L.active[l] = 0;
+  a.L.status[l] = status;
+  a.L.iters[l] = it;
+  atomicSub(&a.g->n_active, 1);
+}
+
+template <typename VT>
+__device__ __forceinline__ void refresh_system(const Args<VT>& a, int sys) {
+  int act = 0;
+  for (int s = 0; s < a.S; s++) act |= a.L.active[sys * a.S + s];
+  a.sys_active[sys] = act;
+}
+
 // ----------------------------------------------------------------- init
-// I1: Jacobi diagonal from the current FP64 values, Dirichlet values into x
+// I1: Jacobi diagonal from the current FP64 values, Dirichlet values into x, counters
 template <typename VT, int LD>
 __global__ void k_i1(Args<VT> a) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.g->iter = 0;
+    a.g->n_active = 0;
+    a.g->n_trigger = 0;
+    a.g->n_reliable = 0;
+  }
   for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < a.n;
        row += (int64_t)gridDim.x * blockDim.x) {
     VT dv[LD];
@@ -174,8 +227,9 @@ __global__ void k_i1(Args<VT> a) {
         else
           h = mid;
       }
-      const double kd = (l < hi && a.A64.indices[l] == row) ? a.A64.K[l] : 0.0;
-      const double md = (a.A64.M && l < hi && a.A64.indices[l] == row) ? a.A64.M[l] : 0.0;
+      const bool found = l < hi && a.A64.indices[l] == row;
+      const double kd = found ? a.A64.K[l] : 0.0;
+      const double md = (a.A64.M && found) ? a.A64.M[l] : 0.0;
 #pragma unroll
       for (int s = 0; s < LD; s++) {
         double d = a.A64.dscale[s] * kd + a.A64.cscale[s] * md;
@@ -187,9 +241,9 @@ __global__ void k_i1(Args<VT> a) {
   }
 }
 
-// FP64 residual r64 = b - A64 x for the rows of one tile pass; shared by I2/RU2/F2
+// FP64 residual r64 = b - A64 x of one row (all G lanes call it)
 template <typename VT, int LD, int G>
-__device__ __forceinline__ void residual64(const Args<VT>& a, int64_t row, int64_t rr, int gl,
+__device__ __forceinline__ void residual64(const Args<VT>& a, int64_t rr, int gl,
                                            double r64[LD]) {
   double ax[LD];
   csr_row<double, LD, G, false>(a.A64, rr, gl, a.x, ax);
@@ -197,16 +251,16 @@ __device__ __forceinline__ void residual64(const Args<VT>& a, int64_t row, int64
   ldv_cg<double, LD>(a.b, rr, bv);
 #pragma unroll
   for (int s = 0; s < LD; s++) r64[s] = (s < a.S) ? bv[s] - ax[s] : 0.0;
-  (void)row;
 }
 
-// I2: r = b - A x, z = D^-1 r, p = z, xi = 0; partials rr, rz, bb
-template <typename VT, int LD, int G>
+// I2: r = b - A x, z = D^-1 r, p = z, xi = 0; per system rr, rz, bb -> lane state
+template <typename VT, int LD, int G, bool COND>
 __global__ void __launch_bounds__(256) k_i2(Args<VT> a) {
   __shared__ double sh[32 * 3 * LD];
   const int gl = threadIdx.x % G;
   const int rpb = blockDim.x / G;
   for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+    const int sys = a.tile_sys[t];
     const int64_t r0 = a.tile_row0[t], r1 = a.tile_row0[t + 1];
     double acc[3 * LD];
 #pragma unroll
@@ -215,7 +269,7 @@ __global__ void __launch_bounds__(256) k_i2(Args<VT> a) {
       const int64_t row = base + threadIdx.x / G;
       const int64_t rr = row < r1 ? row : r1 - 1;
       double r64[LD];
-      residual64<VT, LD, G>(a, row, rr, gl, r64);
+      residual64<VT, LD, G>(a, rr, gl, r64);
       if (row < r1 && gl == 0) {
         VT rv[LD], dv[LD], zv[LD], zero[LD];
         ldv_cg<VT, LD>(a.dinv, row, dv);
@@ -239,53 +293,63 @@ __global__ void __launch_bounds__(256) k_i2(Args<VT> a) {
     block_sum_vec<3 * LD>(acc, sh);
     if (threadIdx.x == 0) {
 #pragma unroll
-      for (int s = 0; s < LD; s++) {
-        a.part[(int64_t)t * PQ + 0 + s] = acc[s];
-        a.part[(int64_t)t * PQ + 4 + s] = acc[LD + s];
-        a.part[(int64_t)t * PQ + 8 + s] = acc[2 * LD + s];
+      for (int s = 0; s < 4; s++) {
+        a.part[(int64_t)t * PQ + 0 + s] = s < LD ? acc[s] : 0.0;
+        a.part[(int64_t)t * PQ + 4 + s] = s < LD ? acc[LD + s] : 0.0;
+        a.part[(int64_t)t * PQ + 8 + s] = s < LD ? acc[2 * LD + s] : 0.0;
+      }
+    }
+    if (finish_tile(a, t, sys, K_I2)) {
+      double tot[12];
+      reduce_system<3>(a, sys, tot);
+      if (threadIdx.x == 0) {
+        int act_all = 0;
+        for (int s = 0; s < a.S; s++) {
+          const int l = sys * a.S + s;
+          const double rr = tot[s], rz = tot[4 + s], bb = tot[8 + s];
+          const double rt = a.rtol[l];
+          a.L.bb[l] = bb;
+          a.L.tol2[l] = rt * rt * bb;
+          a.L.rr[l] = rr;
+          a.L.rtrue[l] = rr;
+          a.L.rmax2[l] = rr;
+          a.L.rz[l] = rz;
+          a.L.alpha[l] = 0.0;
+          a.L.beta[l] = 0.0;
+          a.L.trigger[l] = 0;
+          a.L.iters[l] = 0;
+          const bool fin = isfinite(rr) && isfinite(rz);
+          const bool act = fin && rr > a.L.tol2[l];
+          a.L.active[l] = act;
+          a.L.status[l] = !fin ? LS_NONFINITE : (act ? LS_RUNNING : LS_OK);
+          act_all += act;
+        }
+        a.sys_active[sys] = act_all > 0;
+        a.sys_trig[sys] = 0;
+        if (act_all) atomicAdd(&a.g->n_active, act_all);
       }
     }
   }
-  if (!last_block(&a.g->ticket[0])) return;
-  for_each_lane<3>(a, [&](int l, const double* v) {
-    const double rr = v[0], rz = v[1], bb = v[2];
-    const double rt = a.rtol[l];
-    a.L.bb[l] = bb;
-    a.L.tol2[l] = rt * rt * bb;
-    a.L.rr[l] = rr;
-    a.L.rtrue[l] = rr;
-    a.L.rmax2[l] = rr;
-    a.L.rz[l] = rz;
-    a.L.alpha[l] = 0.0;
-    a.L.beta[l] = 0.0;
-    a.L.trigger[l] = 0;
-    a.L.iters[l] = 0;
-    const bool fin = isfinite(rr) && isfinite(rz);
-    const bool act = fin && rr > a.L.tol2[l];
-    a.L.active[l] = act;
-    a.L.status[l] = !fin ? LS_NONFINITE : (act ? LS_RUNNING : LS_OK);
-  });
-  refresh_activity(a);
-  if (threadIdx.x == 0) {
-    a.g->iter = 0;
-    a.g->n_reliable = 0;
-    a.g->any_trigger = 0;
-    a.g->ticket[0] = 0;
+  if (global_last(&a.g->ticket[K_I2]) && threadIdx.x == 0) {
     const int cont = (a.g->n_active > 0) && (a.g->max_it > 0);
     a.g->cont = cont;
-    if (a.use_cond) cudaGraphSetConditional(a.h_while, cont);
+    if constexpr (COND) cudaGraphSetConditional(a.h_while, cont);
   }
 }
 
 // ----------------------------------------------------------------- iteration
+// B1: q = A p, pq per lane -> alpha
 template <typename VT, int LD, int G>
 __global__ void __launch_bounds__(256) k_b1(Args<VT> a) {
   __shared__ double sh[32 * LD];
   const int gl = threadIdx.x % G;
   const int rpb = blockDim.x / G;
+  const VT* __restrict__ P = a.p;
+  VT* __restrict__ Q = a.q;
+  const bool timing = a.g->timing != 0;  // autotuner / roofline timing: all tiles, no lane updates
   for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
     const int sys = a.tile_sys[t];
-    if (!a.sys_active[sys]) continue;
+    if (!timing && !a.sys_active[sys]) continue;
     const int64_t r0 = a.tile_row0[t], r1 = a.tile_row0[t + 1];
     double acc[LD];
 #pragma unroll
@@ -294,11 +358,11 @@ __global__ void __launch_bounds__(256) k_b1(Args<VT> a) {
       const int64_t row = base + threadIdx.x / G;
       const int64_t rr = row < r1 ? row : r1 - 1;
       VT qv[LD];
-      csr_row<VT, LD, G, true>(a.Ain, rr, gl, a.p, qv);
+      csr_row<VT, LD, G, true>(a.Ain, rr, gl, P, qv);
       if (row < r1 && gl == 0) {
-        stv<VT, LD>(a.q, row, qv);
+        stv<VT, LD>(Q, row, qv);
         VT pv[LD];
-        ldv<VT, LD>(a.p, row, pv);
+        ldv<VT, LD>(P, row, pv);
 #pragma unroll
         for (int s = 0; s < LD; s++) acc[s] += (double)pv[s] * (double)qv[s];
       }
@@ -306,33 +370,42 @@ __global__ void __launch_bounds__(256) k_b1(Args<VT> a) {
     block_sum_vec<LD>(acc, sh);
     if (threadIdx.x == 0) {
 #pragma unroll
-      for (int s = 0; s < LD; s++) a.part[(int64_t)t * PQ + s] = acc[s];
+      for (int s = 0; s < 4; s++) a.part[(int64_t)t * PQ + s] = s < LD ? acc[s] : 0.0;
+    }
+    if (finish_tile(a, t, sys, K_B1)) {
+      double tot[4];
+      reduce_system<1>(a, sys, tot);
+      if (threadIdx.x == 0 && !timing) {
+        for (int s = 0; s < a.S; s++) {
+          const int l = sys * a.S + s;
+          if (!a.L.active[l]) {
+            a.L.alpha[l] = 0.0;
+            continue;
+          }
+          const double pq = tot[s];
+          if (!isfinite(pq) || !(pq > 0.0)) {
+            a.L.alpha[l] = 0.0;
+            set_inactive(a, l, isfinite(pq) ? LS_BREAKDOWN : LS_NONFINITE, a.g->iter);
+            continue;
+          }
+          a.L.alpha[l] = a.L.rz[l] / pq;
+        }
+        refresh_system(a, sys);
+      }
     }
   }
-  if (!last_block(&a.g->ticket[1])) return;
-  for_each_lane<1>(a, [&](int l, const double* v) {
-    if (!a.L.active[l]) {
-      a.L.alpha[l] = 0.0;
-      return;
-    }
-    const double pq = v[0];
-    if (!isfinite(pq) || !(pq > 0.0)) {
-      a.L.alpha[l] = 0.0;
-      a.L.active[l] = 0;
-      a.L.status[l] = isfinite(pq) ? LS_BREAKDOWN : LS_NONFINITE;
-      a.L.iters[l] = a.g->iter;
-      return;
-    }
-    a.L.alpha[l] = a.L.rz[l] / pq;
-  });
-  refresh_activity(a);
-  if (threadIdx.x == 0) a.g->ticket[1] = 0;
 }
 
-template <typename VT, int LD>
+// B2: xi += alpha p, r -= alpha q, z = D^-1 r; rz, rr per lane -> beta, trigger
+template <typename VT, int LD, bool COND>
 __global__ void __launch_bounds__(256) k_b2(Args<VT> a) {
   __shared__ double sh[32 * 2 * LD];
-  const int rpb = blockDim.x;
+  const VT* __restrict__ P = a.p;
+  const VT* __restrict__ Q = a.q;
+  const VT* __restrict__ DI = a.dinv;
+  VT* __restrict__ R = a.r;
+  VT* __restrict__ XI = a.xi;
+  VT* __restrict__ Z = a.z;
   for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
     const int sys = a.tile_sys[t];
     if (!a.sys_active[sys]) continue;
@@ -342,13 +415,13 @@ __global__ void __launch_bounds__(256) k_b2(Args<VT> a) {
     double acc[2 * LD];
 #pragma unroll
     for (int k = 0; k < 2 * LD; k++) acc[k] = 0.0;
-    for (int64_t row = r0 + threadIdx.x; row < r1; row += rpb) {
+    for (int64_t row = r0 + threadIdx.x; row < r1; row += blockDim.x) {
       VT pv[LD], qv[LD], rv[LD], xv[LD], dv[LD], zv[LD];
-      ldv_cg<VT, LD>(a.p, row, pv);
-      ldv_cg<VT, LD>(a.q, row, qv);
-      ldv_cg<VT, LD>(a.r, row, rv);
-      ldv_cg<VT, LD>(a.xi, row, xv);
-      ldv<VT, LD>(a.dinv, row, dv);
+      ldv_cg<VT, LD>(P, row, pv);
+      ldv_cg<VT, LD>(Q, row, qv);
+      ldv_cg<VT, LD>(R, row, rv);
+      ldv_cg<VT, LD>(XI, row, xv);
+      ldv<VT, LD>(DI, row, dv);
 #pragma unroll
       for (int s = 0; s < LD; s++) {
         if (al[s] != 0.0) {
@@ -360,69 +433,68 @@ __global__ void __launch_bounds__(256) k_b2(Args<VT> a) {
         acc[s] += (double)rv[s] * (double)zv[s];
         acc[LD + s] += (double)rv[s] * (double)rv[s];
       }
-      stv<VT, LD>(a.xi, row, xv);
-      stv<VT, LD>(a.r, row, rv);
-      stv<VT, LD>(a.z, row, zv);
+      stv<VT, LD>(XI, row, xv);
+      stv<VT, LD>(R, row, rv);
+      stv<VT, LD>(Z, row, zv);
     }
     block_sum_vec<2 * LD>(acc, sh);
     if (threadIdx.x == 0) {
 #pragma unroll
-      for (int s = 0; s < LD; s++) {
-        a.part[(int64_t)t * PQ + s] = acc[s];
-        a.part[(int64_t)t * PQ + 4 + s] = acc[LD + s];
+      for (int s = 0; s < 4; s++) {
+        a.part[(int64_t)t * PQ + s] = s < LD ? acc[s] : 0.0;
+        a.part[(int64_t)t * PQ + 4 + s] = s < LD ? acc[LD + s] : 0.0;
+      }
+    }
+    if (finish_tile(a, t, sys, K_B2)) {
+      double tot[8];
+      reduce_system<2>(a, sys, tot);
+      if (threadIdx.x == 0) {
+        const int it = a.g->iter + 1;
+        int ntrig = 0;
+        for (int s = 0; s < a.S; s++) {
+          const int l = sys * a.S + s;
+          if (!a.L.active[l]) {
+            a.L.beta[l] = 0.0;
+            a.L.trigger[l] = 0;
+            continue;
+          }
+          const double rz = tot[s], rr = tot[4 + s];
+          if (!isfinite(rz) || !isfinite(rr)) {
+            a.L.trigger[l] = 0;
+            set_inactive(a, l, LS_NONFINITE, it);
+            continue;
+          }
+          const double old = a.L.rz[l];
+          a.L.beta[l] = (old != 0.0) ? rz / old : 0.0;
+          a.L.rz[l] = rz;
+          a.L.rr[l] = rr;
+          const bool trig = (rr <= a.L.tol2[l]) ||
+                            (a.g->delta2 > 0.0 && rr < a.g->delta2 * a.L.rmax2[l]);
+          a.L.trigger[l] = trig;
+          ntrig += trig;
+        }
+        a.sys_trig[sys] = ntrig > 0;
+        if (ntrig) atomicAdd(&a.g->n_trigger, ntrig);
+        refresh_system(a, sys);
       }
     }
   }
-  if (!last_block(&a.g->ticket[2])) return;
-  __shared__ int s_any;
-  if (threadIdx.x == 0) s_any = 0;
-  __syncthreads();
-  const int it = a.g->iter + 1;
-  for_each_lane<2>(a, [&](int l, const double* v) {
-    if (!a.L.active[l]) {
-      a.L.beta[l] = 0.0;
-      a.L.trigger[l] = 0;
-      return;
-    }
-    const double rz = v[0], rr = v[1];
-    if (!isfinite(rz) || !isfinite(rr)) {
-      a.L.active[l] = 0;
-      a.L.status[l] = LS_NONFINITE;
-      a.L.iters[l] = it;
-      a.L.trigger[l] = 0;
-      return;
-    }
-    const double old = a.L.rz[l];
-    a.L.beta[l] = (old != 0.0) ? rz / old : 0.0;
-    a.L.rz[l] = rz;
-    a.L.rr[l] = rr;
-    const bool trig = (rr <= a.L.tol2[l]) || (a.g->delta2 > 0.0 && rr < a.g->delta2 * a.L.rmax2[l]);
-    a.L.trigger[l] = trig;
-    if (trig) atomicOr(&s_any, 1);
-  });
-  refresh_activity(a);
-  if (threadIdx.x == 0) {
-    a.g->iter = it;
-    a.g->any_trigger = s_any;
-    a.g->ticket[2] = 0;
-    if (a.use_cond) cudaGraphSetConditional(a.h_if, s_any ? 1u : 0u);
+  if (global_last(&a.g->ticket[K_B2]) && threadIdx.x == 0) {
+    a.g->iter += 1;
+    if constexpr (COND) cudaGraphSetConditional(a.h_if, a.g->n_trigger > 0 ? 1u : 0u);
   }
 }
 
 // RU1: fold the inner correction of trigger lanes into x (FP64)
 template <typename VT, int LD>
 __global__ void k_ru1(Args<VT> a) {
-  if (!a.use_cond && !a.g->any_trigger) return;
+  if (a.g->n_trigger == 0) return;
   for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
     const int sys = a.tile_sys[t];
+    if (!a.sys_trig[sys]) continue;
     int trig[LD];
-    bool anyt = false;
 #pragma unroll
-    for (int s = 0; s < LD; s++) {
-      trig[s] = (s < a.S) ? a.L.trigger[sys * a.S + s] : 0;
-      anyt |= trig[s] != 0;
-    }
-    if (!anyt) continue;
+    for (int s = 0; s < LD; s++) trig[s] = (s < a.S) ? a.L.trigger[sys * a.S + s] : 0;
     const int64_t r0 = a.tile_row0[t], r1 = a.tile_row0[t + 1];
     for (int64_t row = r0 + threadIdx.x; row < r1; row += blockDim.x) {
       VT xv[LD];
@@ -439,23 +511,19 @@ __global__ void k_ru1(Args<VT> a) {
   }
 }
 
-// RU2: FP64 residual of trigger lanes; converge or replace the FP32 residual
+// RU2: FP64 residual of trigger lanes; converge or replace the inner residual
 template <typename VT, int LD, int G>
 __global__ void __launch_bounds__(256) k_ru2(Args<VT> a) {
   __shared__ double sh[32 * 2 * LD];
-  if (!a.use_cond && !a.g->any_trigger) return;
+  if (a.g->n_trigger == 0) return;
   const int gl = threadIdx.x % G;
   const int rpb = blockDim.x / G;
   for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
     const int sys = a.tile_sys[t];
+    if (!a.sys_trig[sys]) continue;
     int trig[LD];
-    bool anyt = false;
 #pragma unroll
-    for (int s = 0; s < LD; s++) {
-      trig[s] = (s < a.S) ? a.L.trigger[sys * a.S + s] : 0;
-      anyt |= trig[s] != 0;
-    }
-    if (!anyt) continue;
+    for (int s = 0; s < LD; s++) trig[s] = (s < a.S) ? a.L.trigger[sys * a.S + s] : 0;
     const int64_t r0 = a.tile_row0[t], r1 = a.tile_row0[t + 1];
     double acc[2 * LD];
 #pragma unroll
@@ -464,7 +532,7 @@ __global__ void __launch_bounds__(256) k_ru2(Args<VT> a) {
       const int64_t row = base + threadIdx.x / G;
       const int64_t rr = row < r1 ? row : r1 - 1;
       double r64[LD];
-      residual64<VT, LD, G>(a, row, rr, gl, r64);
+      residual64<VT, LD, G>(a, rr, gl, r64);
       if (row < r1 && gl == 0) {
         VT rv[LD], dv[LD], zv[LD];
         ldv_cg<VT, LD>(a.r, row, rv);
@@ -486,46 +554,48 @@ __global__ void __launch_bounds__(256) k_ru2(Args<VT> a) {
     block_sum_vec<2 * LD>(acc, sh);
     if (threadIdx.x == 0) {
 #pragma unroll
-      for (int s = 0; s < LD; s++) {
-        a.part[(int64_t)t * PQ + s] = acc[s];
-        a.part[(int64_t)t * PQ + 4 + s] = acc[LD + s];
+      for (int s = 0; s < 4; s++) {
+        a.part[(int64_t)t * PQ + s] = s < LD ? acc[s] : 0.0;
+        a.part[(int64_t)t * PQ + 4 + s] = s < LD ? acc[LD + s] : 0.0;
+      }
+    }
+    if (finish_tile(a, t, sys, K_RU2)) {
+      double tot[8];
+      reduce_system<2>(a, sys, tot);
+      if (threadIdx.x == 0) {
+        const int it = a.g->iter;
+        for (int s = 0; s < a.S; s++) {
+          const int l = sys * a.S + s;
+          if (!a.L.trigger[l]) continue;
+          a.L.trigger[l] = 0;
+          const double rr = tot[s], rz = tot[4 + s];
+          a.L.rtrue[l] = rr;
+          if (!isfinite(rr)) {
+            set_inactive(a, l, LS_NONFINITE, it);
+          } else if (rr <= a.L.tol2[l]) {
+            set_inactive(a, l, LS_OK, it);
+          } else {
+            a.L.rz[l] = rz;
+            a.L.rr[l] = rr;
+            a.L.rmax2[l] = rr;
+          }
+        }
+        a.sys_trig[sys] = 0;
+        refresh_system(a, sys);
       }
     }
   }
-  if (!last_block(&a.g->ticket[3])) return;
-  const int it = a.g->iter;
-  for_each_lane<2>(a, [&](int l, const double* v) {
-    if (!a.L.trigger[l]) return;
-    a.L.trigger[l] = 0;
-    const double rr = v[0], rz = v[1];
-    a.L.rtrue[l] = rr;
-    if (!isfinite(rr)) {
-      a.L.active[l] = 0;
-      a.L.status[l] = LS_NONFINITE;
-      a.L.iters[l] = it;
-      return;
-    }
-    if (rr <= a.L.tol2[l]) {
-      a.L.active[l] = 0;
-      a.L.status[l] = LS_OK;
-      a.L.iters[l] = it;
-      return;
-    }
-    a.L.rz[l] = rz;
-    a.L.rr[l] = rr;
-    a.L.rmax2[l] = rr;
-  });
-  refresh_activity(a);
-  if (threadIdx.x == 0) {
+  if (global_last(&a.g->ticket[K_RU2]) && threadIdx.x == 0) {
     a.g->n_reliable += 1;
-    a.g->any_trigger = 0;
-    a.g->ticket[3] = 0;
+    a.g->n_trigger = 0;
   }
 }
 
 // B4: p = z + beta p; decide whether the loop continues
-template <typename VT, int LD>
+template <typename VT, int LD, bool COND>
 __global__ void __launch_bounds__(256) k_b4(Args<VT> a) {
+  const VT* __restrict__ Z = a.z;
+  VT* __restrict__ P = a.p;
   for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
     const int sys = a.tile_sys[t];
     if (!a.sys_active[sys]) continue;
@@ -537,18 +607,18 @@ __global__ void __launch_bounds__(256) k_b4(Args<VT> a) {
     const int64_t r0 = a.tile_row0[t], r1 = a.tile_row0[t + 1];
     for (int64_t row = r0 + threadIdx.x; row < r1; row += blockDim.x) {
       VT pv[LD], zv[LD];
-      ldv_cg<VT, LD>(a.p, row, pv);
-      ldv_cg<VT, LD>(a.z, row, zv);
+      ldv_cg<VT, LD>(P, row, pv);
+      ldv_cg<VT, LD>(Z, row, zv);
 #pragma unroll
       for (int s = 0; s < LD; s++)
         if (act[s]) pv[s] = zv[s] + (VT)be[s] * pv[s];
-      stv<VT, LD>(a.p, row, pv);
+      stv<VT, LD>(P, row, pv);
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     const int cont = (a.g->n_active > 0) && (a.g->iter < a.g->max_it);
     a.g->cont = cont;
-    if (a.use_cond) cudaGraphSetConditional(a.h_while, cont);
+    if constexpr (COND) cudaGraphSetConditional(a.h_while, cont);
   }
 }
 
@@ -575,6 +645,7 @@ __global__ void __launch_bounds__(256) k_f2(Args<VT> a) {
   const int gl = threadIdx.x % G;
   const int rpb = blockDim.x / G;
   for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+    const int sys = a.tile_sys[t];
     const int64_t r0 = a.tile_row0[t], r1 = a.tile_row0[t + 1];
     double acc[LD];
 #pragma unroll
@@ -583,7 +654,7 @@ __global__ void __launch_bounds__(256) k_f2(Args<VT> a) {
       const int64_t row = base + threadIdx.x / G;
       const int64_t rr = row < r1 ? row : r1 - 1;
       double r64[LD];
-      residual64<VT, LD, G>(a, row, rr, gl, r64);
+      residual64<VT, LD, G>(a, rr, gl, r64);
       if (row < r1 && gl == 0) {
 #pragma unroll
         for (int s = 0; s < LD; s++) acc[s] += r64[s] * r64[s];
@@ -592,67 +663,108 @@ __global__ void __launch_bounds__(256) k_f2(Args<VT> a) {
     block_sum_vec<LD>(acc, sh);
     if (threadIdx.x == 0) {
 #pragma unroll
-      for (int s = 0; s < LD; s++) a.part[(int64_t)t * PQ + s] = acc[s];
+      for (int s = 0; s < 4; s++) a.part[(int64_t)t * PQ + s] = s < LD ? acc[s] : 0.0;
+    }
+    if (finish_tile(a, t, sys, K_F2)) {
+      double tot[4];
+      reduce_system<1>(a, sys, tot);
+      if (threadIdx.x == 0) {
+        const int it = a.g->iter;
+        for (int s = 0; s < a.S; s++) {
+          const int l = sys * a.S + s;
+          a.L.rtrue[l] = tot[s];
+          if (a.L.status[l] == LS_RUNNING) {
+            a.L.status[l] = (tot[s] <= a.L.tol2[l]) ? LS_OK : LS_MAXIT;
+            a.L.iters[l] = it;
+            a.L.active[l] = 0;
+          }
+        }
+      }
     }
   }
-  if (!last_block(&a.g->ticket[4])) return;
-  const int it = a.g->iter;
-  for_each_lane<1>(a, [&](int l, const double* v) {
-    a.L.rtrue[l] = v[0];
-    if (a.L.status[l] == LS_RUNNING) {
-      a.L.status[l] = (v[0] <= a.L.tol2[l]) ? LS_OK : LS_MAXIT;
-      a.L.iters[l] = it;
-      a.L.active[l] = 0;
-    }
-  });
-  if (threadIdx.x == 0) a.g->ticket[4] = 0;
 }
 
 // ----------------------------------------------------------------- host side
 static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct Layout {
-  size_t vec, part, lanes_d, lanes_i, sysact, glob, trow, tsys, sptr, total;
+  size_t vec, part, lanes_d, lanes_i, sysact, systrig, systicket, glob, trow, tsys, sptr,
+      tchunk, cptr, schptr, cpart, cticket, total;
 };
 
-static int64_t count_tiles(const tp_csr_op* op, int rpt, std::vector<int64_t>* row0,
-                           std::vector<int32_t>* tsys, std::vector<int32_t>* sptr) {
+// Row tiles (never straddling two systems) and chunks of up to CHUNK tiles of one system.
+struct Tiles {
+  std::vector<int64_t> row0;
+  std::vector<int32_t> tsys, sptr, tchunk, cptr, schptr;
+  int64_t nt = 0, nch = 0;
+};
+
+static Tiles make_tiles(const tp_csr_op* op, int rpt) {
+  Tiles T;
   const int nsys = op->n_systems > 0 ? op->n_systems : 1;
-  int64_t nt = 0;
-  if (sptr) sptr->assign(1, 0);
+  T.sptr.push_back(0);
+  T.cptr.push_back(0);
+  T.schptr.push_back(0);
   for (int m = 0; m < nsys; m++) {
     const int64_t a = op->sys_row_ptr ? op->sys_row_ptr[m] : 0;
     const int64_t b = op->sys_row_ptr ? op->sys_row_ptr[m + 1] : op->n_rows;
+    int64_t in_chunk = 0;
     for (int64_t r = a; r < b; r += rpt) {
-      if (row0) {
-        row0->push_back(r);
-        tsys->push_back(m);
+      if (in_chunk == CHUNK) {
+        T.cptr.push_back((int32_t)T.nt);
+        T.nch++;
+        in_chunk = 0;
       }
-      nt++;
+      T.row0.push_back(r);
+      T.tsys.push_back(m);
+      T.tchunk.push_back((int32_t)T.nch);
+      T.nt++;
+      in_chunk++;
     }
-    if (sptr) sptr->push_back((int32_t)nt);
+    if (in_chunk > 0) {
+      T.cptr.push_back((int32_t)T.nt);
+      T.nch++;
+    }
+    T.sptr.push_back((int32_t)T.nt);
+    T.schptr.push_back((int32_t)T.nch);
   }
-  if (row0) row0->push_back(op->n_rows);
-  return nt;
+  T.row0.push_back(op->n_rows);
+  return T;
+}
+
+static int64_t count_tiles(const tp_csr_op* op, int rpt, int64_t* nch) {
+  const Tiles T = make_tiles(op, rpt);
+  if (nch) *nch = T.nch;
+  return T.nt;
 }
 
 static Layout layout(const tp_csr_op* op, const tp_cg_config* cfg) {
   const int nsys = op->n_systems > 0 ? op->n_systems : 1;
   const int NL = nsys * op->S;
   const size_t vt = cfg->inner_fp32 ? 4 : 8;
-  const int64_t nt = count_tiles(op, cfg->rows_per_tile, nullptr, nullptr, nullptr);
+  int64_t nch = 0;
+  const int64_t nt = count_tiles(op, cfg->rows_per_tile, &nch);
+  const size_t nt1 = (size_t)std::max<int64_t>(nt, 1), nc1 = (size_t)std::max<int64_t>(nch, 1);
   Layout L;
   L.vec = al256(vt * op->ld * (size_t)op->n_rows);
-  L.part = al256(sizeof(double) * PQ * (size_t)std::max<int64_t>(nt, 1));
+  L.part = al256(sizeof(double) * PQ * nt1);
   L.lanes_d = al256(sizeof(double) * NL);
   L.lanes_i = al256(sizeof(int32_t) * NL);
   L.sysact = al256(sizeof(int32_t) * nsys);
+  L.systrig = al256(sizeof(int32_t) * nsys);
+  L.systicket = al256(sizeof(uint32_t) * N_KINDS * nsys);
   L.glob = al256(sizeof(Glob));
   L.trow = al256(sizeof(int64_t) * (nt + 1));
-  L.tsys = al256(sizeof(int32_t) * std::max<int64_t>(nt, 1));
+  L.tsys = al256(sizeof(int32_t) * nt1);
   L.sptr = al256(sizeof(int32_t) * (nsys + 1));
-  L.total = 6 * L.vec + L.part + 8 * L.lanes_d + 4 * L.lanes_i + L.sysact + L.glob + L.trow +
-            L.tsys + L.sptr;
+  L.tchunk = al256(sizeof(int32_t) * nt1);
+  L.cptr = al256(sizeof(int32_t) * (nc1 + 1));
+  L.schptr = al256(sizeof(int32_t) * (nsys + 1));
+  L.cpart = al256(sizeof(double) * PQ * nc1);
+  L.cticket = al256(sizeof(uint32_t) * N_KINDS * nc1);
+  L.total = 6 * L.vec + L.part + 8 * L.lanes_d + 4 * L.lanes_i + L.sysact + L.systrig +
+            L.systicket + L.glob + L.trow + L.tsys + L.sptr + L.tchunk + L.cptr + L.schptr +
+            L.cpart + L.cticket;
   return L;
 }
 
@@ -680,41 +792,48 @@ struct KernelSet {
   KFn i1, i2, b1, b2, ru1, ru2, b4, f1, f2;
 };
 
-template <typename VT, int LD, int G>
+// COND: the variant that drives the graph's conditional nodes; the host-loop variant
+// carries no device-side conditional call (profilers can then see every kernel node).
+template <typename VT, int LD, int G, bool COND>
 static KernelSet kset() {
   KernelSet k;
   k.i1 = (KFn)k_i1<VT, LD>;
-  k.i2 = (KFn)k_i2<VT, LD, G>;
+  k.i2 = (KFn)k_i2<VT, LD, G, COND>;
   k.b1 = (KFn)k_b1<VT, LD, G>;
-  k.b2 = (KFn)k_b2<VT, LD>;
+  k.b2 = (KFn)k_b2<VT, LD, COND>;
   k.ru1 = (KFn)k_ru1<VT, LD>;
   k.ru2 = (KFn)k_ru2<VT, LD, G>;
-  k.b4 = (KFn)k_b4<VT, LD>;
+  k.b4 = (KFn)k_b4<VT, LD, COND>;
   k.f1 = (KFn)k_f1<VT, LD>;
   k.f2 = (KFn)k_f2<VT, LD, G>;
   return k;
 }
 
-template <typename VT, int LD>
-static bool kset_g(int G, KernelSet* k) {
+template <typename VT, int LD, bool COND>
+static bool kset_gc(int G, KernelSet* k) {
   switch (G) {
-    case 1: *k = kset<VT, LD, 1>(); return true;
-    case 2: *k = kset<VT, LD, 2>(); return true;
-    case 4: *k = kset<VT, LD, 4>(); return true;
-    case 8: *k = kset<VT, LD, 8>(); return true;
+    case 1: *k = kset<VT, LD, 1, COND>(); return true;
+    case 2: *k = kset<VT, LD, 2, COND>(); return true;
+    case 4: *k = kset<VT, LD, 4, COND>(); return true;
+    case 8: *k = kset<VT, LD, 8, COND>(); return true;
     default: return false;
   }
 }
 
-static bool get_kernels(int fp32, int ld, int G, KernelSet* k) {
+template <typename VT, int LD>
+static bool kset_g(int G, bool cond, KernelSet* k) {
+  return cond ? kset_gc<VT, LD, true>(G, k) : kset_gc<VT, LD, false>(G, k);
+}
+
+static bool get_kernels(int fp32, int ld, int G, bool cond, KernelSet* k) {
   if (fp32) {
-    if (ld == 1) return kset_g<float, 1>(G, k);
-    if (ld == 2) return kset_g<float, 2>(G, k);
-    if (ld == 4) return kset_g<float, 4>(G, k);
+    if (ld == 1) return kset_g<float, 1>(G, cond, k);
+    if (ld == 2) return kset_g<float, 2>(G, cond, k);
+    if (ld == 4) return kset_g<float, 4>(G, cond, k);
   } else {
-    if (ld == 1) return kset_g<double, 1>(G, k);
-    if (ld == 2) return kset_g<double, 2>(G, k);
-    if (ld == 4) return kset_g<double, 4>(G, k);
+    if (ld == 1) return kset_g<double, 1>(G, cond, k);
+    if (ld == 2) return kset_g<double, 2>(G, cond, k);
+    if (ld == 4) return kset_g<double, 4>(G, cond, k);
   }
   return false;
 }
@@ -814,7 +933,7 @@ static int build_graphs(tp_cg_handle* h, const KernelSet& K, void* arg) {
 
 template <typename VT>
 static void fill_args(Args<VT>& a, const tp_csr_op* op, const tp_cg_config* cfg, char* ws,
-                      const Layout& L, int64_t nt, const double* b, double* x,
+                      const Layout& L, int64_t nt, int64_t nch, const double* b, double* x,
                       const double* rtol, int use_cond) {
   const int nsys = op->n_systems > 0 ? op->n_systems : 1;
   a.n = op->n_rows;
@@ -823,7 +942,8 @@ static void fill_args(Args<VT>& a, const tp_csr_op* op, const tp_cg_config* cfg,
   a.nsys = nsys;
   a.NL = nsys * op->S;
   a.ntiles = (int)nt;
-  a.use_cond = use_cond;
+  a.nchunks = (int)nch;
+  (void)use_cond;
   a.Ain.indptr = a.A64.indptr = op->indptr;
   a.Ain.indices = a.A64.indices = op->indices;
   a.Ain.bc = a.A64.bc = op->bc_mask;
@@ -866,6 +986,10 @@ static void fill_args(Args<VT>& a, const tp_csr_op* op, const tp_cg_config* cfg,
   }
   a.sys_active = reinterpret_cast<int32_t*>(p);
   p += L.sysact;
+  a.sys_trig = reinterpret_cast<int32_t*>(p);
+  p += L.systrig;
+  a.sys_ticket = reinterpret_cast<uint32_t*>(p);
+  p += L.systicket;
   a.g = reinterpret_cast<Glob*>(p);
   p += L.glob;
   a.tile_row0 = reinterpret_cast<const int64_t*>(p);
@@ -873,6 +997,16 @@ static void fill_args(Args<VT>& a, const tp_csr_op* op, const tp_cg_config* cfg,
   a.tile_sys = reinterpret_cast<const int32_t*>(p);
   p += L.tsys;
   a.sys_tile_ptr = reinterpret_cast<const int32_t*>(p);
+  p += L.sptr;
+  a.tile_chunk = reinterpret_cast<const int32_t*>(p);
+  p += L.tchunk;
+  a.chunk_tile_ptr = reinterpret_cast<const int32_t*>(p);
+  p += L.cptr;
+  a.sys_chunk_ptr = reinterpret_cast<const int32_t*>(p);
+  p += L.schptr;
+  a.chunk_part = reinterpret_cast<double*>(p);
+  p += L.cpart;
+  a.chunk_ticket = reinterpret_cast<uint32_t*>(p);
   a.x = x;
   a.b = b;
   a.rtol = rtol;
@@ -913,12 +1047,11 @@ extern "C" int tp_cg_create(const tp_csr_op* op, const tp_cg_config* cfg, const 
   const Layout L = layout(op, cfg);
   TP_REQUIRE(workspace_bytes >= L.total, "workspace too small (%zu < %zu)", workspace_bytes,
              L.total);
-  std::vector<int64_t> row0;
-  std::vector<int32_t> tsys, sptr;
-  const int64_t nt = count_tiles(op, cfg->rows_per_tile, &row0, &tsys, &sptr);
+  const Tiles T = make_tiles(op, cfg->rows_per_tile);
+  const int64_t nt = T.nt;
   TP_REQUIRE(nt < INT32_MAX, "too many tiles");
   KernelSet K;
-  if (!get_kernels(cfg->inner_fp32, op->ld, cfg->group, &K)) {
+  if (!get_kernels(cfg->inner_fp32, op->ld, cfg->group, cfg->use_graph_loop != 0, &K)) {
     set_error("no kernel for fp32=%d ld=%d group=%d", cfg->inner_fp32, op->ld, cfg->group);
     return TP_ERR_ARG;
   }
@@ -937,13 +1070,14 @@ extern "C" int tp_cg_create(const tp_csr_op* op, const tp_cg_config* cfg, const 
                                                                  cfg->block, 0);
   if (oe != cudaSuccess || occ < 1) occ = 1;
   const int64_t cap = (int64_t)sm_count() * occ;
-  h->grid = (int)std::max<int64_t>(1, std::min<int64_t>(nt, cap));
+  // one tile per block up to 16 resident waves; beyond that blocks loop over tiles
+  h->grid = (int)std::max<int64_t>(1, std::min<int64_t>(nt, 16 * cap));
   h->row_grid = (int)std::max<int64_t>(1, std::min<int64_t>((op->n_rows + cfg->block - 1) / cfg->block, cap));
   char* ws = static_cast<char*>(workspace);
   if (h->vt_fp32)
-    fill_args(h->af, op, cfg, ws, L, nt, b, x, rtol, h->use_cond);
+    fill_args(h->af, op, cfg, ws, L, nt, T.nch, b, x, rtol, h->use_cond);
   else
-    fill_args(h->ad, op, cfg, ws, L, nt, b, x, rtol, h->use_cond);
+    fill_args(h->ad, op, cfg, ws, L, nt, T.nch, b, x, rtol, h->use_cond);
   Glob* gp = h->vt_fp32 ? h->af.g : h->ad.g;
   h->glob = gp;
   h->lanes = h->vt_fp32 ? h->af.L : h->ad.L;
@@ -952,19 +1086,40 @@ extern "C" int tp_cg_create(const tp_csr_op* op, const tp_cg_config* cfg, const 
   g0.max_it = cfg->max_it;
   const double delta = cfg->inner_fp32 ? (cfg->delta > 0 ? cfg->delta : 0.1) : 0.0;
   g0.delta2 = delta * delta;
-  const int64_t* d_row0 = h->vt_fp32 ? h->af.tile_row0 : h->ad.tile_row0;
-  const int32_t* d_tsys = h->vt_fp32 ? h->af.tile_sys : h->ad.tile_sys;
-  const int32_t* d_sptr = h->vt_fp32 ? h->af.sys_tile_ptr : h->ad.sys_tile_ptr;
+  struct Copy {
+    const void* dst;
+    const void* src;
+    size_t bytes;
+  };
+  const bool f = h->vt_fp32 != 0;
+  const Copy copies[] = {
+      {f ? (const void*)h->af.tile_row0 : (const void*)h->ad.tile_row0, T.row0.data(),
+       sizeof(int64_t) * T.row0.size()},
+      {f ? (const void*)h->af.tile_sys : (const void*)h->ad.tile_sys, T.tsys.data(),
+       sizeof(int32_t) * T.tsys.size()},
+      {f ? (const void*)h->af.sys_tile_ptr : (const void*)h->ad.sys_tile_ptr, T.sptr.data(),
+       sizeof(int32_t) * T.sptr.size()},
+      {f ? (const void*)h->af.tile_chunk : (const void*)h->ad.tile_chunk, T.tchunk.data(),
+       sizeof(int32_t) * T.tchunk.size()},
+      {f ? (const void*)h->af.chunk_tile_ptr : (const void*)h->ad.chunk_tile_ptr, T.cptr.data(),
+       sizeof(int32_t) * T.cptr.size()},
+      {f ? (const void*)h->af.sys_chunk_ptr : (const void*)h->ad.sys_chunk_ptr, T.schptr.data(),
+       sizeof(int32_t) * T.schptr.size()},
+  };
+  uint32_t* d_tick = f ? h->af.sys_ticket : h->ad.sys_ticket;
+  uint32_t* d_ctick = f ? h->af.chunk_ticket : h->ad.chunk_ticket;
   int rc = TP_OK;
-  cudaError_t e;
-  if ((e = cudaMemcpyAsync(gp, &g0, sizeof(Glob), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
-      (e = cudaMemcpyAsync((void*)d_row0, row0.data(), sizeof(int64_t) * row0.size(),
-                           cudaMemcpyHostToDevice, st)) != cudaSuccess ||
-      (e = cudaMemcpyAsync((void*)d_tsys, tsys.data(), sizeof(int32_t) * tsys.size(),
-                           cudaMemcpyHostToDevice, st)) != cudaSuccess ||
-      (e = cudaMemcpyAsync((void*)d_sptr, sptr.data(), sizeof(int32_t) * sptr.size(),
-                           cudaMemcpyHostToDevice, st)) != cudaSuccess ||
-      (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+  cudaError_t e = cudaMemcpyAsync(gp, &g0, sizeof(Glob), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(d_tick, 0, sizeof(uint32_t) * N_KINDS * nsys, st);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(d_ctick, 0, sizeof(uint32_t) * N_KINDS * std::max<int64_t>(T.nch, 1), st);
+  for (const Copy& c : copies) {
+    if (e != cudaSuccess) break;
+    if (c.bytes) e = cudaMemcpyAsync((void*)c.dst, c.src, c.bytes, cudaMemcpyHostToDevice, st);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
     set_error("cg setup copy failed: %s", cudaGetErrorString(e));
     delete h;
     return TP_ERR_CUDA;
@@ -1055,11 +1210,11 @@ extern "C" int tp_cg_time_spmv(tp_cg_handle* h, int reps, float* ms, void* strea
   TP_REQUIRE(h && ms && reps > 0, "bad argument");
   cudaStream_t st = as_stream(stream);
   KernelSet K;
-  if (!get_kernels(h->vt_fp32, h->ld, h->G, &K)) return TP_ERR_ARG;
-  const int nsys = h->vt_fp32 ? h->af.nsys : h->ad.nsys;
-  std::vector<int32_t> ones(nsys, 1);
-  TP_CUDA_TRY(cudaMemcpyAsync(h->sys_active, ones.data(), sizeof(int32_t) * nsys,
-                              cudaMemcpyHostToDevice, st));
+  if (!get_kernels(h->vt_fp32, h->ld, h->G, h->use_cond != 0, &K)) return TP_ERR_ARG;
+  // timing mode: B1 processes every tile and leaves the lane state alone
+  static const int32_t on = 1, off = 0;
+  TP_CUDA_TRY(cudaMemcpyAsync(&h->glob->timing, &on, sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  TP_CUDA_TRY(cudaStreamSynchronize(st));
   void* arg = h->vt_fp32 ? (void*)&h->af : (void*)&h->ad;
   void* args[1] = {arg};
   cudaEvent_t e0, e1;
@@ -1075,6 +1230,8 @@ extern "C" int tp_cg_time_spmv(tp_cg_handle* h, int reps, float* ms, void* strea
   TP_CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  TP_CUDA_TRY(cudaMemcpyAsync(&h->glob->timing, &off, sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  TP_CUDA_TRY(cudaStreamSynchronize(st));
   *ms = t / reps;
   return TP_OK;
 }

@@ -11,15 +11,14 @@ import itertools
 
 _CACHE: dict = {}
 
-GROUPS = (2, 4, 8)
+GROUPS = (1, 2, 4, 8)
 BLOCKS = (128, 256)
-TILE_ROWS = (256, 512, 1024)
+TILE_PASSES = (1, 2)       # rows per tile = passes * block
 
 
 def candidates():
-    for g, b, t in itertools.product(GROUPS, BLOCKS, TILE_ROWS):
-        if t % b == 0:
-            yield {"group": g, "block": b, "rows_per_tile": t}
+    for g, b, k in itertools.product(GROUPS, BLOCKS, TILE_PASSES):
+        yield {"group": g, "block": b, "rows_per_tile": k * b}
 
 
 def tune_cg(op, inner_fp32: bool, reps: int = 10, verbose: bool = False) -> dict:
