@@ -41,6 +41,7 @@ extern "C" const char* tp_status_string(int status) {
     case TP_ERR_NOT_CONVERGED: return "not converged";
     case TP_ERR_BREAKDOWN: return "Krylov breakdown (operator not SPD)";
     case TP_ERR_NONFINITE: return "non-finite value";
+    case TP_ERR_TIMEOUT: return "device wait timed out";
     default: return "unknown status";
   }
 }

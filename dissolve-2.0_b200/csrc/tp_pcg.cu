@@ -1,0 +1,946 @@
+// tp_pcg.cu -- persistent Jacobi-PCG: one cooperative launch per solve.
+//
+// The problem sizes of the transport step (a few 100k rows, operator and vectors
+// resident in the 126 MB L2) make a Krylov iteration latency-bound: what costs is the
+// number of dependent launches and reduction tails, not bytes.  This engine runs the
+// whole solve in ONE cooperative kernel with one CTA group per SM:
+//
+//   init  I1 Jacobi diagonal, Dirichlet values into x      | barrier
+//         I2 r = b - A64 x, z = D^-1 r, p = z, norms        | barrier -> lane state
+//   loop  A  q = A p (SELL-32), p.q                         | barrier -> alpha
+//         B  xi += alpha p, r -= alpha q, z = D^-1 r, r.z, r.r | barrier -> beta, trigger
+//         RU (FP32 inner only, when triggered) x += xi        | barrier
+//            r = b - A64 x in FP64, replace r, z             | barrier -> converge / keep
+//         C  p = z + beta p                                 | barrier
+//   final x += xi | barrier | r = b - A64 x -> true residual norms
+//
+// Every CTA owns a contiguous range of 32-row slices.  Each dot product is one FP64
+// partial per CTA; after the barrier every CTA sums all partials in the same fixed order,
+// so all CTAs hold bit-identical scalars and take the same branches (deterministic for a
+// given grid).  The grid barrier is a counter plus a generation word; its spin is bounded
+// (about two seconds), after which the CTA raises an abort flag that every other spin
+// also watches, so a lost CTA ends the kernel with TP_ERR_TIMEOUT instead of a hang.
+//
+// The inner operator is SELL-32: per slice, entry k of its 32 rows is stored
+// contiguously (col, value), so each load of an index or value is one 128-byte warp
+// access; rows shorter than the slice width are padded with their own column and 0.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "tp_ops.cuh"
+
+namespace tp {
+
+struct PBar {
+  unsigned int count;
+  unsigned int gen;
+  unsigned int abort;
+  unsigned int pad;
+};
+
+struct POut {
+  int32_t iterations, n_reliable, status, timeouts;
+  int32_t lane_iters[4], lane_status[4];
+  double lane_rtrue[4], lane_bb[4];
+};
+
+template <typename VT>
+struct PArgs {
+  int64_t n;
+  int S, ns, max_it;
+  double delta2;
+  // inner operator, SELL-32
+  const int32_t* slice_ptr;
+  const int32_t* sell_col;
+  const VT* sK;
+  const VT* sM;
+  const VT* diag;
+  // outer operator, FP64 CSR
+  CsrView<double> A64;
+  double dscale[4], cscale[4];
+  const uint8_t* bc;
+  const double* b;
+  double* x;
+  const double* rtol;
+  VT *p, *q, *r, *z, *xi, *dinv, *p2;  // p / p2: ping-pong search directions
+  double* part;  // gridDim.x * 16
+  PBar* bar;
+  POut* out;
+  unsigned long long* prof;  // optional: gridDim.x * 8 phase times (ns)
+};
+
+constexpr unsigned long long SPIN_LIMIT = 1ull << 25;  // x ~64 ns sleeps: ~2 s
+
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Read-only matrix stream: no L1 allocation, so the L1 keeps the gathered vectors.
+__device__ __forceinline__ int ld_na(const int32_t* p) {
+  int v;
+  asm("ld.global.nc.L1::no_allocate.s32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ float ld_na(const float* p) {
+  float v;
+  asm("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ double ld_na(const double* p) {
+  double v;
+  asm("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+
+__device__ __forceinline__ unsigned long long gtime() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Phase clock of thread 0 (profiling builds of a run only): adds now - last to slot k.
+struct PhaseClock {
+  unsigned long long last = 0, acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  bool on = false;
+  __device__ __forceinline__ void start(bool enable) {
+    on = enable && threadIdx.x == 0;
+    if (on) last = gtime();
+  }
+  __device__ __forceinline__ void lap(int k) {
+    if (on) {
+      const unsigned long long t = gtime();
+      acc[k] += t - last;
+      last = t;
+    }
+  }
+};
+
+// Grid barrier; returns false in every thread when the grid has aborted.
+__device__ __forceinline__ bool grid_sync(PBar* bar, unsigned int& gen) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    __threadfence();
+    const unsigned int arrived = atomicAdd(&bar->count, 1u);
+    if (arrived == gridDim.x - 1) {
+      bar->count = 0u;
+      __threadfence();
+      atomicExch(&bar->gen, gen + 1u);
+    } else {
+      unsigned long long spins = 0;
+      while (ld_acquire(&bar->gen) == gen) {
+        if (ld_acquire(&bar->abort)) {
+          ok = 0;
+          break;
+        }
+        if (++spins > SPIN_LIMIT) {
+          atomicExch(&bar->abort, 1u);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    gen += 1u;
+    s_ok = ok && !ld_acquire(&bar->abort);
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Sum NV slots of every CTA's partial row (fixed order); result in s_tot for all threads.
+template <int NV>
+__device__ __forceinline__ void grid_totals(const double* part, double* s_tot, double* s_buf) {
+  const int T = blockDim.x;
+  const int groups = T / 16;  // blockDim multiple of 16
+  const int k = threadIdx.x % 16, g = threadIdx.x / 16;
+  double v = 0.0;
+  if (k < NV)
+    for (int b = g; b < (int)gridDim.x; b += groups) v += __ldcg(part + (int64_t)b * 16 + k);
+  s_buf[threadIdx.x] = v;
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double t = 0.0;
+    for (int gg = 0; gg < groups; gg++) t += s_buf[gg * 16 + threadIdx.x];
+    s_tot[threadIdx.x] = t;
+  }
+  __syncthreads();
+}
+
+template <int NV>
+__device__ __forceinline__ void block_partial(double v[NV], double* part, double* sh) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NV; k++) v[k] = warp_sum(v[k]);
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; k++) sh[k * 32 + w] = v[k];
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double t = 0.0;
+    for (int ww = 0; ww < nw; ww++) t += sh[threadIdx.x * 32 + ww];
+    part[(int64_t)blockIdx.x * 16 + threadIdx.x] = t;
+  }
+}
+
+struct LaneState {
+  double rz[4], alpha[4], beta[4], rr[4], rmax2[4], tol2[4], bb[4], rtrue[4];
+  int active[4], trigger[4], status[4], iters[4];
+};
+
+template <typename VT, int LD>
+__device__ __forceinline__ void csr64_residual(const PArgs<VT>& a, int64_t row, double r64[LD]) {
+  double ax[LD];
+#pragma unroll
+  for (int s = 0; s < LD; s++) ax[s] = 0.0;
+  const bool bcr = a.bc && a.bc[row];
+  double xr[LD];
+  ldv_cg<double, LD>(a.x, row, xr);
+  if (bcr) {
+#pragma unroll
+    for (int s = 0; s < LD; s++) ax[s] = xr[s];
+  } else {
+    double ak[LD], am[LD];
+#pragma unroll
+    for (int s = 0; s < LD; s++) ak[s] = am[s] = 0.0;
+    const int beg = a.A64.indptr[row], end = a.A64.indptr[row + 1];
+    for (int p = beg; p < end; p++) {
+      const int j = __ldg(a.A64.indices + p);
+      double xv[LD];
+      ldv_cg<double, LD>(a.x, j, xv);
+      const double kv = __ldg(a.A64.K + p);
+#pragma unroll
+      for (int s = 0; s < LD; s++) ak[s] += kv * xv[s];
+      if (a.A64.M) {
+        const double mv = __ldg(a.A64.M + p);
+#pragma unroll
+        for (int s = 0; s < LD; s++) am[s] += mv * xv[s];
+      }
+    }
+    double dr[LD];
+#pragma unroll
+    for (int s = 0; s < LD; s++) dr[s] = 0.0;
+    if (a.A64.diag) ldv<double, LD>(a.A64.diag, row, dr);
+#pragma unroll
+    for (int s = 0; s < LD; s++) ax[s] = a.dscale[s] * ak[s] + a.cscale[s] * am[s] + dr[s] * xr[s];
+  }
+  double bv[LD];
+  ldv_cg<double, LD>(a.b, row, bv);
+#pragma unroll
+  for (int s = 0; s < LD; s++) r64[s] = (s < a.S) ? bv[s] - ax[s] : 0.0;
+}
+
+template <typename VT, int LD, int UNROLL, int MINB>
+__global__ void __launch_bounds__(512, MINB) k_pcg(PArgs<VT> a) {
+  __shared__ double sh[32 * 12];
+  __shared__ double s_buf[512];
+  __shared__ double s_tot[16];
+  __shared__ LaneState L;
+  unsigned int gen = 0;
+  if (threadIdx.x == 0) gen = ld_acquire(&a.bar->gen);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int sb = (int)((int64_t)blockIdx.x * a.ns / gridDim.x);
+  const int se = (int)((int64_t)(blockIdx.x + 1) * a.ns / gridDim.x);
+  const int S = a.S;
+  PhaseClock clk;
+  clk.start(a.prof != nullptr);
+
+#define FOR_OWN_ROWS                                              \
+  for (int sl = sb + warp; sl < se; sl += nwarps)                 \
+    for (int64_t row = (int64_t)sl * 32 + lane; row < a.n; row = a.n)
+
+  // ---- I1: Jacobi diagonal (FP64 values), Dirichlet values into x
+  FOR_OWN_ROWS {
+    VT dv[LD];
+    const bool bcr = a.bc && a.bc[row];
+    if (bcr) {
+#pragma unroll
+      for (int s = 0; s < LD; s++) {
+        dv[s] = VT(0);
+        a.x[row * LD + s] = a.b[row * LD + s];
+      }
+    } else {
+      const int lo = a.A64.indptr[row], hi = a.A64.indptr[row + 1];
+      int l = lo, h = hi;
+      while (l < h) {
+        const int mid = (l + h) >> 1;
+        if (a.A64.indices[mid] < row)
+          l = mid + 1;
+        else
+          h = mid;
+      }
+      const bool found = l < hi && a.A64.indices[l] == row;
+      const double kd = found ? a.A64.K[l] : 0.0;
+      const double md = (a.A64.M && found) ? a.A64.M[l] : 0.0;
+#pragma unroll
+      for (int s = 0; s < LD; s++) {
+        double d = a.dscale[s] * kd + a.cscale[s] * md;
+        if (a.A64.diag) d += a.A64.diag[row * LD + s];
+        dv[s] = (s < S && d != 0.0) ? VT(1.0 / d) : VT(0);
+      }
+    }
+    stv<VT, LD>(a.dinv, row, dv);
+  }
+  bool ok = grid_sync(a.bar, gen);
+
+  // ---- I2: r = b - A x, z = D^-1 r, p = z, xi = 0; rr, rz, bb
+  {
+    double acc[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) acc[k] = 0.0;
+    if (ok) {
+      FOR_OWN_ROWS {
+        double r64[LD];
+        csr64_residual<VT, LD>(a, row, r64);
+        VT rv[LD], dv[LD], zv[LD], zero[LD];
+        ldv_cg<VT, LD>(a.dinv, row, dv);
+        double bv[LD];
+        ldv_cg<double, LD>(a.b, row, bv);
+#pragma unroll
+        for (int s = 0; s < LD; s++) {
+          rv[s] = (VT)r64[s];
+          zv[s] = dv[s] * rv[s];
+          zero[s] = VT(0);
+          acc[s] += r64[s] * r64[s];
+          acc[4 + s] += (double)rv[s] * (double)zv[s];
+          acc[8 + s] += (s < S) ? bv[s] * bv[s] : 0.0;
+        }
+        stv<VT, LD>(a.r, row, rv);
+        stv<VT, LD>(a.z, row, zv);
+        stv<VT, LD>(a.p, row, zv);
+        stv<VT, LD>(a.xi, row, zero);
+      }
+    }
+    block_partial<12>(acc, a.part, sh);
+  }
+  ok = ok && grid_sync(a.bar, gen);
+  if (ok) grid_totals<12>(a.part, s_tot, s_buf);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < 4; s++) {
+      const bool use = s < S && ok;
+      const double rr = use ? s_tot[s] : 0.0, rz = use ? s_tot[4 + s] : 0.0;
+      const double bb = use ? s_tot[8 + s] : 0.0;
+      const double rt = use ? a.rtol[s] : 0.0;
+      L.bb[s] = bb;
+      L.tol2[s] = rt * rt * bb;
+      L.rr[s] = rr;
+      L.rtrue[s] = rr;
+      L.rmax2[s] = rr;
+      L.rz[s] = rz;
+      L.alpha[s] = 0.0;
+      L.beta[s] = 0.0;
+      L.trigger[s] = 0;
+      L.iters[s] = 0;
+      const bool fin = isfinite(rr) && isfinite(rz);
+      const bool act = use && fin && rr > L.tol2[s];
+      L.active[s] = act;
+      L.status[s] = !use ? TP_OK : (!fin ? TP_ERR_NONFINITE : (act ? -1 : TP_OK));
+    }
+  }
+  __syncthreads();
+
+  clk.lap(7);  // init phases
+  int it = 0, n_rel = 0, par = 0;
+  while (ok && it < a.max_it) {
+    int nact = 0;
+#pragma unroll
+    for (int s = 0; s < 4; s++) nact += L.active[s];
+    if (!nact) break;
+    // ---- A: p_new = z + beta p_old (own rows; recomputed for every gathered neighbour),
+    //         q = A p_new, p_new.q
+    VT* __restrict__ p_old = par ? a.p2 : a.p;
+    VT* __restrict__ p_new = par ? a.p : a.p2;
+    {
+      VT be[LD];
+      bool act[LD];
+#pragma unroll
+      for (int s = 0; s < LD; s++) {
+        act[s] = (s < S) && L.active[s];
+        be[s] = act[s] ? (VT)L.beta[s] : VT(0);
+      }
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+      FOR_OWN_ROWS {
+        const int base = a.slice_ptr[sl], w = (a.slice_ptr[sl + 1] - base) >> 5;
+        VT ak[LD], am[LD];
+#pragma unroll
+        for (int s = 0; s < LD; s++) ak[s] = am[s] = VT(0);
+        for (int k = 0; k < w; k += UNROLL) {
+          int cc[UNROLL];
+          VT vv[UNROLL];
+#pragma unroll
+          for (int u = 0; u < UNROLL; u++) {
+            const int pos = base + min(k + u, w - 1) * 32 + lane;
+            cc[u] = ld_na(a.sell_col + pos);
+            vv[u] = (k + u < w) ? ld_na(a.sK + pos) : VT(0);
+          }
+#pragma unroll
+          for (int u = 0; u < UNROLL; u++) {
+            VT zv[LD], pv[LD];
+            ldv_cg<VT, LD>(a.z, cc[u], zv);
+            ldv_cg<VT, LD>(p_old, cc[u], pv);
+            VT mv = VT(0);
+            if (a.sM && k + u < w) mv = ld_na(a.sM + base + (k + u) * 32 + lane);
+#pragma unroll
+            for (int s = 0; s < LD; s++) {
+              const VT pj = act[s] ? zv[s] + be[s] * pv[s] : pv[s];
+              ak[s] += vv[u] * pj;
+              am[s] += mv * pj;
+            }
+          }
+        }
+        VT zr[LD], por[LD], pr[LD], dr[LD], qv[LD];
+        ldv_cg<VT, LD>(a.z, row, zr);
+        ldv_cg<VT, LD>(p_old, row, por);
+#pragma unroll
+        for (int s = 0; s < LD; s++) {
+          pr[s] = act[s] ? zr[s] + be[s] * por[s] : por[s];
+          dr[s] = VT(0);
+        }
+        stv<VT, LD>(p_new, row, pr);
+        if (a.diag) ldv<VT, LD>(a.diag, row, dr);
+        const bool bcr = a.bc && a.bc[row];
+#pragma unroll
+        for (int s = 0; s < LD; s++) {
+          VT v = VT(a.dscale[s]) * ak[s] + VT(a.cscale[s]) * am[s] + dr[s] * pr[s];
+          qv[s] = bcr ? pr[s] : v;
+          acc[s] += (double)pr[s] * (double)qv[s];
+        }
+        stv<VT, LD>(a.q, row, qv);
+      }
+      block_partial<4>(acc, a.part, sh);
+    }
+    clk.lap(0);
+    ok = grid_sync(a.bar, gen);
+    clk.lap(1);
+    if (!ok) break;
+    grid_totals<4>(a.part, s_tot, s_buf);
+    if (threadIdx.x == 0) {
+      for (int s = 0; s < S; s++) {
+        if (!L.active[s]) {
+          L.alpha[s] = 0.0;
+          continue;
+        }
+        const double pq = s_tot[s];
+        if (!isfinite(pq) || !(pq > 0.0)) {
+          L.alpha[s] = 0.0;
+          L.active[s] = 0;
+          L.status[s] = isfinite(pq) ? TP_ERR_BREAKDOWN : TP_ERR_NONFINITE;
+          L.iters[s] = it;
+          continue;
+        }
+        L.alpha[s] = L.rz[s] / pq;
+      }
+    }
+    __syncthreads();
+    // ---- B: xi += alpha p, r -= alpha q, z = D^-1 r; r.z, r.r
+    {
+      double acc[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) acc[k] = 0.0;
+      VT al[LD];
+#pragma unroll
+      for (int s = 0; s < LD; s++) al[s] = (s < S) ? (VT)L.alpha[s] : VT(0);
+      FOR_OWN_ROWS {
+        VT pv[LD], qv[LD], rv[LD], xv[LD], dv[LD], zv[LD];
+        ldv_cg<VT, LD>(p_new, row, pv);
+        ldv_cg<VT, LD>(a.q, row, qv);
+        ldv_cg<VT, LD>(a.r, row, rv);
+        ldv_cg<VT, LD>(a.xi, row, xv);
+        ldv_cg<VT, LD>(a.dinv, row, dv);
+#pragma unroll
+        for (int s = 0; s < LD; s++) {
+          xv[s] += al[s] * pv[s];
+          rv[s] -= al[s] * qv[s];
+          zv[s] = dv[s] * rv[s];
+          acc[s] += (double)rv[s] * (double)zv[s];
+          acc[4 + s] += (double)rv[s] * (double)rv[s];
+        }
+        stv<VT, LD>(a.xi, row, xv);
+        stv<VT, LD>(a.r, row, rv);
+        stv<VT, LD>(a.z, row, zv);
+      }
+      block_partial<8>(acc, a.part, sh);
+    }
+    clk.lap(2);
+    ok = grid_sync(a.bar, gen);
+    clk.lap(3);
+    if (!ok) break;
+    grid_totals<8>(a.part, s_tot, s_buf);
+    __shared__ int s_anytrig;
+    if (threadIdx.x == 0) {
+      int any = 0;
+      for (int s = 0; s < S; s++) {
+        L.trigger[s] = 0;
+        if (!L.active[s]) {
+          L.beta[s] = 0.0;
+          continue;
+        }
+        const double rz = s_tot[s], rr = s_tot[4 + s];
+        if (!isfinite(rz) || !isfinite(rr)) {
+          L.active[s] = 0;
+          L.status[s] = TP_ERR_NONFINITE;
+          L.iters[s] = it + 1;
+          continue;
+        }
+        const double old = L.rz[s];
+        L.beta[s] = (old != 0.0) ? rz / old : 0.0;
+        L.rz[s] = rz;
+        L.rr[s] = rr;
+        const bool trig = (rr <= L.tol2[s]) || (a.delta2 > 0.0 && rr < a.delta2 * L.rmax2[s]);
+        L.trigger[s] = trig;
+        any |= trig;
+      }
+      s_anytrig = any;
+    }
+    __syncthreads();
+    it++;
+    clk.lap(4);  // scalar updates
+    if (s_anytrig) {
+      // ---- RU1: x += xi on trigger lanes
+      int tr[LD];
+#pragma unroll
+      for (int s = 0; s < LD; s++) tr[s] = (s < S) ? L.trigger[s] : 0;
+      FOR_OWN_ROWS {
+        VT xv[LD];
+        ldv_cg<VT, LD>(a.xi, row, xv);
+#pragma unroll
+        for (int s = 0; s < LD; s++) {
+          if (tr[s]) {
+            a.x[row * LD + s] += (double)xv[s];
+            xv[s] = VT(0);
+          }
+        }
+        stv<VT, LD>(a.xi, row, xv);
+      }
+      ok = grid_sync(a.bar, gen);
+      if (!ok) break;
+      // ---- RU2: FP64 residual on trigger lanes, replace r and z
+      double acc[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) acc[k] = 0.0;
+      FOR_OWN_ROWS {
+        double r64[LD];
+        csr64_residual<VT, LD>(a, row, r64);
+        VT rv[LD], dv[LD], zv[LD];
+        ldv_cg<VT, LD>(a.r, row, rv);
+        ldv_cg<VT, LD>(a.dinv, row, dv);
+        ldv_cg<VT, LD>(a.z, row, zv);
+#pragma unroll
+        for (int s = 0; s < LD; s++) {
+          if (tr[s]) {
+            rv[s] = (VT)r64[s];
+            zv[s] = dv[s] * rv[s];
+            acc[s] += r64[s] * r64[s];
+            acc[4 + s] += (double)rv[s] * (double)zv[s];
+          }
+        }
+        stv<VT, LD>(a.r, row, rv);
+        stv<VT, LD>(a.z, row, zv);
+      }
+      block_partial<8>(acc, a.part, sh);
+      ok = grid_sync(a.bar, gen);
+      if (!ok) break;
+      grid_totals<8>(a.part, s_tot, s_buf);
+      if (threadIdx.x == 0) {
+        n_rel++;
+        for (int s = 0; s < S; s++) {
+          if (!L.trigger[s]) continue;
+          L.trigger[s] = 0;
+          const double rr = s_tot[s], rz = s_tot[4 + s];
+          L.rtrue[s] = rr;
+          if (!isfinite(rr)) {
+            L.active[s] = 0;
+            L.status[s] = TP_ERR_NONFINITE;
+            L.iters[s] = it;
+          } else if (rr <= L.tol2[s]) {
+            L.active[s] = 0;
+            L.status[s] = TP_OK;
+            L.iters[s] = it;
+          } else {
+            L.rz[s] = rz;
+            L.rr[s] = rr;
+            L.rmax2[s] = rr;
+          }
+        }
+      }
+      __syncthreads();
+      clk.lap(5);  // reliable update
+    }
+    par ^= 1;
+  }
+
+  // ---- final: x += xi, true residual norms
+  FOR_OWN_ROWS {
+    VT xv[LD];
+    ldv_cg<VT, LD>(a.xi, row, xv);
+#pragma unroll
+    for (int s = 0; s < LD; s++) {
+      if (s < S) a.x[row * LD + s] += (double)xv[s];
+      xv[s] = VT(0);
+    }
+    stv<VT, LD>(a.xi, row, xv);
+  }
+  bool ok2 = ok && grid_sync(a.bar, gen);
+  {
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    if (ok2) {
+      FOR_OWN_ROWS {
+        double r64[LD];
+        csr64_residual<VT, LD>(a, row, r64);
+#pragma unroll
+        for (int s = 0; s < LD; s++) acc[s] += r64[s] * r64[s];
+      }
+    }
+    block_partial<4>(acc, a.part, sh);
+  }
+  ok2 = ok2 && grid_sync(a.bar, gen);
+  if (ok2) grid_totals<4>(a.part, s_tot, s_buf);
+  if (clk.on) {
+    clk.lap(6);
+#pragma unroll
+    for (int k = 0; k < 8; k++) a.prof[blockIdx.x * 8 + k] = clk.acc[k];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    int status = TP_OK;
+    for (int s = 0; s < 4; s++) {
+      if (s < S) {
+        if (ok2) L.rtrue[s] = s_tot[s];
+        if (L.status[s] == -1) {
+          L.status[s] = (ok2 && L.rtrue[s] <= L.tol2[s]) ? TP_OK : TP_ERR_NOT_CONVERGED;
+          L.iters[s] = it;
+        }
+        if (!ok2) L.status[s] = TP_ERR_TIMEOUT;
+        if (L.status[s] != TP_OK && status == TP_OK) status = L.status[s];
+      }
+      a.out->lane_iters[s] = L.iters[s];
+      a.out->lane_status[s] = L.status[s];
+      a.out->lane_rtrue[s] = L.rtrue[s];
+      a.out->lane_bb[s] = L.bb[s];
+    }
+    a.out->iterations = it;
+    a.out->n_reliable = n_rel;
+    a.out->status = status;
+    a.out->timeouts = ok2 ? 0 : 1;
+  }
+#undef FOR_OWN_ROWS
+}
+
+// ----------------------------------------------------------------- SELL-32 build
+__global__ void k_slice_width(int64_t n, const int32_t* __restrict__ indptr, int ns,
+                              int32_t* __restrict__ width) {
+  const int sl = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x & 31;
+  if (sl >= ns) return;
+  const int64_t row = (int64_t)sl * 32 + lane;
+  int len = (row < n) ? indptr[row + 1] - indptr[row] : 0;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) len = max(len, __shfl_xor_sync(0xffffffffu, len, o));
+  if (lane == 0) width[sl] = len;
+}
+
+__global__ void k_sell_fill_pattern(int64_t n, const int32_t* __restrict__ indptr,
+                                    const int32_t* __restrict__ indices, int ns,
+                                    const int32_t* __restrict__ slice_ptr,
+                                    int32_t* __restrict__ sell_col,
+                                    int32_t* __restrict__ csr2sell) {
+  const int sl = blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  const int lane = threadIdx.x & 31;
+  if (sl >= ns) return;
+  const int64_t row = (int64_t)sl * 32 + lane;
+  const int base = slice_ptr[sl], w = (slice_ptr[sl + 1] - base) >> 5;
+  const int beg = row < n ? indptr[row] : 0, len = row < n ? indptr[row + 1] - beg : 0;
+  const int own = (int)(row < n ? row : n - 1);
+  for (int k = 0; k < w; k++) {
+    const int pos = base + k * 32 + lane;
+    if (k < len) {
+      sell_col[pos] = indices[beg + k];
+      csr2sell[beg + k] = pos;
+    } else {
+      sell_col[pos] = own;  // padding: own column, value 0
+    }
+  }
+}
+
+template <typename T>
+__global__ void k_sell_scatter(int64_t nnz, const int32_t* __restrict__ csr2sell,
+                               const double* __restrict__ v, T* __restrict__ out) {
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < nnz;
+       p += (int64_t)gridDim.x * blockDim.x)
+    out[csr2sell[p]] = (T)v[p];
+}
+
+}  // namespace tp
+
+using namespace tp;
+
+extern "C" int tp_sell_build(int64_t n_rows, const int32_t* indptr, const int32_t* indices,
+                             int32_t* slice_ptr, int32_t* sell_col, int32_t* csr2sell,
+                             int64_t* n_entries, void* stream) {
+  TP_REQUIRE(indptr && slice_ptr && n_entries, "null pointer");
+  cudaStream_t st = as_stream(stream);
+  const int ns = (int)((n_rows + 31) / 32);
+  std::vector<int32_t> w(ns), sp(ns + 1, 0);
+  if (ns > 0) {
+    int32_t* dw = slice_ptr;  // scratch: slice_ptr has ns + 1 entries
+    k_slice_width<<<(ns + 7) / 8, 256, 0, st>>>(n_rows, indptr, ns, dw);
+    TP_LAUNCH_CHECK();
+    TP_CUDA_TRY(cudaMemcpyAsync(w.data(), dw, sizeof(int32_t) * ns, cudaMemcpyDeviceToHost, st));
+    TP_CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  int64_t tot = 0;
+  for (int s = 0; s < ns; s++) {
+    sp[s] = (int32_t)tot;
+    tot += 32 * (int64_t)w[s];
+    if (tot > INT32_MAX) {
+      set_error("SELL storage exceeds int32 offsets");
+      return TP_ERR_CAPACITY;
+    }
+  }
+  sp[ns] = (int32_t)tot;
+  *n_entries = tot;
+  TP_CUDA_TRY(cudaMemcpyAsync(slice_ptr, sp.data(), sizeof(int32_t) * (ns + 1),
+                              cudaMemcpyHostToDevice, st));
+  if (sell_col && csr2sell && ns > 0) {
+    k_sell_fill_pattern<<<(ns + 7) / 8, 256, 0, st>>>(n_rows, indptr, indices, ns, slice_ptr,
+                                                      sell_col, csr2sell);
+    TP_LAUNCH_CHECK();
+  }
+  TP_CUDA_TRY(cudaStreamSynchronize(st));
+  return TP_OK;
+}
+
+extern "C" int tp_sell_scatter(int64_t nnz, const int32_t* csr2sell, const double* csr_vals,
+                               float* sell32, double* sell64, void* stream) {
+  TP_REQUIRE(csr2sell && csr_vals && (sell32 || sell64), "null pointer");
+  if (nnz == 0) return TP_OK;
+  cudaStream_t st = as_stream(stream);
+  const int grid = grid_for(nnz, 256, sm_count() * 16);
+  if (sell32) k_sell_scatter<float><<<grid, 256, 0, st>>>(nnz, csr2sell, csr_vals, sell32);
+  if (sell64) k_sell_scatter<double><<<grid, 256, 0, st>>>(nnz, csr2sell, csr_vals, sell64);
+  TP_LAUNCH_CHECK();
+  return TP_OK;
+}
+
+// ----------------------------------------------------------------- persistent handle
+struct tp_pcg_handle {
+  int fp32, ld, grid, block;
+  void* fn;
+  tp::PArgs<float> af;
+  tp::PArgs<double> ad;
+  tp::POut* out;
+  tp::PBar* bar;
+};
+
+namespace tp {
+template <typename VT, int LD>
+static void* pick_kernel(int minb) {
+  if (minb >= 2) return (void*)k_pcg<VT, LD, (LD == 4 ? 4 : 8), 2>;
+  return (void*)k_pcg<VT, LD, (LD == 4 ? 4 : 8), 1>;
+}
+
+// CTAs per SM: 1 (up to 128 registers per thread) or 2 (64 registers)
+static void* pcg_kernel(int fp32, int ld, int minb) {
+  if (fp32) {
+    if (ld == 1) return pick_kernel<float, 1>(minb);
+    if (ld == 2) return pick_kernel<float, 2>(minb);
+    if (ld == 4) return pick_kernel<float, 4>(minb);
+  } else {
+    if (ld == 1) return pick_kernel<double, 1>(minb);
+    if (ld == 2) return pick_kernel<double, 2>(minb);
+    if (ld == 4) return pick_kernel<double, 4>(minb);
+  }
+  return nullptr;
+}
+
+static size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+template <typename VT>
+static void fill_pargs(PArgs<VT>& a, const tp_csr_op* op, const tp_sell* sl, const double* b,
+                       double* x, const double* rtol, int max_it, double delta, char* ws,
+                       size_t vec_bytes, int grid) {
+  a.n = op->n_rows;
+  a.S = op->S;
+  a.ns = (int)((op->n_rows + 31) / 32);
+  a.max_it = max_it;
+  a.delta2 = delta * delta;
+  a.slice_ptr = sl->slice_ptr;
+  a.sell_col = sl->sell_col;
+  if constexpr (sizeof(VT) == 4) {
+    a.sK = sl->sK32;
+    a.sM = sl->sM32;
+    a.diag = op->diag32;
+  } else {
+    a.sK = sl->sK64;
+    a.sM = sl->sM64;
+    a.diag = op->diag64;
+  }
+  a.A64.indptr = op->indptr;
+  a.A64.indices = op->indices;
+  a.A64.K = op->K64;
+  a.A64.M = op->M64;
+  a.A64.diag = op->diag64;
+  a.A64.bc = op->bc_mask;
+  for (int s = 0; s < 4; s++) {
+    a.dscale[s] = a.A64.dscale[s] = s < op->S ? op->dscale[s] : 0.0;
+    a.cscale[s] = a.A64.cscale[s] = s < op->S ? op->cscale[s] : 0.0;
+  }
+  a.bc = op->bc_mask;
+  a.b = b;
+  a.x = x;
+  a.rtol = rtol;
+  char* p = ws;
+  VT** v[7] = {&a.p, &a.q, &a.r, &a.z, &a.xi, &a.dinv, &a.p2};
+  for (int i = 0; i < 7; i++) {
+    *v[i] = reinterpret_cast<VT*>(p);
+    p += vec_bytes;
+  }
+  a.part = reinterpret_cast<double*>(p);
+  p += a256(sizeof(double) * 16 * grid);
+  a.bar = reinterpret_cast<PBar*>(p);
+  p += a256(sizeof(PBar));
+  a.out = reinterpret_cast<POut*>(p);
+}
+}  // namespace tp
+
+static int default_minb(int ld) { return ld == 4 ? 1 : 2; }
+
+static int pcg_grid(int fp32, int ld, int minb, int block, int* grid) {
+  void* fn = pcg_kernel(fp32, ld, minb);
+  if (!fn) return TP_ERR_ARG;
+  // most of the unified L1/shared storage to L1 (the gathered vectors live there), but
+  // enough shared memory for `minb` CTAs; set before the occupancy query so the
+  // cooperative grid matches what the launch will see
+  TP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   minb >= 2 ? 10 : 5));
+  int occ = 0;
+  TP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, block, 0));
+  if (occ < 1) {
+    set_error("persistent CG kernel does not fit on an SM");
+    return TP_ERR_CAPACITY;
+  }
+  *grid = sm_count() * std::min(occ, minb);
+  return TP_OK;
+}
+
+extern "C" size_t tp_pcg_workspace_bytes(const tp_csr_op* op, int inner_fp32) {
+  if (!op) return 0;
+  int grid = 0;  // partial rows for the largest grid (2 CTAs per SM)
+  if (pcg_grid(inner_fp32, op->ld, 2, 512, &grid) != TP_OK) return 0;
+  grid = std::max(grid, 2 * sm_count());
+  const size_t vt = inner_fp32 ? 4 : 8;
+  return 7 * a256(vt * op->ld * (size_t)op->n_rows) + a256(sizeof(double) * 16 * grid) +
+         a256(sizeof(PBar)) + a256(sizeof(POut));
+}
+
+extern "C" int tp_pcg_create(const tp_csr_op* op, const tp_sell* sell, int max_it,
+                             int inner_fp32, double delta, int ctas_per_sm, const double* b,
+                             double* x, const double* rtol, void* workspace,
+                             size_t workspace_bytes, void* stream, tp_pcg_handle** out) {
+  TP_REQUIRE(op && sell && b && x && rtol && workspace && out, "null pointer");
+  TP_REQUIRE(op->n_systems <= 1, "the persistent engine solves one system (use tp_cg_*)");
+  TP_REQUIRE(op->S >= 1 && op->S <= 4 && (op->ld == 1 || op->ld == 2 || op->ld == 4) &&
+                 op->ld >= op->S,
+             "bad S/ld");
+  TP_REQUIRE(op->indptr && op->indices && op->K64, "operator needs the FP64 CSR values");
+  TP_REQUIRE(sell->slice_ptr && sell->sell_col && (inner_fp32 ? sell->sK32 != nullptr : sell->sK64 != nullptr),
+             "SELL operator incomplete");
+  TP_REQUIRE(!inner_fp32 || !op->diag64 || op->diag32, "FP32 inner solve needs diag32");
+  TP_REQUIRE(!sell->sM64 || op->M64, "SELL mass values need the CSR mass values");
+  TP_REQUIRE(((uintptr_t)workspace & 255) == 0, "workspace must be 256-byte aligned");
+  TP_REQUIRE(workspace_bytes >= tp_pcg_workspace_bytes(op, inner_fp32), "workspace too small");
+  TP_REQUIRE(max_it >= 0, "max_it < 0");
+  tp_pcg_handle* h = new tp_pcg_handle();
+  h->fp32 = inner_fp32 ? 1 : 0;
+  h->ld = op->ld;
+  h->block = 512;
+  const int minb = ctas_per_sm > 0 ? std::min(ctas_per_sm, 2) : default_minb(op->ld);
+  int rc = pcg_grid(h->fp32, h->ld, minb, h->block, &h->grid);
+  if (rc) {
+    delete h;
+    return rc;
+  }
+  h->fn = pcg_kernel(h->fp32, h->ld, minb);
+  const size_t vt = inner_fp32 ? 4 : 8;
+  const size_t vec = a256(vt * op->ld * (size_t)op->n_rows);
+  const double d = inner_fp32 ? (delta > 0 ? delta : 0.1) : 0.0;
+  char* ws = static_cast<char*>(workspace);
+  if (h->fp32)
+    fill_pargs(h->af, op, sell, b, x, rtol, max_it, d, ws, vec, h->grid);
+  else
+    fill_pargs(h->ad, op, sell, b, x, rtol, max_it, d, ws, vec, h->grid);
+  h->bar = h->fp32 ? h->af.bar : h->ad.bar;
+  h->out = h->fp32 ? h->af.out : h->ad.out;
+  cudaStream_t st = as_stream(stream);
+  cudaError_t e = cudaMemsetAsync(h->bar, 0, sizeof(PBar), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(h->out, 0, sizeof(POut), st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    set_error("pcg setup failed: %s", cudaGetErrorString(e));
+    delete h;
+    return TP_ERR_CUDA;
+  }
+  *out = h;
+  return TP_OK;
+}
+
+extern "C" int tp_pcg_run(tp_pcg_handle* h, void* stream) {
+  TP_REQUIRE(h, "null handle");
+  cudaStream_t st = as_stream(stream);
+  // a previous run that timed out leaves the abort flag set: clear the barrier first
+  TP_CUDA_TRY(cudaMemsetAsync(h->bar, 0, sizeof(PBar), st));
+  void* arg = h->fp32 ? (void*)&h->af : (void*)&h->ad;
+  void* args[1] = {arg};
+  TP_CUDA_TRY(cudaLaunchCooperativeKernel(h->fn, dim3(h->grid), dim3(h->block), args, 0, st));
+  return TP_OK;
+}
+
+extern "C" int tp_pcg_result_get(tp_pcg_handle* h, tp_cg_result* res, int32_t* lane_iters,
+                                 int32_t* lane_status, double* lane_rnorm, double* lane_bnorm,
+                                 void* stream) {
+  TP_REQUIRE(h, "null handle");
+  cudaStream_t st = as_stream(stream);
+  POut o;
+  TP_CUDA_TRY(cudaMemcpyAsync(&o, h->out, sizeof(POut), cudaMemcpyDeviceToHost, st));
+  TP_CUDA_TRY(cudaStreamSynchronize(st));
+  const int S = h->fp32 ? h->af.S : h->ad.S;
+  for (int s = 0; s < S; s++) {
+    if (lane_iters) lane_iters[s] = o.lane_iters[s];
+    if (lane_status) lane_status[s] = o.lane_status[s];
+    if (lane_rnorm) lane_rnorm[s] = sqrt(std::max(o.lane_rtrue[s], 0.0));
+    if (lane_bnorm) lane_bnorm[s] = sqrt(std::max(o.lane_bb[s], 0.0));
+  }
+  if (res) {
+    res->status = o.status;
+    res->iterations = o.iterations;
+    res->n_reliable = o.n_reliable;
+    res->n_lanes = S;
+  }
+  return TP_OK;
+}
+
+extern "C" int tp_pcg_grid(tp_pcg_handle* h, int* grid, int* block) {
+  TP_REQUIRE(h, "null handle");
+  if (grid) *grid = h->grid;
+  if (block) *block = h->block;
+  return TP_OK;
+}
+
+extern "C" int tp_pcg_set_profile(tp_pcg_handle* h, unsigned long long* prof) {
+  TP_REQUIRE(h, "null handle");
+  h->af.prof = prof;
+  h->ad.prof = prof;
+  return TP_OK;
+}
+
+extern "C" int tp_pcg_destroy(tp_pcg_handle* h) {
+  delete h;
+  return TP_OK;
+}

@@ -25,6 +25,7 @@ TP_ERR_CAPACITY = 5
 TP_ERR_NOT_CONVERGED = 6
 TP_ERR_BREAKDOWN = 7
 TP_ERR_NONFINITE = 8
+TP_ERR_TIMEOUT = 9
 
 TP_ASM_FULL = 0
 TP_ASM_STIFF = 1
@@ -59,6 +60,11 @@ class TpCgConfig(ctypes.Structure):
     _fields_ = [("max_it", _c_i32), ("inner_fp32", _c_i32), ("delta", _c_dbl),
                 ("group", _c_i32), ("block", _c_i32), ("rows_per_tile", _c_i32),
                 ("use_graph_loop", _c_i32)]
+
+
+class TpSell(ctypes.Structure):
+    _fields_ = [("n_rows", _c_i64), ("n_entries", _c_i64), ("slice_ptr", _vp), ("sell_col", _vp),
+                ("sK32", _vp), ("sK64", _vp), ("sM32", _vp), ("sM64", _vp)]
 
 
 class TpCgResult(ctypes.Structure):
@@ -111,6 +117,17 @@ SIGNATURES = {
     "tp_cg_result_get": (ctypes.c_int, [_vp, _P(TpCgResult), _vp, _vp, _vp, _vp, _vp]),
     "tp_cg_destroy": (ctypes.c_int, [_vp]),
     "tp_cg_time_spmv": (ctypes.c_int, [_vp, ctypes.c_int, _P(ctypes.c_float), _vp]),
+    "tp_sell_build": (ctypes.c_int, [_c_i64, _vp, _vp, _vp, _vp, _vp, _P(_c_i64), _vp]),
+    "tp_sell_scatter": (ctypes.c_int, [_c_i64, _vp, _vp, _vp, _vp, _vp]),
+    "tp_pcg_workspace_bytes": (ctypes.c_size_t, [_P(TpCsrOp), ctypes.c_int]),
+    "tp_pcg_create": (ctypes.c_int, [_P(TpCsrOp), _P(TpSell), ctypes.c_int, ctypes.c_int, _c_dbl,
+                                     ctypes.c_int, _vp, _vp, _vp, _vp, ctypes.c_size_t, _vp,
+                                     _P(_vp)]),
+    "tp_pcg_run": (ctypes.c_int, [_vp, _vp]),
+    "tp_pcg_result_get": (ctypes.c_int, [_vp, _P(TpCgResult), _vp, _vp, _vp, _vp, _vp]),
+    "tp_pcg_grid": (ctypes.c_int, [_vp, _P(ctypes.c_int), _P(ctypes.c_int)]),
+    "tp_pcg_set_profile": (ctypes.c_int, [_vp, _vp]),
+    "tp_pcg_destroy": (ctypes.c_int, [_vp]),
 }
 
 

@@ -141,3 +141,139 @@ class CGSolver:
             self.close()
         except Exception:
             pass
+
+
+class SellPattern:
+    """SELL-32 layout of a CSR pattern (tp_sell_build) plus the CSR->SELL position map."""
+
+    def __init__(self, indptr: torch.Tensor, indices: torch.Tensor):
+        from ._lib import _c_i64
+        dev = indptr.device
+        self.n_rows = int(indptr.numel()) - 1
+        ns = (self.n_rows + 31) // 32
+        self.slice_ptr = torch.empty(ns + 1, dtype=torch.int32, device=dev)
+        ne = _c_i64(0)
+        call("tp_sell_build", self.n_rows, ptr(indptr), ptr(indices), ptr(self.slice_ptr), None,
+             None, ctypes.byref(ne), stream_handle())
+        self.n_entries = int(ne.value)
+        self.nnz = int(indices.numel())
+        self.sell_col = torch.empty(max(self.n_entries, 1), dtype=torch.int32, device=dev)
+        self.csr2sell = torch.empty(max(self.nnz, 1), dtype=torch.int32, device=dev)
+        call("tp_sell_build", self.n_rows, ptr(indptr), ptr(indices), ptr(self.slice_ptr),
+             ptr(self.sell_col), ptr(self.csr2sell), ctypes.byref(ne), stream_handle())
+
+    def values(self, dtype):
+        return torch.zeros(max(self.n_entries, 1), dtype=dtype, device=self.slice_ptr.device)
+
+    def scatter(self, csr_vals64, out32=None, out64=None):
+        call("tp_sell_scatter", self.nnz, ptr(self.csr2sell), ptr(csr_vals64), ptr(out32),
+             ptr(out64), stream_handle())
+
+
+class PersistentCG:
+    """The same Jacobi-PCG as CGSolver for one system, as one cooperative kernel per solve
+    (tp_pcg_*).  The inner operator is read in SELL-32 order: call refresh_values() after the
+    CSR values change (it scatters them)."""
+
+    def __init__(self, op: CsrOperator, rtol=1e-8, max_it=1000, inner_fp32=False, delta=0.1,
+                 sell: SellPattern | None = None, ctas_per_sm: int = 0):
+        from ._lib import TpSell
+        if op.n_systems != 1:
+            raise ValueError("the persistent engine solves one system")
+        self.op = op
+        dev = op.arrays["indptr"].device
+        self.device = dev
+        self.n_lanes = op.S
+        self.inner_fp32 = bool(inner_fp32)
+        self.sell = sell or SellPattern(op.arrays["indptr"], op.arrays["indices"])
+        vdt = torch.float32 if inner_fp32 else torch.float64
+        self.sK = self.sell.values(vdt)
+        self.sM = self.sell.values(vdt) if op.arrays["M64"] is not None else None
+        self.b = torch.zeros((op.n_rows, op.ld), dtype=torch.float64, device=dev)
+        self.x = torch.zeros((op.n_rows, op.ld), dtype=torch.float64, device=dev)
+        self.rtol = torch.empty(self.n_lanes, dtype=torch.float64, device=dev)
+        self.set_rtol(rtol)
+        st = TpSell()
+        st.n_rows, st.n_entries = self.sell.n_rows, self.sell.n_entries
+        st.slice_ptr, st.sell_col = ptr(self.sell.slice_ptr), ptr(self.sell.sell_col)
+        if inner_fp32:
+            st.sK32, st.sM32 = ptr(self.sK), ptr(self.sM)
+        else:
+            st.sK64, st.sM64 = ptr(self.sK), ptr(self.sM)
+        self._sell_struct = st
+        nbytes = _lib.lib.tp_pcg_workspace_bytes(ctypes.byref(op.struct), int(inner_fp32))
+        if nbytes == 0:
+            raise ValueError("invalid persistent solver configuration")
+        self._ws_buf, self._ws = empty_aligned(nbytes, dev)
+        h = ctypes.c_void_p()
+        call("tp_pcg_create", ctypes.byref(op.struct), ctypes.byref(st), int(max_it),
+             int(inner_fp32), float(delta), int(ctas_per_sm), ptr(self.b), ptr(self.x),
+             ptr(self.rtol), self._ws, int(nbytes), stream_handle(), ctypes.byref(h))
+        self._h = h
+        self.refresh_values()
+
+    def set_rtol(self, rtol):
+        r = np.broadcast_to(np.asarray(rtol, dtype=np.float64), (self.n_lanes,))
+        self.rtol.copy_(torch.from_numpy(np.array(r, dtype=np.float64)))
+
+    def refresh_values(self):
+        a = self.op.arrays
+        if self.inner_fp32:
+            self.sell.scatter(a["K64"], out32=self.sK)
+            if self.sM is not None:
+                self.sell.scatter(a["M64"], out32=self.sM)
+        else:
+            self.sell.scatter(a["K64"], out64=self.sK)
+            if self.sM is not None:
+                self.sell.scatter(a["M64"], out64=self.sM)
+
+    def profile_run(self) -> dict:
+        """One solve with per-CTA phase clocks; mean and max over CTAs in microseconds."""
+        g, _ = self.grid()
+        prof = torch.zeros(g * 8, dtype=torch.int64, device=self.device)
+        call("tp_pcg_set_profile", self._h, ptr(prof))
+        try:
+            res = self.solve()
+        finally:
+            call("tp_pcg_set_profile", self._h, None)
+        p = prof.view(g, 8).double().cpu().numpy() / 1e3
+        names = ["A_work", "A_wait", "B_work", "B_wait", "scalars", "reliable", "final", "init"]
+        return {"result": res, "mean_us": dict(zip(names, p.mean(0).round(1).tolist())),
+                "max_us": dict(zip(names, p.max(0).round(1).tolist())),
+                "min_us": dict(zip(names, p.min(0).round(1).tolist()))}
+
+    def grid(self):
+        g, b = ctypes.c_int(0), ctypes.c_int(0)
+        call("tp_pcg_grid", self._h, ctypes.byref(g), ctypes.byref(b))
+        return int(g.value), int(b.value)
+
+    def run(self):
+        call("tp_pcg_run", self._h, stream_handle())
+
+    def result(self) -> dict:
+        res = TpCgResult()
+        n = self.n_lanes
+        it = np.zeros(n, dtype=np.int32)
+        st = np.zeros(n, dtype=np.int32)
+        rn = np.zeros(n, dtype=np.float64)
+        bn = np.zeros(n, dtype=np.float64)
+        call("tp_pcg_result_get", self._h, ctypes.byref(res), it.ctypes.data, st.ctypes.data,
+             rn.ctypes.data, bn.ctypes.data, stream_handle())
+        return {"status": int(res.status), "converged": int(res.status) == 0,
+                "iterations": int(res.iterations), "n_reliable": int(res.n_reliable),
+                "lane_iterations": it, "lane_status": st, "rnorm": rn, "bnorm": bn}
+
+    def solve(self) -> dict:
+        self.run()
+        return self.result()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib.tp_pcg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

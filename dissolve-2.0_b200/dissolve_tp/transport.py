@@ -30,14 +30,14 @@ from ._lib import call
 from .assembler import GPUSparseAssembler
 from .autotune import tune_cg
 from .device import ptr, stream_handle, to_device
-from .krylov import CGSolver, CsrOperator
+from .krylov import CGSolver, CsrOperator, PersistentCG
 
 
 class PlainTransport:
     """The plain FP64 GPU form: per species assemble + RHS + FP64 Jacobi-PCG."""
 
     def __init__(self, mesh, coef_cell, D, k, dt, rtol=1e-8, max_it=5000, lumped=True,
-                 bc=None, cg=None):
+                 bc=None, cg=None, engine="persistent"):
         from . import assembler as A
 
         self.S = len(D)
@@ -62,7 +62,12 @@ class PlainTransport:
             mask = self.asm[0]._dm.bc_mask(self.bc[s][0]) if self.bc[s] is not None else None
             op = CsrOperator(self.asm[s].d_indptr, self.asm[s].d_indices, self.asm[s].d_data,
                              bc_mask=mask)
-            self.solvers.append(CGSolver(op, rtol=rtol, max_it=max_it, **cg))
+            if engine == "persistent":
+                self.solvers.append(PersistentCG(op, rtol=rtol, max_it=max_it,
+                                                 sell=self.solvers[0].sell if s else None))
+            else:
+                self.solvers.append(CGSolver(op, rtol=rtol, max_it=max_it, **cg))
+        self.engine = engine
         nv = self.asm[0].n_dofs
         self.U = [torch.zeros(nv, dtype=torch.float64, device=dev) for _ in range(self.S)]
 
@@ -89,6 +94,8 @@ class PlainTransport:
                                      bc_value=0.0 if bc is None else bc[1])
                 sol.b.view(-1).copy_(b)
                 sol.x.view(-1).copy_(self.U[s])
+                if self.engine == "persistent":
+                    sol.refresh_values()
                 sol.run()
                 self.U[s].copy_(sol.x.view(-1))
         finally:
@@ -111,7 +118,7 @@ class BatchedTransport:
 
     def __init__(self, mesh, coef_cell, D, k, dt, rtol=1e-8, max_it=5000, lumped=True,
                  inner_fp32=True, delta=0.1, guess="previous", bc_dofs=None, bc_values=None,
-                 alpha_cells=None, autotune=True, cg=None, asm=None):
+                 alpha_cells=None, autotune=True, cg=None, asm=None, engine="persistent"):
         if not lumped:
             raise ValueError("the batched form splits the operator into a shared stiffness "
                              "and a per-column lumped diagonal; use PlainTransport for "
@@ -145,13 +152,20 @@ class BatchedTransport:
         self.op = CsrOperator(dm.indptr, dm.indices, self.K64, K32=self.K32, diag64=self.D64,
                               diag32=self.D32, bc_mask=self.bc_mask, dscale=self.D, S=self.S,
                               ld=self.ld)
+        self.engine = engine
         cg = dict(cg or {})
-        if autotune and not {"group", "block", "rows_per_tile"} & set(cg):
-            self.assemble_operator()
-            cg.update(tune_cg(self.op, inner_fp32=inner_fp32))
-        self.cg_config = cg
-        self.solver = CGSolver(self.op, rtol=rtol, max_it=max_it, inner_fp32=inner_fp32,
-                               delta=delta, **cg)
+        if engine == "persistent":
+            self.cg_config = {"engine": "persistent"}
+            self.solver = PersistentCG(self.op, rtol=rtol, max_it=max_it, inner_fp32=inner_fp32,
+                                       delta=delta, ctas_per_sm=int(cg.get("ctas_per_sm", 0)))
+            self.cg_config["grid"], self.cg_config["block"] = self.solver.grid()
+        else:
+            if autotune and not {"group", "block", "rows_per_tile"} & set(cg):
+                self.assemble_operator()
+                cg.update(tune_cg(self.op, inner_fp32=inner_fp32))
+            self.cg_config = dict(cg, engine="graph")
+            self.solver = CGSolver(self.op, rtol=rtol, max_it=max_it, inner_fp32=inner_fp32,
+                                   delta=delta, **cg)
         self.U = torch.zeros((n, self.ld), dtype=torch.float64, device=dev)
         self.U_prev = torch.zeros_like(self.U)
         self.guess = guess
@@ -198,6 +212,8 @@ class BatchedTransport:
 
     def step(self, sync=True):
         self.assemble_operator()
+        if self.engine == "persistent":
+            self.solver.refresh_values()
         self.assemble_rhs()
         self.initial_guess()
         self.solver.run()

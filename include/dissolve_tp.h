@@ -43,6 +43,7 @@ extern "C" {
 #define TP_ERR_NOT_CONVERGED 6 /* Krylov solve stopped at max_it                      */
 #define TP_ERR_BREAKDOWN 7    /* p.Ap <= 0: operator not SPD on the free dofs         */
 #define TP_ERR_NONFINITE 8    /* NaN/Inf in a Krylov scalar                           */
+#define TP_ERR_TIMEOUT 9      /* a bounded device-side wait gave up (grid barrier)     */
 
 /* assembly modes for tp_assemble_csr */
 #define TP_ASM_FULL 0   /* De K + (inv_dt + alpha) M  (gpu_assembler.py:60-139)      */
@@ -278,6 +279,58 @@ TP_API int tp_cg_destroy(tp_cg_handle* h);
 /* time `reps` launches of one inner SpMV+dot with the given config (autotuner support);
  * returns milliseconds per launch through *ms (host). [sync] */
 TP_API int tp_cg_time_spmv(tp_cg_handle* h, int reps, float* ms, void* stream);
+
+/* ------------------------------------------------------------------ SELL-32 operator */
+/* Sliced ELL with slices of 32 rows: entry k of the 32 rows of slice s sits at
+ * slice_ptr[s] + 32 k + lane, so every index/value load of a warp is one 128-byte access.
+ * Rows shorter than their slice are padded with their own column and value 0.
+ * (No reference counterpart: the device layout of the inner Krylov operator.) */
+typedef struct tp_sell {
+  int64_t n_rows;
+  int64_t n_entries;         /* 32 * sum of slice widths                              */
+  const int32_t* slice_ptr;  /* (ceil(n_rows/32) + 1)                                 */
+  const int32_t* sell_col;   /* (n_entries)                                           */
+  const float* sK32;         /* (n_entries) values of K (FP32) or NULL                */
+  const double* sK64;        /* (n_entries) values of K (FP64) or NULL                */
+  const float* sM32;         /* optional mass values                                  */
+  const double* sM64;
+} tp_sell;
+
+/* [sync] SELL-32 pattern of a CSR pattern: slice_ptr always; sell_col and csr2sell
+ * (position of each CSR entry, (nnz)) when both are non-NULL.  *n_entries (host)
+ * receives the storage size; allocate sell_col and the value arrays to it, zeroed. */
+TP_API int tp_sell_build(int64_t n_rows, const int32_t* indptr, const int32_t* indices,
+                         int32_t* slice_ptr, int32_t* sell_col, int32_t* csr2sell,
+                         int64_t* n_entries, void* stream);
+
+/* values of a CSR matrix into SELL order (padding entries are left untouched) */
+TP_API int tp_sell_scatter(int64_t nnz, const int32_t* csr2sell, const double* csr_vals,
+                           float* sell32, double* sell64, void* stream);
+
+/* ------------------------------------------------------------------ persistent solve */
+/* The Jacobi-PCG of tp_cg_* for ONE system (S <= 4 columns) as a single cooperative
+ * kernel: one launch per solve, grid barriers with a bounded wait (TP_ERR_TIMEOUT when a
+ * barrier gives up), the inner operator read in SELL-32 order, the FP64 operator (Jacobi
+ * diagonal, initial / reliable-update / final residuals) in CSR.  Same stopping rule,
+ * reliable updates and lane results as tp_cg_*. */
+typedef struct tp_pcg_handle tp_pcg_handle;
+
+TP_API size_t tp_pcg_workspace_bytes(const tp_csr_op* op, int inner_fp32);
+/* ctas_per_sm: 1 or 2 resident 512-thread CTAs per SM (0 = default for the column count) */
+TP_API int tp_pcg_create(const tp_csr_op* op, const tp_sell* sell, int max_it, int inner_fp32,
+                         double delta, int ctas_per_sm, const double* b, double* x,
+                         const double* rtol, void* workspace, size_t workspace_bytes,
+                         void* stream, tp_pcg_handle** out);
+TP_API int tp_pcg_run(tp_pcg_handle* h, void* stream);
+TP_API int tp_pcg_result_get(tp_pcg_handle* h, tp_cg_result* res, int32_t* lane_iters,
+                             int32_t* lane_status, double* lane_rnorm, double* lane_bnorm,
+                             void* stream);
+TP_API int tp_pcg_grid(tp_pcg_handle* h, int* grid, int* block);
+/* per-CTA phase times of the next runs: prof (grid * 8 device u64, ns) receives per CTA
+ * [A work, A barrier wait, B work, B barrier wait, scalar updates, reliable updates,
+ * final, init]; NULL switches it off */
+TP_API int tp_pcg_set_profile(tp_pcg_handle* h, unsigned long long* prof);
+TP_API int tp_pcg_destroy(tp_pcg_handle* h);
 
 #ifdef __cplusplus
 }
