@@ -1,0 +1,559 @@
+// tp_mlp.cu -- per-vertex MLP that predicts the next backward-Euler state (the Krylov
+// initial guess), BF16 on the tensor cores with FP32 accumulation.
+//
+// Network: 16 inputs (8 used) -> 64 -> ReLU -> 64 -> ReLU -> 1, one network shared by
+// all species; a row is one (vertex, species) pair.  Features (normalised by per-input
+// affine maps fixed at training time):
+//   0 phi, 1 |grad phi|, 2 u^n, 3 u^{n-1}, 4 u^n - u^{n-1}, 5 log D_s, 6 k_s, 7 1
+// The output y predicts (u^{n+1} - u^n) / sigma; the guess is u^n + sigma y.
+//
+// Tensor-core fragments are those of mma.sync.m16n8k16 (row.col, bf16 x bf16 -> f32):
+// a warp owns 16 rows; layer outputs stay in registers and are re-packed from the
+// accumulator layout into the next layer's A layout.  Backward: the weight gradients
+// are GEMMs over the row dimension (dW2 = dZ2^T H1, dW1 = dZ1^T X) fed from transposed
+// tiles staged in shared memory; every CTA writes its partial gradient, and the AdamW
+// kernel sums the partials in CTA order (training is deterministic for a given grid).
+#include <cuda_bf16.h>
+
+#include <algorithm>
+
+#include "tp_common.cuh"
+
+namespace tp {
+
+constexpr int MLP_IN = 16, MLP_H = 64;
+// FP32 master parameter vector layout
+constexpr int OFF_W1 = 0;                      // [64][16]
+constexpr int OFF_B1 = OFF_W1 + MLP_H * MLP_IN;  // [64]
+constexpr int OFF_W2 = OFF_B1 + MLP_H;           // [64][64]
+constexpr int OFF_B2 = OFF_W2 + MLP_H * MLP_H;   // [64]
+constexpr int OFF_W3 = OFF_B2 + MLP_H;           // [64]
+constexpr int OFF_B3 = OFF_W3 + MLP_H;           // [1]
+constexpr int MLP_P = OFF_B3 + 1;
+
+struct MlpFeat {
+  const double* U;      // (V, ld) u^n
+  const double* Up;     // (V, ld) u^{n-1}
+  const double* phi;    // (V) or NULL
+  const double* ngphi;  // (V) or NULL
+  int S, ld;
+  float logD[4], k[4];
+  float mean[8], istd[8];
+};
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&v);
+}
+
+__device__ __forceinline__ void mma_bf16(float c[4], uint32_t a0, uint32_t a1, uint32_t a2,
+                                         uint32_t a3, uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// normalised feature f (0..15) of row r = v * S + s
+__device__ __forceinline__ float feature(const MlpFeat& F, int64_t r, int f) {
+  if (f >= 8) return 0.0f;
+  const int64_t v = r / F.S;
+  const int s = (int)(r - v * F.S);
+  float x;
+  switch (f) {
+    case 0: x = F.phi ? (float)F.phi[v] : 0.0f; break;
+    case 1: x = F.ngphi ? (float)F.ngphi[v] : 0.0f; break;
+    case 2: x = (float)F.U[v * F.ld + s]; break;
+    case 3: x = (float)F.Up[v * F.ld + s]; break;
+    case 4: x = (float)(F.U[v * F.ld + s] - F.Up[v * F.ld + s]); break;
+    case 5: x = F.logD[s]; break;
+    case 6: x = F.k[s]; break;
+    default: return 1.0f;
+  }
+  return (x - F.mean[f]) * F.istd[f];
+}
+
+// shared-memory copy of the BF16 weights; W2T[in][out] is the transpose used by the
+// backward pass
+struct MlpSmem {
+  __nv_bfloat16 W1[MLP_H][MLP_IN];
+  __nv_bfloat16 W2[MLP_H][MLP_H];
+  __nv_bfloat16 W2T[MLP_H][MLP_H];
+  float w3[MLP_H];
+  float b1[MLP_H], b2[MLP_H];
+  float b3;
+};
+
+__device__ void load_weights(MlpSmem& sm, const float* __restrict__ P) {
+  for (int i = threadIdx.x; i < MLP_H * MLP_IN; i += blockDim.x)
+    sm.W1[i / MLP_IN][i % MLP_IN] = __float2bfloat16_rn(P[OFF_W1 + i]);
+  for (int i = threadIdx.x; i < MLP_H * MLP_H; i += blockDim.x) {
+    const __nv_bfloat16 w = __float2bfloat16_rn(P[OFF_W2 + i]);
+    sm.W2[i / MLP_H][i % MLP_H] = w;
+    sm.W2T[i % MLP_H][i / MLP_H] = w;
+  }
+  for (int i = threadIdx.x; i < MLP_H; i += blockDim.x) {
+    sm.w3[i] = __bfloat162float(__float2bfloat16_rn(P[OFF_W3 + i]));
+    sm.b1[i] = P[OFF_B1 + i];
+    sm.b2[i] = P[OFF_B2 + i];
+  }
+  if (threadIdx.x == 0) sm.b3 = P[OFF_B3];
+  __syncthreads();
+}
+
+// B fragment of W^T for W stored [n][k] row-major with row length ldk
+__device__ __forceinline__ void bfrag(const __nv_bfloat16* W, int ldk, int n0, int k0, int g,
+                                      int t, uint32_t& b0, uint32_t& b1) {
+  const __nv_bfloat16* row = W + (n0 + g) * ldk + k0 + 2 * t;
+  b0 = *reinterpret_cast<const uint32_t*>(row);
+  b1 = *reinterpret_cast<const uint32_t*>(row + 8);
+}
+
+// Forward pass of one 16-row tile.  xa: the A fragment of the inputs (K = 16).
+// On return z1/z2 hold the pre-activations (8 n-tiles x 4), y the output of rows g, g+8
+// (valid in every lane of the quad).
+__device__ __forceinline__ void mlp_tile_forward(const MlpSmem& sm, const uint32_t xa[4], int g,
+                                                 int t, float z1[8][4], float z2[8][4],
+                                                 float& y0, float& y1) {
+#pragma unroll
+  for (int n = 0; n < 8; n++) {
+    const float bl = sm.b1[n * 8 + 2 * t], bh = sm.b1[n * 8 + 2 * t + 1];
+    z1[n][0] = bl;
+    z1[n][1] = bh;
+    z1[n][2] = bl;
+    z1[n][3] = bh;
+    uint32_t b0, b1;
+    bfrag(&sm.W1[0][0], MLP_IN, n * 8, 0, g, t, b0, b1);
+    mma_bf16(z1[n], xa[0], xa[1], xa[2], xa[3], b0, b1);
+  }
+  uint32_t ha[4][4];  // h1 as A fragments, 4 k-steps
+#pragma unroll
+  for (int kk = 0; kk < 4; kk++) {
+    const float* lo = z1[2 * kk];
+    const float* hi = z1[2 * kk + 1];
+    ha[kk][0] = pack_bf16(fmaxf(lo[0], 0.f), fmaxf(lo[1], 0.f));
+    ha[kk][1] = pack_bf16(fmaxf(lo[2], 0.f), fmaxf(lo[3], 0.f));
+    ha[kk][2] = pack_bf16(fmaxf(hi[0], 0.f), fmaxf(hi[1], 0.f));
+    ha[kk][3] = pack_bf16(fmaxf(hi[2], 0.f), fmaxf(hi[3], 0.f));
+  }
+#pragma unroll
+  for (int n = 0; n < 8; n++) {
+    const float bl = sm.b2[n * 8 + 2 * t], bh = sm.b2[n * 8 + 2 * t + 1];
+    z2[n][0] = bl;
+    z2[n][1] = bh;
+    z2[n][2] = bl;
+    z2[n][3] = bh;
+#pragma unroll
+    for (int kk = 0; kk < 4; kk++) {
+      uint32_t b0, b1;
+      bfrag(&sm.W2[0][0], MLP_H, n * 8, kk * 16, g, t, b0, b1);
+      mma_bf16(z2[n], ha[kk][0], ha[kk][1], ha[kk][2], ha[kk][3], b0, b1);
+    }
+  }
+  // layer 3 (64 -> 1) on the CUDA cores: BF16-rounded h2 . w3, reduced over the quad
+  float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+  for (int n = 0; n < 8; n++) {
+#pragma unroll
+    for (int e = 0; e < 2; e++) {
+      const float w = sm.w3[n * 8 + 2 * t + e];
+      s0 += __bfloat162float(__float2bfloat16_rn(fmaxf(z2[n][e], 0.f))) * w;
+      s1 += __bfloat162float(__float2bfloat16_rn(fmaxf(z2[n][2 + e], 0.f))) * w;
+    }
+  }
+  s0 += __shfl_xor_sync(0xffffffffu, s0, 1);
+  s0 += __shfl_xor_sync(0xffffffffu, s0, 2);
+  s1 += __shfl_xor_sync(0xffffffffu, s1, 1);
+  s1 += __shfl_xor_sync(0xffffffffu, s1, 2);
+  y0 = s0 + sm.b3;
+  y1 = s1 + sm.b3;
+}
+
+// A fragment of the inputs of rows r0 + g, r0 + g + 8 (16 features)
+__device__ __forceinline__ void input_frag(const MlpFeat& F, int64_t r0, int64_t nrows, int g,
+                                           int t, uint32_t xa[4]) {
+  const int64_t ra = r0 + g, rb = r0 + g + 8;
+  auto f = [&](int64_t r, int c) { return r < nrows ? feature(F, r, c) : 0.0f; };
+  xa[0] = pack_bf16(f(ra, 2 * t), f(ra, 2 * t + 1));
+  xa[1] = pack_bf16(f(rb, 2 * t), f(rb, 2 * t + 1));
+  xa[2] = pack_bf16(f(ra, 2 * t + 8), f(ra, 2 * t + 9));
+  xa[3] = pack_bf16(f(rb, 2 * t + 8), f(rb, 2 * t + 9));
+}
+
+// ----------------------------------------------------------------- inference
+// x_out[v, s] = U[v, s] + sigma * y(v, s)  (or y_out[r] = y when x_out is NULL)
+__global__ void __launch_bounds__(128) k_mlp_predict(MlpFeat F, int64_t nrows,
+                                                     const float* __restrict__ P, float sigma,
+                                                     double* __restrict__ x_out,
+                                                     float* __restrict__ y_out) {
+  __shared__ MlpSmem sm;
+  load_weights(sm, P);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int64_t ntiles = (nrows + 15) / 16;
+  for (int64_t tile = (int64_t)blockIdx.x * 4 + warp; tile < ntiles;
+       tile += (int64_t)gridDim.x * 4) {
+    const int64_t r0 = tile * 16;
+    uint32_t xa[4];
+    input_frag(F, r0, nrows, g, t, xa);
+    float z1[8][4], z2[8][4], y0, y1;
+    mlp_tile_forward(sm, xa, g, t, z1, z2, y0, y1);
+    if (t == 0) {
+      const int64_t rr[2] = {r0 + g, r0 + g + 8};
+      const float yy[2] = {y0, y1};
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        if (rr[h] >= nrows) continue;
+        if (x_out) {
+          const int64_t v = rr[h] / F.S;
+          const int s = (int)(rr[h] - v * F.S);
+          x_out[v * F.ld + s] = F.U[v * F.ld + s] + (double)sigma * (double)yy[h];
+        } else {
+          y_out[rr[h]] = yy[h];
+        }
+      }
+    }
+  }
+}
+
+// features of every row, materialised (training set), BF16 (nrows, 16)
+__global__ void k_mlp_features(MlpFeat F, int64_t nrows, __nv_bfloat16* __restrict__ X) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nrows * MLP_IN;
+       i += (int64_t)gridDim.x * blockDim.x)
+    X[i] = __float2bfloat16_rn(feature(F, i / MLP_IN, (int)(i % MLP_IN)));
+}
+
+// training target (u^{n+1} - u^n) / sigma per row
+__global__ void k_mlp_target(int64_t nrows, int S, int ld, const double* __restrict__ Un,
+                             const double* __restrict__ Unext, float inv_sigma,
+                             float* __restrict__ T) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nrows;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t v = r / S;
+    const int s = (int)(r - v * S);
+    T[r] = (float)((Unext[v * ld + s] - Un[v * ld + s]) * inv_sigma);
+  }
+}
+
+// ----------------------------------------------------------------- training
+struct GradSmem {
+  __nv_bfloat16 dz2T[MLP_H][64];  // [out unit][chunk row]
+  __nv_bfloat16 h1T[MLP_H][64];   // [hidden unit][chunk row]
+  __nv_bfloat16 dz1T[MLP_H][64];
+  __nv_bfloat16 xT[MLP_IN][64];
+  float dw3[4][MLP_H];  // per warp
+  float db3[4];
+  float loss[4];
+};
+
+// One CTA = 4 warps = 64-row chunks.  Partial gradients (MLP_P floats) and the loss
+// partial (sum of squared errors) per CTA.  wscale = 2 / (rows in the batch).
+__global__ void __launch_bounds__(128) k_mlp_grad(const __nv_bfloat16* __restrict__ X,
+                                                  const float* __restrict__ T, int64_t row0,
+                                                  int64_t nrows, const float* __restrict__ P,
+                                                  float wscale, float* __restrict__ part,
+                                                  float* __restrict__ loss_part) {
+  __shared__ MlpSmem sm;
+  __shared__ GradSmem gs;
+  load_weights(sm, P);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  for (int i = threadIdx.x; i < 4 * MLP_H; i += blockDim.x) gs.dw3[i / MLP_H][i % MLP_H] = 0.f;
+  if (threadIdx.x < 4) {
+    gs.db3[threadIdx.x] = 0.f;
+    gs.loss[threadIdx.x] = 0.f;
+  }
+  // dW2 rows [16 warp, 16 warp + 16) x 64 cols; dW1 rows [16 warp, +16) x 16 cols
+  float dW2[8][4], dW1[2][4];
+#pragma unroll
+  for (int n = 0; n < 8; n++) dW2[n][0] = dW2[n][1] = dW2[n][2] = dW2[n][3] = 0.f;
+#pragma unroll
+  for (int n = 0; n < 2; n++) dW1[n][0] = dW1[n][1] = dW1[n][2] = dW1[n][3] = 0.f;
+  float db1 = 0.f, db2 = 0.f;  // thread i < 64: db2[i]; 64 <= i < 128: db1[i - 64]
+  __syncthreads();
+  const int64_t nchunks = (nrows + 63) / 64;
+  for (int64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const int64_t r0 = ch * 64 + warp * 16;  // this warp's 16 rows (relative)
+    // inputs of rows r0 + g, r0 + g + 8
+    uint32_t xa[4];
+    {
+      const int64_t ra = r0 + g, rb = r0 + g + 8;
+      const uint32_t* Xa = reinterpret_cast<const uint32_t*>(X + (row0 + ra) * MLP_IN);
+      const uint32_t* Xb = reinterpret_cast<const uint32_t*>(X + (row0 + rb) * MLP_IN);
+      xa[0] = ra < nrows ? Xa[t] : 0u;
+      xa[1] = rb < nrows ? Xb[t] : 0u;
+      xa[2] = ra < nrows ? Xa[t + 4] : 0u;
+      xa[3] = rb < nrows ? Xb[t + 4] : 0u;
+    }
+    float z1[8][4], z2[8][4], y0, y1;
+    mlp_tile_forward(sm, xa, g, t, z1, z2, y0, y1);
+    const int64_t ra = r0 + g, rb = r0 + g + 8;
+    const float e0 = ra < nrows ? y0 - T[row0 + ra] : 0.f;
+    const float e1 = rb < nrows ? y1 - T[row0 + rb] : 0.f;
+    const float d0 = wscale * e0, d1 = wscale * e1;  // dL/dy
+    {
+      // every lane of a quad holds its rows' errors: sum over the 8 quads of the warp
+      float ls = e0 * e0 + e1 * e1, bs = d0 + d1;
+      ls += __shfl_xor_sync(0xffffffffu, ls, 4);
+      ls += __shfl_xor_sync(0xffffffffu, ls, 8);
+      ls += __shfl_xor_sync(0xffffffffu, ls, 16);
+      bs += __shfl_xor_sync(0xffffffffu, bs, 4);
+      bs += __shfl_xor_sync(0xffffffffu, bs, 8);
+      bs += __shfl_xor_sync(0xffffffffu, bs, 16);
+      if (lane == 0) {
+        gs.loss[warp] += ls;
+        gs.db3[warp] += bs;
+      }
+    }
+    // layer 3 and dZ2 = dy w3 [z2 > 0]
+    float dz2[8][4];
+#pragma unroll
+    for (int n = 0; n < 8; n++) {
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        const int j = n * 8 + 2 * t + e;
+        const float h0 = __bfloat162float(__float2bfloat16_rn(fmaxf(z2[n][e], 0.f)));
+        const float h1v = __bfloat162float(__float2bfloat16_rn(fmaxf(z2[n][2 + e], 0.f)));
+        float pw = d0 * h0 + d1 * h1v;  // dw3[j] partial over rows g, g+8
+        pw += __shfl_xor_sync(0xffffffffu, pw, 4);
+        pw += __shfl_xor_sync(0xffffffffu, pw, 8);
+        pw += __shfl_xor_sync(0xffffffffu, pw, 16);
+        if (g == 0) gs.dw3[warp][j] += pw;
+        dz2[n][e] = z2[n][e] > 0.f ? d0 * sm.w3[j] : 0.f;
+        dz2[n][2 + e] = z2[n][2 + e] > 0.f ? d1 * sm.w3[j] : 0.f;
+      }
+    }
+    // dH1 = dZ2 W2 (A = dZ2 as bf16 fragments, B = W2 via its transpose)
+    uint32_t da[4][4];
+#pragma unroll
+    for (int kk = 0; kk < 4; kk++) {
+      da[kk][0] = pack_bf16(dz2[2 * kk][0], dz2[2 * kk][1]);
+      da[kk][1] = pack_bf16(dz2[2 * kk][2], dz2[2 * kk][3]);
+      da[kk][2] = pack_bf16(dz2[2 * kk + 1][0], dz2[2 * kk + 1][1]);
+      da[kk][3] = pack_bf16(dz2[2 * kk + 1][2], dz2[2 * kk + 1][3]);
+    }
+    float dz1[8][4];
+#pragma unroll
+    for (int n = 0; n < 8; n++) {
+      dz1[n][0] = dz1[n][1] = dz1[n][2] = dz1[n][3] = 0.f;
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++) {
+        uint32_t b0, b1;
+        bfrag(&sm.W2T[0][0], MLP_H, n * 8, kk * 16, g, t, b0, b1);
+        mma_bf16(dz1[n], da[kk][0], da[kk][1], da[kk][2], da[kk][3], b0, b1);
+      }
+#pragma unroll
+      for (int e = 0; e < 4; e++) dz1[n][e] = z1[n][e] > 0.f ? dz1[n][e] : 0.f;
+    }
+    // stage transposed tiles (columns = this chunk's 64 rows)
+    const int ca = warp * 16 + g, cb = warp * 16 + g + 8;
+#pragma unroll
+    for (int n = 0; n < 8; n++) {
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        const int j = n * 8 + 2 * t + e;
+        gs.dz2T[j][ca] = __float2bfloat16_rn(dz2[n][e]);
+        gs.dz2T[j][cb] = __float2bfloat16_rn(dz2[n][2 + e]);
+        gs.dz1T[j][ca] = __float2bfloat16_rn(dz1[n][e]);
+        gs.dz1T[j][cb] = __float2bfloat16_rn(dz1[n][2 + e]);
+        gs.h1T[j][ca] = __float2bfloat16_rn(fmaxf(z1[n][e], 0.f));
+        gs.h1T[j][cb] = __float2bfloat16_rn(fmaxf(z1[n][2 + e], 0.f));
+      }
+    }
+    {
+      const __nv_bfloat162* xa2 = reinterpret_cast<const __nv_bfloat162*>(xa);
+      gs.xT[2 * t][ca] = xa2[0].x;
+      gs.xT[2 * t + 1][ca] = xa2[0].y;
+      gs.xT[2 * t][cb] = xa2[1].x;
+      gs.xT[2 * t + 1][cb] = xa2[1].y;
+      gs.xT[2 * t + 8][ca] = xa2[2].x;
+      gs.xT[2 * t + 9][ca] = xa2[2].y;
+      gs.xT[2 * t + 8][cb] = xa2[3].x;
+      gs.xT[2 * t + 9][cb] = xa2[3].y;
+    }
+    __syncthreads();
+    // dW2[i][j] += sum_r dZ2T[i][r] H1T[j][r];  dW1[i][j] += sum_r dZ1T[i][r] XT[j][r]
+    const int i0 = warp * 16;
+#pragma unroll
+    for (int kk = 0; kk < 4; kk++) {
+      const int k0 = kk * 16;
+      uint32_t a[4], a1[4];
+      a[0] = *reinterpret_cast<const uint32_t*>(&gs.dz2T[i0 + g][k0 + 2 * t]);
+      a[1] = *reinterpret_cast<const uint32_t*>(&gs.dz2T[i0 + g + 8][k0 + 2 * t]);
+      a[2] = *reinterpret_cast<const uint32_t*>(&gs.dz2T[i0 + g][k0 + 2 * t + 8]);
+      a[3] = *reinterpret_cast<const uint32_t*>(&gs.dz2T[i0 + g + 8][k0 + 2 * t + 8]);
+      a1[0] = *reinterpret_cast<const uint32_t*>(&gs.dz1T[i0 + g][k0 + 2 * t]);
+      a1[1] = *reinterpret_cast<const uint32_t*>(&gs.dz1T[i0 + g + 8][k0 + 2 * t]);
+      a1[2] = *reinterpret_cast<const uint32_t*>(&gs.dz1T[i0 + g][k0 + 2 * t + 8]);
+      a1[3] = *reinterpret_cast<const uint32_t*>(&gs.dz1T[i0 + g + 8][k0 + 2 * t + 8]);
+#pragma unroll
+      for (int n = 0; n < 8; n++) {
+        uint32_t b0, b1;
+        bfrag(&gs.h1T[0][0], 64, n * 8, k0, g, t, b0, b1);
+        mma_bf16(dW2[n], a[0], a[1], a[2], a[3], b0, b1);
+      }
+#pragma unroll
+      for (int n = 0; n < 2; n++) {
+        uint32_t b0, b1;
+        bfrag(&gs.xT[0][0], 64, n * 8, k0, g, t, b0, b1);
+        mma_bf16(dW1[n], a1[0], a1[1], a1[2], a1[3], b0, b1);
+      }
+    }
+    // bias gradients: thread i < 64 owns db2[i], 64 <= i < 128 owns db1[i - 64]
+    {
+      const int i = threadIdx.x & 63;
+      const __nv_bfloat16* rowp = threadIdx.x < 64 ? gs.dz2T[i] : gs.dz1T[i];
+      float sacc = 0.f;
+      for (int c = 0; c < 64; c++) sacc += __bfloat162float(rowp[c]);
+      if (threadIdx.x < 64)
+        db2 += sacc;
+      else
+        db1 += sacc;
+    }
+    __syncthreads();
+  }
+  // write this CTA's partial gradient
+  float* out = part + (int64_t)blockIdx.x * MLP_P;
+  const int i0 = warp * 16;
+#pragma unroll
+  for (int n = 0; n < 8; n++) {
+    const int j = n * 8 + 2 * t;
+    out[OFF_W2 + (i0 + g) * MLP_H + j] = dW2[n][0];
+    out[OFF_W2 + (i0 + g) * MLP_H + j + 1] = dW2[n][1];
+    out[OFF_W2 + (i0 + g + 8) * MLP_H + j] = dW2[n][2];
+    out[OFF_W2 + (i0 + g + 8) * MLP_H + j + 1] = dW2[n][3];
+  }
+#pragma unroll
+  for (int n = 0; n < 2; n++) {
+    const int j = n * 8 + 2 * t;
+    out[OFF_W1 + (i0 + g) * MLP_IN + j] = dW1[n][0];
+    out[OFF_W1 + (i0 + g) * MLP_IN + j + 1] = dW1[n][1];
+    out[OFF_W1 + (i0 + g + 8) * MLP_IN + j] = dW1[n][2];
+    out[OFF_W1 + (i0 + g + 8) * MLP_IN + j + 1] = dW1[n][3];
+  }
+  if (threadIdx.x < 64)
+    out[OFF_B2 + threadIdx.x] = db2;
+  else
+    out[OFF_B1 + threadIdx.x - 64] = db1;
+  __syncthreads();
+  if (threadIdx.x < MLP_H)
+    out[OFF_W3 + threadIdx.x] = ((gs.dw3[0][threadIdx.x] + gs.dw3[1][threadIdx.x]) +
+                                 gs.dw3[2][threadIdx.x]) + gs.dw3[3][threadIdx.x];
+  if (threadIdx.x == 0) {
+    out[OFF_B3] = ((gs.db3[0] + gs.db3[1]) + gs.db3[2]) + gs.db3[3];
+    loss_part[blockIdx.x] = ((gs.loss[0] + gs.loss[1]) + gs.loss[2]) + gs.loss[3];
+  }
+}
+
+// Sum the CTA partials in CTA order, AdamW on the FP32 master parameters.
+__global__ void k_mlp_adamw(const float* __restrict__ part, int nparts,
+                            const float* __restrict__ loss_part, float* __restrict__ P,
+                            float* __restrict__ m, float* __restrict__ v, float lr, float b1,
+                            float b2, float eps, float wd, float bc1, float bc2,
+                            float* __restrict__ grad_out, float* __restrict__ loss_out) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < MLP_P; p += gridDim.x * blockDim.x) {
+    float gsum = 0.f;
+    for (int c = 0; c < nparts; c++) gsum += part[(int64_t)c * MLP_P + p];
+    if (grad_out) grad_out[p] = gsum;
+    if (lr > 0.f) {
+      const float mm = b1 * m[p] + (1.f - b1) * gsum;
+      const float vv = b2 * v[p] + (1.f - b2) * gsum * gsum;
+      m[p] = mm;
+      v[p] = vv;
+      const bool decay = !((p >= OFF_B1 && p < OFF_W2) || (p >= OFF_B2 && p < OFF_W3) ||
+                           p == OFF_B3);
+      P[p] -= lr * ((mm / bc1) / (sqrtf(vv / bc2) + eps) + (decay ? wd * P[p] : 0.f));
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && loss_out) {
+    float l = 0.f;
+    for (int c = 0; c < nparts; c++) l += loss_part[c];
+    *loss_out = l;
+  }
+}
+
+}  // namespace tp
+
+using namespace tp;
+
+static MlpFeat make_feat(const tp_mlp_inputs* in) {
+  MlpFeat F;
+  F.U = in->U;
+  F.Up = in->U_prev;
+  F.phi = in->phi;
+  F.ngphi = in->normgradphi;
+  F.S = in->S;
+  F.ld = in->ld;
+  for (int s = 0; s < 4; s++) {
+    F.logD[s] = (float)in->logD[s];
+    F.k[s] = (float)in->k[s];
+  }
+  for (int f = 0; f < 8; f++) {
+    F.mean[f] = (float)in->mean[f];
+    F.istd[f] = (float)in->istd[f];
+  }
+  return F;
+}
+
+extern "C" int tp_mlp_param_count(void) { return MLP_P; }
+
+extern "C" int tp_mlp_predict(const tp_mlp_inputs* in, const float* params, float sigma,
+                              double* x_out, float* y_out, void* stream) {
+  TP_REQUIRE(in && in->U && in->U_prev && params && (x_out || y_out), "null pointer");
+  TP_REQUIRE(in->S >= 1 && in->S <= 4 && in->ld >= in->S, "bad S/ld");
+  const int64_t nrows = in->n_verts * in->S;
+  if (nrows == 0) return TP_OK;
+  const int64_t ntiles = (nrows + 15) / 16;
+  const int grid = (int)std::min<int64_t>((ntiles + 3) / 4, (int64_t)sm_count() * 16);
+  k_mlp_predict<<<grid, 128, 0, as_stream(stream)>>>(make_feat(in), nrows, params, sigma, x_out,
+                                                      y_out);
+  TP_LAUNCH_CHECK();
+  return TP_OK;
+}
+
+extern "C" int tp_mlp_features(const tp_mlp_inputs* in, void* X, void* stream) {
+  TP_REQUIRE(in && in->U && in->U_prev && X, "null pointer");
+  const int64_t nrows = in->n_verts * in->S;
+  if (nrows == 0) return TP_OK;
+  k_mlp_features<<<grid_for(nrows * MLP_IN, 256, 65535), 256, 0, as_stream(stream)>>>(
+      make_feat(in), nrows, static_cast<__nv_bfloat16*>(X));
+  TP_LAUNCH_CHECK();
+  return TP_OK;
+}
+
+extern "C" int tp_mlp_target(int64_t n_verts, int S, int ld, const double* U_n,
+                             const double* U_next, double sigma, float* T, void* stream) {
+  TP_REQUIRE(U_n && U_next && T && sigma > 0, "bad argument");
+  const int64_t nrows = n_verts * S;
+  if (nrows == 0) return TP_OK;
+  k_mlp_target<<<grid_for(nrows, 256, 65535), 256, 0, as_stream(stream)>>>(
+      nrows, S, ld, U_n, U_next, (float)(1.0 / sigma), T);
+  TP_LAUNCH_CHECK();
+  return TP_OK;
+}
+
+extern "C" size_t tp_mlp_grad_workspace_floats(int grid) { return (size_t)grid * (MLP_P + 1); }
+
+extern "C" int tp_mlp_train_step(const void* X, const float* T, int64_t row0, int64_t nrows,
+                                 float* params, float* adam_m, float* adam_v, int step,
+                                 float lr, float beta1, float beta2, float eps,
+                                 float weight_decay, int grid, float* workspace,
+                                 float* grad_out, float* loss_out, void* stream) {
+  TP_REQUIRE(X && T && params && workspace && grid >= 1, "bad argument");
+  TP_REQUIRE(lr <= 0.f || (adam_m && adam_v && step >= 1), "AdamW state required");
+  cudaStream_t st = as_stream(stream);
+  float* part = workspace;
+  float* loss_part = workspace + (size_t)grid * MLP_P;
+  const float wscale = nrows > 0 ? 2.0f / (float)nrows : 0.f;
+  k_mlp_grad<<<grid, 128, 0, st>>>(static_cast<const __nv_bfloat16*>(X), T, row0, nrows, params,
+                                   wscale, part, loss_part);
+  TP_LAUNCH_CHECK();
+  const float bc1 = 1.f - powf(beta1, (float)std::max(step, 1));
+  const float bc2 = 1.f - powf(beta2, (float)std::max(step, 1));
+  k_mlp_adamw<<<(MLP_P + 255) / 256, 256, 0, st>>>(part, grid, loss_part, params, adam_m, adam_v,
+                                                   lr, beta1, beta2, eps, weight_decay, bc1,
+                                                   bc2, grad_out, loss_out);
+  TP_LAUNCH_CHECK();
+  return TP_OK;
+}

@@ -67,6 +67,12 @@ class TpSell(ctypes.Structure):
                 ("sK32", _vp), ("sK64", _vp), ("sM32", _vp), ("sM64", _vp)]
 
 
+class TpMlpInputs(ctypes.Structure):
+    _fields_ = [("n_verts", _c_i64), ("S", _c_i32), ("ld", _c_i32), ("U", _vp), ("U_prev", _vp),
+                ("phi", _vp), ("normgradphi", _vp), ("logD", _c_dbl * 4), ("k", _c_dbl * 4),
+                ("mean", _c_dbl * 8), ("istd", _c_dbl * 8)]
+
+
 class TpCgResult(ctypes.Structure):
     _fields_ = [("status", _c_i32), ("iterations", _c_i32), ("n_reliable", _c_i32),
                 ("n_lanes", _c_i32)]
@@ -128,6 +134,16 @@ SIGNATURES = {
     "tp_pcg_grid": (ctypes.c_int, [_vp, _P(ctypes.c_int), _P(ctypes.c_int)]),
     "tp_pcg_set_profile": (ctypes.c_int, [_vp, _vp]),
     "tp_pcg_destroy": (ctypes.c_int, [_vp]),
+    "tp_mlp_param_count": (ctypes.c_int, []),
+    "tp_mlp_predict": (ctypes.c_int, [_P(TpMlpInputs), _vp, ctypes.c_float, _vp, _vp, _vp]),
+    "tp_mlp_features": (ctypes.c_int, [_P(TpMlpInputs), _vp, _vp]),
+    "tp_mlp_target": (ctypes.c_int, [_c_i64, ctypes.c_int, ctypes.c_int, _vp, _vp, _c_dbl, _vp,
+                                     _vp]),
+    "tp_mlp_grad_workspace_floats": (ctypes.c_size_t, [ctypes.c_int]),
+    "tp_mlp_train_step": (ctypes.c_int, [_vp, _vp, _c_i64, _c_i64, _vp, _vp, _vp, ctypes.c_int,
+                                         ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                         ctypes.c_float, ctypes.c_float, ctypes.c_int, _vp, _vp,
+                                         _vp, _vp]),
 }
 
 

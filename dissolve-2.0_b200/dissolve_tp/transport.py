@@ -232,6 +232,8 @@ class BatchedTransport:
         guess = 1 if (self.guess != "previous" and self.steps_done > 1) else 0
         if self.guess == "learned" and self.predictor is not None:
             guess = self.predictor.launches
+        if self.engine == "persistent":
+            return 3 + 1 + guess + 1  # assembly, diagonal, RHS, SELL scatter, guess, solve
         return 3 + guess + 4 + 3 * int(res["iterations"]) + 2 * int(res["n_reliable"])
 
     def step_host(self, u_host: torch.Tensor, out_host: torch.Tensor):

@@ -332,6 +332,44 @@ TP_API int tp_pcg_grid(tp_pcg_handle* h, int* grid, int* block);
 TP_API int tp_pcg_set_profile(tp_pcg_handle* h, unsigned long long* prof);
 TP_API int tp_pcg_destroy(tp_pcg_handle* h);
 
+/* ------------------------------------------------------------------ learned guess */
+/* Per-vertex MLP predicting the next backward-Euler state as the Krylov initial guess
+ * (no reference counterpart).  One network for all species; a row is (vertex, species).
+ * Inputs (normalised: (x - mean[f]) * istd[f]): phi, |grad phi|, u^n, u^{n-1},
+ * u^n - u^{n-1}, log D_s, k_s, 1; 16 -> 64 -> ReLU -> 64 -> ReLU -> 1, BF16 weights and
+ * activations on the tensor cores, FP32 accumulation.  Parameters: one FP32 vector of
+ * tp_mlp_param_count() floats [W1 (64x16) | b1 | W2 (64x64) | b2 | w3 (64) | b3]. */
+typedef struct tp_mlp_inputs {
+  int64_t n_verts;
+  int32_t S, ld;
+  const double* U;           /* (n_verts, ld) u^n      */
+  const double* U_prev;      /* (n_verts, ld) u^{n-1}  */
+  const double* phi;         /* (n_verts) or NULL       */
+  const double* normgradphi; /* (n_verts) or NULL       */
+  double logD[4], k[4];      /* per species             */
+  double mean[8], istd[8];   /* input normalisation     */
+} tp_mlp_inputs;
+
+TP_API int tp_mlp_param_count(void);
+/* x_out[v, s] = U[v, s] + sigma * y(v, s) (the guess, written into a solver's x), or
+ * y_out[v * S + s] = y when x_out is NULL */
+TP_API int tp_mlp_predict(const tp_mlp_inputs* in, const float* params, float sigma,
+                          double* x_out, float* y_out, void* stream);
+/* the normalised inputs as BF16 rows of 16 (training set) */
+TP_API int tp_mlp_features(const tp_mlp_inputs* in, void* X_bf16, void* stream);
+/* training target (U_next - U_n) / sigma per row */
+TP_API int tp_mlp_target(int64_t n_verts, int S, int ld, const double* U_n,
+                         const double* U_next, double sigma, float* T, void* stream);
+TP_API size_t tp_mlp_grad_workspace_floats(int grid);
+/* one AdamW step on rows [row0, row0 + nrows) of (X, T), loss = mean squared error.
+ * grid CTAs write partial gradients into workspace (tp_mlp_grad_workspace_floats(grid)).
+ * lr <= 0: gradient only (grad_out, the summed gradient, may be NULL otherwise).
+ * loss_out: sum of squared errors (device float) or NULL. */
+TP_API int tp_mlp_train_step(const void* X_bf16, const float* T, int64_t row0, int64_t nrows,
+                             float* params, float* adam_m, float* adam_v, int step, float lr,
+                             float beta1, float beta2, float eps, float weight_decay, int grid,
+                             float* workspace, float* grad_out, float* loss_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,155 @@
+"""Warm-start MLP: the oracle's backward pass against central differences (CPU) and the
+tensor-core kernels against the oracle (GPU).
+
+Bars: FP64 analytic gradient within 1e-4 relative of central differences (step 1e-5); GPU forward
+outputs within 2e-3 relative (max-norm) of the oracle, which rounds to BF16 at the same
+points as the kernels; GPU gradients within 5e-3 relative (norm-wise per parameter
+block); AdamW update within 1e-6 of the oracle's given the same gradient."""
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as mo
+
+
+def test_oracle_backward_matches_finite_differences():
+    for seed in (0, 1, 2):
+        assert mo.fd_check(seed=seed, h=1e-5) < 1e-4
+    assert mo.fd_check(seed=3, n=17, h=1e-5) < 1e-4
+
+
+def test_bf16_rounding_helper():
+    x = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -9, -2.5e-3, 65504.0])
+    r = mo.bf16(x)
+    assert r[0] == 1.0 and r[1] == 1.0  # tie to even
+    assert r[2] == 1.0 + 2 ** -7
+    assert abs(r[3] - x[3]) <= 2 ** -8 * abs(x[3])
+
+
+def test_product_init_matches_oracle_init():
+    from dissolve_tp import mlp
+    assert np.array_equal(mlp.initial_params(3), mo.init_params(3))
+    assert mlp.P == mo.P
+
+
+def _random_setup(seed, rows):
+    rng = np.random.default_rng(seed)
+    p = mo.init_params(seed).astype(np.float64)
+    p[mo.OFF_B1:mo.OFF_W2] = rng.normal(0, 0.2, mo.H)
+    p[mo.OFF_B2:mo.OFF_W3] = rng.normal(0, 0.2, mo.H)
+    p[mo.OFF_B3] = 0.1
+    p = p.astype(np.float32)
+    X = rng.normal(0, 1, (rows, mo.IN))
+    X[:, 7] = 1.0
+    X[:, 8:] = 0.0
+    X = mo.bf16(X)
+    T = rng.normal(0, 1, rows).astype(np.float32)
+    return p, X, T
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rows", [64, 1000, 20011])
+def test_gpu_gradient_matches_oracle(cuda_device, rows):
+    import torch
+
+    from dissolve_tp.mlp import WarmStartMLP
+    p, X, T = _random_setup(7, rows)
+    m = WarmStartMLP(cuda_device, capacity_rows=rows)
+    m.params.copy_(torch.from_numpy(p))
+    m.X[:rows].copy_(torch.from_numpy(X.astype(np.float32)).to(torch.bfloat16))
+    m.T[:rows].copy_(torch.from_numpy(T))
+    m.rows = rows
+    g, loss = m.gradient(0, rows)
+    g = g.cpu().numpy().astype(np.float64)
+    lo, go = mo.loss_and_grad(p, X, T.astype(np.float64))
+    assert abs(float(loss.item()) - lo) <= 2e-3 * lo
+    blocks = {"W1": (mo.OFF_W1, mo.OFF_B1), "b1": (mo.OFF_B1, mo.OFF_W2),
+              "W2": (mo.OFF_W2, mo.OFF_B2), "b2": (mo.OFF_B2, mo.OFF_W3),
+              "w3": (mo.OFF_W3, mo.OFF_B3), "b3": (mo.OFF_B3, mo.P)}
+    for name, (a, b) in blocks.items():
+        err = np.linalg.norm(g[a:b] - go[a:b]) / max(np.linalg.norm(go[a:b]), 1e-30)
+        assert err < 5e-3, (name, err)
+    # determinism: same inputs -> same gradient bits
+    g2, _ = m.gradient(0, rows)
+    assert np.array_equal(g2.cpu().numpy().astype(np.float64), g)
+
+
+@pytest.mark.gpu
+def test_gpu_adamw_step_matches_oracle(cuda_device):
+    import torch
+
+    from dissolve_tp.mlp import WarmStartMLP
+    rows = 5000
+    p, X, T = _random_setup(11, rows)
+    m = WarmStartMLP(cuda_device, capacity_rows=rows)
+    m.params.copy_(torch.from_numpy(p))
+    m.X[:rows].copy_(torch.from_numpy(X.astype(np.float32)).to(torch.bfloat16))
+    m.T[:rows].copy_(torch.from_numpy(T))
+    m.rows = rows
+    g, _ = m.gradient(0, rows)
+    g = g.cpu().numpy().astype(np.float64)
+    m.train(steps=1, batch_rows=rows, lr=1e-3, wd=1e-4)
+    # train() uses a cosine schedule: lr at step 0 is the full lr
+    po, _, _ = mo.adamw(p.astype(np.float64), np.zeros(mo.P), np.zeros(mo.P), g, 1, 1e-3)
+    assert np.abs(m.params.cpu().numpy() - po).max() < 1e-6
+
+
+@pytest.mark.gpu
+def test_gpu_forward_from_fields_matches_oracle(cuda_device):
+    import torch
+
+    from dissolve_tp.mlp import WarmStartMLP
+    rng = np.random.default_rng(5)
+    V, S, ld = 3001, 3, 4
+    U = rng.uniform(0, 1, (V, S))
+    Up = U + rng.normal(0, 0.05, (V, S))
+    phi = rng.normal(0, 1, V)
+    ng = np.abs(rng.normal(1, 0.2, V))
+    D, k = [1.0, 1.0, 2.6], [0.5, 0.0, 0.2]
+    m = WarmStartMLP(cuda_device)
+    m.mean = np.array([0.0, 1.0, 0.5, 0.5, 0.0, 0.3, 0.2, 0.0])
+    m.istd = np.array([1.0, 5.0, 3.0, 3.0, 20.0, 2.0, 4.0, 1.0])
+    m.sigma = 0.01
+    Ud = torch.zeros((V, ld), dtype=torch.float64, device=cuda_device)
+    Upd = torch.zeros_like(Ud)
+    Ud[:, :S] = torch.from_numpy(U)
+    Upd[:, :S] = torch.from_numpy(Up)
+    phid = torch.from_numpy(phi).to(cuda_device)
+    ngd = torch.from_numpy(ng).to(cuda_device)
+    y = m.predict(Ud, Upd, S, ld, D, k, phid, ngd).cpu().numpy().astype(np.float64)
+    X = mo.features(U, Up, phi, ng, np.log(D), k, m.mean, m.istd)
+    yo, _ = mo.forward(m.params.cpu().numpy(), X)
+    assert np.abs(y - yo).max() <= 2e-3 * np.abs(yo).max()
+    x = torch.zeros_like(Ud)
+    m.predict(Ud, Upd, S, ld, D, k, phid, ngd, x_out=x)
+    xo = U + m.sigma * yo.reshape(V, S)
+    assert np.abs(x[:, :S].cpu().numpy() - xo).max() <= 2e-3 * m.sigma * np.abs(yo).max() + 1e-12
+
+
+@pytest.mark.gpu
+def test_learned_guess_reduces_iterations(cuda_device):
+    """Train on one trajectory, evaluate on another: same tolerance, fewer iterations."""
+    from dissolve_tp import mlp
+    from dissolve_tp.mesh import kuhn_cube
+    from dissolve_tp.transport import BatchedTransport
+    m = kuhn_cube(16, 0.2, seed=0)
+    rng = np.random.default_rng(1)
+    coef = np.exp(0.3 * rng.standard_normal(m.n_cells))
+    D, K, dt = (1.0, 1.0, 2.6), (0.5, 0.0, 0.2), 0.02
+    u_eval = np.random.default_rng(2).uniform(0, 1, (m.n_verts, 3))
+    runs = {}
+    for guess in ("previous", "learned"):
+        tr = BatchedTransport(m, coef, D, K, dt, rtol=1e-8, inner_fp32=True)
+        if guess == "learned":
+            mlp.attach_trained_predictor(tr, m, coef, u_eval, D, K, dt, train_steps=10,
+                                         epochs=300)
+        tr.set_state(u_eval)
+        its = []
+        for _ in range(8):
+            r = tr.step()
+            assert r["converged"], r
+            its.append(r["iterations"])
+        runs[guess] = (its, tr.state())
+    prev, learned = runs["previous"], runs["learned"]
+    assert sum(learned[0][1:]) < sum(prev[0][1:]), (prev[0], learned[0])
+    # the guess only changes the iteration count: both solves meet the same tolerance
+    assert np.linalg.norm(learned[1] - prev[1]) / np.linalg.norm(prev[1]) < 1e-7
