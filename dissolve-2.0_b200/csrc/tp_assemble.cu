@@ -8,6 +8,8 @@
 // and -- because the walk follows cell order and every product/sum is rounded
 // separately (__dmul_rn/__dadd_rn, no FMA contraction) in the reference's operation
 // order -- equal to the reference kernel executed in cell order.
+#include <mutex>
+
 #include "tp_common.cuh"
 
 namespace tp {
@@ -609,6 +611,57 @@ extern "C" int tp_scaffold_volume(const tp_mesh* m, const double* phi, double ep
   cudaStream_t st = as_stream(stream);
   const int grid = grid_for(m->n_cells, 256, 1024);
   double* part = static_cast<double*>(scratch);
+  const double qa = (5.0 + 3.0 * sqrt(5.0)) / 20.0, qb = (5.0 - sqrt(5.0)) / 20.0;
+  k_scaffold_volume<<<grid, 256, 0, st>>>(m->n_cells, reinterpret_cast<const int4*>(m->cells),
+                                          m->geo, phi, eps, qa, qb, part);
+  TP_LAUNCH_CHECK();
+  k_sum_parts<<<1, 256, 0, st>>>(grid, part, out_dev);
+  TP_LAUNCH_CHECK();
+  return TP_OK;
+}
+
+// ----------------------------------------------------------------- scaffold volume, fixed scratch
+// tp_scaffold_volume_static keeps its block partials in this module-resident array instead
+// of a caller buffer.  The launch uses at most kSvMaxParts blocks (the same cap as
+// tp_scaffold_volume), so every mesh size fits; nothing in the array has to start at zero
+// because every partial is written before the second kernel reads it.  One array per
+// device, shared by all callers: calls that overlap on one device (two streams, two host
+// threads) race on it.
+static constexpr int kSvMaxParts = 1024;  // 8 KiB of doubles
+static constexpr int kSvMaxDevices = 64;
+static __device__ __align__(256) double g_sv_parts[kSvMaxParts];
+static std::mutex g_sv_mu;
+static double* g_sv_ptr[kSvMaxDevices] = {};
+
+// device address of g_sv_parts on the current device, looked up on the first call there
+static int sv_parts_on_current_device(double** out) {
+  int dev = -1;
+  TP_CUDA_TRY(cudaGetDevice(&dev));
+  TP_REQUIRE(dev >= 0 && dev < kSvMaxDevices,
+             "tp_scaffold_volume_static: device ordinal %d beyond the %d supported", dev,
+             kSvMaxDevices);
+  std::lock_guard<std::mutex> lock(g_sv_mu);
+  if (g_sv_ptr[dev] == nullptr) {
+    void* p = nullptr;
+    TP_CUDA_TRY(cudaGetSymbolAddress(&p, g_sv_parts));
+    g_sv_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_sv_ptr[dev];
+  return TP_OK;
+}
+
+extern "C" int tp_scaffold_volume_static(const tp_mesh* m, const double* phi, double eps,
+                                         double* out_dev, void* stream) {
+  TP_REQUIRE(mesh_ok(m) && phi && out_dev, "null pointer");
+  TP_REQUIRE(eps > 0.0, "epsilon must be positive");
+  const int grid = grid_for(m->n_cells, 256, kSvMaxParts);
+  TP_REQUIRE(grid <= kSvMaxParts,
+             "tp_scaffold_volume_static: %d block partials exceed the fixed scratch of %d",
+             grid, kSvMaxParts);
+  double* part = nullptr;
+  const int rc = sv_parts_on_current_device(&part);
+  if (rc != TP_OK) return rc;
+  cudaStream_t st = as_stream(stream);
   const double qa = (5.0 + 3.0 * sqrt(5.0)) / 20.0, qb = (5.0 - sqrt(5.0)) / 20.0;
   k_scaffold_volume<<<grid, 256, 0, st>>>(m->n_cells, reinterpret_cast<const int4*>(m->cells),
                                           m->geo, phi, eps, qa, qb, part);

@@ -106,6 +106,7 @@ SIGNATURES = {
                                        ctypes.c_int, _c_i64, _vp, _P(_c_dbl), _vp, _vp]),
     "tp_nodal_gradient": (ctypes.c_int, [_P(TpMesh), _vp, _vp, _vp, _vp]),
     "tp_scaffold_volume": (ctypes.c_int, [_P(TpMesh), _vp, _c_dbl, _vp, _vp, _vp]),
+    "tp_scaffold_volume_static": (ctypes.c_int, [_P(TpMesh), _vp, _c_dbl, _vp, _vp]),
     "tp_o2_alpha": (ctypes.c_int, [_c_i64, _vp, _vp, _c_dbl, _c_dbl, _vp, _vp]),
     "tp_oh_source": (ctypes.c_int, [_c_i64, _vp, _vp, _vp, _vp, _vp, _c_dbl, _c_dbl, _c_dbl,
                                     _c_dbl, _vp, _vp]),

@@ -166,6 +166,22 @@ TP_API int tp_nodal_gradient(const tp_mesh* m, const double* JinvT, const double
 TP_API int tp_scaffold_volume(const tp_mesh* m, const double* phi, double eps, double* out_dev,
                        void* scratch, void* stream);
 
+/* tp_scaffold_volume without the scratch argument: it allocates no device memory and needs
+ * no buffer from the caller (no counterpart in the reference, whose volume integral runs
+ * through CuPy's allocator).  For callers that cannot hand over a device temporary: hosts
+ * that bind plain pointers and own no device allocator (a cgo/JNI/FFI embedding that only
+ * passes the mesh and phi it already holds), and per-step loops that must not call
+ * cudaMalloc/cudaFree, which synchronise the device.
+ * Scratch: a fixed 8 KiB array compiled into this library, one per device, holding the at
+ * most 1024 block partials; any mesh size fits, and a launch that would need more partials
+ * is rejected with TP_ERR_ARG.  Nothing in it has to start at zero.  The first call on each
+ * device looks up the array's address (cudaGetSymbolAddress) with that device current and
+ * keeps it; a caller that records calls into a stream capture makes one call on that device
+ * before the capture begins.  Calls that overlap on one device (two streams, or two host
+ * threads) share the array and race: serialise them.  Result as tp_scaffold_volume. */
+TP_API int tp_scaffold_volume_static(const tp_mesh* m, const double* phi, double eps,
+                              double* out_dev, void* stream);
+
 /* dissolve.py:866-875: alpha_O2 = delta_eps(phi) |grad phi| k_orr (per vertex) */
 TP_API int tp_o2_alpha(int64_t n, const double* phi, const double* normgradphi, double eps,
                 double k_orr, double* alpha, void* stream);
