@@ -2,31 +2,48 @@
 //
 // The problem sizes of the transport step (a few 100k rows, operator and vectors
 // resident in the 126 MB L2) make a Krylov iteration latency-bound: what costs is the
-// number of dependent launches and reduction tails, not bytes.  This engine runs the
-// whole solve in ONE cooperative kernel with one CTA group per SM:
+// number of dependent launches, dependent memory round trips and reduction tails, not
+// bytes.  This engine runs the whole solve in ONE cooperative kernel with one CTA group
+// per SM:
 //
 //   init  I1 Jacobi diagonal, Dirichlet values into x      | barrier
 //         I2 r = b - A64 x, z = D^-1 r, p = z, norms        | barrier -> lane state
-//   loop  A  q = A p (SELL-32), p.q                         | barrier -> alpha
+//   loop  A  p = z + beta p (recomputed at every gathered neighbour), q = A p, p.q
+//                                                            | barrier -> alpha
 //         B  xi += alpha p, r -= alpha q, z = D^-1 r, r.z, r.r | barrier -> beta, trigger
 //         RU (FP32 inner only, when triggered) x += xi        | barrier
 //            r = b - A64 x in FP64, replace r, z             | barrier -> converge / keep
-//         C  p = z + beta p                                 | barrier
 //   final x += xi | barrier | r = b - A64 x -> true residual norms
 //
-// Every CTA owns a contiguous range of 32-row slices.  Each dot product is one FP64
-// partial per CTA; after the barrier every CTA sums all partials in the same fixed order,
-// so all CTAs hold bit-identical scalars and take the same branches (deterministic for a
-// given grid).  The grid barrier is a counter plus a generation word; its spin is bounded
-// (about two seconds), after which the CTA raises an abort flag that every other spin
-// also watches, so a lost CTA ends the kernel with TP_ERR_TIMEOUT instead of a hang.
+// Layout.  z and p of a row sit side by side in one record [z_0..z_{LD-1} | p_0..p_{LD-1}]
+// (32 bytes for 4 FP32 columns: one sector per gathered neighbour), double-buffered: phase
+// A of iteration k reads record k and writes p into record k+1, phase B writes z into
+// record k+1.  Every CTA owns a contiguous range of 32-row slices (its slice offsets are
+// staged in shared memory at launch).
 //
-// The inner operator is SELL-32: per slice, entry k of its 32 rows is stored
-// contiguously (col, value), so each load of an index or value is one 128-byte warp
-// access; rows shorter than the slice width are padded with their own column and 0.
+// Phase A walks a warp's (slice, group-of-U-entries) sequence as one flat loop and loads
+// the SELL stream (column, value) of the NEXT group before gathering the records of the
+// current one, so the dependent chain per group is one gather, not a stream load followed
+// by a gather.  Phase B handles two rows per thread per step so their loads overlap.
+//
+// Reductions.  Each dot product is one FP64 partial per CTA; after the barrier every CTA
+// sums all partials in the same fixed order, so all CTAs hold bit-identical scalars and
+// take the same branches (deterministic for a given grid).
+//
+// Barrier.  A monotonic arrival counter: each CTA adds 1 (release) and waits until the
+// counter reaches (barriers so far) x gridDim.  The wait is bounded in time (2 s of
+// %globaltimer); a CTA that gives up raises an abort flag that every other wait also
+// watches, so a lost CTA ends the kernel with TP_ERR_TIMEOUT instead of a hang.
+//
+// Reliable updates (FP32 inner solve).  When any lane's recurrence residual has dropped
+// by delta since its last refresh (or reached the tolerance), every active lane is
+// refreshed in the same pass: the FP64 residual costs one operator sweep whatever the
+// number of lanes, and refreshing together keeps the number of sweeps at that of the
+// fastest-converging lane.
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <cstring>
 #include <vector>
 
 #include "tp_ops.cuh"
@@ -34,10 +51,9 @@
 namespace tp {
 
 struct PBar {
-  unsigned int count;
-  unsigned int gen;
+  unsigned int count;  // arrivals since the launch (reset by tp_pcg_run)
   unsigned int abort;
-  unsigned int pad;
+  unsigned int pad[2];
 };
 
 struct POut {
@@ -64,14 +80,15 @@ struct PArgs {
   const double* b;
   double* x;
   const double* rtol;
-  VT *p, *q, *r, *z, *xi, *dinv, *p2;  // p / p2: ping-pong search directions
+  VT *rec0, *rec1;  // [z | p] records, double-buffered
+  VT *q, *r, *xi, *dinv;
   double* part;  // gridDim.x * 16
   PBar* bar;
   POut* out;
   unsigned long long* prof;  // optional: gridDim.x * 8 phase times (ns)
 };
 
-constexpr unsigned long long SPIN_LIMIT = 1ull << 25;  // x ~64 ns sleeps: ~2 s
+constexpr unsigned long long WAIT_LIMIT_NS = 2000000000ull;  // one barrier wait: 2 s
 
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
   unsigned int v;
@@ -79,7 +96,11 @@ __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
   return v;
 }
 
-// Read-only matrix stream: no L1 allocation, so the L1 keeps the gathered vectors.
+__device__ __forceinline__ void red_release_add(unsigned int* p, unsigned int v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Read-only matrix stream: no L1 allocation, so the L1 keeps the gathered records.
 __device__ __forceinline__ int ld_na(const int32_t* p) {
   int v;
   asm("ld.global.nc.L1::no_allocate.s32 %0, [%1];" : "=r"(v) : "l"(p));
@@ -119,36 +140,37 @@ struct PhaseClock {
   }
 };
 
-// Grid barrier; returns false in every thread when the grid has aborted.
-__device__ __forceinline__ bool grid_sync(PBar* bar, unsigned int& gen) {
+// Grid barrier; returns false in every thread of the CTA when the grid has aborted.
+// `target` (thread 0 only) counts the arrivals this CTA has waited for so far.
+__device__ __forceinline__ bool grid_sync(PBar* bar, unsigned int& target) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
+    target += gridDim.x;
     __threadfence();
-    const unsigned int arrived = atomicAdd(&bar->count, 1u);
-    if (arrived == gridDim.x - 1) {
-      bar->count = 0u;
-      __threadfence();
-      atomicExch(&bar->gen, gen + 1u);
-    } else {
-      unsigned long long spins = 0;
-      while (ld_acquire(&bar->gen) == gen) {
+    red_release_add(&bar->count, 1u);
+    unsigned int spins = 0;
+    unsigned long long t0 = 0;
+    while ((int)(ld_acquire(&bar->count) - target) < 0) {
+      if ((++spins & 31u) == 0u) {
         if (ld_acquire(&bar->abort)) {
           ok = 0;
           break;
         }
-        if (++spins > SPIN_LIMIT) {
+        const unsigned long long t = gtime();
+        if (t0 == 0) {
+          t0 = t;
+        } else if (t - t0 > WAIT_LIMIT_NS) {
           atomicExch(&bar->abort, 1u);
           ok = 0;
           break;
         }
-        __nanosleep(64);
       }
+      __nanosleep(32);
     }
     __threadfence();
-    gen += 1u;
-    s_ok = ok && !ld_acquire(&bar->abort);
+    s_ok = ok;
   }
   __syncthreads();
   return s_ok != 0;
@@ -196,6 +218,43 @@ struct LaneState {
   int active[4], trigger[4], status[4], iters[4];
 };
 
+// z and p of row j from a [z | p] record buffer (plain loads: written by this kernel)
+template <typename VT, int LD>
+__device__ __forceinline__ void ld_rec(const VT* rec, int64_t j, VT z[LD], VT p[LD]) {
+  constexpr int NB = 2 * LD * (int)sizeof(VT);
+  VT t[2 * LD];
+  const VT* src = rec + j * 2 * LD;
+  if constexpr (NB == 8) {
+    const uint2 u = *reinterpret_cast<const uint2*>(src);
+    memcpy(t, &u, 8);
+  } else {
+    uint4 u[NB / 16];
+#pragma unroll
+    for (int i = 0; i < NB / 16; i++) u[i] = reinterpret_cast<const uint4*>(src)[i];
+    memcpy(t, u, NB);
+  }
+#pragma unroll
+  for (int s = 0; s < LD; s++) {
+    z[s] = t[s];
+    p[s] = t[LD + s];
+  }
+}
+
+// SELL stream of entries k .. k+U-1 of a slice (base, width w) for this lane; entries past
+// the width read the slice's last column with value 0.
+template <typename VT, int U, bool HASM>
+__device__ __forceinline__ void stage_group(const PArgs<VT>& a, int base, int w, int k, int lane,
+                                            int cc[U], VT vv[U], VT mm[]) {
+#pragma unroll
+  for (int u = 0; u < U; u++) {
+    const bool in = k + u < w;
+    const int pos = base + (in ? k + u : w - 1) * 32 + lane;
+    cc[u] = (w > 0) ? ld_na(a.sell_col + pos) : 0;
+    vv[u] = in ? ld_na(a.sK + pos) : VT(0);
+    if constexpr (HASM) mm[u] = in ? ld_na(a.sM + pos) : VT(0);
+  }
+}
+
 template <typename VT, int LD>
 __device__ __forceinline__ void csr64_residual(const PArgs<VT>& a, int64_t row, double r64[LD]) {
   double ax[LD];
@@ -238,20 +297,23 @@ __device__ __forceinline__ void csr64_residual(const PArgs<VT>& a, int64_t row, 
   for (int s = 0; s < LD; s++) r64[s] = (s < a.S) ? bv[s] - ax[s] : 0.0;
 }
 
-template <typename VT, int LD, int UNROLL, int MINB>
+template <typename VT, int LD, int U, int MINB, bool HASM>
 __global__ void __launch_bounds__(512, MINB) k_pcg(PArgs<VT> a) {
+  extern __shared__ int32_t s_sp[];  // slice offsets of this CTA's range, se - sb + 1
   __shared__ double sh[32 * 12];
   __shared__ double s_buf[512];
   __shared__ double s_tot[16];
   __shared__ LaneState L;
-  unsigned int gen = 0;
-  if (threadIdx.x == 0) gen = ld_acquire(&a.bar->gen);
+  __shared__ int s_anytrig;
+  unsigned int target = 0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int sb = (int)((int64_t)blockIdx.x * a.ns / gridDim.x);
   const int se = (int)((int64_t)(blockIdx.x + 1) * a.ns / gridDim.x);
   const int S = a.S;
   PhaseClock clk;
   clk.start(a.prof != nullptr);
+  // read only after the first barrier (whose __syncthreads orders these stores)
+  for (int i = threadIdx.x; i <= se - sb; i += blockDim.x) s_sp[i] = a.slice_ptr[sb + i];
 
 #define FOR_OWN_ROWS                                              \
   for (int sl = sb + warp; sl < se; sl += nwarps)                 \
@@ -289,9 +351,9 @@ __global__ void __launch_bounds__(512, MINB) k_pcg(PArgs<VT> a) {
     }
     stv<VT, LD>(a.dinv, row, dv);
   }
-  bool ok = grid_sync(a.bar, gen);
+  bool ok = grid_sync(a.bar, target);
 
-  // ---- I2: r = b - A x, z = D^-1 r, p = z, xi = 0; rr, rz, bb
+  // ---- I2: r = b - A x, z = D^-1 r, record 0 = [z | z], xi = 0; rr, rz, bb
   {
     double acc[12];
 #pragma unroll
@@ -314,14 +376,14 @@ __global__ void __launch_bounds__(512, MINB) k_pcg(PArgs<VT> a) {
           acc[8 + s] += (s < S) ? bv[s] * bv[s] : 0.0;
         }
         stv<VT, LD>(a.r, row, rv);
-        stv<VT, LD>(a.z, row, zv);
-        stv<VT, LD>(a.p, row, zv);
+        stv<VT, LD>(a.rec0, 2 * row, zv);
+        stv<VT, LD>(a.rec0, 2 * row + 1, zv);
         stv<VT, LD>(a.xi, row, zero);
       }
     }
     block_partial<12>(acc, a.part, sh);
   }
-  ok = ok && grid_sync(a.bar, gen);
+  ok = ok && grid_sync(a.bar, target);
   if (ok) grid_totals<12>(a.part, s_tot, s_buf);
   if (threadIdx.x == 0) {
     for (int s = 0; s < 4; s++) {
@@ -354,10 +416,10 @@ __global__ void __launch_bounds__(512, MINB) k_pcg(PArgs<VT> a) {
 #pragma unroll
     for (int s = 0; s < 4; s++) nact += L.active[s];
     if (!nact) break;
-    // ---- A: p_new = z + beta p_old (own rows; recomputed for every gathered neighbour),
-    //         q = A p_new, p_new.q
-    VT* __restrict__ p_old = par ? a.p2 : a.p;
-    VT* __restrict__ p_new = par ? a.p : a.p2;
+    const VT* __restrict__ rec_o = par ? a.rec1 : a.rec0;
+    VT* rec_n = par ? a.rec0 : a.rec1;
+    // ---- A: p = z + beta p_old for own rows and, on the fly, for every gathered
+    //         neighbour; q = A p; p.q
     {
       VT be[LD];
       bool act[LD];
@@ -367,58 +429,85 @@ __global__ void __launch_bounds__(512, MINB) k_pcg(PArgs<VT> a) {
         be[s] = act[s] ? (VT)L.beta[s] : VT(0);
       }
       double acc[4] = {0.0, 0.0, 0.0, 0.0};
-      FOR_OWN_ROWS {
-        const int base = a.slice_ptr[sl], w = (a.slice_ptr[sl + 1] - base) >> 5;
+      int sl = sb + warp;
+      if (sl < se) {
+        int base = s_sp[sl - sb], w = (s_sp[sl - sb + 1] - base) >> 5, k = 0;
+        int cc[U];
+        VT vv[U], mm[HASM ? U : 1];
+        stage_group<VT, U, HASM>(a, base, w, 0, lane, cc, vv, mm);
         VT ak[LD], am[LD];
 #pragma unroll
         for (int s = 0; s < LD; s++) ak[s] = am[s] = VT(0);
-        for (int k = 0; k < w; k += UNROLL) {
-          int cc[UNROLL];
-          VT vv[UNROLL];
-#pragma unroll
-          for (int u = 0; u < UNROLL; u++) {
-            const int pos = base + min(k + u, w - 1) * 32 + lane;
-            cc[u] = ld_na(a.sell_col + pos);
-            vv[u] = (k + u < w) ? ld_na(a.sK + pos) : VT(0);
+        while (true) {
+          const bool last = k + U >= w;  // last group of this slice
+          const int nsl = last ? sl + nwarps : sl;
+          const int nk = last ? 0 : k + U;
+          const bool more = nsl < se;
+          int nbase = base, nw = w;
+          if (last && more) {
+            nbase = s_sp[nsl - sb];
+            nw = (s_sp[nsl - sb + 1] - nbase) >> 5;
           }
+          int cn[U];
+          VT vn[U], mn[HASM ? U : 1];
+          if (more) stage_group<VT, U, HASM>(a, nbase, nw, nk, lane, cn, vn, mn);
+          const int64_t row = (int64_t)sl * 32 + lane;
+          const bool own = last && row < a.n;
+          VT zr[LD], por[LD], dr[LD];
 #pragma unroll
-          for (int u = 0; u < UNROLL; u++) {
-            VT zv[LD], pv[LD];
-            ldv_cg<VT, LD>(a.z, cc[u], zv);
-            ldv_cg<VT, LD>(p_old, cc[u], pv);
-            VT mv = VT(0);
-            if (a.sM && k + u < w) mv = ld_na(a.sM + base + (k + u) * 32 + lane);
+          for (int s = 0; s < LD; s++) zr[s] = por[s] = dr[s] = VT(0);
+          bool bcr = false;
+          if (own) {
+            ld_rec<VT, LD>(rec_o, row, zr, por);
+            if (a.diag) ldv<VT, LD>(a.diag, row, dr);
+            bcr = a.bc && a.bc[row];
+          }
+          VT zg[U][LD], pg[U][LD];
+#pragma unroll
+          for (int u = 0; u < U; u++) ld_rec<VT, LD>(rec_o, cc[u], zg[u], pg[u]);
+#pragma unroll
+          for (int u = 0; u < U; u++) {
 #pragma unroll
             for (int s = 0; s < LD; s++) {
-              const VT pj = act[s] ? zv[s] + be[s] * pv[s] : pv[s];
+              const VT pj = act[s] ? zg[u][s] + be[s] * pg[u][s] : pg[u][s];
               ak[s] += vv[u] * pj;
-              am[s] += mv * pj;
+              if constexpr (HASM) am[s] += mm[u] * pj;
             }
           }
-        }
-        VT zr[LD], por[LD], pr[LD], dr[LD], qv[LD];
-        ldv_cg<VT, LD>(a.z, row, zr);
-        ldv_cg<VT, LD>(p_old, row, por);
+          if (last) {
+            if (own) {
+              VT pr[LD], qv[LD];
 #pragma unroll
-        for (int s = 0; s < LD; s++) {
-          pr[s] = act[s] ? zr[s] + be[s] * por[s] : por[s];
-          dr[s] = VT(0);
-        }
-        stv<VT, LD>(p_new, row, pr);
-        if (a.diag) ldv<VT, LD>(a.diag, row, dr);
-        const bool bcr = a.bc && a.bc[row];
+              for (int s = 0; s < LD; s++) pr[s] = act[s] ? zr[s] + be[s] * por[s] : por[s];
+              stv<VT, LD>(rec_n, 2 * row + 1, pr);
 #pragma unroll
-        for (int s = 0; s < LD; s++) {
-          VT v = VT(a.dscale[s]) * ak[s] + VT(a.cscale[s]) * am[s] + dr[s] * pr[s];
-          qv[s] = bcr ? pr[s] : v;
-          acc[s] += (double)pr[s] * (double)qv[s];
+              for (int s = 0; s < LD; s++) {
+                const VT v = VT(a.dscale[s]) * ak[s] + VT(a.cscale[s]) * am[s] + dr[s] * pr[s];
+                qv[s] = bcr ? pr[s] : v;
+                acc[s] += (double)pr[s] * (double)qv[s];
+              }
+              stv<VT, LD>(a.q, row, qv);
+            }
+#pragma unroll
+            for (int s = 0; s < LD; s++) ak[s] = am[s] = VT(0);
+          }
+          if (!more) break;
+          sl = nsl;
+          k = nk;
+          base = nbase;
+          w = nw;
+#pragma unroll
+          for (int u = 0; u < U; u++) {
+            cc[u] = cn[u];
+            vv[u] = vn[u];
+            if constexpr (HASM) mm[u] = mn[u];
+          }
         }
-        stv<VT, LD>(a.q, row, qv);
       }
       block_partial<4>(acc, a.part, sh);
     }
     clk.lap(0);
-    ok = grid_sync(a.bar, gen);
+    ok = grid_sync(a.bar, target);
     clk.lap(1);
     if (!ok) break;
     grid_totals<4>(a.part, s_tot, s_buf);
@@ -448,33 +537,47 @@ __global__ void __launch_bounds__(512, MINB) k_pcg(PArgs<VT> a) {
       VT al[LD];
 #pragma unroll
       for (int s = 0; s < LD; s++) al[s] = (s < S) ? (VT)L.alpha[s] : VT(0);
-      FOR_OWN_ROWS {
-        VT pv[LD], qv[LD], rv[LD], xv[LD], dv[LD], zv[LD];
-        ldv_cg<VT, LD>(p_new, row, pv);
-        ldv_cg<VT, LD>(a.q, row, qv);
-        ldv_cg<VT, LD>(a.r, row, rv);
-        ldv_cg<VT, LD>(a.xi, row, xv);
-        ldv_cg<VT, LD>(a.dinv, row, dv);
+      constexpr int RS = (LD * sizeof(VT) <= 8) ? 2 : 1;  // rows per step (registers)
+      for (int sl = sb + warp; sl < se; sl += RS * nwarps) {
+        const int sl1 = (RS == 2) ? sl + nwarps : se;
+        const int64_t rw[2] = {(int64_t)sl * 32 + lane, (int64_t)sl1 * 32 + lane};
+        const bool vr[2] = {rw[0] < a.n, sl1 < se && rw[1] < a.n};
+        VT pv[2][LD], qv[2][LD], rv[2][LD], xv[2][LD], dv[2][LD];
 #pragma unroll
-        for (int s = 0; s < LD; s++) {
-          xv[s] += al[s] * pv[s];
-          rv[s] -= al[s] * qv[s];
-          zv[s] = dv[s] * rv[s];
-          acc[s] += (double)rv[s] * (double)zv[s];
-          acc[4 + s] += (double)rv[s] * (double)rv[s];
+        for (int h = 0; h < 2; h++) {
+          if (vr[h]) {
+            ldv_cg<VT, LD>(rec_n, 2 * rw[h] + 1, pv[h]);
+            ldv_cg<VT, LD>(a.q, rw[h], qv[h]);
+            ldv_cg<VT, LD>(a.r, rw[h], rv[h]);
+            ldv_cg<VT, LD>(a.xi, rw[h], xv[h]);
+            ldv_cg<VT, LD>(a.dinv, rw[h], dv[h]);
+          }
         }
-        stv<VT, LD>(a.xi, row, xv);
-        stv<VT, LD>(a.r, row, rv);
-        stv<VT, LD>(a.z, row, zv);
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          if (vr[h]) {
+            VT zv[LD];
+#pragma unroll
+            for (int s = 0; s < LD; s++) {
+              xv[h][s] += al[s] * pv[h][s];
+              rv[h][s] -= al[s] * qv[h][s];
+              zv[s] = dv[h][s] * rv[h][s];
+              acc[s] += (double)rv[h][s] * (double)zv[s];
+              acc[4 + s] += (double)rv[h][s] * (double)rv[h][s];
+            }
+            stv<VT, LD>(a.xi, rw[h], xv[h]);
+            stv<VT, LD>(a.r, rw[h], rv[h]);
+            stv<VT, LD>(rec_n, 2 * rw[h], zv);
+          }
+        }
       }
       block_partial<8>(acc, a.part, sh);
     }
     clk.lap(2);
-    ok = grid_sync(a.bar, gen);
+    ok = grid_sync(a.bar, target);
     clk.lap(3);
     if (!ok) break;
     grid_totals<8>(a.part, s_tot, s_buf);
-    __shared__ int s_anytrig;
     if (threadIdx.x == 0) {
       int any = 0;
       for (int s = 0; s < S; s++) {
@@ -495,9 +598,11 @@ __global__ void __launch_bounds__(512, MINB) k_pcg(PArgs<VT> a) {
         L.rz[s] = rz;
         L.rr[s] = rr;
         const bool trig = (rr <= L.tol2[s]) || (a.delta2 > 0.0 && rr < a.delta2 * L.rmax2[s]);
-        L.trigger[s] = trig;
         any |= trig;
       }
+      // one FP64 sweep refreshes every active lane
+      if (any)
+        for (int s = 0; s < S; s++) L.trigger[s] = L.active[s];
       s_anytrig = any;
     }
     __syncthreads();
@@ -520,9 +625,9 @@ __global__ void __launch_bounds__(512, MINB) k_pcg(PArgs<VT> a) {
         }
         stv<VT, LD>(a.xi, row, xv);
       }
-      ok = grid_sync(a.bar, gen);
+      ok = grid_sync(a.bar, target);
       if (!ok) break;
-      // ---- RU2: FP64 residual on trigger lanes, replace r and z
+      // ---- RU2: FP64 residual on trigger lanes, replace r and z (z of the next record)
       double acc[8];
 #pragma unroll
       for (int k = 0; k < 8; k++) acc[k] = 0.0;
@@ -532,7 +637,7 @@ __global__ void __launch_bounds__(512, MINB) k_pcg(PArgs<VT> a) {
         VT rv[LD], dv[LD], zv[LD];
         ldv_cg<VT, LD>(a.r, row, rv);
         ldv_cg<VT, LD>(a.dinv, row, dv);
-        ldv_cg<VT, LD>(a.z, row, zv);
+        ldv_cg<VT, LD>(rec_n, 2 * row, zv);
 #pragma unroll
         for (int s = 0; s < LD; s++) {
           if (tr[s]) {
@@ -543,10 +648,10 @@ __global__ void __launch_bounds__(512, MINB) k_pcg(PArgs<VT> a) {
           }
         }
         stv<VT, LD>(a.r, row, rv);
-        stv<VT, LD>(a.z, row, zv);
+        stv<VT, LD>(rec_n, 2 * row, zv);
       }
       block_partial<8>(acc, a.part, sh);
-      ok = grid_sync(a.bar, gen);
+      ok = grid_sync(a.bar, target);
       if (!ok) break;
       grid_totals<8>(a.part, s_tot, s_buf);
       if (threadIdx.x == 0) {
@@ -588,7 +693,7 @@ __global__ void __launch_bounds__(512, MINB) k_pcg(PArgs<VT> a) {
     }
     stv<VT, LD>(a.xi, row, xv);
   }
-  bool ok2 = ok && grid_sync(a.bar, gen);
+  bool ok2 = ok && grid_sync(a.bar, target);
   {
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     if (ok2) {
@@ -601,7 +706,7 @@ __global__ void __launch_bounds__(512, MINB) k_pcg(PArgs<VT> a) {
     }
     block_partial<4>(acc, a.part, sh);
   }
-  ok2 = ok2 && grid_sync(a.bar, gen);
+  ok2 = ok2 && grid_sync(a.bar, target);
   if (ok2) grid_totals<4>(a.part, s_tot, s_buf);
   if (clk.on) {
     clk.lap(6);
@@ -609,6 +714,8 @@ __global__ void __launch_bounds__(512, MINB) k_pcg(PArgs<VT> a) {
     for (int k = 0; k < 8; k++) a.prof[blockIdx.x * 8 + k] = clk.acc[k];
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
+    // a CTA that gave up at the last barrier leaves only the flag behind
+    if (ld_acquire(&a.bar->abort)) ok2 = false;
     int status = TP_OK;
     for (int s = 0; s < 4; s++) {
       if (s < S) {
@@ -732,6 +839,7 @@ extern "C" int tp_sell_scatter(int64_t nnz, const int32_t* csr2sell, const doubl
 // ----------------------------------------------------------------- persistent handle
 struct tp_pcg_handle {
   int fp32, ld, grid, block;
+  size_t dyn_smem;  // slice offsets staged per CTA
   void* fn;
   tp::PArgs<float> af;
   tp::PArgs<double> ad;
@@ -740,22 +848,31 @@ struct tp_pcg_handle {
 };
 
 namespace tp {
+// SELL entries per pipelined group: the current and next group's stream entries and the
+// current group's gathered records stay in registers (about 48 per thread: 2 to 8
+// entries).  Two CTAs per SM
+// (64 registers) only for records of at most 16 bytes.
 template <typename VT, int LD>
-static void* pick_kernel(int minb) {
-  if (minb >= 2) return (void*)k_pcg<VT, LD, (LD == 4 ? 4 : 8), 2>;
-  return (void*)k_pcg<VT, LD, (LD == 4 ? 4 : 8), 1>;
+static void* pick_kernel(int minb, bool hasM) {
+  constexpr int RB = 2 * LD * (int)sizeof(VT);
+  constexpr int cost = 2 * (1 + (int)sizeof(VT) / 4) + RB / 4;  // registers per entry
+  constexpr int U = std::max(2, std::min(8, 48 / cost));
+  if constexpr (RB <= 16) {
+    if (minb >= 2) return hasM ? (void*)k_pcg<VT, LD, U, 2, true> : (void*)k_pcg<VT, LD, U, 2, false>;
+  }
+  return hasM ? (void*)k_pcg<VT, LD, U, 1, true> : (void*)k_pcg<VT, LD, U, 1, false>;
 }
 
 // CTAs per SM: 1 (up to 128 registers per thread) or 2 (64 registers)
-static void* pcg_kernel(int fp32, int ld, int minb) {
+static void* pcg_kernel(int fp32, int ld, int minb, bool hasM) {
   if (fp32) {
-    if (ld == 1) return pick_kernel<float, 1>(minb);
-    if (ld == 2) return pick_kernel<float, 2>(minb);
-    if (ld == 4) return pick_kernel<float, 4>(minb);
+    if (ld == 1) return pick_kernel<float, 1>(minb, hasM);
+    if (ld == 2) return pick_kernel<float, 2>(minb, hasM);
+    if (ld == 4) return pick_kernel<float, 4>(minb, hasM);
   } else {
-    if (ld == 1) return pick_kernel<double, 1>(minb);
-    if (ld == 2) return pick_kernel<double, 2>(minb);
-    if (ld == 4) return pick_kernel<double, 4>(minb);
+    if (ld == 1) return pick_kernel<double, 1>(minb, hasM);
+    if (ld == 2) return pick_kernel<double, 2>(minb, hasM);
+    if (ld == 4) return pick_kernel<double, 4>(minb, hasM);
   }
   return nullptr;
 }
@@ -797,11 +914,15 @@ static void fill_pargs(PArgs<VT>& a, const tp_csr_op* op, const tp_sell* sl, con
   a.x = x;
   a.rtol = rtol;
   char* p = ws;
-  VT** v[7] = {&a.p, &a.q, &a.r, &a.z, &a.xi, &a.dinv, &a.p2};
-  for (int i = 0; i < 7; i++) {
+  VT** v[4] = {&a.q, &a.r, &a.xi, &a.dinv};
+  for (int i = 0; i < 4; i++) {
     *v[i] = reinterpret_cast<VT*>(p);
     p += vec_bytes;
   }
+  a.rec0 = reinterpret_cast<VT*>(p);
+  p += 2 * vec_bytes;
+  a.rec1 = reinterpret_cast<VT*>(p);
+  p += 2 * vec_bytes;
   a.part = reinterpret_cast<double*>(p);
   p += a256(sizeof(double) * 16 * grid);
   a.bar = reinterpret_cast<PBar*>(p);
@@ -810,33 +931,50 @@ static void fill_pargs(PArgs<VT>& a, const tp_csr_op* op, const tp_sell* sl, con
 }
 }  // namespace tp
 
-static int default_minb(int ld) { return ld == 4 ? 1 : 2; }
+static int default_minb(int) { return 1; }
 
-static int pcg_grid(int fp32, int ld, int minb, int block, int* grid) {
-  void* fn = pcg_kernel(fp32, ld, minb);
-  if (!fn) return TP_ERR_ARG;
-  // most of the unified L1/shared storage to L1 (the gathered vectors live there), but
-  // enough shared memory for `minb` CTAs; set before the occupancy query so the
-  // cooperative grid matches what the launch will see
-  TP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                   minb >= 2 ? 10 : 5));
-  int occ = 0;
-  TP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, block, 0));
-  if (occ < 1) {
-    set_error("persistent CG kernel does not fit on an SM");
-    return TP_ERR_CAPACITY;
+// Grid of `minb` CTAs per SM (fewer if they do not fit) and the dynamic shared memory
+// (slice offsets of one CTA's range) for n_rows rows.
+static int pcg_grid(int fp32, int ld, int minb, bool hasM, int block, int64_t n_rows, int* grid,
+                    size_t* dyn) {
+  const int64_t ns = (n_rows + 31) / 32;
+  for (int m = minb; m >= 1; m--) {
+    void* fn = pcg_kernel(fp32, ld, m, hasM);
+    if (!fn) return TP_ERR_ARG;
+    const int g = sm_count() * m;
+    const size_t d = sizeof(int32_t) * (size_t)((ns + g - 1) / g + 2);
+    if (d > 160 * 1024) {
+      set_error("persistent CG: %lld rows exceed the slice table of one CTA", (long long)n_rows);
+      return TP_ERR_CAPACITY;
+    }
+    cudaFuncAttributes fa;
+    TP_CUDA_TRY(cudaFuncGetAttributes(&fa, fn));
+    if (d > 48 * 1024)
+      TP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d));
+    // the rest of the unified L1/shared storage stays L1 (the gathered records live
+    // there); set before the occupancy query so the cooperative grid matches the launch
+    const size_t per_sm = (fa.sharedSizeBytes + d + 1024) * m;
+    const int pct = (int)std::min<size_t>(100, (per_sm * 100 + 228 * 1024 - 1) / (228 * 1024));
+    TP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     std::max(pct, 1)));
+    int occ = 0;
+    TP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, block, d));
+    if (occ >= m) {
+      *grid = g;
+      *dyn = d;
+      return TP_OK;
+    }
   }
-  *grid = sm_count() * std::min(occ, minb);
-  return TP_OK;
+  set_error("persistent CG kernel does not fit on an SM");
+  return TP_ERR_CAPACITY;
 }
 
 extern "C" size_t tp_pcg_workspace_bytes(const tp_csr_op* op, int inner_fp32) {
   if (!op) return 0;
-  int grid = 0;  // partial rows for the largest grid (2 CTAs per SM)
-  if (pcg_grid(inner_fp32, op->ld, 2, 512, &grid) != TP_OK) return 0;
-  grid = std::max(grid, 2 * sm_count());
+  // partial rows for the largest grid (2 CTAs per SM)
+  const int grid = 2 * sm_count();
   const size_t vt = inner_fp32 ? 4 : 8;
-  return 7 * a256(vt * op->ld * (size_t)op->n_rows) + a256(sizeof(double) * 16 * grid) +
+  return 8 * a256(vt * op->ld * (size_t)op->n_rows) + a256(sizeof(double) * 16 * grid) +
          a256(sizeof(PBar)) + a256(sizeof(POut));
 }
 
@@ -862,15 +1000,16 @@ extern "C" int tp_pcg_create(const tp_csr_op* op, const tp_sell* sell, int max_i
   h->ld = op->ld;
   h->block = 512;
   const int minb = ctas_per_sm > 0 ? std::min(ctas_per_sm, 2) : default_minb(op->ld);
-  int rc = pcg_grid(h->fp32, h->ld, minb, h->block, &h->grid);
+  const bool hasM = inner_fp32 ? sell->sM32 != nullptr : sell->sM64 != nullptr;
+  int rc = pcg_grid(h->fp32, h->ld, minb, hasM, h->block, op->n_rows, &h->grid, &h->dyn_smem);
   if (rc) {
     delete h;
     return rc;
   }
-  h->fn = pcg_kernel(h->fp32, h->ld, minb);
+  h->fn = pcg_kernel(h->fp32, h->ld, h->grid / sm_count(), hasM);
   const size_t vt = inner_fp32 ? 4 : 8;
   const size_t vec = a256(vt * op->ld * (size_t)op->n_rows);
-  const double d = inner_fp32 ? (delta > 0 ? delta : 0.1) : 0.0;
+  const double d = inner_fp32 ? (delta > 0 ? delta : 0.01) : 0.0;
   char* ws = static_cast<char*>(workspace);
   if (h->fp32)
     fill_pargs(h->af, op, sell, b, x, rtol, max_it, d, ws, vec, h->grid);
@@ -898,7 +1037,8 @@ extern "C" int tp_pcg_run(tp_pcg_handle* h, void* stream) {
   TP_CUDA_TRY(cudaMemsetAsync(h->bar, 0, sizeof(PBar), st));
   void* arg = h->fp32 ? (void*)&h->af : (void*)&h->ad;
   void* args[1] = {arg};
-  TP_CUDA_TRY(cudaLaunchCooperativeKernel(h->fn, dim3(h->grid), dim3(h->block), args, 0, st));
+  TP_CUDA_TRY(cudaLaunchCooperativeKernel(h->fn, dim3(h->grid), dim3(h->block), args,
+                                          h->dyn_smem, st));
   return TP_OK;
 }
 

@@ -326,13 +326,16 @@ TP_API int tp_sell_scatter(int64_t nnz, const int32_t* csr2sell, const double* c
 /* ------------------------------------------------------------------ persistent solve */
 /* The Jacobi-PCG of tp_cg_* for ONE system (S <= 4 columns) as a single cooperative
  * kernel: one launch per solve, grid barriers with a bounded wait (TP_ERR_TIMEOUT when a
- * barrier gives up), the inner operator read in SELL-32 order, the FP64 operator (Jacobi
- * diagonal, initial / reliable-update / final residuals) in CSR.  Same stopping rule,
- * reliable updates and lane results as tp_cg_*. */
+ * barrier wait exceeds 2 s), the inner operator read in SELL-32 order, the FP64 operator
+ * (Jacobi diagonal, initial / reliable-update / final residuals) in CSR.  Same stopping
+ * rule and lane results as tp_cg_*.  Reliable updates (FP32 inner): when any lane's
+ * recurrence residual has dropped by `delta` (<= 0 -> 0.01) since its last update, every
+ * active lane is updated in the same FP64 sweep. */
 typedef struct tp_pcg_handle tp_pcg_handle;
 
 TP_API size_t tp_pcg_workspace_bytes(const tp_csr_op* op, int inner_fp32);
-/* ctas_per_sm: 1 or 2 resident 512-thread CTAs per SM (0 = default for the column count) */
+/* ctas_per_sm: 1 or 2 resident 512-thread CTAs per SM (0 = 1; 2 only for rows of at most
+ * 8 bytes per column set, i.e. 1-2 FP32 or 1 FP64 column) */
 TP_API int tp_pcg_create(const tp_csr_op* op, const tp_sell* sell, int max_it, int inner_fp32,
                          double delta, int ctas_per_sm, const double* b, double* x,
                          const double* rtol, void* workspace, size_t workspace_bytes,
