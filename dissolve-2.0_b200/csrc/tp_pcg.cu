@@ -43,6 +43,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -82,6 +83,13 @@ struct PArgs {
   const double* rtol;
   VT *rec0, *rec1;  // [z | p] records, double-buffered
   VT *q, *r, *xi, *dinv;
+  VT *u, *w, *p, *s;  // window engine (Chronopoulos-Gear CG): u = D^-1 r, w = A u
+  // window engine: per-CTA halo lists and window-local SELL columns
+  const int32_t* halo_ptr;  // gridDim.x + 1
+  const int32_t* halo;      // sorted columns outside each CTA's row range
+  const uint16_t* loc_col;  // (n_entries) window-local column of every SELL entry
+  int sp_cap, halo_cap, col_cap;  // shared-memory capacities (entries)
+  int reg_values;                 // every slice at most 16 wide: values via registers
   double* part;  // gridDim.x * 16
   PBar* bar;
   POut* out;
@@ -123,13 +131,19 @@ __device__ __forceinline__ unsigned long long gtime() {
   return t;
 }
 
-// Phase clock of thread 0 (profiling builds of a run only): adds now - last to slot k.
+// Phase clock of thread 0 (profiled runs only): adds now - last to slot k of a shared
+// array (kept out of registers: the solve loop needs them).
 struct PhaseClock {
-  unsigned long long last = 0, acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  unsigned long long last = 0;
+  unsigned long long* acc = nullptr;
   bool on = false;
-  __device__ __forceinline__ void start(bool enable) {
+  __device__ __forceinline__ void start(bool enable, unsigned long long* sacc) {
     on = enable && threadIdx.x == 0;
-    if (on) last = gtime();
+    acc = sacc;
+    if (on) {
+      for (int k = 0; k < 8; k++) acc[k] = 0;
+      last = gtime();
+    }
   }
   __device__ __forceinline__ void lap(int k) {
     if (on) {
@@ -255,6 +269,39 @@ __device__ __forceinline__ void stage_group(const PArgs<VT>& a, int base, int w,
   }
 }
 
+// LD values of entry i of a shared-memory window
+template <typename VT, int LD>
+__device__ __forceinline__ void ld_win(const VT* w, int i, VT v[LD]) {
+  constexpr int NB = LD * (int)sizeof(VT);
+  const VT* src = w + i * LD;
+  if constexpr (NB == 4 || NB == 8) {
+#pragma unroll
+    for (int s = 0; s < LD; s++) v[s] = src[s];
+  } else {
+    VT t[LD];
+    uint4 u[NB / 16];
+#pragma unroll
+    for (int k = 0; k < NB / 16; k++) u[k] = reinterpret_cast<const uint4*>(src)[k];
+    memcpy(t, u, NB);
+#pragma unroll
+    for (int s = 0; s < LD; s++) v[s] = t[s];
+  }
+}
+
+// values only of entries k .. k+U-1 of a slice (the window engine reads its columns from
+// shared memory); entries past the width are 0 and not loaded
+template <typename VT, int U, bool HASM>
+__device__ __forceinline__ void stage_values(const PArgs<VT>& a, int base, int w, int k, int lane,
+                                             VT vv[U], VT mm[]) {
+#pragma unroll
+  for (int u = 0; u < U; u++) {
+    const bool in = k + u < w;
+    const int pos = base + (k + u) * 32 + lane;
+    vv[u] = in ? ld_na(a.sK + pos) : VT(0);
+    if constexpr (HASM) mm[u] = in ? ld_na(a.sM + pos) : VT(0);
+  }
+}
+
 template <typename VT, int LD>
 __device__ __forceinline__ void csr64_residual(const PArgs<VT>& a, int64_t row, double r64[LD]) {
   double ax[LD];
@@ -305,13 +352,14 @@ __global__ void __launch_bounds__(512, MINB) k_pcg(PArgs<VT> a) {
   __shared__ double s_tot[16];
   __shared__ LaneState L;
   __shared__ int s_anytrig;
+  __shared__ unsigned long long s_clk[8];
   unsigned int target = 0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int sb = (int)((int64_t)blockIdx.x * a.ns / gridDim.x);
   const int se = (int)((int64_t)(blockIdx.x + 1) * a.ns / gridDim.x);
   const int S = a.S;
   PhaseClock clk;
-  clk.start(a.prof != nullptr);
+  clk.start(a.prof != nullptr, s_clk);
   // read only after the first barrier (whose __syncthreads orders these stores)
   for (int i = threadIdx.x; i <= se - sb; i += blockDim.x) s_sp[i] = a.slice_ptr[sb + i];
 
@@ -740,6 +788,592 @@ __global__ void __launch_bounds__(512, MINB) k_pcg(PArgs<VT> a) {
 #undef FOR_OWN_ROWS
 }
 
+// ================================================================= window engine
+// Chronopoulos-Gear form of the same Jacobi-PCG: one operator product and one reduction
+// step per iteration, algebraically the same iterates as the standard recurrences:
+//   u = D^-1 r, w = A u, gamma = r.u, delta = w.u,
+//   beta = gamma / gamma_old, alpha = gamma / (delta - beta gamma / alpha_old),
+//   p = u + beta p, s = w + beta s, xi += alpha p, r -= alpha s.
+// The only vector another CTA reads is u.  Every other vector is touched by its owning
+// CTA only, and the operator product runs from shared memory: each CTA copies u of its
+// own rows plus its halo (the columns outside its row range that its rows reference) into
+// a shared-memory window with asynchronous copies, and reads the window through CTA-local
+// 16-bit column indices that stay resident for the whole solve.  The SELL values are
+// staged in registers, MAXS slices per warp at a time (one memory round trip for all).
+//
+//   init  I1 Jacobi diagonal, Dirichlet values, p = s = xi = 0 | barrier
+//         I2 r = b - A64 x, u = D^-1 r, publish u; r.u, r.r, b.b | barrier
+//         W  w = A u; w.u                                    | barrier -> alpha, beta = 0
+//   loop  P  p = u + beta p, s = w + beta s, xi += alpha p, r -= alpha s, u = D^-1 r,
+//            publish u; r.u, r.r                             | barrier
+//         W  w = A u; w.u                                    | barrier -> convergence /
+//                                                              trigger, beta, alpha
+//         RU (when triggered) x += xi | barrier | r = b - A64 x, u = D^-1 r; r.u, r.r |
+//            barrier | W | barrier -> convergence on the FP64 residual, beta, alpha
+//   final x += xi | barrier | r = b - A64 x -> true residual norms
+
+// beta = gamma / gamma_old, alpha = gamma / (delta - beta gamma / alpha_old).  The
+// denominator equals p.Ap; when rounding makes the difference non-positive the direction
+// restarts (beta = 0, alpha = gamma / delta); delta = u.Au itself not positive means the
+// operator is not SPD on the free dofs.
+__device__ __forceinline__ void cg_coefficients(LaneState& L, int s, double gm, double dl,
+                                                int it) {
+  if (!(dl > 0.0)) {
+    L.active[s] = 0;
+    L.status[s] = TP_ERR_BREAKDOWN;
+    L.iters[s] = it;
+    return;
+  }
+  double beta = (L.rz[s] != 0.0) ? gm / L.rz[s] : 0.0;
+  double den = (L.alpha[s] != 0.0) ? dl - beta * gm / L.alpha[s] : dl;
+  if (!(den > 0.0)) {
+    beta = 0.0;
+    den = dl;
+  }
+  L.beta[s] = beta;
+  L.alpha[s] = gm / den;
+  L.rz[s] = gm;
+}
+
+// lane results and status (block 0, thread 0); s_tot holds the final true r.r
+template <typename VT>
+__device__ void write_result(const PArgs<VT>& a, LaneState& L, bool ok2, const double* s_tot,
+                             int it, int n_rel) {
+  // a CTA that gave up at the last barrier leaves only the flag behind
+  if (ld_acquire(&a.bar->abort)) ok2 = false;
+  int status = TP_OK;
+  for (int s = 0; s < 4; s++) {
+    if (s < a.S) {
+      if (ok2) L.rtrue[s] = s_tot[s];
+      if (L.status[s] == -1) {
+        L.status[s] = (ok2 && L.rtrue[s] <= L.tol2[s]) ? TP_OK : TP_ERR_NOT_CONVERGED;
+        L.iters[s] = it;
+      }
+      if (!ok2) L.status[s] = TP_ERR_TIMEOUT;
+      if (L.status[s] != TP_OK && status == TP_OK) status = L.status[s];
+    }
+    a.out->lane_iters[s] = L.iters[s];
+    a.out->lane_status[s] = L.status[s];
+    a.out->lane_rtrue[s] = L.rtrue[s];
+    a.out->lane_bb[s] = L.bb[s];
+  }
+  a.out->iterations = it;
+  a.out->n_reliable = n_rel;
+  a.out->status = status;
+  a.out->timeouts = ok2 ? 0 : 1;
+}
+
+template <int NB>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  if constexpr (NB == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(sa), "l"(gmem), "n"(NB)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+template <typename VT, int LD, int U, bool HASM>
+__global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
+  // dynamic shared memory: slice offsets (sp_cap), halo list (halo_cap), window-local
+  // columns (col_cap), then the window of u (own rows, then halo; LD values each)
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  int32_t* s_sp = reinterpret_cast<int32_t*>(s_dyn);
+  int32_t* s_halo = s_sp + a.sp_cap;
+  uint16_t* s_col = reinterpret_cast<uint16_t*>(s_halo + a.halo_cap);
+  VT* s_win = reinterpret_cast<VT*>(
+      s_dyn + ((4 * (size_t)(a.sp_cap + a.halo_cap) + 2 * (size_t)a.col_cap + 15) & ~(size_t)15));
+  __shared__ double sh[32 * 12];
+  __shared__ double s_buf[512];
+  __shared__ double s_tot[16];
+  __shared__ LaneState L;
+  __shared__ double s_gam[4];
+  __shared__ int s_anytrig;
+  __shared__ unsigned long long s_clk[8];
+  constexpr int WMAX = 16;  // register-staged slices: at most WMAX entries per row
+  constexpr int MAXS = std::max(1, 64 / (WMAX * (int)sizeof(VT) / 4 * (HASM ? 2 : 1)));
+  constexpr int RB = LD * (int)sizeof(VT);  // bytes of one row of u
+  unsigned int target = 0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int sb = (int)((int64_t)blockIdx.x * a.ns / gridDim.x);
+  const int se = (int)((int64_t)(blockIdx.x + 1) * a.ns / gridDim.x);
+  const int S = a.S;
+  const int r0 = sb * 32;
+  const int nown = (se > sb) ? (int)(min((int64_t)se * 32, a.n) - r0) : 0;
+  const int nhalo = a.halo_ptr[blockIdx.x + 1] - a.halo_ptr[blockIdx.x];
+  PhaseClock clk;
+  clk.start(a.prof != nullptr, s_clk);
+  // resident tables; read only after the first barrier (whose __syncthreads orders them)
+  for (int i = threadIdx.x; i <= se - sb; i += blockDim.x) s_sp[i] = a.slice_ptr[sb + i];
+  {
+    const int hb = a.halo_ptr[blockIdx.x];
+    for (int i = threadIdx.x; i < nhalo; i += blockDim.x) s_halo[i] = a.halo[hb + i];
+    if (se > sb) {
+      // this CTA's SELL columns: a multiple of 32 entries starting at a multiple of 32
+      const int e0 = a.slice_ptr[sb], ne = a.slice_ptr[se] - e0;
+      const uint4* src = reinterpret_cast<const uint4*>(a.loc_col + e0);
+      uint4* dst = reinterpret_cast<uint4*>(s_col);
+      for (int i = threadIdx.x; i < ne / 8; i += blockDim.x) dst[i] = src[i];
+    }
+  }
+
+#define FOR_OWN_ROWS                                              \
+  for (int sl = sb + warp; sl < se; sl += nwarps)                 \
+    for (int64_t row = (int64_t)sl * 32 + lane; row < a.n; row = a.n)
+
+  // w = A u for the own rows from the window (filled first); w.u partials into acc
+  auto product = [&](double acc[4]) {
+    const int W = nown + nhalo;
+    for (int i = threadIdx.x; i < W; i += blockDim.x) {
+      const int64_t g = (i < nown) ? (int64_t)(r0 + i) : (int64_t)s_halo[i - nown];
+      const VT* src = a.u + g * LD;
+      VT* dst = s_win + (size_t)i * LD;
+      if constexpr (RB <= 16) {
+        cp_async<RB>(dst, src);
+      } else {
+        constexpr int E = 16 / (int)sizeof(VT);
+#pragma unroll
+        for (int k = 0; k < RB / 16; k++) cp_async<16>(dst + k * E, src + k * E);
+      }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const int e0 = s_sp[0];
+    auto row_done = [&](int sl, const VT ak[LD], const VT am[LD]) {
+      const int64_t row = (int64_t)sl * 32 + lane;
+      if (row < a.n) {
+        VT ur[LD], dr[LD], wv[LD];
+        ld_win<VT, LD>(s_win, (int)(row - r0), ur);
+#pragma unroll
+        for (int s = 0; s < LD; s++) dr[s] = VT(0);
+        if (a.diag) ldv<VT, LD>(a.diag, row, dr);
+        const bool bcr = a.bc && a.bc[row];
+#pragma unroll
+        for (int s = 0; s < LD; s++) {
+          const VT v = VT(a.dscale[s]) * ak[s] + VT(a.cscale[s]) * am[s] + dr[s] * ur[s];
+          wv[s] = bcr ? ur[s] : v;
+          acc[s] += (double)wv[s] * (double)ur[s];
+        }
+        stv<VT, LD>(a.w, row, wv);
+      }
+    };
+    if (a.reg_values) {
+      for (int slb = sb + warp; slb < se; slb += MAXS * nwarps) {
+        VT vals[MAXS][WMAX];
+        VT mvals[HASM ? MAXS : 1][HASM ? WMAX : 1];
+#pragma unroll
+        for (int j = 0; j < MAXS; j++) {
+          const int sl = slb + j * nwarps;
+          const int base = (sl < se) ? s_sp[sl - sb] : 0;
+          const int w = (sl < se) ? (s_sp[sl - sb + 1] - base) >> 5 : 0;
+#pragma unroll
+          for (int k = 0; k < WMAX; k++) {
+            vals[j][k] = (k < w) ? ld_na(a.sK + base + k * 32 + lane) : VT(0);
+            if constexpr (HASM) mvals[j][k] = (k < w) ? ld_na(a.sM + base + k * 32 + lane) : VT(0);
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < MAXS; j++) {
+          const int sl = slb + j * nwarps;
+          if (sl < se) {
+            const int base = s_sp[sl - sb], w = (s_sp[sl - sb + 1] - base) >> 5;
+            const int lb = base - e0;
+            VT ak[LD], am[LD];
+#pragma unroll
+            for (int s = 0; s < LD; s++) ak[s] = am[s] = VT(0);
+#pragma unroll
+            for (int k = 0; k < WMAX; k++) {
+              if (k < w) {
+                VT pv[LD];
+                ld_win<VT, LD>(s_win, s_col[lb + k * 32 + lane], pv);
+#pragma unroll
+                for (int s = 0; s < LD; s++) {
+                  ak[s] += vals[j][k] * pv[s];
+                  if constexpr (HASM) am[s] += mvals[j][k] * pv[s];
+                }
+              }
+            }
+            row_done(sl, ak, am);
+          }
+        }
+      }
+    } else {
+      for (int sl = sb + warp; sl < se; sl += nwarps) {
+        const int base = s_sp[sl - sb], w = (s_sp[sl - sb + 1] - base) >> 5;
+        const int lb = base - e0;
+        VT ak[LD], am[LD];
+#pragma unroll
+        for (int s = 0; s < LD; s++) ak[s] = am[s] = VT(0);
+        VT vv[U], mm[HASM ? U : 1];
+        stage_values<VT, U, HASM>(a, base, w, 0, lane, vv, mm);
+        for (int k = 0; k < w; k += U) {
+          VT vn[U], mn[HASM ? U : 1];
+          if (k + U < w) stage_values<VT, U, HASM>(a, base, w, k + U, lane, vn, mn);
+#pragma unroll
+          for (int u = 0; u < U; u++) {
+            if (k + u < w) {
+              VT pv[LD];
+              ld_win<VT, LD>(s_win, s_col[lb + (k + u) * 32 + lane], pv);
+#pragma unroll
+              for (int s = 0; s < LD; s++) {
+                ak[s] += vv[u] * pv[s];
+                if constexpr (HASM) am[s] += mm[u] * pv[s];
+              }
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < U; u++) {
+            vv[u] = vn[u];
+            if constexpr (HASM) mm[u] = mn[u];
+          }
+        }
+        row_done(sl, ak, am);
+      }
+    }
+  };
+
+  // residual refresh of the lanes in tr: r = b - A64 x (FP64), u = D^-1 r, publish u;
+  // partials [r.u | r.r (FP64) | b.b]
+  auto refresh = [&](const int tr[LD], double acc[12]) {
+    FOR_OWN_ROWS {
+      double r64[LD];
+      csr64_residual<VT, LD>(a, row, r64);
+      VT rv[LD], dv[LD], uv[LD];
+      ldv_cg<VT, LD>(a.r, row, rv);
+      ldv_cg<VT, LD>(a.dinv, row, dv);
+      ldv_cg<VT, LD>(a.u, row, uv);
+      double bv[LD];
+      ldv_cg<double, LD>(a.b, row, bv);
+#pragma unroll
+      for (int s = 0; s < LD; s++) {
+        if (tr[s]) {
+          rv[s] = (VT)r64[s];
+          uv[s] = dv[s] * rv[s];
+          acc[s] += (double)rv[s] * (double)uv[s];
+          acc[4 + s] += r64[s] * r64[s];
+          acc[8 + s] += (s < S) ? bv[s] * bv[s] : 0.0;
+        }
+      }
+      stv<VT, LD>(a.r, row, rv);
+      stv<VT, LD>(a.u, row, uv);
+    }
+  };
+
+  // ---- I1: Jacobi diagonal (FP64 values), Dirichlet values into x, p = s = xi = 0
+  FOR_OWN_ROWS {
+    VT dv[LD], zero[LD], rz[LD];
+    const bool bcr = a.bc && a.bc[row];
+#pragma unroll
+    for (int s = 0; s < LD; s++) zero[s] = rz[s] = VT(0);
+    if (bcr) {
+#pragma unroll
+      for (int s = 0; s < LD; s++) {
+        dv[s] = VT(0);
+        a.x[row * LD + s] = a.b[row * LD + s];
+      }
+    } else {
+      const int lo = a.A64.indptr[row], hi = a.A64.indptr[row + 1];
+      int l = lo, h = hi;
+      while (l < h) {
+        const int mid = (l + h) >> 1;
+        if (a.A64.indices[mid] < row)
+          l = mid + 1;
+        else
+          h = mid;
+      }
+      const bool found = l < hi && a.A64.indices[l] == row;
+      const double kd = found ? a.A64.K[l] : 0.0;
+      const double md = (a.A64.M && found) ? a.A64.M[l] : 0.0;
+#pragma unroll
+      for (int s = 0; s < LD; s++) {
+        double d = a.dscale[s] * kd + a.cscale[s] * md;
+        if (a.A64.diag) d += a.A64.diag[row * LD + s];
+        dv[s] = (s < S && d != 0.0) ? VT(1.0 / d) : VT(0);
+      }
+    }
+    stv<VT, LD>(a.dinv, row, dv);
+    stv<VT, LD>(a.p, row, zero);
+    stv<VT, LD>(a.s, row, zero);
+    stv<VT, LD>(a.xi, row, zero);
+    stv<VT, LD>(a.r, row, rz);
+    stv<VT, LD>(a.u, row, rz);
+  }
+  bool ok = grid_sync(a.bar, target);
+
+  // ---- I2: r = b - A x, u = D^-1 r; r.u, r.r, b.b
+  {
+    double acc[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) acc[k] = 0.0;
+    int tr[LD];
+#pragma unroll
+    for (int s = 0; s < LD; s++) tr[s] = 1;
+    if (ok) refresh(tr, acc);
+    block_partial<12>(acc, a.part, sh);
+  }
+  ok = ok && grid_sync(a.bar, target);
+  if (ok) grid_totals<12>(a.part, s_tot, s_buf);
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < 4; s++) {
+      const bool use = s < S && ok;
+      const double rz = use ? s_tot[s] : 0.0, rr = use ? s_tot[4 + s] : 0.0;
+      const double bb = use ? s_tot[8 + s] : 0.0;
+      const double rt = use ? a.rtol[s] : 0.0;
+      L.bb[s] = bb;
+      L.tol2[s] = rt * rt * bb;
+      L.rr[s] = rr;
+      L.rtrue[s] = rr;
+      L.rmax2[s] = rr;
+      L.rz[s] = rz;
+      L.alpha[s] = 0.0;
+      L.beta[s] = 0.0;
+      L.trigger[s] = 0;
+      L.iters[s] = 0;
+      const bool fin = isfinite(rr) && isfinite(rz);
+      const bool act = use && fin && rr > L.tol2[s];
+      L.active[s] = act;
+      L.status[s] = !use ? TP_OK : (!fin ? TP_ERR_NONFINITE : (act ? -1 : TP_OK));
+    }
+  }
+  // ---- W: w = A u; w.u -> alpha = r.u / w.u
+  {
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    if (ok) product(acc);
+    block_partial<4>(acc, a.part, sh);
+  }
+  ok = ok && grid_sync(a.bar, target);
+  if (ok) grid_totals<4>(a.part, s_tot, s_buf);
+  if (threadIdx.x == 0 && ok) {
+    for (int s = 0; s < S; s++) {
+      if (!L.active[s]) continue;
+      const double dl = s_tot[s];
+      if (!isfinite(dl)) {
+        L.active[s] = 0;
+        L.status[s] = TP_ERR_NONFINITE;
+        continue;
+      }
+      const double gm = L.rz[s];
+      L.rz[s] = 0.0;  // no previous gamma: beta = 0
+      L.alpha[s] = 0.0;
+      cg_coefficients(L, s, gm, dl, 0);
+    }
+  }
+  __syncthreads();
+
+  clk.lap(7);  // init phases
+  int it = 0, n_rel = 0;
+  while (ok && it < a.max_it) {
+    int nact = 0;
+#pragma unroll
+    for (int s = 0; s < 4; s++) nact += L.active[s];
+    if (!nact) break;
+    // ---- P: p = u + beta p, s = w + beta s, xi += alpha p, r -= alpha s, u = D^-1 r
+    {
+      VT al[LD], be[LD];
+#pragma unroll
+      for (int s = 0; s < LD; s++) {
+        const bool act = (s < S) && L.active[s];
+        al[s] = act ? (VT)L.alpha[s] : VT(0);
+        be[s] = act ? (VT)L.beta[s] : VT(0);
+      }
+      double acc[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) acc[k] = 0.0;
+      FOR_OWN_ROWS {
+        VT uv[LD], wv[LD], pv[LD], sv[LD], xv[LD], rv[LD], dv[LD];
+        ld_win<VT, LD>(s_win, (int)(row - r0), uv);  // u of the own rows, last window
+        ldv_cg<VT, LD>(a.w, row, wv);
+        ldv_cg<VT, LD>(a.p, row, pv);
+        ldv_cg<VT, LD>(a.s, row, sv);
+        ldv_cg<VT, LD>(a.xi, row, xv);
+        ldv_cg<VT, LD>(a.r, row, rv);
+        ldv_cg<VT, LD>(a.dinv, row, dv);
+#pragma unroll
+        for (int s = 0; s < LD; s++) {
+          pv[s] = uv[s] + be[s] * pv[s];
+          sv[s] = wv[s] + be[s] * sv[s];
+          xv[s] += al[s] * pv[s];
+          rv[s] -= al[s] * sv[s];
+          uv[s] = dv[s] * rv[s];
+          acc[s] += (double)rv[s] * (double)uv[s];
+          acc[4 + s] += (double)rv[s] * (double)rv[s];
+        }
+        stv<VT, LD>(a.p, row, pv);
+        stv<VT, LD>(a.s, row, sv);
+        stv<VT, LD>(a.xi, row, xv);
+        stv<VT, LD>(a.r, row, rv);
+        stv<VT, LD>(a.u, row, uv);
+      }
+      block_partial<8>(acc, a.part, sh);
+    }
+    clk.lap(2);
+    ok = grid_sync(a.bar, target);
+    clk.lap(3);
+    if (!ok) break;
+    // r.u and r.r of the new residual, kept until the w.u of the product is known
+    grid_totals<8>(a.part, s_tot, s_buf);
+    if (threadIdx.x == 0) {
+      for (int s = 0; s < S; s++) {
+        s_gam[s] = s_tot[s];
+        L.rr[s] = s_tot[4 + s];
+      }
+    }
+    // ---- W: w = A u; w.u
+    {
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+      product(acc);
+      block_partial<4>(acc, a.part, sh);
+    }
+    clk.lap(0);
+    ok = grid_sync(a.bar, target);
+    clk.lap(1);
+    if (!ok) break;
+    grid_totals<4>(a.part, s_tot, s_buf);
+    it++;
+    if (threadIdx.x == 0) {
+      int any = 0;
+      for (int s = 0; s < S; s++) {
+        L.trigger[s] = 0;
+        if (!L.active[s]) continue;
+        const double gm = s_gam[s], rr = L.rr[s], dl = s_tot[s];
+        if (!isfinite(gm) || !isfinite(rr) || !isfinite(dl)) {
+          L.active[s] = 0;
+          L.status[s] = TP_ERR_NONFINITE;
+          L.iters[s] = it;
+          continue;
+        }
+        s_tot[8 + s] = dl;  // delta, kept for the coefficient update
+        any |= (rr <= L.tol2[s]) || (a.delta2 > 0.0 && rr < a.delta2 * L.rmax2[s]);
+      }
+      if (any) {
+        // one FP64 sweep refreshes every active lane
+        for (int s = 0; s < S; s++) L.trigger[s] = L.active[s];
+      } else {
+        for (int s = 0; s < S; s++)
+          if (L.active[s]) cg_coefficients(L, s, s_gam[s], s_tot[8 + s], it);
+      }
+      s_anytrig = any;
+    }
+    __syncthreads();
+    clk.lap(4);  // scalar updates
+    if (s_anytrig) {
+      // ---- RU: x += xi, then the FP64 residual replaces r, u, w and gamma, delta
+      int tr[LD];
+#pragma unroll
+      for (int s = 0; s < LD; s++) tr[s] = (s < S) ? L.trigger[s] : 0;
+      FOR_OWN_ROWS {
+        VT xv[LD];
+        ldv_cg<VT, LD>(a.xi, row, xv);
+#pragma unroll
+        for (int s = 0; s < LD; s++) {
+          if (tr[s]) {
+            a.x[row * LD + s] += (double)xv[s];
+            xv[s] = VT(0);
+          }
+        }
+        stv<VT, LD>(a.xi, row, xv);
+      }
+      ok = grid_sync(a.bar, target);
+      if (!ok) break;
+      {
+        double acc[12];
+#pragma unroll
+        for (int k = 0; k < 12; k++) acc[k] = 0.0;
+        refresh(tr, acc);
+        block_partial<12>(acc, a.part, sh);
+      }
+      ok = grid_sync(a.bar, target);
+      if (!ok) break;
+      grid_totals<12>(a.part, s_tot, s_buf);
+      if (threadIdx.x == 0) {
+        n_rel++;
+        for (int s = 0; s < S; s++) {
+          if (!L.trigger[s]) continue;
+          const double rr = s_tot[4 + s];
+          s_gam[s] = s_tot[s];
+          L.rtrue[s] = rr;
+          if (!isfinite(rr) || !isfinite(s_tot[s])) {
+            L.active[s] = 0;
+            L.status[s] = TP_ERR_NONFINITE;
+            L.iters[s] = it;
+            L.trigger[s] = 0;
+          } else if (rr <= L.tol2[s]) {
+            L.active[s] = 0;
+            L.status[s] = TP_OK;
+            L.iters[s] = it;
+            L.trigger[s] = 0;
+          } else {
+            L.rr[s] = rr;
+            L.rmax2[s] = rr;
+          }
+        }
+      }
+      __syncthreads();
+      {
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        product(acc);
+        block_partial<4>(acc, a.part, sh);
+      }
+      ok = grid_sync(a.bar, target);
+      if (!ok) break;
+      grid_totals<4>(a.part, s_tot, s_buf);
+      if (threadIdx.x == 0) {
+        for (int s = 0; s < S; s++) {
+          if (!L.trigger[s]) continue;
+          L.trigger[s] = 0;
+          if (!isfinite(s_tot[s])) {
+            L.active[s] = 0;
+            L.status[s] = TP_ERR_NONFINITE;
+            L.iters[s] = it;
+            continue;
+          }
+          cg_coefficients(L, s, s_gam[s], s_tot[s], it);
+        }
+      }
+      __syncthreads();
+      clk.lap(5);  // reliable update
+    }
+  }
+
+  // ---- final: x += xi, true residual norms
+  FOR_OWN_ROWS {
+    VT xv[LD];
+    ldv_cg<VT, LD>(a.xi, row, xv);
+#pragma unroll
+    for (int s = 0; s < LD; s++) {
+      if (s < S) a.x[row * LD + s] += (double)xv[s];
+      xv[s] = VT(0);
+    }
+    stv<VT, LD>(a.xi, row, xv);
+  }
+  bool ok2 = ok && grid_sync(a.bar, target);
+  {
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    if (ok2) {
+      FOR_OWN_ROWS {
+        double r64[LD];
+        csr64_residual<VT, LD>(a, row, r64);
+#pragma unroll
+        for (int s = 0; s < LD; s++) acc[s] += r64[s] * r64[s];
+      }
+    }
+    block_partial<4>(acc, a.part, sh);
+  }
+  ok2 = ok2 && grid_sync(a.bar, target);
+  if (ok2) grid_totals<4>(a.part, s_tot, s_buf);
+  if (clk.on) {
+    clk.lap(6);
+#pragma unroll
+    for (int k = 0; k < 8; k++) a.prof[blockIdx.x * 8 + k] = clk.acc[k];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) write_result(a, L, ok2, s_tot, it, n_rel);
+#undef FOR_OWN_ROWS
+}
+
 // ----------------------------------------------------------------- SELL-32 build
 __global__ void k_slice_width(int64_t n, const int32_t* __restrict__ indptr, int ns,
                               int32_t* __restrict__ width) {
@@ -838,25 +1472,35 @@ extern "C" int tp_sell_scatter(int64_t nnz, const int32_t* csr2sell, const doubl
 
 // ----------------------------------------------------------------- persistent handle
 struct tp_pcg_handle {
-  int fp32, ld, grid, block;
-  size_t dyn_smem;  // slice offsets staged per CTA
+  int fp32, ld, grid, block, window;
+  size_t dyn_smem;  // slice offsets (+ window engine tables and window) per CTA
   void* fn;
   tp::PArgs<float> af;
   tp::PArgs<double> ad;
   tp::POut* out;
   tp::PBar* bar;
+  // window engine tables (owned by the handle)
+  int32_t* d_halo_ptr = nullptr;
+  int32_t* d_halo = nullptr;
+  uint16_t* d_loc_col = nullptr;
+  ~tp_pcg_handle() {
+    if (d_halo_ptr) cudaFree(d_halo_ptr);
+    if (d_halo) cudaFree(d_halo);
+    if (d_loc_col) cudaFree(d_loc_col);
+  }
 };
 
 namespace tp {
 // SELL entries per pipelined group: the current and next group's stream entries and the
 // current group's gathered records stay in registers (about 48 per thread: 2 to 8
-// entries).  Two CTAs per SM
-// (64 registers) only for records of at most 16 bytes.
+// entries).  Two CTAs per SM (64 registers) only for records of at most 16 bytes.  The
+// window engine (k_cgw) runs one CTA per SM.
 template <typename VT, int LD>
-static void* pick_kernel(int minb, bool hasM) {
+static void* pick_kernel(int minb, bool hasM, bool win) {
   constexpr int RB = 2 * LD * (int)sizeof(VT);
   constexpr int cost = 2 * (1 + (int)sizeof(VT) / 4) + RB / 4;  // registers per entry
   constexpr int U = std::max(2, std::min(8, 48 / cost));
+  if (win) return hasM ? (void*)k_cgw<VT, LD, U, true> : (void*)k_cgw<VT, LD, U, false>;
   if constexpr (RB <= 16) {
     if (minb >= 2) return hasM ? (void*)k_pcg<VT, LD, U, 2, true> : (void*)k_pcg<VT, LD, U, 2, false>;
   }
@@ -864,15 +1508,15 @@ static void* pick_kernel(int minb, bool hasM) {
 }
 
 // CTAs per SM: 1 (up to 128 registers per thread) or 2 (64 registers)
-static void* pcg_kernel(int fp32, int ld, int minb, bool hasM) {
+static void* pcg_kernel(int fp32, int ld, int minb, bool hasM, bool win = false) {
   if (fp32) {
-    if (ld == 1) return pick_kernel<float, 1>(minb, hasM);
-    if (ld == 2) return pick_kernel<float, 2>(minb, hasM);
-    if (ld == 4) return pick_kernel<float, 4>(minb, hasM);
+    if (ld == 1) return pick_kernel<float, 1>(minb, hasM, win);
+    if (ld == 2) return pick_kernel<float, 2>(minb, hasM, win);
+    if (ld == 4) return pick_kernel<float, 4>(minb, hasM, win);
   } else {
-    if (ld == 1) return pick_kernel<double, 1>(minb, hasM);
-    if (ld == 2) return pick_kernel<double, 2>(minb, hasM);
-    if (ld == 4) return pick_kernel<double, 4>(minb, hasM);
+    if (ld == 1) return pick_kernel<double, 1>(minb, hasM, win);
+    if (ld == 2) return pick_kernel<double, 2>(minb, hasM, win);
+    if (ld == 4) return pick_kernel<double, 4>(minb, hasM, win);
   }
   return nullptr;
 }
@@ -923,11 +1567,85 @@ static void fill_pargs(PArgs<VT>& a, const tp_csr_op* op, const tp_sell* sl, con
   p += 2 * vec_bytes;
   a.rec1 = reinterpret_cast<VT*>(p);
   p += 2 * vec_bytes;
+  // the window engine's vectors share the record buffers
+  a.p = a.rec0;
+  a.s = a.rec0 + vec_bytes / sizeof(VT);
+  a.u = a.rec1;
+  a.w = a.rec1 + vec_bytes / sizeof(VT);
+  a.halo_ptr = nullptr;
+  a.halo = nullptr;
+  a.loc_col = nullptr;
+  a.sp_cap = a.halo_cap = a.col_cap = 0;
+  a.reg_values = 0;
   a.part = reinterpret_cast<double*>(p);
   p += a256(sizeof(double) * 16 * grid);
   a.bar = reinterpret_cast<PBar*>(p);
   p += a256(sizeof(PBar));
   a.out = reinterpret_cast<POut*>(p);
+}
+static int round4(int64_t x) { return (int)((x + 3) & ~(int64_t)3); }
+
+// Window tables for a grid of `grid` CTAs over contiguous slice ranges: for CTA c (rows
+// [r0, r1)) the sorted columns outside [r0, r1) that its rows reference (its halo) and
+// every SELL entry's column as a window index (own rows 0 .. r1-r0-1, then the halo in
+// order).  ok = false (no error) when a window would exceed 65535 entries.
+struct WinTables {
+  std::vector<int32_t> halo_ptr, halo;
+  std::vector<uint16_t> loc_col;
+  int sp_cap = 0, halo_cap = 0, col_cap = 0, win_cap = 0, max_width = 0;
+};
+
+static int build_window(const tp_sell* sell, int grid, cudaStream_t st, WinTables& w, bool* ok) {
+  *ok = false;
+  const int64_t n = sell->n_rows;
+  const int ns = (int)((n + 31) / 32);
+  std::vector<int32_t> sp(ns + 1);
+  std::vector<int32_t> col(sell->n_entries);
+  TP_CUDA_TRY(cudaMemcpyAsync(sp.data(), sell->slice_ptr, sizeof(int32_t) * (ns + 1),
+                              cudaMemcpyDeviceToHost, st));
+  if (sell->n_entries > 0)
+    TP_CUDA_TRY(cudaMemcpyAsync(col.data(), sell->sell_col, sizeof(int32_t) * sell->n_entries,
+                                cudaMemcpyDeviceToHost, st));
+  TP_CUDA_TRY(cudaStreamSynchronize(st));
+  std::vector<int32_t> mark(n, -1), pos(n, 0);
+  w.halo_ptr.assign(grid + 1, 0);
+  w.halo.clear();
+  w.loc_col.assign(sell->n_entries, 0);
+  int max_sl = 0, max_h = 0, max_e = 0, max_w = 0;
+  for (int s = 0; s < ns; s++) w.max_width = std::max(w.max_width, (sp[s + 1] - sp[s]) / 32);
+  for (int c = 0; c < grid; c++) {
+    const int sb = (int)((int64_t)c * ns / grid), se = (int)((int64_t)(c + 1) * ns / grid);
+    const int64_t r0 = (int64_t)sb * 32, r1 = std::min<int64_t>((int64_t)se * 32, n);
+    const int e0 = sp[sb], e1 = sp[se];
+    const size_t h0 = w.halo.size();
+    for (int e = e0; e < e1; e++) {
+      const int j = col[e];
+      if ((j < r0 || j >= r1) && mark[j] != c) {
+        mark[j] = c;
+        w.halo.push_back(j);
+      }
+    }
+    std::sort(w.halo.begin() + h0, w.halo.end());
+    const int64_t nown = se > sb ? r1 - r0 : 0;
+    const int64_t nh = (int64_t)(w.halo.size() - h0);
+    if (nown + nh > 65535) return TP_OK;  // *ok stays false
+    for (int64_t k = 0; k < nh; k++) pos[w.halo[h0 + k]] = (int32_t)(nown + k);
+    for (int e = e0; e < e1; e++) {
+      const int j = col[e];
+      w.loc_col[e] = (uint16_t)((j >= r0 && j < r1) ? j - r0 : pos[j]);
+    }
+    w.halo_ptr[c + 1] = (int32_t)w.halo.size();
+    max_sl = std::max(max_sl, se - sb + 1);
+    max_h = std::max(max_h, (int)nh);
+    max_e = std::max(max_e, e1 - e0);
+    max_w = std::max(max_w, (int)(nown + nh));
+  }
+  w.sp_cap = round4(max_sl);
+  w.halo_cap = round4(max_h);
+  w.col_cap = max_e;  // a multiple of 32
+  w.win_cap = max_w;
+  *ok = true;
+  return TP_OK;
 }
 }  // namespace tp
 
@@ -978,6 +1696,63 @@ extern "C" size_t tp_pcg_workspace_bytes(const tp_csr_op* op, int inner_fp32) {
          a256(sizeof(PBar)) + a256(sizeof(POut));
 }
 
+// Window engine for a one-CTA-per-SM grid when its tables and window fit in shared
+// memory; leaves h on the streaming engine otherwise.  DISSOLVE_PCG_ENGINE=stream at
+// create keeps the streaming engine.
+static int try_window(tp_pcg_handle* h, const tp_sell* sell, bool hasM, cudaStream_t st) {
+  const char* env = getenv("DISSOLVE_PCG_ENGINE");
+  if (env && strcmp(env, "stream") == 0) return TP_OK;
+  if (h->grid != sm_count()) return TP_OK;
+  WinTables w;
+  bool ok = false;
+  int rc = build_window(sell, h->grid, st, w, &ok);
+  if (rc != TP_OK || !ok) return rc;
+  const size_t vt = h->fp32 ? 4 : 8;
+  const size_t head = (4 * (size_t)(w.sp_cap + w.halo_cap) + 2 * (size_t)w.col_cap + 15) & ~(size_t)15;
+  const size_t d = head + (size_t)w.win_cap * h->ld * vt;
+  void* fn = pcg_kernel(h->fp32, h->ld, 1, hasM, true);
+  cudaFuncAttributes fa;
+  TP_CUDA_TRY(cudaFuncGetAttributes(&fa, fn));
+  int optin = 0, dev = 0;
+  TP_CUDA_TRY(cudaGetDevice(&dev));
+  TP_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  if (fa.sharedSizeBytes + d + 1024 > (size_t)optin) return TP_OK;  // does not fit
+  TP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d));
+  TP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  int occ = 0;
+  TP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, h->block, d));
+  if (occ < 1) return TP_OK;
+  TP_CUDA_TRY(cudaMalloc(&h->d_halo_ptr, sizeof(int32_t) * w.halo_ptr.size()));
+  TP_CUDA_TRY(cudaMalloc(&h->d_halo, sizeof(int32_t) * std::max<size_t>(w.halo.size(), 1)));
+  TP_CUDA_TRY(cudaMalloc(&h->d_loc_col, sizeof(uint16_t) * std::max<size_t>(w.loc_col.size(), 8)));
+  TP_CUDA_TRY(cudaMemcpyAsync(h->d_halo_ptr, w.halo_ptr.data(),
+                              sizeof(int32_t) * w.halo_ptr.size(), cudaMemcpyHostToDevice, st));
+  if (!w.halo.empty())
+    TP_CUDA_TRY(cudaMemcpyAsync(h->d_halo, w.halo.data(), sizeof(int32_t) * w.halo.size(),
+                                cudaMemcpyHostToDevice, st));
+  if (!w.loc_col.empty())
+    TP_CUDA_TRY(cudaMemcpyAsync(h->d_loc_col, w.loc_col.data(),
+                                sizeof(uint16_t) * w.loc_col.size(), cudaMemcpyHostToDevice, st));
+  TP_CUDA_TRY(cudaStreamSynchronize(st));
+  auto set = [&](auto& a) {
+    a.halo_ptr = h->d_halo_ptr;
+    a.halo = h->d_halo;
+    a.loc_col = h->d_loc_col;
+    a.sp_cap = w.sp_cap;
+    a.halo_cap = w.halo_cap;
+    a.col_cap = w.col_cap;
+    a.reg_values = w.max_width <= 16 ? 1 : 0;  // the kernel's register-staging width
+  };
+  if (h->fp32)
+    set(h->af);
+  else
+    set(h->ad);
+  h->fn = fn;
+  h->dyn_smem = d;
+  h->window = 1;
+  return TP_OK;
+}
+
 extern "C" int tp_pcg_create(const tp_csr_op* op, const tp_sell* sell, int max_it,
                              int inner_fp32, double delta, int ctas_per_sm, const double* b,
                              double* x, const double* rtol, void* workspace,
@@ -999,6 +1774,8 @@ extern "C" int tp_pcg_create(const tp_csr_op* op, const tp_sell* sell, int max_i
   h->fp32 = inner_fp32 ? 1 : 0;
   h->ld = op->ld;
   h->block = 512;
+  h->window = 0;
+  TP_REQUIRE(sell->n_rows == op->n_rows, "SELL and CSR row counts differ");
   const int minb = ctas_per_sm > 0 ? std::min(ctas_per_sm, 2) : default_minb(op->ld);
   const bool hasM = inner_fp32 ? sell->sM32 != nullptr : sell->sM64 != nullptr;
   int rc = pcg_grid(h->fp32, h->ld, minb, hasM, h->block, op->n_rows, &h->grid, &h->dyn_smem);
@@ -1018,6 +1795,11 @@ extern "C" int tp_pcg_create(const tp_csr_op* op, const tp_sell* sell, int max_i
   h->bar = h->fp32 ? h->af.bar : h->ad.bar;
   h->out = h->fp32 ? h->af.out : h->ad.out;
   cudaStream_t st = as_stream(stream);
+  rc = try_window(h, sell, hasM, st);
+  if (rc != TP_OK) {
+    delete h;
+    return rc;
+  }
   cudaError_t e = cudaMemsetAsync(h->bar, 0, sizeof(PBar), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(h->out, 0, sizeof(POut), st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -1070,6 +1852,13 @@ extern "C" int tp_pcg_grid(tp_pcg_handle* h, int* grid, int* block) {
   TP_REQUIRE(h, "null handle");
   if (grid) *grid = h->grid;
   if (block) *block = h->block;
+  return TP_OK;
+}
+
+extern "C" int tp_pcg_engine(tp_pcg_handle* h, int* window, size_t* smem_bytes) {
+  TP_REQUIRE(h, "null handle");
+  if (window) *window = h->window;
+  if (smem_bytes) *smem_bytes = h->dyn_smem;
   return TP_OK;
 }
 

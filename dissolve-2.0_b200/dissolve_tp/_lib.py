@@ -133,6 +133,7 @@ SIGNATURES = {
     "tp_pcg_run": (ctypes.c_int, [_vp, _vp]),
     "tp_pcg_result_get": (ctypes.c_int, [_vp, _P(TpCgResult), _vp, _vp, _vp, _vp, _vp]),
     "tp_pcg_grid": (ctypes.c_int, [_vp, _P(ctypes.c_int), _P(ctypes.c_int)]),
+    "tp_pcg_engine": (ctypes.c_int, [_vp, _P(ctypes.c_int), _P(ctypes.c_size_t)]),
     "tp_pcg_set_profile": (ctypes.c_int, [_vp, _vp]),
     "tp_pcg_destroy": (ctypes.c_int, [_vp]),
     "tp_mlp_param_count": (ctypes.c_int, []),

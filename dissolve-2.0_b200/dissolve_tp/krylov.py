@@ -247,6 +247,12 @@ class PersistentCG:
         call("tp_pcg_grid", self._h, ctypes.byref(g), ctypes.byref(b))
         return int(g.value), int(b.value)
 
+    def engine(self) -> dict:
+        """Engine of the handle: shared-memory window (Chronopoulos-Gear) or streaming."""
+        w, sm = ctypes.c_int(0), ctypes.c_size_t(0)
+        call("tp_pcg_engine", self._h, ctypes.byref(w), ctypes.byref(sm))
+        return {"window": bool(w.value), "smem_bytes": int(sm.value)}
+
     def run(self):
         call("tp_pcg_run", self._h, stream_handle())
 

@@ -159,6 +159,8 @@ class BatchedTransport:
             self.solver = PersistentCG(self.op, rtol=rtol, max_it=max_it, inner_fp32=inner_fp32,
                                        delta=delta, ctas_per_sm=int(cg.get("ctas_per_sm", 0)))
             self.cg_config["grid"], self.cg_config["block"] = self.solver.grid()
+            self.cg_config["form"] = ("window (Chronopoulos-Gear)" if self.solver.engine()["window"]
+                                      else "streaming")
         else:
             if autotune and not {"group", "block", "rows_per_tile"} & set(cg):
                 self.assemble_operator()

@@ -345,6 +345,16 @@ TP_API int tp_pcg_result_get(tp_pcg_handle* h, tp_cg_result* res, int32_t* lane_
                              int32_t* lane_status, double* lane_rnorm, double* lane_bnorm,
                              void* stream);
 TP_API int tp_pcg_grid(tp_pcg_handle* h, int* grid, int* block);
+/* Engine the handle runs (chosen at create).  *window = 1: the window engine -- the
+ * Chronopoulos-Gear form of the same Jacobi-PCG, in which the only vector shared between
+ * CTAs is u = D^-1 r; every CTA keeps u of its rows plus its halo (the columns outside its
+ * row range that its rows reference) and 16-bit window-local column indices in shared
+ * memory (one CTA per SM, at most 65535 window entries per CTA, the tables within the
+ * per-block shared-memory limit).  *window = 0: the streaming engine (standard
+ * recurrences, columns and gathers from global memory).  *smem_bytes: dynamic shared
+ * memory per CTA.  The environment variable DISSOLVE_PCG_ENGINE=stream at create forces
+ * the streaming engine. */
+TP_API int tp_pcg_engine(tp_pcg_handle* h, int* window, size_t* smem_bytes);
 /* per-CTA phase times of the next runs: prof (grid * 8 device u64, ns) receives per CTA
  * [A work, A barrier wait, B work, B barrier wait, scalar updates, reliable updates,
  * final, init]; NULL switches it off */
