@@ -39,6 +39,8 @@ import numpy as np  # noqa: E402
 METRIC = "3-species BE steps/s at 1.57M P1 tets, rtol 1e-8: mixed+learned vs plain FP64"
 N_SIDE, JITTER = 64, 0.2
 D_S, K_S, DT, RTOL = (1.0, 1.0, 2.6), (0.5, 0.0, 0.2), 0.02, 1e-8
+# measured with ncu on this workload (see profiles/); None until captured
+DRAM_BYTES_PER_ITERATION = 13.40e6  # 3.592 GB over a 268-iteration launch
 WORKLOAD = ("3-species backward-Euler step, 64^3 Kuhn cube (1,572,864 P1 tets, 274,625 "
             "vertices), jitter 0.2h, De = D_s exp(0.3 xi), rtol 1e-8")
 
@@ -201,10 +203,24 @@ def run_ours(args, rank, world, local_rank):
     solve_ms = e0.elapsed_time(e1)
     rk = fast.solver.result()
     its = max(int(rk["iterations"]), 1)
-    # algorithmic bytes per iteration: SELL/CSR matrix (int32 col + FP32 value per nonzero)
-    # and 12 vector passes of (V, 4) FP32: A reads z, p and writes p, q; B reads p, q, r,
-    # xi, D^-1 and writes xi, r, z
-    bytes_it = nnz * 8 + 12 * nv * 16
+    window = fast.cg_config.get("form", "").startswith("window")
+    if window:
+        # window engine, per iteration: FP32 value per nonzero (columns stay in shared
+        # memory for the whole solve) and 14 passes of (V, 4) FP32: u read once into the
+        # windows; P reads w, p, s, xi, r, D^-1 and writes p, s, xi, r, u; the product
+        # writes w and reads the row diagonal
+        bytes_it = nnz * 4 + 14 * nv * 16
+        kernel = ("k_cgw<float,4> (persistent 3-column Jacobi-PCG, Chronopoulos-Gear form, "
+                  "shared-memory windows, one cooperative launch per solve)")
+    else:
+        # streaming engine: int32 column + FP32 value per nonzero and 12 passes of (V, 4)
+        # FP32: A reads z, p and writes p, q; B reads p, q, r, xi, D^-1, writes xi, r, z
+        bytes_it = nnz * 8 + 12 * nv * 16
+        kernel = ("k_pcg<float,4> (persistent 3-column Jacobi-PCG, one cooperative launch "
+                  "per solve)")
+    # DRAM bytes per iteration of the same kernel on this workload, from an ncu capture
+    # (dram__bytes_read.sum + dram__bytes_write.sum of one launch / its iterations)
+    traffic = (DRAM_BYTES_PER_ITERATION * its) if (window and DRAM_BYTES_PER_ITERATION) else None
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
@@ -297,14 +313,15 @@ def run_ours(args, rank, world, local_rank):
                    "cg_launch": fast.cg_config},
         "converged": conv, "cg_iterations": iters,
         "gpu_launches": launches,
-        "roofline": {"bound": "hbm", "kernel": "k_pcg<float,4> (persistent 3-column "
-                     "Jacobi-PCG, one cooperative launch per solve)",
+        "roofline": {"bound": "hbm", "kernel": kernel,
                      "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None,
+                     "frac": achieved / hbm, "traffic": traffic,
                      "algorithmic_bytes": bytes_it * its, "bytes_per_iteration": bytes_it,
                      "iterations": its, "launch_us": solve_ms * 1e3,
-                     "note": "peak = measured HBM copy bandwidth; the operator and vectors "
-                             "(about 85 MB) stay in the 126 MB L2 between iterations"},
+                     "note": "peak = measured HBM copy bandwidth (of measured); the "
+                             "operator and vectors stay in the 126 MB L2 between "
+                             "iterations; traffic = ncu DRAM bytes per iteration x "
+                             "iterations of this launch"},
         "clocks": clk.summary(),
         "e2e": e2e,
         "forms": forms,
