@@ -1651,6 +1651,25 @@ static int build_window(const tp_sell* sell, int grid, cudaStream_t st, WinTable
 
 static int default_minb(int) { return 1; }
 
+// Kernel attributes are per function and shared by every handle, so they only ever grow:
+// the dynamic shared-memory limit to the largest request so far, the shared-memory
+// carveout to what `ctas` CTAs of that size need (the rest of the unified storage stays
+// L1).  Set before occupancy queries so cooperative grids match the launches.
+static cudaError_t raise_smem_limits(void* fn, size_t dyn, int ctas) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, fn);
+  if (e != cudaSuccess) return e;
+  if ((int)dyn > fa.maxDynamicSharedSizeBytes) {
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    if (e != cudaSuccess) return e;
+  }
+  const size_t per_sm = (fa.sharedSizeBytes + dyn + 1024) * ctas;
+  const int pct = (int)std::min<size_t>(100, (per_sm * 100 + 228 * 1024 - 1) / (228 * 1024));
+  if (pct > fa.preferredShmemCarveout)
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
+  return e;
+}
+
 // Grid of `minb` CTAs per SM (fewer if they do not fit) and the dynamic shared memory
 // (slice offsets of one CTA's range) for n_rows rows.
 static int pcg_grid(int fp32, int ld, int minb, bool hasM, int block, int64_t n_rows, int* grid,
@@ -1665,16 +1684,7 @@ static int pcg_grid(int fp32, int ld, int minb, bool hasM, int block, int64_t n_
       set_error("persistent CG: %lld rows exceed the slice table of one CTA", (long long)n_rows);
       return TP_ERR_CAPACITY;
     }
-    cudaFuncAttributes fa;
-    TP_CUDA_TRY(cudaFuncGetAttributes(&fa, fn));
-    if (d > 48 * 1024)
-      TP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d));
-    // the rest of the unified L1/shared storage stays L1 (the gathered records live
-    // there); set before the occupancy query so the cooperative grid matches the launch
-    const size_t per_sm = (fa.sharedSizeBytes + d + 1024) * m;
-    const int pct = (int)std::min<size_t>(100, (per_sm * 100 + 228 * 1024 - 1) / (228 * 1024));
-    TP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                     std::max(pct, 1)));
+    TP_CUDA_TRY(raise_smem_limits(fn, d, m));
     int occ = 0;
     TP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, block, d));
     if (occ >= m) {
@@ -1717,8 +1727,7 @@ static int try_window(tp_pcg_handle* h, const tp_sell* sell, bool hasM, cudaStre
   TP_CUDA_TRY(cudaGetDevice(&dev));
   TP_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   if (fa.sharedSizeBytes + d + 1024 > (size_t)optin) return TP_OK;  // does not fit
-  TP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)d));
-  TP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  TP_CUDA_TRY(raise_smem_limits(fn, d, 1));
   int occ = 0;
   TP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, h->block, d));
   if (occ < 1) return TP_OK;
