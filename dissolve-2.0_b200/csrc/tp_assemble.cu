@@ -419,6 +419,59 @@ __global__ void k_oh_source(int64_t n, const double* __restrict__ phi,
   }
 }
 
+
+// ----------------------------------------------------------------- coupled gyroid step
+// Smoothed Heaviside of the scaffold indicator (the integrand of tp_scaffold_volume).
+__device__ __forceinline__ double heaviside_eps(double phi, double eps) {
+  const double pi = 3.141592653589793;
+  if (phi < -eps) return 0.0;
+  if (phi > eps) return 1.0;
+  return 0.5 * (1.0 + phi / eps + sin(pi * phi / eps) / pi);
+}
+
+// hv = k_orr H_eps(phi); ngphi = |grad phi| (grad may be NULL); f[:, col_oh] = orr_factor
+// hv U[:, col_o2], other columns of f zero
+__global__ void k_interface_terms(int64_t n, const double* __restrict__ phi,
+                                  const double* __restrict__ grad, double eps, double k_orr,
+                                  double orr_factor, int ld, const double* __restrict__ U,
+                                  int col_o2, int col_oh, double* __restrict__ f,
+                                  double* __restrict__ hv, double* __restrict__ ngphi) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double h = k_orr * heaviside_eps(phi[i], eps);
+    if (hv) hv[i] = h;
+    if (ngphi && grad) {
+      const double gx = grad[3 * i], gy = grad[3 * i + 1], gz = grad[3 * i + 2];
+      ngphi[i] = sqrt(gx * gx + gy * gy + gz * gz);
+    }
+    if (f) {
+      for (int s = 0; s < ld; s++) f[i * ld + s] = 0.0;
+      f[i * ld + col_oh] = orr_factor * h * U[i * ld + col_o2];
+    }
+  }
+}
+
+// out[c, col] (leading dim ld) = mean of the 4 vertex values (gpu_assembler.py:465-466)
+__global__ void k_cell_average_col(int64_t n, const int4* __restrict__ cells,
+                                   const double* __restrict__ vv, int ld, int col,
+                                   double* __restrict__ out) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    const int4 v = cells[c];
+    const double s = __dadd_rn(__dadd_rn(__dadd_rn(vv[v.x], vv[v.y]), vv[v.z]), vv[v.w]);
+    out[c * ld + col] = __ddiv_rn(s, 4.0);
+  }
+}
+
+// phi -= dt rate (1 + gain U[:, col])
+__global__ void k_levelset_advance(int64_t n, double* __restrict__ phi, int ld,
+                                   const double* __restrict__ U, int col, double dt, double rate,
+                                   double gain) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    phi[i] -= dt * rate * (1.0 + gain * U[i * ld + col]);
+}
+
 __global__ void k_axpby(int64_t n, double a, const double* __restrict__ x, double b,
                         double* __restrict__ y) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
@@ -688,6 +741,45 @@ extern "C" int tp_oh_source(int64_t n, const double* phi, const double* normgrad
   if (n == 0) return TP_OK;
   k_oh_source<<<grid_for(n, 256, 65535), 256, 0, as_stream(stream)>>>(
       n, phi, normgradphi, F, Cl, O2, eps, kd, k_orr, orr_factor, f);
+  TP_LAUNCH_CHECK();
+  return TP_OK;
+}
+
+
+extern "C" int tp_interface_terms(int64_t n, const double* phi, const double* grad, double eps,
+                                  double k_orr, double orr_factor, int ld, const double* U,
+                                  int col_o2, int col_oh, double* f, double* hv, double* ngphi,
+                                  void* stream) {
+  TP_REQUIRE(phi, "null pointer");
+  TP_REQUIRE(eps > 0.0, "epsilon must be positive");
+  TP_REQUIRE(!f || (U && ld >= 1 && ld <= TP_MAX_COLS && col_o2 >= 0 && col_o2 < ld &&
+                    col_oh >= 0 && col_oh < ld),
+             "bad column layout");
+  if (n == 0) return TP_OK;
+  k_interface_terms<<<grid_for(n, 256, 65535), 256, 0, as_stream(stream)>>>(
+      n, phi, grad, eps, k_orr, orr_factor, ld, U, col_o2, col_oh, f, hv, ngphi);
+  TP_LAUNCH_CHECK();
+  return TP_OK;
+}
+
+extern "C" int tp_cell_average_col(int64_t n_cells, const int32_t* cells, const double* vert_vals,
+                                   int ld, int col, double* out, void* stream) {
+  TP_REQUIRE(cells && vert_vals && out, "null pointer");
+  TP_REQUIRE(ld >= 1 && col >= 0 && col < ld, "bad column");
+  if (n_cells == 0) return TP_OK;
+  k_cell_average_col<<<grid_for(n_cells, 256, 65535), 256, 0, as_stream(stream)>>>(
+      n_cells, reinterpret_cast<const int4*>(cells), vert_vals, ld, col, out);
+  TP_LAUNCH_CHECK();
+  return TP_OK;
+}
+
+extern "C" int tp_levelset_advance(int64_t n, double* phi, int ld, const double* U, int col,
+                                   double dt, double rate, double gain, void* stream) {
+  TP_REQUIRE(phi && U, "null pointer");
+  TP_REQUIRE(ld >= 1 && col >= 0 && col < ld, "bad column");
+  if (n == 0) return TP_OK;
+  k_levelset_advance<<<grid_for(n, 256, 65535), 256, 0, as_stream(stream)>>>(n, phi, ld, U, col,
+                                                                          dt, rate, gain);
   TP_LAUNCH_CHECK();
   return TP_OK;
 }

@@ -110,6 +110,11 @@ SIGNATURES = {
     "tp_o2_alpha": (ctypes.c_int, [_c_i64, _vp, _vp, _c_dbl, _c_dbl, _vp, _vp]),
     "tp_oh_source": (ctypes.c_int, [_c_i64, _vp, _vp, _vp, _vp, _vp, _c_dbl, _c_dbl, _c_dbl,
                                     _c_dbl, _vp, _vp]),
+    "tp_interface_terms": (ctypes.c_int, [_c_i64, _vp, _vp, _c_dbl, _c_dbl, _c_dbl, ctypes.c_int, _vp,
+                                          ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]),
+    "tp_cell_average_col": (ctypes.c_int, [_c_i64, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    "tp_levelset_advance": (ctypes.c_int, [_c_i64, _vp, ctypes.c_int, _vp, ctypes.c_int, _c_dbl,
+                                           _c_dbl, _c_dbl, _vp]),
     "tp_axpby": (ctypes.c_int, [_c_i64, _c_dbl, _vp, _c_dbl, _vp, _vp]),
     "tp_pack_columns": (ctypes.c_int, [_c_i64, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
     "tp_unpack_columns": (ctypes.c_int, [_c_i64, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),

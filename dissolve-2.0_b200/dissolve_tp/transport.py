@@ -176,19 +176,27 @@ class BatchedTransport:
 
     # -- per-step pieces -------------------------------------------------------------
     def assemble_operator(self):
-        st = stream_handle()
+        self.assemble_stiffness()
+        self.assemble_diagonal()
+
+    def assemble_stiffness(self):
+        """Shared stiffness K_xi (FP64 and FP32 values)."""
         call("tp_assemble_csr", ctypes.byref(self.dm.tpm), ptr(self.coef), None, 0.0, 1,
-             _lib.TP_ASM_STIFF, None, ptr(self.K64), ptr(self.K32), st)
+             _lib.TP_ASM_STIFF, None, ptr(self.K64), ptr(self.K32), stream_handle())
+
+    def assemble_diagonal(self):
+        """Per-column lumped (1/dt + k_s + alpha_s) m."""
         shift = (ctypes.c_double * 4)(*([self.inv_dt + kk for kk in self.k] +
                                         [0.0] * (4 - self.S)))
         call("tp_lumped_diag", ctypes.byref(self.dm.tpm), self.S, self.ld, ptr(self.alpha),
-             shift, ptr(self.bc_mask), ptr(self.D64), ptr(self.D32), st)
+             shift, ptr(self.bc_mask), ptr(self.D64), ptr(self.D32), stream_handle())
 
     def assemble_rhs(self):
+        """b = M (U/dt + f) per column; f (V, ld) when a source is set (self.f)."""
         n_bc = 0 if self.bc_dofs is None else int(self.bc_dofs.numel())
-        call("tp_assemble_rhs", ctypes.byref(self.dm.tpm), self.S, self.ld, ptr(self.U), None,
-             self.inv_dt, 1, n_bc, ptr(self.bc_dofs), self.bc_values, ptr(self.solver.b),
-             stream_handle())
+        call("tp_assemble_rhs", ctypes.byref(self.dm.tpm), self.S, self.ld, ptr(self.U),
+             ptr(getattr(self, "f", None)), self.inv_dt, 1, n_bc, ptr(self.bc_dofs),
+             self.bc_values, ptr(self.solver.b), stream_handle())
 
     def initial_guess(self):
         x = self.solver.x

@@ -191,6 +191,27 @@ TP_API int tp_oh_source(int64_t n, const double* phi, const double* normgradphi,
                  const double* Cl, const double* O2, double eps, double kd, double k_orr,
                  double orr_factor, double* f, void* stream);
 
+/* Interface reaction of the gyroid-scaffold step (the per-vertex analogue of
+ * dissolve.py:866-875 and :923-936 with the smoothed Heaviside H_eps of
+ * gpu_assembler.py:605-644 in place of delta_eps |grad phi|):
+ * hv = k_orr H_eps(phi); ngphi = |grad phi| (grad (n, 3), may be NULL); f (n, ld) =
+ * 0 except f[:, col_oh] = orr_factor hv U[:, col_o2] (explicit OH- production from O2).
+ * f, hv, ngphi may each be NULL. */
+TP_API int tp_interface_terms(int64_t n, const double* phi, const double* grad, double eps,
+                              double k_orr, double orr_factor, int ld, const double* U,
+                              int col_o2, int col_oh, double* f, double* hv, double* ngphi,
+                              void* stream);
+
+/* tp_cell_average into column `col` of an (n_cells, ld) array (per-cell, per-column
+ * reaction for tp_lumped_diag). */
+TP_API int tp_cell_average_col(int64_t n_cells, const int32_t* cells, const double* vert_vals,
+                               int ld, int col, double* out, void* stream);
+
+/* Level-set update phi -= dt rate (1 + gain U[:, col]) (the algebraic part of the
+ * level-set step, dissolve.py:684-730, with the configured dissolution law). */
+TP_API int tp_levelset_advance(int64_t n, double* phi, int ld, const double* U, int col,
+                               double dt, double rate, double gain, void* stream);
+
 /* y = a x + b y (n doubles): numerics/solvers.py:278-279 under-relaxation */
 TP_API int tp_axpby(int64_t n, double a, const double* x, double b, double* y, void* stream);
 

@@ -248,6 +248,28 @@ def oh_source(phi, normgradphi, F, Cl, O2, epsilon, kd, k_orr, orr_factor=4.0):
     return medium * kd * F * Cl ** 2 + orr_factor * delta_eps(phi, epsilon) * normgradphi * k_orr * O2
 
 
+
+def heaviside_eps(phi, epsilon):
+    """Smoothed Heaviside of gpu_assembler.py:605-644 (scaffold_volume's integrand)."""
+    phi = np.asarray(phi, dtype=np.float64)
+    mid = 0.5 * (1.0 + phi / epsilon + np.sin(np.pi * phi / epsilon) / np.pi)
+    return np.where(phi < -epsilon, 0.0, np.where(phi > epsilon, 1.0, mid))
+
+
+def interface_terms(phi, grad, epsilon, k_orr, orr_factor, U, col_o2=0, col_oh=2):
+    """Gyroid-step interface reaction: hv = k_orr H_eps(phi), |grad phi|, and the explicit
+    OH- source f[:, col_oh] = orr_factor hv U[:, col_o2] (zero elsewhere)."""
+    hv = k_orr * heaviside_eps(phi, epsilon)
+    ng = None if grad is None else np.sqrt((np.asarray(grad) ** 2).sum(axis=1))
+    f = np.zeros_like(np.asarray(U, dtype=np.float64))
+    f[:, col_oh] = orr_factor * hv * U[:, col_o2]
+    return hv, ng, f
+
+
+def levelset_advance(phi, U, col, dt, rate, gain):
+    """phi - dt rate (1 + gain U[:, col])."""
+    return phi - dt * rate * (1.0 + gain * U[:, col])
+
 def under_relax(u_new, u_old, omega):
     """numerics/solvers.py:278-279."""
     return omega * u_new + (1.0 - omega) * u_old
