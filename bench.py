@@ -326,10 +326,194 @@ def run_ours(args, rank, world, local_rank):
         "e2e": e2e,
         "forms": forms,
     }
+    if args.kernels and world == 1:
+        line["kernels"] = kernel_table(m, coef, u0, flush)
+    if args.configs and world == 1:
+        line["other_configs"] = other_configs(flush)
     if rank == 0 and world == 1 and args.cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(m, coef, u0, sample_steps=args.cpu_sample_steps)
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ other kernels / configs
+def _event_ms(fn, reps, flush, torch):
+    ts = []
+    for _ in range(reps + 2):
+        flush()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return float(np.median(ts[2:]))
+
+
+def kernel_table(m, coef, u0, flush):
+    """Assembly, right-hand side and matrix-free apply at this workload: CUDA-event time
+    (median of 10, L2 flushed before each) and algorithmic bytes as in the per-unit
+    formulas of the design notes, against the measured HBM bandwidth."""
+    import ctypes
+
+    import torch
+
+    from dissolve_tp import _lib
+    from dissolve_tp.assembler import DeviceMesh
+    from dissolve_tp.device import ptr, stream_handle
+    dev = torch.device("cuda", torch.cuda.current_device())
+    dm = DeviceMesh(m.coords, m.cells)
+    n, V, nnz = m.n_cells, m.n_verts, dm.nnz
+    st, tpm = stream_handle(), ctypes.byref(dm.tpm)
+    hbm = _peaks().get("hbm_gbs", 6650.0)
+    De = torch.from_numpy(coef).to(dev)
+    al = torch.full((n,), 0.5, dtype=torch.float64, device=dev)
+    o64 = torch.empty(nnz, dtype=torch.float64, device=dev)
+    o32 = torch.empty(nnz, dtype=torch.float32, device=dev)
+    U = torch.zeros((V, 4), dtype=torch.float64, device=dev)
+    U[:, :3] = torch.from_numpy(u0)
+    b = torch.empty_like(U)
+    x32 = torch.randn((V, 4), dtype=torch.float32, device=dev)
+    y32 = torch.empty_like(x32)
+    x64, y64 = x32.double(), torch.empty((V, 4), dtype=torch.float64, device=dev)
+    ds = (ctypes.c_double * 4)(*D_S, 0.0)
+    sh = (ctypes.c_double * 4)(*K_S, 0.0)
+    rows = {
+        "assemble_full_fp64": (lambda: _lib.call("tp_assemble_csr", tpm, ptr(De), ptr(al), 50.0,
+                                                 1, 0, None, ptr(o64), None, st),
+                               n * (16 + 64 + 16) + V * 24 + nnz * 8),
+        "assemble_stiffness_fp64_fp32": (lambda: _lib.call("tp_assemble_csr", tpm, ptr(De), None,
+                                                           0.0, 1, 1, None, ptr(o64), ptr(o32),
+                                                           st),
+                                         n * (16 + 64 + 8) + V * 24 + nnz * 12),
+        "rhs_3col": (lambda: _lib.call("tp_assemble_rhs", tpm, 3, 4, ptr(U), None, 50.0, 1, 0,
+                                       None, None, ptr(b), st), n * 24 + V * 64),
+        "matfree_3col_fp64": (lambda: _lib.call("tp_matfree_apply", tpm, 3, 4, 0, ptr(De), None,
+                                                ds, sh, 50.0, 0, 0, ptr(x64), ptr(y64), st),
+                              n * 40 + V * 72),
+        "matfree_3col_fp32": (lambda: _lib.call("tp_matfree_apply", tpm, 3, 4, 1, ptr(De), None,
+                                                ds, sh, 50.0, 0, 0, ptr(x32), ptr(y32), st),
+                              n * 28 + V * 48),
+    }
+    out = {}
+    for name, (fn, nbytes) in rows.items():
+        ms = _event_ms(fn, 10, flush, torch)
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        out[name] = {"us": round(ms * 1e3, 1), "algorithmic_MB": round(nbytes / 1e6, 1),
+                     "GB_s": round(gbs, 1), "frac_hbm": round(gbs / hbm, 3)}
+    return out
+
+
+def _peaks():
+    try:
+        return json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+    except OSError:
+        return {}
+
+
+def other_configs(flush):
+    """The other workloads at their own shapes, each timed with CUDA events after warm-up:
+    256 uneven meshes as one batch vs one mesh at a time; the gyroid coupled step with the
+    learned guess trained on 300 steps and evaluated on 100 (N=48) against the
+    previous-step guess; the gyroid step at N=96 with the learned guess, eager and
+    CUDA-graph captured, against the plain FP64 step."""
+    import torch
+    out = {}
+
+    def run(name, fn):
+        try:
+            out[name] = fn()
+        except Exception as e:  # reported, not fatal for the headline line
+            out[name] = {"error": repr(e)[:300]}
+
+    def batch():
+        from dissolve_tp.batch import MeshBatch, MeshBatchPlain, uneven_batch_inputs
+        meshes, D, k = uneven_batch_inputs(256)
+        mb = MeshBatch(meshes, D, k, 0.02, rtol=1e-8, inner_fp32=True)
+        u0 = np.random.default_rng(2).uniform(0, 1, int(mb.vert_ptr[-1]))
+        mb.set_state(u0)
+        for _ in range(3):
+            mb.step()
+        ms = _event_ms(lambda: mb.step(sync=False), 3, flush, torch)
+        r = mb.solver.result()
+        tets = mb.n_cells
+        cfg = mb.cg_config
+        del mb
+        pl = MeshBatchPlain(meshes, D, k, 0.02, rtol=1e-8)
+        vp = np.concatenate([[0], np.cumsum([m_.n_verts for m_ in meshes])])
+        pl.set_state(u0, vp)
+        for _ in range(3):
+            pl.step(sync=False)
+        ms_p = _event_ms(lambda: pl.step(sync=False), 3, flush, torch)
+        return {"workload": "256 Kuhn cubes, N ~ U{8..40}, one species each, rtol 1e-8",
+                "tets": int(tets), "batch_ms_per_step": round(ms, 2),
+                "batch_tets_per_s": round(tets / (ms * 1e-3), 1),
+                "one_at_a_time_plain_fp64_ms_per_step": round(ms_p, 2),
+                "speedup": round(ms_p / ms, 2), "max_lane_iterations": int(r["iterations"]),
+                "converged": bool(r["converged"]), "cg_launch": cfg}
+
+    def gyroid48():
+        from dissolve_tp.coupled import GyroidStep, gyroid_inputs
+        mesh, phi, coef, u0 = gyroid_inputs(48, 0.15)
+        g = GyroidStep(mesh, phi, coef)
+        g.set_state(u0)
+        g.train_predictor(300, every=10, epochs=400)
+        p = GyroidStep(mesh, phi, coef)
+        p.tr.set_state(g.state(), g.tr.U_prev[:, :3].cpu().numpy())
+        p.phi.copy_(g.phi)
+        res = {}
+        for name, obj in (("learned", g), ("previous", p)):
+            its = []
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(100):
+                its.append(obj.step()["iterations"])
+            e1.record()
+            e1.synchronize()
+            res[name] = {"ms_per_step": round(e0.elapsed_time(e1) / 100, 3),
+                         "mean_iterations": round(float(np.mean(its)), 1)}
+        a, b_ = g.state(), p.state()
+        res["rel_l2_learned_vs_previous"] = float(np.linalg.norm(a - b_) / np.linalg.norm(b_))
+        res["workload"] = ("gyroid 48^3 (663,552 tets), k_ORR H_eps interface reaction, 300 "
+                           "training steps, 100 evaluated steps, rtol 1e-8")
+        return res
+
+    def gyroid96():
+        from dissolve_tp.coupled import GyroidStep, GyroidStepPlain, gyroid_inputs
+        mesh, phi, coef, u0 = gyroid_inputs(96, 0.2)
+        g = GyroidStep(mesh, phi, coef)
+        g.set_state(u0)
+        g.train_predictor(40, every=5, epochs=300)
+        ms_e = _event_ms(lambda: g.step(sync=False), 10, flush, torch)
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            for _ in range(2):
+                g.step(sync=False)
+        torch.cuda.current_stream().wait_stream(s)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            g.step(sync=False)
+        ms_g = _event_ms(graph.replay, 10, flush, torch)
+        r = g.tr.solver.result()
+        del graph
+        p = GyroidStepPlain(mesh, phi, coef)
+        p.set_state(u0)
+        for _ in range(3):
+            p.step(sync=False)
+        ms_p = _event_ms(lambda: p.step(sync=False), 10, flush, torch)
+        return {"workload": "gyroid 96^3 (5,308,416 tets), coupled step, rtol 1e-8",
+                "fast_learned_eager_ms": round(ms_e, 2), "fast_learned_graph_ms": round(ms_g, 2),
+                "plain_fp64_ms": round(ms_p, 2), "speedup_graph_vs_plain": round(ms_p / ms_g, 2),
+                "iterations": int(r["iterations"]), "converged": bool(r["converged"])}
+
+    run("uneven_batch_256", batch)
+    run("gyroid_48_learned", gyroid48)
+    run("gyroid_96_coupled", gyroid96)
+    return out
 
 
 # ------------------------------------------------------------------ CPU legs
@@ -412,6 +596,10 @@ def main():
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-sample-steps", type=int, default=3)
+    ap.add_argument("--no-kernels", dest="kernels", action="store_false",
+                    help="skip the assembly / RHS / apply bandwidth table")
+    ap.add_argument("--no-configs", dest="configs", action="store_false",
+                    help="skip the multi-mesh batch and gyroid coupled-step workloads")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
