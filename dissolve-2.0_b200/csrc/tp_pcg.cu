@@ -89,6 +89,7 @@ struct PArgs {
   const int32_t* halo;      // sorted columns outside each CTA's row range
   const uint16_t* loc_col;  // (n_entries) window-local column of every SELL entry
   int sp_cap, halo_cap, col_cap;  // shared-memory capacities (entries)
+  int win_cap;                    // window entries (own rows + halo) of the largest CTA
   int reg_values;                 // every slice at most 16 wide: values via registers
   double* part;  // gridDim.x * 16
   PBar* bar;
@@ -201,10 +202,13 @@ __device__ __forceinline__ void grid_totals(const double* part, double* s_tot, d
     for (int b = g; b < (int)gridDim.x; b += groups) v += __ldcg(part + (int64_t)b * 16 + k);
   s_buf[threadIdx.x] = v;
   __syncthreads();
-  if (threadIdx.x < NV) {
+  // warp w < NV sums slot w over the groups with a fixed shuffle tree
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (w < NV) {
     double t = 0.0;
-    for (int gg = 0; gg < groups; gg++) t += s_buf[gg * 16 + threadIdx.x];
-    s_tot[threadIdx.x] = t;
+    for (int gg = lane; gg < groups; gg += 32) t += s_buf[gg * 16 + w];
+    t = warp_sum(t);
+    if (lane == 0) s_tot[w] = t;
   }
   __syncthreads();
 }
@@ -285,6 +289,22 @@ __device__ __forceinline__ void ld_win(const VT* w, int i, VT v[LD]) {
     memcpy(t, u, NB);
 #pragma unroll
     for (int s = 0; s < LD; s++) v[s] = t[s];
+  }
+}
+
+// store LD values into entry i of a shared-memory window
+template <typename VT, int LD>
+__device__ __forceinline__ void st_win(VT* w, int i, const VT v[LD]) {
+  constexpr int NB = LD * (int)sizeof(VT);
+  VT* dst = w + i * LD;
+  if constexpr (NB == 4 || NB == 8) {
+#pragma unroll
+    for (int s = 0; s < LD; s++) dst[s] = v[s];
+  } else {
+    uint4 u[NB / 16];
+    memcpy(u, v, NB);
+#pragma unroll
+    for (int k = 0; k < NB / 16; k++) reinterpret_cast<uint4*>(dst)[k] = u[k];
   }
 }
 
@@ -887,11 +907,11 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
   uint16_t* s_col = reinterpret_cast<uint16_t*>(s_halo + a.halo_cap);
   VT* s_win = reinterpret_cast<VT*>(
       s_dyn + ((4 * (size_t)(a.sp_cap + a.halo_cap) + 2 * (size_t)a.col_cap + 15) & ~(size_t)15));
+  VT* s_w = s_win + (size_t)a.win_cap * LD;  // w = A u of the own rows
   __shared__ double sh[32 * 12];
   __shared__ double s_buf[512];
   __shared__ double s_tot[16];
   __shared__ LaneState L;
-  __shared__ double s_gam[4];
   __shared__ int s_anytrig;
   __shared__ unsigned long long s_clk[8];
   constexpr int WMAX = 16;  // register-staged slices: at most WMAX entries per row
@@ -958,7 +978,7 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
           wv[s] = bcr ? ur[s] : v;
           acc[s] += (double)wv[s] * (double)ur[s];
         }
-        stv<VT, LD>(a.w, row, wv);
+        st_win<VT, LD>(s_w, (int)(row - r0), wv);
       }
     };
     if (a.reg_values) {
@@ -1171,7 +1191,8 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
 #pragma unroll
     for (int s = 0; s < 4; s++) nact += L.active[s];
     if (!nact) break;
-    // ---- P: p = u + beta p, s = w + beta s, xi += alpha p, r -= alpha s, u = D^-1 r
+    // ---- P: p = u + beta p, s = w + beta s, xi += alpha p, r -= alpha s, u = D^-1 r;
+    //         partials r.u, r.r into slots 0..7
     {
       VT al[LD], be[LD];
 #pragma unroll
@@ -1184,9 +1205,10 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
 #pragma unroll
       for (int k = 0; k < 8; k++) acc[k] = 0.0;
       FOR_OWN_ROWS {
+        const int lr = (int)(row - r0);
         VT uv[LD], wv[LD], pv[LD], sv[LD], xv[LD], rv[LD], dv[LD];
-        ld_win<VT, LD>(s_win, (int)(row - r0), uv);  // u of the own rows, last window
-        ldv_cg<VT, LD>(a.w, row, wv);
+        ld_win<VT, LD>(s_win, lr, uv);  // u of the own rows, last window
+        ld_win<VT, LD>(s_w, lr, wv);    // w = A u of the own rows, last product
         ldv_cg<VT, LD>(a.p, row, pv);
         ldv_cg<VT, LD>(a.s, row, sv);
         ldv_cg<VT, LD>(a.xi, row, xv);
@@ -1211,42 +1233,34 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
       block_partial<8>(acc, a.part, sh);
     }
     clk.lap(2);
-    ok = grid_sync(a.bar, target);
+    ok = grid_sync(a.bar, target);  // u published
     clk.lap(3);
     if (!ok) break;
-    // r.u and r.r of the new residual, kept until the w.u of the product is known
-    grid_totals<8>(a.part, s_tot, s_buf);
-    if (threadIdx.x == 0) {
-      for (int s = 0; s < S; s++) {
-        s_gam[s] = s_tot[s];
-        L.rr[s] = s_tot[4 + s];
-      }
-    }
-    // ---- W: w = A u; w.u
+    // ---- W: w = A u; w.u into slots 8..11.  The three sums are read together below.
     {
       double acc[4] = {0.0, 0.0, 0.0, 0.0};
       product(acc);
-      block_partial<4>(acc, a.part, sh);
+      block_partial<4>(acc, a.part + 8, sh);
     }
     clk.lap(0);
     ok = grid_sync(a.bar, target);
     clk.lap(1);
     if (!ok) break;
-    grid_totals<4>(a.part, s_tot, s_buf);
+    grid_totals<12>(a.part, s_tot, s_buf);
     it++;
     if (threadIdx.x == 0) {
       int any = 0;
       for (int s = 0; s < S; s++) {
         L.trigger[s] = 0;
         if (!L.active[s]) continue;
-        const double gm = s_gam[s], rr = L.rr[s], dl = s_tot[s];
+        const double gm = s_tot[s], rr = s_tot[4 + s], dl = s_tot[8 + s];
         if (!isfinite(gm) || !isfinite(rr) || !isfinite(dl)) {
           L.active[s] = 0;
           L.status[s] = TP_ERR_NONFINITE;
           L.iters[s] = it;
           continue;
         }
-        s_tot[8 + s] = dl;  // delta, kept for the coefficient update
+        L.rr[s] = rr;
         any |= (rr <= L.tol2[s]) || (a.delta2 > 0.0 && rr < a.delta2 * L.rmax2[s]);
       }
       if (any) {
@@ -1254,7 +1268,7 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
         for (int s = 0; s < S; s++) L.trigger[s] = L.active[s];
       } else {
         for (int s = 0; s < S; s++)
-          if (L.active[s]) cg_coefficients(L, s, s_gam[s], s_tot[8 + s], it);
+          if (L.active[s]) cg_coefficients(L, s, s_tot[s], s_tot[8 + s], it);
       }
       s_anytrig = any;
     }
@@ -1284,7 +1298,14 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
 #pragma unroll
         for (int k = 0; k < 12; k++) acc[k] = 0.0;
         refresh(tr, acc);
-        block_partial<12>(acc, a.part, sh);
+        block_partial<12>(acc, a.part, sh);  // slots 8..11 (b.b) are replaced by w.u
+      }
+      ok = grid_sync(a.bar, target);
+      if (!ok) break;
+      {
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        product(acc);
+        block_partial<4>(acc, a.part + 8, sh);
       }
       ok = grid_sync(a.bar, target);
       if (!ok) break;
@@ -1293,45 +1314,22 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
         n_rel++;
         for (int s = 0; s < S; s++) {
           if (!L.trigger[s]) continue;
-          const double rr = s_tot[4 + s];
-          s_gam[s] = s_tot[s];
+          L.trigger[s] = 0;
+          const double gm = s_tot[s], rr = s_tot[4 + s], dl = s_tot[8 + s];
           L.rtrue[s] = rr;
-          if (!isfinite(rr) || !isfinite(s_tot[s])) {
+          if (!isfinite(rr) || !isfinite(gm) || !isfinite(dl)) {
             L.active[s] = 0;
             L.status[s] = TP_ERR_NONFINITE;
             L.iters[s] = it;
-            L.trigger[s] = 0;
           } else if (rr <= L.tol2[s]) {
             L.active[s] = 0;
             L.status[s] = TP_OK;
             L.iters[s] = it;
-            L.trigger[s] = 0;
           } else {
             L.rr[s] = rr;
             L.rmax2[s] = rr;
+            cg_coefficients(L, s, gm, dl, it);
           }
-        }
-      }
-      __syncthreads();
-      {
-        double acc[4] = {0.0, 0.0, 0.0, 0.0};
-        product(acc);
-        block_partial<4>(acc, a.part, sh);
-      }
-      ok = grid_sync(a.bar, target);
-      if (!ok) break;
-      grid_totals<4>(a.part, s_tot, s_buf);
-      if (threadIdx.x == 0) {
-        for (int s = 0; s < S; s++) {
-          if (!L.trigger[s]) continue;
-          L.trigger[s] = 0;
-          if (!isfinite(s_tot[s])) {
-            L.active[s] = 0;
-            L.status[s] = TP_ERR_NONFINITE;
-            L.iters[s] = it;
-            continue;
-          }
-          cg_coefficients(L, s, s_gam[s], s_tot[s], it);
         }
       }
       __syncthreads();
@@ -1575,7 +1573,7 @@ static void fill_pargs(PArgs<VT>& a, const tp_csr_op* op, const tp_sell* sl, con
   a.halo_ptr = nullptr;
   a.halo = nullptr;
   a.loc_col = nullptr;
-  a.sp_cap = a.halo_cap = a.col_cap = 0;
+  a.sp_cap = a.halo_cap = a.col_cap = a.win_cap = 0;
   a.reg_values = 0;
   a.part = reinterpret_cast<double*>(p);
   p += a256(sizeof(double) * 16 * grid);
@@ -1719,7 +1717,8 @@ static int try_window(tp_pcg_handle* h, const tp_sell* sell, bool hasM, cudaStre
   if (rc != TP_OK || !ok) return rc;
   const size_t vt = h->fp32 ? 4 : 8;
   const size_t head = (4 * (size_t)(w.sp_cap + w.halo_cap) + 2 * (size_t)w.col_cap + 15) & ~(size_t)15;
-  const size_t d = head + (size_t)w.win_cap * h->ld * vt;
+  // window (own rows + halo), then w of the own rows (at most 32 per slice)
+  const size_t d = head + ((size_t)w.win_cap + 32 * (size_t)w.sp_cap) * h->ld * vt;
   void* fn = pcg_kernel(h->fp32, h->ld, 1, hasM, true);
   cudaFuncAttributes fa;
   TP_CUDA_TRY(cudaFuncGetAttributes(&fa, fn));
@@ -1750,6 +1749,7 @@ static int try_window(tp_pcg_handle* h, const tp_sell* sell, bool hasM, cudaStre
     a.sp_cap = w.sp_cap;
     a.halo_cap = w.halo_cap;
     a.col_cap = w.col_cap;
+    a.win_cap = w.win_cap;
     a.reg_values = w.max_width <= 16 ? 1 : 0;  // the kernel's register-staging width
   };
   if (h->fp32)
@@ -1795,7 +1795,7 @@ extern "C" int tp_pcg_create(const tp_csr_op* op, const tp_sell* sell, int max_i
   h->fn = pcg_kernel(h->fp32, h->ld, h->grid / sm_count(), hasM);
   const size_t vt = inner_fp32 ? 4 : 8;
   const size_t vec = a256(vt * op->ld * (size_t)op->n_rows);
-  const double d = inner_fp32 ? (delta > 0 ? delta : 0.01) : 0.0;
+  const double d = inner_fp32 ? (delta > 0 ? delta : 0.001) : 0.0;
   char* ws = static_cast<char*>(workspace);
   if (h->fp32)
     fill_pargs(h->af, op, sell, b, x, rtol, max_it, d, ws, vec, h->grid);

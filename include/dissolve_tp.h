@@ -350,7 +350,7 @@ TP_API int tp_sell_scatter(int64_t nnz, const int32_t* csr2sell, const double* c
  * barrier wait exceeds 2 s), the inner operator read in SELL-32 order, the FP64 operator
  * (Jacobi diagonal, initial / reliable-update / final residuals) in CSR.  Same stopping
  * rule and lane results as tp_cg_*.  Reliable updates (FP32 inner): when any lane's
- * recurrence residual has dropped by `delta` (<= 0 -> 0.01) since its last update, every
+ * recurrence residual has dropped by `delta` (<= 0 -> 0.001) since its last update, every
  * active lane is updated in the same FP64 sweep. */
 typedef struct tp_pcg_handle tp_pcg_handle;
 
