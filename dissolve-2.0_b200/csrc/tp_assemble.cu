@@ -472,6 +472,99 @@ __global__ void k_levelset_advance(int64_t n, double* __restrict__ phi, int ld,
     phi[i] -= dt * rate * (1.0 + gain * U[i * ld + col]);
 }
 
+
+// ----------------------------------------------------------------- film / Zn / level set
+// interface_velocity.py:90-155 (compute_effective_diffusion), per vertex:
+//   sat = clip(F / max(Fmax, 1e-20), 0, 1), ff = (1 - sat) + sat floor,
+//   De_Zn = D_Zn ff, De_s = D_s ff [phi <= 0] for Cl-, OH-, O2;
+// flags |= 1 on a non-finite result, 2 on a negative one
+__global__ void k_effective_diffusion(int64_t n, const double* __restrict__ phi,
+                                      const double* __restrict__ F, double Fmax, double floor_,
+                                      double4 d0, double* __restrict__ zn, double* __restrict__ cl,
+                                      double* __restrict__ oh, double* __restrict__ o2,
+                                      int32_t* __restrict__ flags) {
+  const double fm = fmax(Fmax, 1e-20);
+  int bad = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double x = F[i] / fm;
+    const double sat = (x < 0.0) ? 0.0 : ((x > 1.0) ? 1.0 : x);  // clip; NaN stays NaN
+    const double ff = (1.0 - sat) + sat * floor_;
+    const double med = (phi[i] <= 0.0) ? 1.0 : 0.0;
+    const double v[4] = {d0.x * ff, d0.y * ff * med, d0.z * ff * med, d0.w * ff * med};
+    double* out[4] = {zn, cl, oh, o2};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      if (!isfinite(v[k])) bad |= 1;
+      if (v[k] < 0.0) bad |= 2;
+      if (out[k]) out[k][i] = v[k];
+    }
+  }
+  if (bad) atomicOr(flags, bad);
+}
+
+// dissolve.py:746-755: medium = [phi <= 0]; alpha = medium kf (1 - F / Fmax);
+// f = medium kd F Cl^2
+__global__ void k_zn_coefficients(int64_t n, const double* __restrict__ phi,
+                                  const double* __restrict__ F, const double* __restrict__ Cl,
+                                  double kf, double kd, double Fmax, double* __restrict__ alpha,
+                                  double* __restrict__ src) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double med = (phi[i] <= 0.0) ? 1.0 : 0.0;
+    if (alpha) alpha[i] = med * kf * (1.0 - F[i] / Fmax);
+    if (src) src[i] = med * kd * F[i] * (Cl[i] * Cl[i]);
+  }
+}
+
+// mesh_utils.py:478-484: s = phi0 / sqrt(phi0^2 + eps_sign^2), 0 inside the frozen band
+// |phi0| < band (the update there is exactly zero in the reference too)
+__global__ void k_redistance_init(int64_t n, const double* __restrict__ phi, double band,
+                                  double eps_sign, double* __restrict__ s) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double p = phi[i];
+    s[i] = (fabs(p) < band) ? 0.0 : p / sqrt(p * p + eps_sign * eps_sign);
+  }
+}
+
+// mesh_utils.py:515-519: gm = sqrt(|grad|^2 + 1e-12), dtau = h/2 / max(gm, 1/2),
+// phi += dtau s (1 - gm)
+__global__ void k_redistance_update(int64_t n, double* __restrict__ phi,
+                                    const double* __restrict__ grad,
+                                    const double* __restrict__ s, double h) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double gx = grad[3 * i], gy = grad[3 * i + 1], gz = grad[3 * i + 2];
+    const double gm = sqrt(gx * gx + gy * gy + gz * gz + 1e-12);
+    const double dtau = 0.5 * h / fmax(gm, 0.5);
+    if (s[i] != 0.0) phi[i] += dtau * s[i] * (1.0 - gm);
+  }
+}
+
+// longest edge of every cell (the cell diameter of a tetrahedron), summed per block
+__global__ void k_cell_diameter(int64_t n, const int4* __restrict__ cells,
+                                const double4* __restrict__ X, double* __restrict__ part) {
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    const int4 v = cells[c];
+    const double4 p[4] = {X[v.x], X[v.y], X[v.z], X[v.w]};
+    double h2 = 0.0;
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = a + 1; b < 4; b++) {
+        const double dx = p[a].x - p[b].x, dy = p[a].y - p[b].y, dz = p[a].z - p[b].z;
+        h2 = fmax(h2, dx * dx + dy * dy + dz * dz);
+      }
+    s += sqrt(h2);
+  }
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
 __global__ void k_axpby(int64_t n, double a, const double* __restrict__ x, double b,
                         double* __restrict__ y) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
@@ -780,6 +873,84 @@ extern "C" int tp_levelset_advance(int64_t n, double* phi, int ld, const double*
   if (n == 0) return TP_OK;
   k_levelset_advance<<<grid_for(n, 256, 65535), 256, 0, as_stream(stream)>>>(n, phi, ld, U, col,
                                                                           dt, rate, gain);
+  TP_LAUNCH_CHECK();
+  return TP_OK;
+}
+
+
+extern "C" int tp_effective_diffusion(int64_t n, const double* phi, const double* F, double Fmax,
+                                      double film_floor, const double* D0, double* De_zn,
+                                      double* De_cl, double* De_oh, double* De_o2,
+                                      int32_t* flags_dev, void* stream) {
+  TP_REQUIRE(phi && F && D0 && flags_dev, "null pointer");
+  if (n == 0) return TP_OK;
+  cudaStream_t st = as_stream(stream);
+  TP_CUDA_TRY(cudaMemsetAsync(flags_dev, 0, sizeof(int32_t), st));
+  k_effective_diffusion<<<grid_for(n, 256, 65535), 256, 0, st>>>(
+      n, phi, F, Fmax, film_floor, make_double4(D0[0], D0[1], D0[2], D0[3]), De_zn, De_cl, De_oh,
+      De_o2, flags_dev);
+  TP_LAUNCH_CHECK();
+  int32_t fl = 0;
+  TP_CUDA_TRY(cudaMemcpyAsync(&fl, flags_dev, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  TP_CUDA_TRY(cudaStreamSynchronize(st));
+  if (fl & 1) {
+    set_error("effective diffusion contains NaN/Inf (check F against Fmax)");
+    return TP_ERR_NONFINITE;
+  }
+  if (fl & 2) {
+    set_error("effective diffusion has negative values (unphysical film saturation)");
+    return TP_ERR_ARG;
+  }
+  return TP_OK;
+}
+
+extern "C" int tp_zn_coefficients(int64_t n, const double* phi, const double* F, const double* Cl,
+                                  double kf, double kd, double Fmax, double* alpha, double* src,
+                                  void* stream) {
+  TP_REQUIRE(phi && F && (Cl || !src), "null pointer");
+  if (n == 0) return TP_OK;
+  k_zn_coefficients<<<grid_for(n, 256, 65535), 256, 0, as_stream(stream)>>>(n, phi, F, Cl, kf, kd,
+                                                                         Fmax, alpha, src);
+  TP_LAUNCH_CHECK();
+  return TP_OK;
+}
+
+extern "C" size_t tp_redistance_scratch_bytes(int64_t n_verts) {
+  return sizeof(double) * 4 * (size_t)n_verts;
+}
+
+extern "C" int tp_redistance(const tp_mesh* m, double* phi, int iters, double h_avg,
+                             double band_factor, double eps_factor, void* scratch,
+                             void* stream) {
+  TP_REQUIRE(mesh_ok(m) && m->coords4 && phi && scratch, "null pointer");
+  TP_REQUIRE(iters >= 0 && h_avg > 0.0, "bad redistancing parameters");
+  if (m->n_verts == 0) return TP_OK;
+  cudaStream_t st = as_stream(stream);
+  double* grad = static_cast<double*>(scratch);
+  double* s = grad + 3 * m->n_verts;
+  const int g = grid_for(m->n_verts, 256, 65535);
+  k_redistance_init<<<g, 256, 0, st>>>(m->n_verts, phi, band_factor * h_avg, eps_factor * h_avg, s);
+  TP_LAUNCH_CHECK();
+  for (int k = 0; k < iters; k++) {
+    const int rc = tp_nodal_gradient(m, nullptr, phi, grad, stream);
+    if (rc != TP_OK) return rc;
+    k_redistance_update<<<g, 256, 0, st>>>(m->n_verts, phi, grad, s, h_avg);
+    TP_LAUNCH_CHECK();
+  }
+  return TP_OK;
+}
+
+extern "C" int tp_mean_cell_diameter(const tp_mesh* m, double* out_dev, void* scratch,
+                                     void* stream) {
+  TP_REQUIRE(mesh_ok(m) && m->coords4 && out_dev && scratch, "null pointer");
+  if (m->n_cells == 0) return TP_OK;
+  cudaStream_t st = as_stream(stream);
+  const int grid = grid_for(m->n_cells, 256, 1024);
+  double* part = static_cast<double*>(scratch);
+  k_cell_diameter<<<grid, 256, 0, st>>>(m->n_cells, reinterpret_cast<const int4*>(m->cells),
+                                        reinterpret_cast<const double4*>(m->coords4), part);
+  TP_LAUNCH_CHECK();
+  k_sum_parts<<<1, 256, 0, st>>>(grid, part, out_dev);  // the sum; the caller divides by n
   TP_LAUNCH_CHECK();
   return TP_OK;
 }

@@ -115,6 +115,14 @@ SIGNATURES = {
     "tp_cell_average_col": (ctypes.c_int, [_c_i64, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
     "tp_levelset_advance": (ctypes.c_int, [_c_i64, _vp, ctypes.c_int, _vp, ctypes.c_int, _c_dbl,
                                            _c_dbl, _c_dbl, _vp]),
+    "tp_effective_diffusion": (ctypes.c_int, [_c_i64, _vp, _vp, _c_dbl, _c_dbl, _vp, _vp, _vp, _vp,
+                                              _vp, _vp, _vp]),
+    "tp_zn_coefficients": (ctypes.c_int, [_c_i64, _vp, _vp, _vp, _c_dbl, _c_dbl, _c_dbl, _vp, _vp,
+                                          _vp]),
+    "tp_redistance_scratch_bytes": (ctypes.c_size_t, [_c_i64]),
+    "tp_redistance": (ctypes.c_int, [_P(TpMesh), _vp, ctypes.c_int, _c_dbl, _c_dbl, _c_dbl, _vp,
+                                     _vp]),
+    "tp_mean_cell_diameter": (ctypes.c_int, [_P(TpMesh), _vp, _vp, _vp]),
     "tp_axpby": (ctypes.c_int, [_c_i64, _c_dbl, _vp, _c_dbl, _vp, _vp]),
     "tp_pack_columns": (ctypes.c_int, [_c_i64, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
     "tp_unpack_columns": (ctypes.c_int, [_c_i64, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),

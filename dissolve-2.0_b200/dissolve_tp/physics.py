@@ -1,0 +1,73 @@
+"""Per-vertex builders around the transport step, on the GPU (the CuPy/numpy element-wise
+code of the reference's time loop): effective film diffusivity, Zn transport
+coefficients, Sussman redistancing of the level set and the mean cell diameter."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import call
+from .device import ptr, stream_handle, to_device
+
+
+def film_floor(porosity: float = 0.25, constrictivity: float = 1.0,
+               tortuosity: float = 2.0) -> float:
+    """eps delta / tau^2 (physics/interface_velocity.py:118-127; parameters.py:119-121)."""
+    return porosity * constrictivity / (tortuosity * tortuosity)
+
+
+def effective_diffusion(phi, F, Fmax, D0=(2.72, 7.78, 20.16, 9.36), floor=None):
+    """(De_Zn, De_Cl, De_OH, De_O2) per vertex (compute_effective_diffusion,
+    interface_velocity.py:90-155); raises like the reference on NaN/Inf or negatives."""
+    phi_d = to_device(phi, torch.float64, torch.device("cuda"))
+    dev = phi_d.device
+    F_d = to_device(F, torch.float64, dev)
+    n = int(phi_d.numel())
+    out = [torch.empty(n, dtype=torch.float64, device=dev) for _ in range(4)]
+    flags = torch.zeros(1, dtype=torch.int32, device=dev)
+    d0 = (ctypes.c_double * 4)(*[float(v) for v in D0])
+    fl = film_floor() if floor is None else float(floor)
+    rc = _lib.lib.tp_effective_diffusion(n, ptr(phi_d), ptr(F_d), float(Fmax), fl, d0,
+                                         *(ptr(o) for o in out), ptr(flags), stream_handle())
+    if rc != _lib.TP_OK:
+        raise RuntimeError(f"[bounds] {_lib.last_error()}")
+    return tuple(out)
+
+
+def zn_coefficients(phi, F, Cl, kf, kd, Fmax):
+    """(alpha, source) of the Zn transport (dissolve.py:746-755) and the scaffold
+    Dirichlet dofs phi > 0 (dissolve.py:745) as an int32 numpy array."""
+    phi_d = to_device(phi, torch.float64, torch.device("cuda"))
+    dev = phi_d.device
+    n = int(phi_d.numel())
+    alpha = torch.empty(n, dtype=torch.float64, device=dev)
+    src = torch.empty(n, dtype=torch.float64, device=dev)
+    # keep the device copies referenced until the kernel has been enqueued
+    F_d, Cl_d = to_device(F, torch.float64, dev), to_device(Cl, torch.float64, dev)
+    call("tp_zn_coefficients", n, ptr(phi_d), ptr(F_d), ptr(Cl_d), float(kf), float(kd),
+         float(Fmax), ptr(alpha), ptr(src), stream_handle())
+    scaffold = np.nonzero(phi_d.cpu().numpy() > 0.0)[0].astype(np.int32)
+    return alpha, src, scaffold
+
+
+def mean_cell_diameter(dm) -> float:
+    """h_avg of a DeviceMesh (domain/mesh_utils.py:559-575)."""
+    out = torch.zeros(1, dtype=torch.float64, device=dm.device)
+    scratch = torch.empty(1024, dtype=torch.float64, device=dm.device)
+    call("tp_mean_cell_diameter", ctypes.byref(dm.tpm), ptr(out), ptr(scratch), stream_handle())
+    return float(out.item()) / dm.n_cells
+
+
+def redistance(dm, phi: torch.Tensor, num_iters: int = 8, h_avg: float | None = None,
+               band_factor: float = 3.0, eps_factor: float = 1.5) -> torch.Tensor:
+    """Sussman redistancing of phi (device, in place) on a DeviceMesh
+    (domain/mesh_utils.py:450-542, GPU branch)."""
+    h = mean_cell_diameter(dm) if h_avg is None else float(h_avg)
+    scratch = torch.empty(int(_lib.lib.tp_redistance_scratch_bytes(dm.n_verts)) // 8,
+                          dtype=torch.float64, device=dm.device)
+    call("tp_redistance", ctypes.byref(dm.tpm), ptr(phi), int(num_iters), h, float(band_factor),
+         float(eps_factor), ptr(scratch), stream_handle())
+    return phi

@@ -207,6 +207,40 @@ TP_API int tp_interface_terms(int64_t n, const double* phi, const double* grad, 
 TP_API int tp_cell_average_col(int64_t n_cells, const int32_t* cells, const double* vert_vals,
                                int ld, int col, double* out, void* stream);
 
+/* [sync] physics/interface_velocity.py:90-155 (compute_effective_diffusion) per vertex:
+ * sat = clip(F / max(Fmax, 1e-20), 0, 1), ff = (1 - sat) + sat film_floor
+ * (film_floor = porosity constrictivity / tortuosity^2); De_Zn = D0[0] ff and, where
+ * phi <= 0 (medium), De_Cl/OH/O2 = D0[1..3] ff (0 in the scaffold).  Any output may be
+ * NULL.  TP_ERR_NONFINITE on NaN/Inf, TP_ERR_ARG on a negative value (the reference's
+ * RuntimeErrors).  flags_dev: 1 int32 of device scratch. */
+TP_API int tp_effective_diffusion(int64_t n, const double* phi, const double* F, double Fmax,
+                                  double film_floor, const double* D0 /* host, 4 */,
+                                  double* De_zn, double* De_cl, double* De_oh, double* De_o2,
+                                  int32_t* flags_dev, void* stream);
+
+/* dissolve.py:746-755, Zn transport coefficients per vertex: medium = [phi <= 0],
+ * alpha = medium kf (1 - F / Fmax), src = medium kd F Cl^2 (either output may be NULL).
+ * The scaffold vertices (phi > 0) are the Dirichlet set of the Zn solve (dissolve.py:
+ * 745, 764-770). */
+TP_API int tp_zn_coefficients(int64_t n, const double* phi, const double* F, const double* Cl,
+                              double kf, double kd, double Fmax, double* alpha, double* src,
+                              void* stream);
+
+/* domain/mesh_utils.py:450-542 (redistance, GPU branch): `iters` Sussman pseudo-time steps
+ * psi += dtau sign(phi0) (1 - |grad psi|), sign(phi0) = phi0 / sqrt(phi0^2 + (eps_factor
+ * h_avg)^2), dtau = h_avg / 2 / max(|grad psi|, 1/2), nodes with |phi0| < band_factor h_avg
+ * frozen; |grad psi| from tp_nodal_gradient (volume-weighted, coords4).  In place on phi.
+ * scratch >= tp_redistance_scratch_bytes(n_verts).  The reference uses band_factor 3 and
+ * eps_factor 1.5. */
+TP_API size_t tp_redistance_scratch_bytes(int64_t n_verts);
+TP_API int tp_redistance(const tp_mesh* m, double* phi, int iters, double h_avg,
+                         double band_factor, double eps_factor, void* scratch, void* stream);
+
+/* Sum over cells of the cell diameter (longest edge), into out_dev (1 double); divided by
+ * n_cells it is the h_avg of domain/mesh_utils.py:559-575 (dolfinx mesh.h).
+ * scratch >= 1024 doubles. */
+TP_API int tp_mean_cell_diameter(const tp_mesh* m, double* out_dev, void* scratch, void* stream);
+
 /* Level-set update phi -= dt rate (1 + gain U[:, col]) (the algebraic part of the
  * level-set step, dissolve.py:684-730, with the configured dissolution law). */
 TP_API int tp_levelset_advance(int64_t n, double* phi, int ld, const double* U, int col,

@@ -270,6 +270,45 @@ def levelset_advance(phi, U, col, dt, rate, gain):
     """phi - dt rate (1 + gain U[:, col])."""
     return phi - dt * rate * (1.0 + gain * U[:, col])
 
+
+def effective_diffusion(phi, F, Fmax, film_floor, D0):
+    """physics/interface_velocity.py:90-155: (De_Zn, De_Cl, De_OH, De_O2)."""
+    fm = max(Fmax, 1e-20)
+    sat = np.clip(F / fm, 0.0, 1.0)
+    ff = (1.0 - sat) + sat * film_floor
+    med = np.where(phi <= 0.0, 1.0, 0.0)
+    return D0[0] * ff, D0[1] * ff * med, D0[2] * ff * med, D0[3] * ff * med
+
+
+def zn_coefficients(phi, F, Cl, kf, kd, Fmax):
+    """dissolve.py:746-755: alpha and source of the Zn transport."""
+    med = np.where(phi <= 0.0, 1.0, 0.0)
+    return med * kf * (1.0 - F / Fmax), med * kd * F * (Cl * Cl)
+
+
+def mean_cell_diameter(coords, cells):
+    """domain/mesh_utils.py:559-575 (dolfinx mesh.h of a tetrahedron: longest edge)."""
+    p = coords[cells]
+    h2 = np.zeros(cells.shape[0])
+    for a in range(4):
+        for b in range(a + 1, 4):
+            h2 = np.maximum(h2, ((p[:, a] - p[:, b]) ** 2).sum(axis=1))
+    return float(np.sqrt(h2).mean())
+
+
+def redistance(cells, detJ, JinvT, phi, iters, h_avg, band_factor=3.0, eps_factor=1.5):
+    """domain/mesh_utils.py:450-542: Sussman pseudo-time steps with the frozen band."""
+    phi = np.array(phi, dtype=np.float64)
+    mask = np.abs(phi) < band_factor * h_avg
+    eps = eps_factor * h_avg
+    sign = phi / np.sqrt(phi ** 2 + eps ** 2)
+    for _ in range(iters):
+        g = nodal_gradient(cells, detJ, JinvT, phi)
+        gm = np.sqrt(g[:, 0] ** 2 + g[:, 1] ** 2 + g[:, 2] ** 2 + 1e-12)
+        dtau = 0.5 * h_avg / np.maximum(gm, 0.5)
+        phi = phi + np.where(mask, 0.0, dtau * sign * (1.0 - gm))
+    return phi
+
 def under_relax(u_new, u_old, omega):
     """numerics/solvers.py:278-279."""
     return omega * u_new + (1.0 - omega) * u_old
