@@ -221,9 +221,17 @@ class BatchedTransport:
         return out
 
     def step(self, sync=True):
+        self.step_operator()
+        return self.step_state(sync)
+
+    def step_operator(self):
+        """The part of a step that does not read the state: the operator."""
         self.assemble_operator()
         if self.engine == "persistent":
             self.solver.refresh_values()
+
+    def step_state(self, sync=True):
+        """The rest of a step: right-hand sides, initial guess, solve, state update."""
         self.assemble_rhs()
         self.initial_guess()
         self.solver.run()
@@ -253,9 +261,19 @@ class BatchedTransport:
         n = self.U.shape[0]
         if getattr(self, "_stage", None) is None:
             self._stage = torch.empty((n, self.S), dtype=torch.float64, device=self.device)
+            self._copy_stream = torch.cuda.Stream(device=self.device)
+            self._copied = torch.cuda.Event()
+        main = torch.cuda.current_stream(self.device)
+        # the H2D copy overlaps the operator assembly, which does not read the state
+        self._copy_stream.wait_stream(main)
+        with torch.cuda.stream(self._copy_stream):
+            self._stage.copy_(u_host, non_blocking=True)
+            self._copied.record()
+        self._stage.record_stream(self._copy_stream)
+        self.step_operator()
+        main.wait_event(self._copied)
         st = stream_handle()
-        self._stage.copy_(u_host, non_blocking=True)
         call("tp_pack_columns", n, self.S, self.ld, ptr(self._stage), ptr(self.U), st)
-        self.step(sync=False)
+        self.step_state(sync=False)
         call("tp_unpack_columns", n, self.S, self.ld, ptr(self.U), ptr(self._stage), st)
         out_host.copy_(self._stage, non_blocking=True)
