@@ -206,10 +206,10 @@ def run_ours(args, rank, world, local_rank):
     window = fast.cg_config.get("form", "").startswith("window")
     if window:
         # window engine, per iteration: FP32 value per nonzero (columns stay in shared
-        # memory for the whole solve) and 14 passes of (V, 4) FP32: u read once into the
-        # windows; P reads w, p, s, xi, r, D^-1 and writes p, s, xi, r, u; the product
-        # writes w and reads the row diagonal
-        bytes_it = nnz * 4 + 14 * nv * 16
+        # memory for the whole solve) and 12 passes of (V, 4) FP32: u read once into the
+        # windows; P reads p, s, xi, r, D^-1 and writes p, s, xi, r, u; the product reads
+        # the row diagonal (w = A u of the own rows stays in shared memory)
+        bytes_it = nnz * 4 + 12 * nv * 16
         kernel = ("k_cgw<float,4> (persistent 3-column Jacobi-PCG, Chronopoulos-Gear form, "
                   "shared-memory windows, one cooperative launch per solve)")
     else:

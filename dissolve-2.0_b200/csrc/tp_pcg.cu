@@ -192,6 +192,9 @@ __device__ __forceinline__ bool grid_sync(PBar* bar, unsigned int& target) {
 }
 
 // Sum NV slots of every CTA's partial row (fixed order); result in s_tot for all threads.
+// Thread (group g, slot k) adds the partials of CTAs g, g + groups, ... (a half-warp reads
+// one CTA's 16 slots: one 128-byte line), then warp k sums slot k over the groups with a
+// fixed shuffle tree; every CTA computes the same bits.
 template <int NV>
 __device__ __forceinline__ void grid_totals(const double* part, double* s_tot, double* s_buf) {
   const int T = blockDim.x;
@@ -202,7 +205,6 @@ __device__ __forceinline__ void grid_totals(const double* part, double* s_tot, d
     for (int b = g; b < (int)gridDim.x; b += groups) v += __ldcg(part + (int64_t)b * 16 + k);
   s_buf[threadIdx.x] = v;
   __syncthreads();
-  // warp w < NV sums slot w over the groups with a fixed shuffle tree
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (w < NV) {
     double t = 0.0;
@@ -1248,30 +1250,33 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
     if (!ok) break;
     grid_totals<12>(a.part, s_tot, s_buf);
     it++;
-    if (threadIdx.x == 0) {
-      int any = 0;
-      for (int s = 0; s < S; s++) {
-        L.trigger[s] = 0;
-        if (!L.active[s]) continue;
+    // lanes in parallel: thread s owns lane s
+    int trig = 0;
+    if (threadIdx.x < S) {
+      const int s = threadIdx.x;
+      L.trigger[s] = 0;
+      if (L.active[s]) {
         const double gm = s_tot[s], rr = s_tot[4 + s], dl = s_tot[8 + s];
         if (!isfinite(gm) || !isfinite(rr) || !isfinite(dl)) {
           L.active[s] = 0;
           L.status[s] = TP_ERR_NONFINITE;
           L.iters[s] = it;
-          continue;
+        } else {
+          L.rr[s] = rr;
+          trig = (rr <= L.tol2[s]) || (a.delta2 > 0.0 && rr < a.delta2 * L.rmax2[s]);
         }
-        L.rr[s] = rr;
-        any |= (rr <= L.tol2[s]) || (a.delta2 > 0.0 && rr < a.delta2 * L.rmax2[s]);
       }
-      if (any) {
-        // one FP64 sweep refreshes every active lane
-        for (int s = 0; s < S; s++) L.trigger[s] = L.active[s];
-      } else {
-        for (int s = 0; s < S; s++)
-          if (L.active[s]) cg_coefficients(L, s, s_tot[s], s_tot[8 + s], it);
-      }
-      s_anytrig = any;
     }
+    // one FP64 sweep refreshes every active lane when any lane asks for it
+    const int any = __syncthreads_or(trig);
+    if (threadIdx.x < S && L.active[threadIdx.x]) {
+      const int s = threadIdx.x;
+      if (any)
+        L.trigger[s] = 1;
+      else
+        cg_coefficients(L, s, s_tot[s], s_tot[8 + s], it);
+    }
+    if (threadIdx.x == 0) s_anytrig = any;
     __syncthreads();
     clk.lap(4);  // scalar updates
     if (s_anytrig) {
