@@ -340,17 +340,30 @@ __device__ __forceinline__ void csr64_residual(const PArgs<VT>& a, int64_t row, 
 #pragma unroll
     for (int s = 0; s < LD; s++) ak[s] = am[s] = 0.0;
     const int beg = a.A64.indptr[row], end = a.A64.indptr[row + 1];
-    for (int p = beg; p < end; p++) {
-      const int j = __ldg(a.A64.indices + p);
-      double xv[LD];
-      ldv_cg<double, LD>(a.x, j, xv);
-      const double kv = __ldg(a.A64.K + p);
+    // RP entries at a time: their index, value and x loads are in flight together; the
+    // sums still run entry by entry in CSR order
+    constexpr int RP = (LD == 4) ? 2 : 4;
+    for (int p0 = beg; p0 < end; p0 += RP) {
+      int jj[RP];
+      double kv[RP], mv[RP], xv[RP][LD];
 #pragma unroll
-      for (int s = 0; s < LD; s++) ak[s] += kv * xv[s];
-      if (a.A64.M) {
-        const double mv = __ldg(a.A64.M + p);
+      for (int u = 0; u < RP; u++) {
+        const bool in = p0 + u < end;
+        jj[u] = in ? __ldg(a.A64.indices + p0 + u) : (int)row;
+        kv[u] = in ? __ldg(a.A64.K + p0 + u) : 0.0;
+        mv[u] = (in && a.A64.M) ? __ldg(a.A64.M + p0 + u) : 0.0;
+      }
 #pragma unroll
-        for (int s = 0; s < LD; s++) am[s] += mv * xv[s];
+      for (int u = 0; u < RP; u++) ldv_cg<double, LD>(a.x, jj[u], xv[u]);
+#pragma unroll
+      for (int u = 0; u < RP; u++) {
+        if (p0 + u >= end) break;
+#pragma unroll
+        for (int s = 0; s < LD; s++) ak[s] += kv[u] * xv[u][s];
+        if (a.A64.M) {
+#pragma unroll
+          for (int s = 0; s < LD; s++) am[s] += mv[u] * xv[u][s];
+        }
       }
     }
     double dr[LD];
@@ -1206,16 +1219,27 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
       double acc[8];
 #pragma unroll
       for (int k = 0; k < 8; k++) acc[k] = 0.0;
-      FOR_OWN_ROWS {
+      // distinct arrays: declared non-aliasing so loads of the next row may be issued
+      // before the stores of this one
+      VT* __restrict__ pP = a.p;
+      VT* __restrict__ pS = a.s;
+      VT* __restrict__ pX = a.xi;
+      VT* __restrict__ pR = a.r;
+      VT* __restrict__ pU = a.u;
+      const VT* __restrict__ pD = a.dinv;
+#pragma unroll 2
+      for (int sl = sb + warp; sl < se; sl += nwarps) {
+        const int64_t row = (int64_t)sl * 32 + lane;
+        if (row >= a.n) continue;
         const int lr = (int)(row - r0);
         VT uv[LD], wv[LD], pv[LD], sv[LD], xv[LD], rv[LD], dv[LD];
+        ldv_cg<VT, LD>(pP, row, pv);
+        ldv_cg<VT, LD>(pS, row, sv);
+        ldv_cg<VT, LD>(pX, row, xv);
+        ldv_cg<VT, LD>(pR, row, rv);
+        ldv_cg<VT, LD>(pD, row, dv);
         ld_win<VT, LD>(s_win, lr, uv);  // u of the own rows, last window
         ld_win<VT, LD>(s_w, lr, wv);    // w = A u of the own rows, last product
-        ldv_cg<VT, LD>(a.p, row, pv);
-        ldv_cg<VT, LD>(a.s, row, sv);
-        ldv_cg<VT, LD>(a.xi, row, xv);
-        ldv_cg<VT, LD>(a.r, row, rv);
-        ldv_cg<VT, LD>(a.dinv, row, dv);
 #pragma unroll
         for (int s = 0; s < LD; s++) {
           pv[s] = uv[s] + be[s] * pv[s];
@@ -1226,11 +1250,11 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
           acc[s] += (double)rv[s] * (double)uv[s];
           acc[4 + s] += (double)rv[s] * (double)rv[s];
         }
-        stv<VT, LD>(a.p, row, pv);
-        stv<VT, LD>(a.s, row, sv);
-        stv<VT, LD>(a.xi, row, xv);
-        stv<VT, LD>(a.r, row, rv);
-        stv<VT, LD>(a.u, row, uv);
+        stv<VT, LD>(pP, row, pv);
+        stv<VT, LD>(pS, row, sv);
+        stv<VT, LD>(pX, row, xv);
+        stv<VT, LD>(pR, row, rv);
+        stv<VT, LD>(pU, row, uv);
       }
       block_partial<8>(acc, a.part, sh);
     }
