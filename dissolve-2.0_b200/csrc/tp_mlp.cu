@@ -1,10 +1,12 @@
 // tp_mlp.cu -- per-vertex MLP that predicts the next backward-Euler state (the Krylov
 // initial guess), BF16 on the tensor cores with FP32 accumulation.
 //
-// Network: 16 inputs (8 used) -> 64 -> ReLU -> 64 -> ReLU -> 1, one network shared by
+// Network: 16 inputs (10 used) -> 64 -> ReLU -> 64 -> ReLU -> 1, one network shared by
 // all species; a row is one (vertex, species) pair.  Features (normalised by per-input
 // affine maps fixed at training time):
-//   0 phi, 1 |grad phi|, 2 u^n, 3 u^{n-1}, 4 u^n - u^{n-1}, 5 log D_s, 6 k_s, 7 1
+//   0 phi, 1 |grad phi|, 2 u^n, 3 u^{n-1}, 4 u^n - u^{n-1}, 5 log D_s, 6 k_s, 7 1,
+//   8 (D_s K u^n)_v, 9 (D_s K (u^n - u^{n-1}))_v -- the stiffness images give the
+//   network the local curvature that decides how fast each part of the change decays
 // The output y predicts (u^{n+1} - u^n) / sigma; the guess is u^n + sigma y.
 //
 // Tensor-core fragments are those of mma.sync.m16n8k16 (row.col, bf16 x bf16 -> f32):
@@ -31,14 +33,18 @@ constexpr int OFF_W3 = OFF_B2 + MLP_H;           // [64]
 constexpr int OFF_B3 = OFF_W3 + MLP_H;           // [1]
 constexpr int MLP_P = OFF_B3 + 1;
 
+constexpr int NFEAT = 10;  // used inputs: 0..6 fields, 7 bias, 8..9 operator images
+
 struct MlpFeat {
   const double* U;      // (V, ld) u^n
   const double* Up;     // (V, ld) u^{n-1}
   const double* phi;    // (V) or NULL
   const double* ngphi;  // (V) or NULL
+  const double* opU;    // (V, ld) D_s K u^n or NULL
+  const double* opDU;   // (V, ld) D_s K (u^n - u^{n-1}) or NULL
   int S, ld;
   float logD[4], k[4];
-  float mean[8], istd[8];
+  float mean[NFEAT], istd[NFEAT];
 };
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
@@ -57,7 +63,7 @@ __device__ __forceinline__ void mma_bf16(float c[4], uint32_t a0, uint32_t a1, u
 
 // normalised feature f (0..15) of row r = v * S + s
 __device__ __forceinline__ float feature(const MlpFeat& F, int64_t r, int f) {
-  if (f >= 8) return 0.0f;
+  if (f >= NFEAT) return 0.0f;
   const int64_t v = r / F.S;
   const int s = (int)(r - v * F.S);
   float x;
@@ -69,7 +75,9 @@ __device__ __forceinline__ float feature(const MlpFeat& F, int64_t r, int f) {
     case 4: x = (float)(F.U[v * F.ld + s] - F.Up[v * F.ld + s]); break;
     case 5: x = F.logD[s]; break;
     case 6: x = F.k[s]; break;
-    default: return 1.0f;
+    case 7: return 1.0f;
+    case 8: x = F.opU ? (float)F.opU[v * F.ld + s] : 0.0f; break;
+    default: x = F.opDU ? (float)F.opDU[v * F.ld + s] : 0.0f; break;
   }
   return (x - F.mean[f]) * F.istd[f];
 }
@@ -483,13 +491,15 @@ static MlpFeat make_feat(const tp_mlp_inputs* in) {
   F.Up = in->U_prev;
   F.phi = in->phi;
   F.ngphi = in->normgradphi;
+  F.opU = in->opU;
+  F.opDU = in->opDU;
   F.S = in->S;
   F.ld = in->ld;
   for (int s = 0; s < 4; s++) {
     F.logD[s] = (float)in->logD[s];
     F.k[s] = (float)in->k[s];
   }
-  for (int f = 0; f < 8; f++) {
+  for (int f = 0; f < NFEAT; f++) {
     F.mean[f] = (float)in->mean[f];
     F.istd[f] = (float)in->istd[f];
   }

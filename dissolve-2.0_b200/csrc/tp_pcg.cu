@@ -1824,7 +1824,7 @@ extern "C" int tp_pcg_create(const tp_csr_op* op, const tp_sell* sell, int max_i
   h->fn = pcg_kernel(h->fp32, h->ld, h->grid / sm_count(), hasM);
   const size_t vt = inner_fp32 ? 4 : 8;
   const size_t vec = a256(vt * op->ld * (size_t)op->n_rows);
-  const double d = inner_fp32 ? (delta > 0 ? delta : 0.001) : 0.0;
+  const double d = inner_fp32 ? (delta > 0 ? delta : 0.01) : 0.0;
   char* ws = static_cast<char*>(workspace);
   if (h->fp32)
     fill_pargs(h->af, op, sell, b, x, rtol, max_it, d, ws, vec, h->grid);

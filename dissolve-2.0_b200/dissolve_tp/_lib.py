@@ -69,8 +69,9 @@ class TpSell(ctypes.Structure):
 
 class TpMlpInputs(ctypes.Structure):
     _fields_ = [("n_verts", _c_i64), ("S", _c_i32), ("ld", _c_i32), ("U", _vp), ("U_prev", _vp),
-                ("phi", _vp), ("normgradphi", _vp), ("logD", _c_dbl * 4), ("k", _c_dbl * 4),
-                ("mean", _c_dbl * 8), ("istd", _c_dbl * 8)]
+                ("phi", _vp), ("normgradphi", _vp), ("opU", _vp), ("opDU", _vp),
+                ("logD", _c_dbl * 4), ("k", _c_dbl * 4), ("mean", _c_dbl * 10),
+                ("istd", _c_dbl * 10)]
 
 
 class TpCgResult(ctypes.Structure):

@@ -126,19 +126,21 @@ class GyroidStep:
         for i in range(steps):
             keep = (i % every == every - 1) and tr.steps_done >= 1
             if keep:
-                # the step's inputs: u^{n-1}, u^n and the phi its coefficients use
+                # the step's inputs: u^{n-1}, u^n, their stiffness images and the phi its
+                # coefficients use
                 up, un, ph = tr.U_prev.clone(), tr.U.clone(), self.phi.clone()
+                op = tr.operator_images(un, up, fresh=True)
             res = self.step()
             results.append(res)
             if not res["converged"]:
                 raise RuntimeError(f"training trajectory did not converge at step {i}: {res}")
             if keep:
-                samples.append((up, un, tr.U.clone(), ph, self.ngphi.clone()))
+                samples.append((up, un, tr.U.clone(), ph, self.ngphi.clone(), op))
         mlp = WarmStartMLP(self.device, seed=seed)
         mlp.fit_normalization([s[:3] for s in samples], tr.S, tr.D, tr.k, samples[-1][3],
-                              samples[-1][4])
+                              samples[-1][4], ops=[s[5] for s in samples])
         for s in samples:
-            mlp.add_pairs([s[:3]], tr.S, tr.ld, tr.D, tr.k, s[3], s[4])
+            mlp.add_pairs([s[:3]], tr.S, tr.ld, tr.D, tr.k, s[3], s[4], ops=[s[5]])
         log = mlp.train(steps=epochs, log_every=100 if verbose else 0)
         if verbose:
             print("mlp training loss", log)

@@ -175,7 +175,7 @@ class PersistentCG:
     (tp_pcg_*).  The inner operator is read in SELL-32 order: call refresh_values() after the
     CSR values change (it scatters them)."""
 
-    def __init__(self, op: CsrOperator, rtol=1e-8, max_it=1000, inner_fp32=False, delta=0.001,
+    def __init__(self, op: CsrOperator, rtol=1e-8, max_it=1000, inner_fp32=False, delta=0.01,
                  sell: SellPattern | None = None, ctas_per_sm: int = 0):
         from ._lib import TpSell
         if op.n_systems != 1:

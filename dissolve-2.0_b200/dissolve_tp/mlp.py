@@ -20,6 +20,7 @@ from ._lib import TpMlpInputs, call
 from .device import ptr, stream_handle
 
 H, IN = 64, 16
+NFEAT = 10  # used inputs: fields 0..6, bias 7, stiffness images 8..9
 P = H * IN + H + H * H + H + H + 1
 OFF_W1, OFF_B1 = 0, H * IN
 OFF_W2, OFF_B2 = OFF_B1 + H, OFF_B1 + H + H * H
@@ -29,8 +30,8 @@ OFF_W3, OFF_B3 = OFF_B2 + H, OFF_B2 + 2 * H
 def initial_params(seed: int = 3) -> np.ndarray:
     rng = np.random.default_rng(seed)
     p = np.zeros(P, dtype=np.float32)
-    w1 = rng.normal(0, np.sqrt(2.0 / 8), (H, IN))
-    w1[:, 8:] = 0.0
+    w1 = rng.normal(0, np.sqrt(2.0 / NFEAT), (H, IN))
+    w1[:, NFEAT:] = 0.0
     p[OFF_W1:OFF_B1] = w1.reshape(-1)
     p[OFF_W2:OFF_B2] = rng.normal(0, np.sqrt(2.0 / H), H * H)
     p[OFF_W3:OFF_B3] = rng.normal(0, 0.1 / np.sqrt(H), H)
@@ -46,8 +47,8 @@ class WarmStartMLP:
         self.m = torch.zeros(P, dtype=torch.float32, device=device)
         self.v = torch.zeros(P, dtype=torch.float32, device=device)
         self.step = 0
-        self.mean = np.zeros(8)
-        self.istd = np.ones(8)
+        self.mean = np.zeros(NFEAT)
+        self.istd = np.ones(NFEAT)
         self.sigma = 1.0
         self.grid = grid or 2 * int(_lib.lib.tp_device_sm_count())
         self.ws = torch.empty(int(_lib.lib.tp_mlp_grad_workspace_floats(self.grid)),
@@ -60,30 +61,37 @@ class WarmStartMLP:
         self.launches = 1
 
     # ---- inputs -----------------------------------------------------------------
-    def inputs(self, U, Up, S, ld, D, k, phi=None, ngphi=None) -> TpMlpInputs:
+    def inputs(self, U, Up, S, ld, D, k, phi=None, ngphi=None, ops=None) -> TpMlpInputs:
         st = TpMlpInputs()
         st.n_verts = int(U.shape[0])
         st.S, st.ld = int(S), int(ld)
         st.U, st.U_prev = ptr(U), ptr(Up)
         st.phi, st.normgradphi = ptr(phi), ptr(ngphi)
+        opU, opDU = ops if ops is not None else (None, None)
+        st.opU, st.opDU = ptr(opU), ptr(opDU)
         for s in range(S):
             st.logD[s] = math.log(float(D[s]))
             st.k[s] = float(k[s])
-        for f in range(8):
+        for f in range(NFEAT):
             st.mean[f] = float(self.mean[f])
             st.istd[f] = float(self.istd[f])
-        self._keep = (U, Up, phi, ngphi)
+        self._keep = (U, Up, phi, ngphi, opU, opDU)
         return st
 
-    def fit_normalization(self, pairs, S, D, k, phi=None, ngphi=None):
-        """Input/target scales from training pairs [(U_prev, U_n, U_next)] (device)."""
+    def fit_normalization(self, pairs, S, D, k, phi=None, ngphi=None, ops=None):
+        """Input/target scales from training pairs [(U_prev, U_n, U_next)] (device) and,
+        when given, their stiffness images ops [(opU, opDU)]."""
         up = np.concatenate([p[0][:, :S].cpu().numpy().reshape(-1) for p in pairs])
         un = np.concatenate([p[1][:, :S].cpu().numpy().reshape(-1) for p in pairs])
         nx = np.concatenate([p[2][:, :S].cpu().numpy().reshape(-1) for p in pairs])
         du, tg = un - up, nx - un
         raw = [np.zeros(1) if phi is None else phi.cpu().numpy(),
                np.zeros(1) if ngphi is None else ngphi.cpu().numpy(), un, up, du,
-               np.log(np.asarray(D, dtype=np.float64)), np.asarray(k, dtype=np.float64)]
+               np.log(np.asarray(D, dtype=np.float64)), np.asarray(k, dtype=np.float64),
+               np.zeros(1)]
+        for j in range(2):
+            raw.append(np.zeros(1) if ops is None else
+                       np.concatenate([o[j][:, :S].cpu().numpy().reshape(-1) for o in ops]))
         for f, r in enumerate(raw):
             self.mean[f] = float(np.mean(r))
             sd = float(np.std(r))
@@ -91,7 +99,7 @@ class WarmStartMLP:
         self.mean[7], self.istd[7] = 0.0, 1.0
         self.sigma = float(np.std(tg)) if np.std(tg) > 0 else 1.0
 
-    def add_pairs(self, pairs, S, ld, D, k, phi=None, ngphi=None):
+    def add_pairs(self, pairs, S, ld, D, k, phi=None, ngphi=None, ops=None):
         n_new = sum(int(p[1].shape[0]) * S for p in pairs)
         need = self.rows + n_new
         if need > self.X.shape[0]:
@@ -102,9 +110,10 @@ class WarmStartMLP:
                 T[: self.rows].copy_(self.T[: self.rows])
             self.X, self.T = X, T
         st = stream_handle()
-        for Up, Un, Unx in pairs:
+        for i, (Up, Un, Unx) in enumerate(pairs):
             V = int(Un.shape[0])
-            inp = self.inputs(Un, Up, S, ld, D, k, phi, ngphi)
+            inp = self.inputs(Un, Up, S, ld, D, k, phi, ngphi,
+                              None if ops is None else ops[i])
             r0 = self.rows
             call("tp_mlp_features", ctypes.byref(inp), ptr(self.X) + r0 * IN * 2, st)
             call("tp_mlp_target", V, S, ld, ptr(Un), ptr(Unx), float(self.sigma),
@@ -137,8 +146,8 @@ class WarmStartMLP:
         return g, self.loss_dev
 
     # ---- inference --------------------------------------------------------------
-    def predict(self, U, Up, S, ld, D, k, phi=None, ngphi=None, x_out=None):
-        inp = self.inputs(U, Up, S, ld, D, k, phi, ngphi)
+    def predict(self, U, Up, S, ld, D, k, phi=None, ngphi=None, x_out=None, ops=None):
+        inp = self.inputs(U, Up, S, ld, D, k, phi, ngphi, ops)
         if x_out is not None:
             call("tp_mlp_predict", ctypes.byref(inp), ptr(self.params), float(self.sigma),
                  ptr(x_out), None, stream_handle())
@@ -151,23 +160,27 @@ class WarmStartMLP:
     def predict_into(self, tr, x):
         """The transport driver's hook: guess for tr's next step written into x."""
         self.predict(tr.U, tr.U_prev, tr.S, tr.ld, tr.D, tr.k, getattr(tr, "phi", None),
-                     getattr(tr, "ngphi", None), x_out=x)
+                     getattr(tr, "ngphi", None), x_out=x, ops=tr.operator_images())
 
 
 def trajectory_pairs(tr, steps):
     """Run `steps` steps of a transport object from its current state, returning the
-    (U^{n-1}, U^n, U^{n+1}) triples that have a real history (n >= 1)."""
-    pairs = []
+    (U^{n-1}, U^n, U^{n+1}) triples that have a real history (n >= 1) and the stiffness
+    images (D_s K U^n, D_s K (U^n - U^{n-1})) of each."""
+    pairs, ops = [], []
     prev = None
     for _ in range(steps):
         cur = tr.U.clone()
+        if prev is not None:
+            op = tr.operator_images(cur, prev, fresh=True)
         res = tr.step()
         if not res["converged"]:
             raise RuntimeError(f"training trajectory did not converge: {res}")
         if prev is not None:
             pairs.append((prev, cur, tr.U.clone()))
+            ops.append(op)
         prev = cur
-    return pairs
+    return pairs, ops
 
 
 def attach_trained_predictor(fast, mesh, coef, u_ref, D, K, DT, train_steps=12,
@@ -180,10 +193,10 @@ def attach_trained_predictor(fast, mesh, coef, u_ref, D, K, DT, train_steps=12,
                            guess="previous", asm=fast.asm)
     u_train = np.random.default_rng(seed).uniform(0.0, 1.0, np.asarray(u_ref).shape)
     gen.set_state(u_train)
-    pairs = trajectory_pairs(gen, train_steps + 1)
+    pairs, ops = trajectory_pairs(gen, train_steps + 1)
     mlp = WarmStartMLP(fast.device, seed=seed)
-    mlp.fit_normalization(pairs, fast.S, D, K)
-    mlp.add_pairs(pairs, fast.S, fast.ld, D, K)
+    mlp.fit_normalization(pairs, fast.S, D, K, ops=ops)
+    mlp.add_pairs(pairs, fast.S, fast.ld, D, K, ops=ops)
     log = mlp.train(steps=epochs, log_every=100 if verbose else 0)
     if verbose:
         print("mlp training loss", log)

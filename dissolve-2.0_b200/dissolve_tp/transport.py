@@ -117,7 +117,7 @@ class BatchedTransport:
     """All species in one multi-column solve (shared stiffness, per-column diagonal)."""
 
     def __init__(self, mesh, coef_cell, D, k, dt, rtol=1e-8, max_it=5000, lumped=True,
-                 inner_fp32=True, delta=0.001, guess="previous", bc_dofs=None, bc_values=None,
+                 inner_fp32=True, delta=0.01, guess="previous", bc_dofs=None, bc_values=None,
                  alpha_cells=None, autotune=True, cg=None, asm=None, engine="persistent"):
         if not lumped:
             raise ValueError("the batched form splits the operator into a shared stiffness "
@@ -170,6 +170,10 @@ class BatchedTransport:
                                    delta=delta, **cg)
         self.U = torch.zeros((n, self.ld), dtype=torch.float64, device=dev)
         self.U_prev = torch.zeros_like(self.U)
+        # D_s K_xi alone (no diagonal): the stiffness images the learned guess reads
+        self.stiff_op = CsrOperator(dm.indptr, dm.indices, self.K64, dscale=self.D, S=self.S,
+                                    ld=self.ld)
+        self._op_bufs = None
         self.guess = guess
         self.predictor = None
         self.steps_done = 0
@@ -207,6 +211,24 @@ class BatchedTransport:
             call("tp_axpby", x.numel(), -1.0, ptr(self.U_prev), 2.0, ptr(x), stream_handle())
         else:
             x.copy_(self.U)
+
+    def operator_images(self, U=None, U_prev=None, fresh=False):
+        """(D_s K U, D_s K (U - U_prev)) with the current stiffness; defaults to the state.
+        Reuses two buffers unless fresh=True."""
+        U = self.U if U is None else U
+        Up = self.U_prev if U_prev is None else U_prev
+        if fresh or self._op_bufs is None:
+            bufs = tuple(torch.empty_like(self.U) for _ in range(3))
+            if not fresh:
+                self._op_bufs = bufs
+        else:
+            bufs = self._op_bufs
+        opU, opDU, dU = bufs
+        dU.copy_(U)
+        call("tp_axpby", dU.numel(), -1.0, ptr(Up), 1.0, ptr(dU), stream_handle())
+        self.stiff_op.apply(U, opU)
+        self.stiff_op.apply(dU, opDU)
+        return opU, opDU
 
     def set_state(self, U, U_prev=None):
         u = to_device(U, torch.float64, self.device).reshape(-1, self.S)

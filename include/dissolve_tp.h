@@ -384,7 +384,7 @@ TP_API int tp_sell_scatter(int64_t nnz, const int32_t* csr2sell, const double* c
  * barrier wait exceeds 2 s), the inner operator read in SELL-32 order, the FP64 operator
  * (Jacobi diagonal, initial / reliable-update / final residuals) in CSR.  Same stopping
  * rule and lane results as tp_cg_*.  Reliable updates (FP32 inner): when any lane's
- * recurrence residual has dropped by `delta` (<= 0 -> 0.001) since its last update, every
+ * recurrence residual has dropped by `delta` (<= 0 -> 0.01) since its last update, every
  * active lane is updated in the same FP64 sweep. */
 typedef struct tp_pcg_handle tp_pcg_handle;
 
@@ -430,8 +430,10 @@ typedef struct tp_mlp_inputs {
   const double* U_prev;      /* (n_verts, ld) u^{n-1}  */
   const double* phi;         /* (n_verts) or NULL       */
   const double* normgradphi; /* (n_verts) or NULL       */
+  const double* opU;         /* (n_verts, ld) stiffness image D_s K u^n, or NULL        */
+  const double* opDU;        /* (n_verts, ld) D_s K (u^n - u^{n-1}), or NULL           */
   double logD[4], k[4];      /* per species             */
-  double mean[8], istd[8];   /* input normalisation     */
+  double mean[10], istd[10]; /* input normalisation (features 0..9) */
 } tp_mlp_inputs;
 
 TP_API int tp_mlp_param_count(void);

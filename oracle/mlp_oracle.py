@@ -11,6 +11,7 @@ from __future__ import annotations
 import numpy as np
 
 IN, H = 16, 64
+NFEAT = 10  # used inputs (the rest of the 16 are zero)
 OFF_W1 = 0
 OFF_B1 = OFF_W1 + H * IN
 OFF_W2 = OFF_B1 + H
@@ -42,15 +43,17 @@ def init_params(seed=3):
     """He-style initial weights (the same formula as dissolve_tp.mlp)."""
     rng = np.random.default_rng(seed)
     p = np.zeros(P, dtype=np.float32)
-    p[OFF_W1:OFF_B1] = rng.normal(0, np.sqrt(2.0 / 8), H * IN)
-    p[OFF_W1:OFF_B1].reshape(H, IN)[:, 8:] = 0.0
+    p[OFF_W1:OFF_B1] = rng.normal(0, np.sqrt(2.0 / NFEAT), H * IN)
+    p[OFF_W1:OFF_B1].reshape(H, IN)[:, NFEAT:] = 0.0
     p[OFF_W2:OFF_B2] = rng.normal(0, np.sqrt(2.0 / H), H * H)
     p[OFF_W3:OFF_B3] = rng.normal(0, 0.1 / np.sqrt(H), H)
     return p
 
 
-def features(U, Up, phi, ngphi, logD, k, mean, istd):
-    """Normalised inputs (rows = vertex * S + species), FP32 then BF16 as on the GPU."""
+def features(U, Up, phi, ngphi, logD, k, mean, istd, opU=None, opDU=None):
+    """Normalised inputs (rows = vertex * S + species), FP32 then BF16 as on the GPU:
+    0 phi, 1 |grad phi|, 2 u^n, 3 u^{n-1}, 4 u^n - u^{n-1}, 5 log D, 6 k, 7 1,
+    8 stiffness image of u^n, 9 of u^n - u^{n-1} (both (V, S) or None)."""
     V, S = U.shape
     rows = V * S
     x = np.zeros((rows, IN), dtype=np.float64)
@@ -61,7 +64,11 @@ def features(U, Up, phi, ngphi, logD, k, mean, istd):
     raw = [phi[vid] if phi is not None else np.zeros(rows),
            ngphi[vid] if ngphi is not None else np.zeros(rows),
            u, up, (U - Up).reshape(-1), np.asarray(logD)[sid], np.asarray(k)[sid]]
-    for f in range(7):
+    raw += [None, np.zeros(rows) if opU is None else opU.reshape(-1),
+            np.zeros(rows) if opDU is None else opDU.reshape(-1)]
+    for f in range(NFEAT):
+        if f == 7:
+            continue
         x[:, f] = (f32(raw[f]) - f32(mean[f])) * f32(istd[f])
         x[:, f] = f32(x[:, f])
     x[:, 7] = 1.0

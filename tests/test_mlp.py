@@ -40,7 +40,7 @@ def _random_setup(seed, rows):
     p = p.astype(np.float32)
     X = rng.normal(0, 1, (rows, mo.IN))
     X[:, 7] = 1.0
-    X[:, 8:] = 0.0
+    X[:, mo.NFEAT:] = 0.0
     X = mo.bf16(X)
     T = rng.normal(0, 1, rows).astype(np.float32)
     return p, X, T
@@ -106,8 +106,8 @@ def test_gpu_forward_from_fields_matches_oracle(cuda_device):
     ng = np.abs(rng.normal(1, 0.2, V))
     D, k = [1.0, 1.0, 2.6], [0.5, 0.0, 0.2]
     m = WarmStartMLP(cuda_device)
-    m.mean = np.array([0.0, 1.0, 0.5, 0.5, 0.0, 0.3, 0.2, 0.0])
-    m.istd = np.array([1.0, 5.0, 3.0, 3.0, 20.0, 2.0, 4.0, 1.0])
+    m.mean = np.array([0.0, 1.0, 0.5, 0.5, 0.0, 0.3, 0.2, 0.0, 0.1, -0.1])
+    m.istd = np.array([1.0, 5.0, 3.0, 3.0, 20.0, 2.0, 4.0, 1.0, 0.5, 2.0])
     m.sigma = 0.01
     Ud = torch.zeros((V, ld), dtype=torch.float64, device=cuda_device)
     Upd = torch.zeros_like(Ud)
@@ -115,12 +115,18 @@ def test_gpu_forward_from_fields_matches_oracle(cuda_device):
     Upd[:, :S] = torch.from_numpy(Up)
     phid = torch.from_numpy(phi).to(cuda_device)
     ngd = torch.from_numpy(ng).to(cuda_device)
-    y = m.predict(Ud, Upd, S, ld, D, k, phid, ngd).cpu().numpy().astype(np.float64)
-    X = mo.features(U, Up, phi, ng, np.log(D), k, m.mean, m.istd)
+    oU, oDU = rng.normal(0, 2, (V, S)), rng.normal(0, 0.5, (V, S))
+    ops = []
+    for o in (oU, oDU):
+        t = torch.zeros((V, ld), dtype=torch.float64, device=cuda_device)
+        t[:, :S] = torch.from_numpy(o)
+        ops.append(t)
+    y = m.predict(Ud, Upd, S, ld, D, k, phid, ngd, ops=ops).cpu().numpy().astype(np.float64)
+    X = mo.features(U, Up, phi, ng, np.log(D), k, m.mean, m.istd, oU, oDU)
     yo, _ = mo.forward(m.params.cpu().numpy(), X)
     assert np.abs(y - yo).max() <= 2e-3 * np.abs(yo).max()
     x = torch.zeros_like(Ud)
-    m.predict(Ud, Upd, S, ld, D, k, phid, ngd, x_out=x)
+    m.predict(Ud, Upd, S, ld, D, k, phid, ngd, x_out=x, ops=ops)
     xo = U + m.sigma * yo.reshape(V, S)
     assert np.abs(x[:, :S].cpu().numpy() - xo).max() <= 2e-3 * m.sigma * np.abs(yo).max() + 1e-12
 
