@@ -24,31 +24,25 @@ __device__ __forceinline__ GeoRec load_geo(const double* __restrict__ geo, int64
   return GeoRec{a.x, a.y, a.z, a.w, b.x, b.y, b.z};
 }
 
-// K_ij / ((dJ De)/6) in the reference's order (gpu_assembler.py:108-119): with
-// reference gradients g_0 = (-1,-1,-1), g_k = e_{k-1}, every product is exact and
+// Row li of K / ((dJ De)/6), K_li,j for j = 0..3, in the reference's order
+// (gpu_assembler.py:108-119): with reference gradients g_0 = (-1,-1,-1), g_k = e_{k-1},
+// every product is exact and
 //   Gg_j[a] = -((G[a][0] + G[a][1]) + G[a][2])  (j = 0),   G[a][j-1]  (j > 0)
 //   K_ij    = -((Gg_j[0] + Gg_j[1]) + Gg_j[2])  (i = 0),   Gg_j[i-1]  (i > 0)
-__device__ __forceinline__ double kref(int i, int j, const double G[3][3], const double S[3]) {
-  if (i == 0) {
-    if (j == 0) return __dadd_rn(__dadd_rn(S[0], S[1]), S[2]);
-    return -__dadd_rn(__dadd_rn(G[0][j - 1], G[1][j - 1]), G[2][j - 1]);
-  }
-  if (j == 0) return -S[i - 1];
-  return G[i - 1][j - 1];
-}
-
-__device__ __forceinline__ void unpack_G(const GeoRec& g, double G[3][3], double S[3]) {
-  G[0][0] = g.G00;
-  G[0][1] = g.G01;
-  G[0][2] = g.G02;
-  G[1][0] = g.G01;
-  G[1][1] = g.G11;
-  G[1][2] = g.G12;
-  G[2][0] = g.G02;
-  G[2][1] = g.G12;
-  G[2][2] = g.G22;
-#pragma unroll
-  for (int a = 0; a < 3; a++) S[a] = __dadd_rn(__dadd_rn(G[a][0], G[a][1]), G[a][2]);
+// G is symmetric, so the column sums of the first row are the row sums
+// S[a] = (G[a][0] + G[a][1]) + G[a][2] (same operands, same order).  li is a runtime
+// value: the row comes from selects, not from an indexed array (which would live in
+// local memory).
+__device__ __forceinline__ void kref_row(int li, const GeoRec& g, double k[4]) {
+  const double S0 = __dadd_rn(__dadd_rn(g.G00, g.G01), g.G02);
+  const double S1 = __dadd_rn(__dadd_rn(g.G01, g.G11), g.G12);
+  const double S2 = __dadd_rn(__dadd_rn(g.G02, g.G12), g.G22);
+  const double T = __dadd_rn(__dadd_rn(S0, S1), S2);
+  const bool l0 = li == 0, l1 = li == 1, l2 = li == 2;
+  k[0] = l0 ? T : -(l1 ? S0 : (l2 ? S1 : S2));
+  k[1] = l0 ? -S0 : (l1 ? g.G00 : (l2 ? g.G01 : g.G02));
+  k[2] = l0 ? -S1 : (l1 ? g.G01 : (l2 ? g.G11 : g.G12));
+  k[3] = l0 ? -S2 : (l1 ? g.G02 : (l2 ? g.G12 : g.G22));
 }
 
 // ----------------------------------------------------------------- CSR assembly
@@ -104,15 +98,15 @@ __global__ void __launch_bounds__(128) k_assemble_rows(
         if (k0 + u >= kend) break;
         const int li = ev[u] & 3;
         const GeoRec& g = gv[u];
-        double G[3][3], S[3];
-        unpack_G(g, G, S);
+        double kr[4];
+        kref_row(li, g, kr);
         const double kscale = (MODE == TP_ASM_MASS) ? 0.0
                                                     : __ddiv_rn(__dmul_rn(g.dJ, dev[u]), 6.0);
         const double react = (MODE == TP_ASM_FULL) ? __dadd_rn(inv_dt, alv[u]) : 1.0;
 #pragma unroll
         for (int j = 0; j < 4; j++) {
           double a = 0.0;
-          if (MODE != TP_ASM_MASS) a = __dmul_rn(kref(li, j, G, S), kscale);
+          if (MODE != TP_ASM_MASS) a = __dmul_rn(kr[j], kscale);
           if (MODE != TP_ASM_STIFF) {
             double M;
             if (lumped)
@@ -206,17 +200,23 @@ __global__ void k_lumped_diag(int64_t nv, int S, int ld, const int32_t* __restri
         for (int u = 0; u < PF; u++) {
           if (k0 + u >= kend) break;
           const double Ld = __dmul_rn(__ddiv_rn(dJ[u], 120.0), 5.0);
-          for (int s = 0; s < S; s++) {
-            const double w = __dadd_rn(sh[s], alpha ? alpha[cv[u] * ld + s] : 0.0);
-            acc[s] = __dadd_rn(acc[s], __dmul_rn(w, Ld));
+#pragma unroll
+          for (int s = 0; s < 4; s++) {
+            if (s < S) {
+              const double w = __dadd_rn(sh[s], alpha ? alpha[cv[u] * ld + s] : 0.0);
+              acc[s] = __dadd_rn(acc[s], __dmul_rn(w, Ld));
+            }
           }
         }
       }
     }
-    for (int s = 0; s < ld; s++) {
-      const double v = is_bc ? 1.0 : (s < S ? acc[s] : 0.0);
-      if (d64) d64[r * ld + s] = v;
-      if (d32) d32[r * ld + s] = (float)v;
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+      if (s < ld) {
+        const double v = is_bc ? 1.0 : (s < S ? acc[s] : 0.0);
+        if (d64) d64[r * ld + s] = v;
+        if (d32) d32[r * ld + s] = (float)v;
+      }
     }
   }
 }
@@ -232,9 +232,10 @@ __global__ void k_rhs_rows(int64_t nv, int S, int ld, const int32_t* __restrict_
        r += (int64_t)gridDim.x * blockDim.x) {
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     double ur[4], fr[4];
-    for (int s = 0; s < S; s++) {
-      ur[s] = u[r * ld + s];
-      fr[s] = f ? f[r * ld + s] : 0.0;
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+      ur[s] = (s < S) ? u[r * ld + s] : 0.0;
+      fr[s] = (s < S && f) ? f[r * ld + s] : 0.0;
     }
     constexpr int PF = 8;
     const int kbeg = v2c_ptr[r], kend = v2c_ptr[r + 1];
@@ -252,13 +253,17 @@ __global__ void k_rhs_rows(int64_t nv, int S, int ld, const int32_t* __restrict_
         const double base = __ddiv_rn(dJv[q], 120.0);
         if (lumped) {
           const double Ld = __dmul_rn(base, 5.0);
-          for (int s = 0; s < S; s++)
-            acc[s] = __dadd_rn(acc[s],
-                               __dmul_rn(Ld, __dadd_rn(__dmul_rn(inv_dt, ur[s]), fr[s])));
+#pragma unroll
+          for (int s = 0; s < 4; s++)
+            if (s < S)
+              acc[s] = __dadd_rn(acc[s],
+                                 __dmul_rn(Ld, __dadd_rn(__dmul_rn(inv_dt, ur[s]), fr[s])));
         } else {
           const int4 cv = reinterpret_cast<const int4*>(cells)[c];
           const double mdt = __dmul_rn(base, inv_dt);
-          for (int s = 0; s < S; s++) {
+#pragma unroll
+          for (int s = 0; s < 4; s++) {
+            if (s >= S) continue;
             const double su = __dadd_rn(
                 __dadd_rn(__dadd_rn(u[(int64_t)cv.x * ld + s], u[(int64_t)cv.y * ld + s]),
                           u[(int64_t)cv.z * ld + s]),
@@ -275,7 +280,9 @@ __global__ void k_rhs_rows(int64_t nv, int S, int ld, const int32_t* __restrict_
         }
       }
     }
-    for (int s = 0; s < ld; s++) b[r * ld + s] = (s < S) ? acc[s] : 0.0;
+#pragma unroll
+    for (int s = 0; s < 4; s++)
+      if (s < ld) b[r * ld + s] = (s < S) ? acc[s] : 0.0;
   }
 }
 
