@@ -112,6 +112,60 @@ __global__ void __launch_bounds__(256) k_csr_apply(int64_t n, CsrView<T> A,
   }
 }
 
+// y1 = D K x1 and y2 = D K (x1 - x2) in one pass over the CSR operator (no mass, no
+// diagonal, no identity rows): the stiffness images of u^n and of the last increment.
+// G lanes per row, FP64.
+template <int LD, int G>
+__global__ void __launch_bounds__(256) k_csr_images(int64_t n, const int32_t* __restrict__ indptr,
+                                                    const int32_t* __restrict__ indices,
+                                                    const double* __restrict__ K, double4 dsc,
+                                                    const double* __restrict__ x1,
+                                                    const double* __restrict__ x2,
+                                                    double* __restrict__ y1,
+                                                    double* __restrict__ y2) {
+  const double dscale[4] = {dsc.x, dsc.y, dsc.z, dsc.w};
+  const int gl = threadIdx.x % G;
+  const int64_t rpb = blockDim.x / G;
+  for (int64_t base = blockIdx.x * rpb; base < n; base += (int64_t)gridDim.x * rpb) {
+    const int64_t row = base + threadIdx.x / G;
+    const int64_t rr = row < n ? row : n - 1;
+    double a1[LD], a2[LD];
+#pragma unroll
+    for (int s = 0; s < LD; s++) a1[s] = a2[s] = 0.0;
+    const int beg = indptr[rr], end = indptr[rr + 1];
+    for (int p = beg + gl; p < end; p += G) {
+      const int j = __ldg(indices + p);
+      const double kv = __ldg(K + p);
+      double u[LD], up[LD];
+      ldv<double, LD>(x1, j, u);
+      ldv<double, LD>(x2, j, up);
+#pragma unroll
+      for (int s = 0; s < LD; s++) {
+        a1[s] += kv * u[s];
+        a2[s] += kv * (u[s] - up[s]);
+      }
+    }
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) {
+#pragma unroll
+      for (int s = 0; s < LD; s++) {
+        a1[s] += __shfl_xor_sync(0xffffffffu, a1[s], o, G);
+        a2[s] += __shfl_xor_sync(0xffffffffu, a2[s], o, G);
+      }
+    }
+    if (row < n && gl == 0) {
+      double o1[LD], o2[LD];
+#pragma unroll
+      for (int s = 0; s < LD; s++) {
+        o1[s] = dscale[s] * a1[s];
+        o2[s] = dscale[s] * a2[s];
+      }
+      stv<double, LD>(y1, row, o1);
+      stv<double, LD>(y2, row, o2);
+    }
+  }
+}
+
 template <typename T>
 static int launch_matfree(const tp_mesh* m, int S, int ld, const double* De, const double* al,
                           double4 dsc, double4 shf, double inv_dt, int lumped, int legacy,
@@ -218,6 +272,30 @@ extern "C" int tp_csr_apply(const tp_csr_op* op, int fp32, const void* x, void* 
     else if (op->ld == 2) launch_csr<double, 2>(op, x, y, st);
     else launch_csr<double, 4>(op, x, y, st);
   }
+  TP_LAUNCH_CHECK();
+  return TP_OK;
+}
+
+extern "C" int tp_csr_images(const tp_csr_op* op, const double* x1, const double* x2,
+                             double* y1, double* y2, void* stream) {
+  TP_REQUIRE(op && op->indptr && op->indices && op->K64 && x1 && x2 && y1 && y2,
+             "null pointer");
+  TP_REQUIRE(op->ld == 1 || op->ld == 2 || op->ld == 4, "ld must be 1, 2 or 4");
+  if (op->n_rows == 0) return TP_OK;
+  cudaStream_t st = as_stream(stream);
+  constexpr int G = 4;
+  const int grid = grid_for(op->n_rows, 256 / G, sm_count() * 16);
+  const double4 dsc = make_double4(op->S > 0 ? op->dscale[0] : 0.0, op->S > 1 ? op->dscale[1] : 0.0,
+                                   op->S > 2 ? op->dscale[2] : 0.0, op->S > 3 ? op->dscale[3] : 0.0);
+  if (op->ld == 1)
+    k_csr_images<1, G><<<grid, 256, 0, st>>>(op->n_rows, op->indptr, op->indices, op->K64, dsc,
+                                             x1, x2, y1, y2);
+  else if (op->ld == 2)
+    k_csr_images<2, G><<<grid, 256, 0, st>>>(op->n_rows, op->indptr, op->indices, op->K64, dsc,
+                                             x1, x2, y1, y2);
+  else
+    k_csr_images<4, G><<<grid, 256, 0, st>>>(op->n_rows, op->indptr, op->indices, op->K64, dsc,
+                                             x1, x2, y1, y2);
   TP_LAUNCH_CHECK();
   return TP_OK;
 }

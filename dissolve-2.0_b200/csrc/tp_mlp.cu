@@ -24,6 +24,10 @@
 namespace tp {
 
 constexpr int MLP_IN = 16, MLP_H = 64;
+// shared-memory row strides (bf16 elements) of the weight and staging tiles: 24 and 72
+// put the 8 rows a B-fragment load touches into 8 different bank groups (16 and 64
+// would hit the same banks 2 and 8 times)
+constexpr int W1S = 24, W2S = 72, GS = 72;
 // FP32 master parameter vector layout
 constexpr int OFF_W1 = 0;                      // [64][16]
 constexpr int OFF_B1 = OFF_W1 + MLP_H * MLP_IN;  // [64]
@@ -61,45 +65,43 @@ __device__ __forceinline__ void mma_bf16(float c[4], uint32_t a0, uint32_t a1, u
       : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-// normalised feature f (0..15) of row r = v * S + s
-__device__ __forceinline__ float feature(const MlpFeat& F, int64_t r, int f) {
-  if (f >= NFEAT) return 0.0f;
-  const int64_t v = r / F.S;
-  const int s = (int)(r - v * F.S);
-  float x;
-  switch (f) {
-    case 0: x = F.phi ? (float)F.phi[v] : 0.0f; break;
-    case 1: x = F.ngphi ? (float)F.ngphi[v] : 0.0f; break;
-    case 2: x = (float)F.U[v * F.ld + s]; break;
-    case 3: x = (float)F.Up[v * F.ld + s]; break;
-    case 4: x = (float)(F.U[v * F.ld + s] - F.Up[v * F.ld + s]); break;
-    case 5: x = F.logD[s]; break;
-    case 6: x = F.k[s]; break;
-    case 7: return 1.0f;
-    case 8: x = F.opU ? (float)F.opU[v * F.ld + s] : 0.0f; break;
-    default: x = F.opDU ? (float)F.opDU[v * F.ld + s] : 0.0f; break;
-  }
-  return (x - F.mean[f]) * F.istd[f];
+// all NFEAT normalised features of row r = v * S + s (r < number of rows), branch-free
+__device__ __forceinline__ void row_features(const MlpFeat& F, int64_t v, int s,
+                                             float f[NFEAT]) {
+  const int64_t i = v * F.ld + s;
+  const double u = F.U[i], up = F.Up[i];
+  float x[NFEAT];
+  x[0] = F.phi ? (float)F.phi[v] : 0.0f;
+  x[1] = F.ngphi ? (float)F.ngphi[v] : 0.0f;
+  x[2] = (float)u;
+  x[3] = (float)up;
+  x[4] = (float)(u - up);
+  x[5] = F.logD[s];
+  x[6] = F.k[s];
+  x[8] = F.opU ? (float)F.opU[i] : 0.0f;
+  x[9] = F.opDU ? (float)F.opDU[i] : 0.0f;
+#pragma unroll
+  for (int k = 0; k < NFEAT; k++) f[k] = (k == 7) ? 1.0f : (x[k] - F.mean[k]) * F.istd[k];
 }
 
-// shared-memory copy of the BF16 weights; W2T[in][out] is the transpose used by the
-// backward pass
+// shared-memory copy of the BF16 weights
 struct MlpSmem {
-  __nv_bfloat16 W1[MLP_H][MLP_IN];
-  __nv_bfloat16 W2[MLP_H][MLP_H];
-  __nv_bfloat16 W2T[MLP_H][MLP_H];
+  __nv_bfloat16 W1[MLP_H][W1S];
+  __nv_bfloat16 W2[MLP_H][W2S];
   float w3[MLP_H];
   float b1[MLP_H], b2[MLP_H];
   float b3;
 };
 
-__device__ void load_weights(MlpSmem& sm, const float* __restrict__ P) {
+// W2T (optional, the backward pass): W2 transposed, [in][out]
+__device__ void load_weights(MlpSmem& sm, const float* __restrict__ P,
+                             __nv_bfloat16 (*W2T)[W2S] = nullptr) {
   for (int i = threadIdx.x; i < MLP_H * MLP_IN; i += blockDim.x)
     sm.W1[i / MLP_IN][i % MLP_IN] = __float2bfloat16_rn(P[OFF_W1 + i]);
   for (int i = threadIdx.x; i < MLP_H * MLP_H; i += blockDim.x) {
     const __nv_bfloat16 w = __float2bfloat16_rn(P[OFF_W2 + i]);
     sm.W2[i / MLP_H][i % MLP_H] = w;
-    sm.W2T[i % MLP_H][i / MLP_H] = w;
+    if (W2T) W2T[i % MLP_H][i / MLP_H] = w;
   }
   for (int i = threadIdx.x; i < MLP_H; i += blockDim.x) {
     sm.w3[i] = __bfloat162float(__float2bfloat16_rn(P[OFF_W3 + i]));
@@ -132,7 +134,7 @@ __device__ __forceinline__ void mlp_tile_forward(const MlpSmem& sm, const uint32
     z1[n][2] = bl;
     z1[n][3] = bh;
     uint32_t b0, b1;
-    bfrag(&sm.W1[0][0], MLP_IN, n * 8, 0, g, t, b0, b1);
+    bfrag(&sm.W1[0][0], W1S, n * 8, 0, g, t, b0, b1);
     mma_bf16(z1[n], xa[0], xa[1], xa[2], xa[3], b0, b1);
   }
   uint32_t ha[4][4];  // h1 as A fragments, 4 k-steps
@@ -155,7 +157,7 @@ __device__ __forceinline__ void mlp_tile_forward(const MlpSmem& sm, const uint32
 #pragma unroll
     for (int kk = 0; kk < 4; kk++) {
       uint32_t b0, b1;
-      bfrag(&sm.W2[0][0], MLP_H, n * 8, kk * 16, g, t, b0, b1);
+      bfrag(&sm.W2[0][0], W2S, n * 8, kk * 16, g, t, b0, b1);
       mma_bf16(z2[n], ha[kk][0], ha[kk][1], ha[kk][2], ha[kk][3], b0, b1);
     }
   }
@@ -178,19 +180,11 @@ __device__ __forceinline__ void mlp_tile_forward(const MlpSmem& sm, const uint32
   y1 = s1 + sm.b3;
 }
 
-// A fragment of the inputs of rows r0 + g, r0 + g + 8 (16 features)
-__device__ __forceinline__ void input_frag(const MlpFeat& F, int64_t r0, int64_t nrows, int g,
-                                           int t, uint32_t xa[4]) {
-  const int64_t ra = r0 + g, rb = r0 + g + 8;
-  auto f = [&](int64_t r, int c) { return r < nrows ? feature(F, r, c) : 0.0f; };
-  xa[0] = pack_bf16(f(ra, 2 * t), f(ra, 2 * t + 1));
-  xa[1] = pack_bf16(f(rb, 2 * t), f(rb, 2 * t + 1));
-  xa[2] = pack_bf16(f(ra, 2 * t + 8), f(ra, 2 * t + 9));
-  xa[3] = pack_bf16(f(rb, 2 * t + 8), f(rb, 2 * t + 9));
-}
-
 // ----------------------------------------------------------------- inference
-// x_out[v, s] = U[v, s] + sigma * y(v, s)  (or y_out[r] = y when x_out is NULL)
+// x_out[v, s] = U[v, s] + sigma * y(v, s)  (or y_out[r] = y when x_out is NULL).
+// Persistent warps over 16-row tiles.  Every lane of a quad gathers all features of its
+// two rows (the quad's loads hit the same addresses) and keeps the four its A fragment
+// holds: no divergent per-feature branches.
 __global__ void __launch_bounds__(128) k_mlp_predict(MlpFeat F, int64_t nrows,
                                                      const float* __restrict__ P, float sigma,
                                                      double* __restrict__ x_out,
@@ -204,32 +198,73 @@ __global__ void __launch_bounds__(128) k_mlp_predict(MlpFeat F, int64_t nrows,
        tile += (int64_t)gridDim.x * 4) {
     const int64_t r0 = tile * 16;
     uint32_t xa[4];
-    input_frag(F, r0, nrows, g, t, xa);
+    int64_t vv[2];
+    int ss[2];
+    float fa[2][4];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int64_t r = r0 + g + 8 * h;
+      const bool in = r < nrows;
+      // 32-bit division while the row index fits
+      const int64_t v = !in ? 0
+                            : (r < (int64_t)UINT32_MAX ? (int64_t)((uint32_t)r / (uint32_t)F.S)
+                                                       : r / F.S);
+      const int s = in ? (int)(r - v * F.S) : 0;
+      vv[h] = v;
+      ss[h] = s;
+      float f[NFEAT];
+      row_features(F, v, s, f);
+      // this lane's features 2t, 2t+1, 2t+8, 2t+9 (10..15 are zero)
+      const float lo = (t == 0) ? f[0] : (t == 1) ? f[2] : (t == 2) ? f[4] : f[6];
+      const float hi = (t == 0) ? f[1] : (t == 1) ? f[3] : (t == 2) ? f[5] : f[7];
+      fa[h][0] = in ? lo : 0.f;
+      fa[h][1] = in ? hi : 0.f;
+      fa[h][2] = (in && t == 0) ? f[8] : 0.f;
+      fa[h][3] = (in && t == 0) ? f[9] : 0.f;
+    }
+    xa[0] = pack_bf16(fa[0][0], fa[0][1]);
+    xa[1] = pack_bf16(fa[1][0], fa[1][1]);
+    xa[2] = pack_bf16(fa[0][2], fa[0][3]);
+    xa[3] = pack_bf16(fa[1][2], fa[1][3]);
     float z1[8][4], z2[8][4], y0, y1;
     mlp_tile_forward(sm, xa, g, t, z1, z2, y0, y1);
-    if (t == 0) {
-      const int64_t rr[2] = {r0 + g, r0 + g + 8};
-      const float yy[2] = {y0, y1};
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        if (rr[h] >= nrows) continue;
+    // lane t < 2 of each quad writes row g + 8t
+    if (t < 2) {
+      const int h = t;
+      const int64_t r = r0 + g + 8 * h;
+      const float y = h ? y1 : y0;
+      if (r < nrows) {
         if (x_out) {
-          const int64_t v = rr[h] / F.S;
-          const int s = (int)(rr[h] - v * F.S);
-          x_out[v * F.ld + s] = F.U[v * F.ld + s] + (double)sigma * (double)yy[h];
+          const int64_t i = (h ? vv[1] : vv[0]) * F.ld + (h ? ss[1] : ss[0]);
+          x_out[i] = F.U[i] + (double)sigma * (double)y;
         } else {
-          y_out[rr[h]] = yy[h];
+          y_out[r] = y;
         }
       }
     }
   }
 }
 
-// features of every row, materialised (training set), BF16 (nrows, 16)
+// features of every row, materialised (training set), BF16 (nrows, 16): one thread per
+// row, one 32-byte store
 __global__ void k_mlp_features(MlpFeat F, int64_t nrows, __nv_bfloat16* __restrict__ X) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nrows * MLP_IN;
-       i += (int64_t)gridDim.x * blockDim.x)
-    X[i] = __float2bfloat16_rn(feature(F, i / MLP_IN, (int)(i % MLP_IN)));
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nrows;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t v = r / F.S;
+    const int s = (int)(r - v * F.S);
+    float f[NFEAT];
+    row_features(F, v, s, f);
+    uint32_t w[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const float lo = (2 * k < NFEAT) ? f[2 * k] : 0.f;
+      const float hi = (2 * k + 1 < NFEAT) ? f[2 * k + 1] : 0.f;
+      w[k] = pack_bf16(lo, hi);
+    }
+    uint4* dst = reinterpret_cast<uint4*>(X + r * MLP_IN);
+    dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
+    dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
+  }
 }
 
 // training target (u^{n+1} - u^n) / sigma per row
@@ -246,10 +281,11 @@ __global__ void k_mlp_target(int64_t nrows, int S, int ld, const double* __restr
 
 // ----------------------------------------------------------------- training
 struct GradSmem {
-  __nv_bfloat16 dz2T[MLP_H][64];  // [out unit][chunk row]
-  __nv_bfloat16 h1T[MLP_H][64];   // [hidden unit][chunk row]
-  __nv_bfloat16 dz1T[MLP_H][64];
-  __nv_bfloat16 xT[MLP_IN][64];
+  __nv_bfloat16 dz2T[MLP_H][GS];  // [out unit][chunk row]
+  __nv_bfloat16 h1T[MLP_H][GS];   // [hidden unit][chunk row]
+  __nv_bfloat16 dz1T[MLP_H][GS];
+  __nv_bfloat16 xT[MLP_IN][GS];
+  __nv_bfloat16 W2T[MLP_H][W2S];  // W2 transposed: B operand of dH1 = dZ2 W2
   float dw3[4][MLP_H];  // per warp
   float db3[4];
   float loss[4];
@@ -263,8 +299,9 @@ __global__ void __launch_bounds__(128) k_mlp_grad(const __nv_bfloat16* __restric
                                                   float wscale, float* __restrict__ part,
                                                   float* __restrict__ loss_part) {
   __shared__ MlpSmem sm;
-  __shared__ GradSmem gs;
-  load_weights(sm, P);
+  extern __shared__ __align__(16) unsigned char grad_dyn[];  // GradSmem (> 48 KB static)
+  GradSmem& gs = *reinterpret_cast<GradSmem*>(grad_dyn);
+  load_weights(sm, P, gs.W2T);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, t = lane & 3;
   for (int i = threadIdx.x; i < 4 * MLP_H; i += blockDim.x) gs.dw3[i / MLP_H][i % MLP_H] = 0.f;
@@ -348,7 +385,7 @@ __global__ void __launch_bounds__(128) k_mlp_grad(const __nv_bfloat16* __restric
 #pragma unroll
       for (int kk = 0; kk < 4; kk++) {
         uint32_t b0, b1;
-        bfrag(&sm.W2T[0][0], MLP_H, n * 8, kk * 16, g, t, b0, b1);
+        bfrag(&gs.W2T[0][0], W2S, n * 8, kk * 16, g, t, b0, b1);
         mma_bf16(dz1[n], da[kk][0], da[kk][1], da[kk][2], da[kk][3], b0, b1);
       }
 #pragma unroll
@@ -398,13 +435,13 @@ __global__ void __launch_bounds__(128) k_mlp_grad(const __nv_bfloat16* __restric
 #pragma unroll
       for (int n = 0; n < 8; n++) {
         uint32_t b0, b1;
-        bfrag(&gs.h1T[0][0], 64, n * 8, k0, g, t, b0, b1);
+        bfrag(&gs.h1T[0][0], GS, n * 8, k0, g, t, b0, b1);
         mma_bf16(dW2[n], a[0], a[1], a[2], a[3], b0, b1);
       }
 #pragma unroll
       for (int n = 0; n < 2; n++) {
         uint32_t b0, b1;
-        bfrag(&gs.xT[0][0], 64, n * 8, k0, g, t, b0, b1);
+        bfrag(&gs.xT[0][0], GS, n * 8, k0, g, t, b0, b1);
         mma_bf16(dW1[n], a1[0], a1[1], a1[2], a1[3], b0, b1);
       }
     }
@@ -515,7 +552,7 @@ extern "C" int tp_mlp_predict(const tp_mlp_inputs* in, const float* params, floa
   const int64_t nrows = in->n_verts * in->S;
   if (nrows == 0) return TP_OK;
   const int64_t ntiles = (nrows + 15) / 16;
-  const int grid = (int)std::min<int64_t>((ntiles + 3) / 4, (int64_t)sm_count() * 16);
+  const int grid = (int)std::min<int64_t>((ntiles + 3) / 4, (int64_t)sm_count() * 6);
   k_mlp_predict<<<grid, 128, 0, as_stream(stream)>>>(make_feat(in), nrows, params, sigma, x_out,
                                                       y_out);
   TP_LAUNCH_CHECK();
@@ -556,8 +593,10 @@ extern "C" int tp_mlp_train_step(const void* X, const float* T, int64_t row0, in
   float* part = workspace;
   float* loss_part = workspace + (size_t)grid * MLP_P;
   const float wscale = nrows > 0 ? 2.0f / (float)nrows : 0.f;
-  k_mlp_grad<<<grid, 128, 0, st>>>(static_cast<const __nv_bfloat16*>(X), T, row0, nrows, params,
-                                   wscale, part, loss_part);
+  TP_CUDA_TRY(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)sizeof(GradSmem)));
+  k_mlp_grad<<<grid, 128, sizeof(GradSmem), st>>>(static_cast<const __nv_bfloat16*>(X), T, row0,
+                                                  nrows, params, wscale, part, loss_part);
   TP_LAUNCH_CHECK();
   const float bc1 = 1.f - powf(beta1, (float)std::max(step, 1));
   const float bc2 = 1.f - powf(beta2, (float)std::max(step, 1));

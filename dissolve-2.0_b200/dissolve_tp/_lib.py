@@ -131,6 +131,7 @@ SIGNATURES = {
                                         _vp, _P(_c_dbl), _P(_c_dbl), _c_dbl, ctypes.c_int,
                                         ctypes.c_int, _vp, _vp, _vp]),
     "tp_csr_apply": (ctypes.c_int, [_P(TpCsrOp), ctypes.c_int, _vp, _vp, _vp]),
+    "tp_csr_images": (ctypes.c_int, [_P(TpCsrOp), _vp, _vp, _vp, _vp, _vp]),
     "tp_cg_workspace_bytes": (ctypes.c_size_t, [_P(TpCsrOp), _P(TpCgConfig)]),
     "tp_cg_create": (ctypes.c_int, [_P(TpCsrOp), _P(TpCgConfig), _vp, _vp, _vp, _vp,
                                     ctypes.c_size_t, _vp, _P(_vp)]),

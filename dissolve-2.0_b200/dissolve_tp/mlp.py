@@ -58,7 +58,7 @@ class WarmStartMLP:
         self.T = torch.empty(max(capacity_rows, 1), dtype=torch.float32, device=device)
         self.rows = 0
         self.rng = np.random.default_rng(seed)
-        self.launches = 1
+        self.launches = 2  # per guess: the stiffness images, the network
 
     # ---- inputs -----------------------------------------------------------------
     def inputs(self, U, Up, S, ld, D, k, phi=None, ngphi=None, ops=None) -> TpMlpInputs:

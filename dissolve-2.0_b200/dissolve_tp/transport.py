@@ -213,21 +213,19 @@ class BatchedTransport:
             x.copy_(self.U)
 
     def operator_images(self, U=None, U_prev=None, fresh=False):
-        """(D_s K U, D_s K (U - U_prev)) with the current stiffness; defaults to the state.
-        Reuses two buffers unless fresh=True."""
+        """(D_s K U, D_s K (U - U_prev)) with the current stiffness, one launch
+        (tp_csr_images); defaults to the state.  Reuses two buffers unless fresh=True."""
         U = self.U if U is None else U
         Up = self.U_prev if U_prev is None else U_prev
         if fresh or self._op_bufs is None:
-            bufs = tuple(torch.empty_like(self.U) for _ in range(3))
+            bufs = tuple(torch.empty_like(self.U) for _ in range(2))
             if not fresh:
                 self._op_bufs = bufs
         else:
             bufs = self._op_bufs
-        opU, opDU, dU = bufs
-        dU.copy_(U)
-        call("tp_axpby", dU.numel(), -1.0, ptr(Up), 1.0, ptr(dU), stream_handle())
-        self.stiff_op.apply(U, opU)
-        self.stiff_op.apply(dU, opDU)
+        opU, opDU = bufs
+        call("tp_csr_images", ctypes.byref(self.stiff_op.struct), ptr(U), ptr(Up), ptr(opU),
+             ptr(opDU), stream_handle())
         return opU, opDU
 
     def set_state(self, U, U_prev=None):

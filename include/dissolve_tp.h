@@ -296,6 +296,12 @@ typedef struct tp_csr_op {
 /* y = A x with the FP64 (fp32 = 0) or FP32 (fp32 = 1) values of op */
 TP_API int tp_csr_apply(const tp_csr_op* op, int fp32, const void* x, void* y, void* stream);
 
+/* y1 = D K x1 and y2 = D K (x1 - x2) with the FP64 values K64 of op (D = op->dscale; no
+ * mass, diagonal or identity rows) in one pass: the stiffness images of u^n and of the
+ * last increment that the learned initial guess reads (no reference counterpart). */
+TP_API int tp_csr_images(const tp_csr_op* op, const double* x1, const double* x2, double* y1,
+                         double* y2, void* stream);
+
 /* ------------------------------------------------------------------ Krylov solve */
 /* Jacobi-preconditioned CG on every (system, column) lane at once, captured in a CUDA
  * graph whose device-side while loop runs until every lane converges or max_it.
