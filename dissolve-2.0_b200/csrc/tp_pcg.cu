@@ -156,14 +156,15 @@ struct PhaseClock {
 };
 
 // Grid barrier; returns false in every thread of the CTA when the grid has aborted.
-// `target` (thread 0 only) counts the arrivals this CTA has waited for so far.
+// `target` (thread 0 only) counts the arrivals this CTA has waited for so far.  The CTA's
+// writes are ordered by __syncthreads and published by thread 0's gpu-scope release add;
+// the acquire poll and the closing __syncthreads make the other CTAs' writes visible.
 __device__ __forceinline__ bool grid_sync(PBar* bar, unsigned int& target) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
     target += gridDim.x;
-    __threadfence();
     red_release_add(&bar->count, 1u);
     unsigned int spins = 0;
     unsigned long long t0 = 0;
@@ -182,31 +183,42 @@ __device__ __forceinline__ bool grid_sync(PBar* bar, unsigned int& target) {
           break;
         }
       }
-      __nanosleep(32);
     }
-    __threadfence();
     s_ok = ok;
   }
   __syncthreads();
   return s_ok != 0;
 }
 
-// Sum NV slots of every CTA's partial row (fixed order); result in s_tot for all threads.
-// Thread (group g, slot k) adds the partials of CTAs g, g + groups, ... (a half-warp reads
-// one CTA's 16 slots: one 128-byte line), then warp k sums slot k over the groups with a
-// fixed shuffle tree; every CTA computes the same bits.
-template <int NV>
+// Sum slots K0 .. K0+NV-1 of every CTA's partial row (fixed order) into s_tot[K0 ..] for
+// all threads.  Thread (group g, slot k) adds the partials of CTAs g, g + groups, ... (a
+// half-warp reads one CTA's 16 slots: one 128-byte line; the first 8 loads are issued
+// together), then warp k sums slot k over the groups with a fixed shuffle tree; every
+// CTA computes the same bits.
+template <int NV, int K0 = 0>
 __device__ __forceinline__ void grid_totals(const double* part, double* s_tot, double* s_buf) {
   const int T = blockDim.x;
   const int groups = T / 16;  // blockDim multiple of 16
   const int k = threadIdx.x % 16, g = threadIdx.x / 16;
+  const int nb = (int)gridDim.x;
   double v = 0.0;
-  if (k < NV)
-    for (int b = g; b < (int)gridDim.x; b += groups) v += __ldcg(part + (int64_t)b * 16 + k);
+  if (k >= K0 && k < K0 + NV) {
+    constexpr int Q = 8;
+    double x[Q];
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+      const int b = g + q * groups;
+      x[q] = (b < nb) ? __ldcg(part + (int64_t)b * 16 + k) : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < Q; q++)
+      if (g + q * groups < nb) v += x[q];
+    for (int b = g + Q * groups; b < nb; b += groups) v += __ldcg(part + (int64_t)b * 16 + k);
+  }
   s_buf[threadIdx.x] = v;
   __syncthreads();
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (w < NV) {
+  if (w >= K0 && w < K0 + NV) {
     double t = 0.0;
     for (int gg = lane; gg < groups; gg += 32) t += s_buf[gg * 16 + w];
     t = warp_sum(t);
@@ -960,10 +972,12 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
   for (int sl = sb + warp; sl < se; sl += nwarps)                 \
     for (int64_t row = (int64_t)sl * 32 + lane; row < a.n; row = a.n)
 
-  // w = A u for the own rows from the window (filled first); w.u partials into acc
-  auto product = [&](double acc[4]) {
+  // w = A u for the own rows from the window; w.u partials into acc.  fill_window issues
+  // the copies (own_done: the own rows of the window already hold u -- the P phase wrote
+  // them -- only the halo is copied); product_rows waits for them and multiplies.
+  auto fill_window = [&](bool own_done) {
     const int W = nown + nhalo;
-    for (int i = threadIdx.x; i < W; i += blockDim.x) {
+    for (int i = (own_done ? nown : 0) + threadIdx.x; i < W; i += blockDim.x) {
       const int64_t g = (i < nown) ? (int64_t)(r0 + i) : (int64_t)s_halo[i - nown];
       const VT* src = a.u + g * LD;
       VT* dst = s_win + (size_t)i * LD;
@@ -975,6 +989,8 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
         for (int k = 0; k < RB / 16; k++) cp_async<16>(dst + k * E, src + k * E);
       }
     }
+  };
+  auto product_rows = [&](double acc[4]) {
     cp_async_wait_all();
     __syncthreads();
     const int e0 = s_sp[0];
@@ -1069,6 +1085,11 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
         row_done(sl, ak, am);
       }
     }
+  };
+
+  auto product = [&](double acc[4], bool own_done) {
+    fill_window(own_done);
+    product_rows(acc);
   };
 
   // residual refresh of the lanes in tr: r = b - A64 x (FP64), u = D^-1 r, publish u;
@@ -1177,7 +1198,7 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
   // ---- W: w = A u; w.u -> alpha = r.u / w.u
   {
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    if (ok) product(acc);
+    if (ok) product(acc, false);
     block_partial<4>(acc, a.part, sh);
   }
   ok = ok && grid_sync(a.bar, target);
@@ -1255,6 +1276,7 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
         stv<VT, LD>(pX, row, xv);
         stv<VT, LD>(pR, row, rv);
         stv<VT, LD>(pU, row, uv);
+        st_win<VT, LD>(s_win, lr, uv);  // the next product reads it from here
       }
       block_partial<8>(acc, a.part, sh);
     }
@@ -1265,14 +1287,16 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
     // ---- W: w = A u; w.u into slots 8..11.  The three sums are read together below.
     {
       double acc[4] = {0.0, 0.0, 0.0, 0.0};
-      product(acc);
+      fill_window(true);
+      grid_totals<8, 0>(a.part, s_tot, s_buf);  // r.u, r.r of this P phase: final already
+      product_rows(acc);
       block_partial<4>(acc, a.part + 8, sh);
     }
     clk.lap(0);
     ok = grid_sync(a.bar, target);
     clk.lap(1);
     if (!ok) break;
-    grid_totals<12>(a.part, s_tot, s_buf);
+    grid_totals<4, 8>(a.part, s_tot, s_buf);
     it++;
     // lanes in parallel: thread s owns lane s
     int trig = 0;
@@ -1333,7 +1357,7 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
       if (!ok) break;
       {
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
-        product(acc);
+        product(acc, false);
         block_partial<4>(acc, a.part + 8, sh);
       }
       ok = grid_sync(a.bar, target);
