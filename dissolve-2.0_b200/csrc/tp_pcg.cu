@@ -1119,6 +1119,89 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
     }
   };
 
+  // The FP64 residual with x read through the shared-memory window (own rows + halo at
+  // their window-local columns) instead of CSR gathers from global memory.  x is FP64, so
+  // a window entry holds CP = RB / 8 of its columns and the own rows are walked LD / CP
+  // times.  Each row sums its CSR entries in order (the SELL entries k < row length of a
+  // row are its CSR entries, in order), as csr64_residual does.
+  //   final = false: the refresh above (lanes in tr): r, u and partials [r.u | r.r | b.b]
+  //   final = true:  partials r.r of every lane into acc[0..3], nothing written
+  constexpr int CP = (RB >= 8) ? RB / 8 : 1;
+  constexpr bool WINRES = (RB % 8 == 0) && (LD % CP == 0);
+  auto refresh_win = [&](const int tr[LD], double* acc, bool final) {
+    const int W = nown + nhalo;
+    const int e0 = s_sp[0];
+    double* s_x = reinterpret_cast<double*>(s_win);  // entry i: CP doubles at s_x + i CP
+#pragma unroll
+    for (int c0 = 0; c0 < LD; c0 += CP) {
+      __syncthreads();  // the window may still be read (previous pass or product)
+      for (int i = threadIdx.x; i < W; i += blockDim.x) {
+        const int64_t g = (i < nown) ? (int64_t)(r0 + i) : (int64_t)s_halo[i - nown];
+        double* dst = s_x + (size_t)i * CP;
+        const double* src = a.x + g * LD + c0;
+        if constexpr (CP == 1) {
+          cp_async<8>(dst, src);
+        } else {
+#pragma unroll
+          for (int k = 0; k < CP / 2; k++) cp_async<16>(dst + 2 * k, src + 2 * k);
+        }
+      }
+      cp_async_wait_all();
+      __syncthreads();
+      FOR_OWN_ROWS {
+        const int lr = (int)(row - r0);
+        double xo[CP], ax[CP];
+#pragma unroll
+        for (int c = 0; c < CP; c++) xo[c] = s_x[lr * CP + c];
+        const bool bcr = a.bc && a.bc[row];
+        if (bcr) {
+#pragma unroll
+          for (int c = 0; c < CP; c++) ax[c] = xo[c];
+        } else {
+          double ak[CP], am[CP];
+#pragma unroll
+          for (int c = 0; c < CP; c++) ak[c] = am[c] = 0.0;
+          const int p0 = a.A64.indptr[row], len = a.A64.indptr[row + 1] - p0;
+          const int lb = s_sp[sl - sb] - e0;
+#pragma unroll 4
+          for (int k = 0; k < len; k++) {
+            const int loc = s_col[lb + k * 32 + lane];
+            const double kv = __ldg(a.A64.K + p0 + k);
+            const double mv = a.A64.M ? __ldg(a.A64.M + p0 + k) : 0.0;
+#pragma unroll
+            for (int c = 0; c < CP; c++) {
+              const double xv = s_x[loc * CP + c];
+              ak[c] += kv * xv;
+              if (a.A64.M) am[c] += mv * xv;
+            }
+          }
+#pragma unroll
+          for (int c = 0; c < CP; c++) {
+            const double dr = a.A64.diag ? a.A64.diag[row * LD + c0 + c] : 0.0;
+            ax[c] = a.dscale[c0 + c] * ak[c] + a.cscale[c0 + c] * am[c] + dr * xo[c];
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < CP; c++) {
+          const int s = c0 + c;
+          const double bv = (s < S) ? a.b[row * LD + s] : 0.0;
+          const double r64 = (s < S) ? bv - ax[c] : 0.0;
+          if (final) {
+            acc[s] += r64 * r64;
+          } else if (tr[s]) {
+            const VT rv = (VT)r64;
+            const VT uv = a.dinv[row * LD + s] * rv;
+            acc[s] += (double)rv * (double)uv;
+            acc[4 + s] += r64 * r64;
+            acc[8 + s] += bv * bv;
+            a.r[row * LD + s] = rv;
+            a.u[row * LD + s] = uv;
+          }
+        }
+      }
+    }
+  };
+
   // ---- I1: Jacobi diagonal (FP64 values), Dirichlet values into x, p = s = xi = 0
   FOR_OWN_ROWS {
     VT dv[LD], zero[LD], rz[LD];
@@ -1168,7 +1251,12 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
     int tr[LD];
 #pragma unroll
     for (int s = 0; s < LD; s++) tr[s] = 1;
-    if (ok) refresh(tr, acc);
+    if (ok) {
+      if constexpr (WINRES)
+        refresh_win(tr, acc, false);
+      else
+        refresh(tr, acc);
+    }
     block_partial<12>(acc, a.part, sh);
   }
   ok = ok && grid_sync(a.bar, target);
@@ -1350,7 +1438,10 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
         double acc[12];
 #pragma unroll
         for (int k = 0; k < 12; k++) acc[k] = 0.0;
-        refresh(tr, acc);
+        if constexpr (WINRES)
+          refresh_win(tr, acc, false);
+        else
+          refresh(tr, acc);
         block_partial<12>(acc, a.part, sh);  // slots 8..11 (b.b) are replaced by w.u
       }
       ok = grid_sync(a.bar, target);
@@ -1405,11 +1496,18 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
   {
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     if (ok2) {
-      FOR_OWN_ROWS {
-        double r64[LD];
-        csr64_residual<VT, LD>(a, row, r64);
+      if constexpr (WINRES) {
+        int none[LD];
 #pragma unroll
-        for (int s = 0; s < LD; s++) acc[s] += r64[s] * r64[s];
+        for (int s = 0; s < LD; s++) none[s] = 0;
+        refresh_win(none, acc, true);
+      } else {
+        FOR_OWN_ROWS {
+          double r64[LD];
+          csr64_residual<VT, LD>(a, row, r64);
+#pragma unroll
+          for (int s = 0; s < LD; s++) acc[s] += r64[s] * r64[s];
+        }
       }
     }
     block_partial<4>(acc, a.part, sh);
