@@ -40,7 +40,7 @@ METRIC = "3-species BE steps/s at 1.57M P1 tets, rtol 1e-8: mixed+learned vs pla
 N_SIDE, JITTER = 64, 0.2
 D_S, K_S, DT, RTOL = (1.0, 1.0, 2.6), (0.5, 0.0, 0.2), 0.02, 1e-8
 # measured with ncu on this workload (see profiles/); None until captured
-DRAM_BYTES_PER_ITERATION = 13.40e6  # 3.592 GB over a 268-iteration launch
+DRAM_BYTES_PER_ITERATION = 11.30e6  # 3.040 GB over a 269-iteration launch of k_cgw
 WORKLOAD = ("3-species backward-Euler step, 64^3 Kuhn cube (1,572,864 P1 tets, 274,625 "
             "vertices), jitter 0.2h, De = D_s exp(0.3 xi), rtol 1e-8")
 
