@@ -166,6 +166,141 @@ __global__ void __launch_bounds__(256) k_csr_images(int64_t n, const int32_t* __
   }
 }
 
+// ---------------------------------------------------------------- guess projection
+// The learned guess projected in the energy norm.  With A = D K + diag (identity rows
+// where bc), u = u^n, du = u^n - u^{n-1} and the network's direction d, the guess is
+// x = u + a du + c d on the free rows, (a, c) per column from the 2x2 Galerkin system
+//   [du.A du  du.A d] [a]   [du.r0]
+//   [ d.A du   d.A d] [c] = [ d.r0],   r0 = b - A u,
+// which minimises the A-norm of the error over that plane: the guess is never worse than
+// u^n in that norm (a = c = 0 is in the plane).  Sums run over the free rows; d is taken
+// as zero on the Dirichlet rows, which keep x = b.
+constexpr int GP_BLOCKS = 512, GP_Q = 5;  // 5 sums per column: du.Adu du.Ad d.Ad du.r0 d.r0
+
+template <int LD, int G>
+__global__ void __launch_bounds__(256) k_guess_dots(
+    int64_t n, int S, const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+    const double* __restrict__ K, double4 dsc, const double* __restrict__ diag,
+    const uint8_t* __restrict__ bc, const double* __restrict__ b, const double* __restrict__ U,
+    const double* __restrict__ Up, const double* __restrict__ opU,
+    const double* __restrict__ opDU, const double* __restrict__ d, double* __restrict__ part) {
+  __shared__ double sh[32];
+  const double dscale[4] = {dsc.x, dsc.y, dsc.z, dsc.w};
+  const int gl = threadIdx.x % G;
+  const int64_t rpb = blockDim.x / G;
+  double acc[GP_Q][LD];
+#pragma unroll
+  for (int q = 0; q < GP_Q; q++)
+#pragma unroll
+    for (int s = 0; s < LD; s++) acc[q][s] = 0.0;
+  for (int64_t base = blockIdx.x * rpb; base < n; base += (int64_t)gridDim.x * rpb) {
+    const int64_t row = base + threadIdx.x / G;
+    const int64_t rr = row < n ? row : n - 1;
+    double kd[LD];
+#pragma unroll
+    for (int s = 0; s < LD; s++) kd[s] = 0.0;
+    const int beg = indptr[rr], end = indptr[rr + 1];
+    for (int p = beg + gl; p < end; p += G) {
+      const int j = __ldg(indices + p);
+      if (bc && bc[j]) continue;
+      const double kv = __ldg(K + p);
+      double dv[LD];
+      ldv<double, LD>(d, j, dv);
+#pragma unroll
+      for (int s = 0; s < LD; s++) kd[s] += kv * dv[s];
+    }
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1)
+#pragma unroll
+      for (int s = 0; s < LD; s++) kd[s] += __shfl_xor_sync(0xffffffffu, kd[s], o, G);
+    if (row < n && gl == 0 && !(bc && bc[row])) {
+      double u[LD], up[LD], dd[LD], dg[LD], bv[LD], iu[LD], idu[LD];
+      ldv<double, LD>(U, row, u);
+      ldv<double, LD>(Up, row, up);
+      ldv<double, LD>(d, row, dd);
+      ldv<double, LD>(diag, row, dg);
+      ldv<double, LD>(b, row, bv);
+      ldv<double, LD>(opU, row, iu);
+      ldv<double, LD>(opDU, row, idu);
+#pragma unroll
+      for (int s = 0; s < LD; s++) {
+        if (s >= S) continue;
+        const double du = u[s] - up[s];
+        const double Au = iu[s] + dg[s] * u[s];
+        const double Adu = idu[s] + dg[s] * du;
+        const double Ad = dscale[s] * kd[s] + dg[s] * dd[s];
+        const double r0 = bv[s] - Au;
+        acc[0][s] += du * Adu;
+        acc[1][s] += du * Ad;
+        acc[2][s] += dd[s] * Ad;
+        acc[3][s] += du * r0;
+        acc[4][s] += dd[s] * r0;
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < GP_Q; q++)
+#pragma unroll
+    for (int s = 0; s < LD; s++) {
+      const double v = block_sum(acc[q][s], sh);
+      if (threadIdx.x == 0) part[(int64_t)blockIdx.x * GP_Q * 4 + q * 4 + s] = v;
+    }
+}
+
+// one block: the sums over the partials in a fixed order, then (a, c) per column into
+// coef[2 s], coef[2 s + 1]
+__global__ void __launch_bounds__(256) k_guess_coeffs(int nparts, int S,
+                                                      const double* __restrict__ part,
+                                                      double* __restrict__ coef) {
+  __shared__ double sh[32];
+  __shared__ double tot[GP_Q * 4];
+  for (int k = 0; k < GP_Q * 4; k++) {
+    double v = 0.0;
+    for (int bl = threadIdx.x; bl < nparts; bl += blockDim.x) v += part[(int64_t)bl * GP_Q * 4 + k];
+    v = block_sum(v, sh);
+    if (threadIdx.x == 0) tot[k] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    const int s = threadIdx.x;
+    double a = 0.0, c = 0.0;
+    if (s < S) {
+      const double g11 = tot[0 * 4 + s], g12 = tot[1 * 4 + s], g22 = tot[2 * 4 + s];
+      const double h1 = tot[3 * 4 + s], h2 = tot[4 * 4 + s];
+      const double det = g11 * g22 - g12 * g12;
+      if (g11 > 0.0 && g22 > 0.0 && det > 1e-12 * g11 * g22) {
+        a = (h1 * g22 - h2 * g12) / det;
+        c = (g11 * h2 - g12 * h1) / det;
+      } else if (g11 > 0.0 && (!(g22 > 0.0) || h1 * h1 / g11 >= h2 * h2 / g22)) {
+        a = h1 / g11;  // (nearly) collinear directions: the better single one
+      } else if (g22 > 0.0) {
+        c = h2 / g22;
+      }
+      if (!isfinite(a) || !isfinite(c)) a = c = 0.0;
+    }
+    coef[2 * s] = a;
+    coef[2 * s + 1] = c;
+  }
+}
+
+template <int LD>
+__global__ void k_guess_update(int64_t n, int S, const uint8_t* __restrict__ bc,
+                               const double* __restrict__ b, const double* __restrict__ U,
+                               const double* __restrict__ Up, const double* __restrict__ d,
+                               const double* __restrict__ coef, double* __restrict__ x) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n * LD;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = i / LD;
+    const int s = (int)(i - row * LD);
+    double v = U[i];
+    if (bc && bc[row])
+      v = (s < S) ? b[i] : v;
+    else if (s < S)
+      v = v + coef[2 * s] * (v - Up[i]) + coef[2 * s + 1] * d[i];
+    x[i] = v;
+  }
+}
+
 template <typename T>
 static int launch_matfree(const tp_mesh* m, int S, int ld, const double* De, const double* al,
                           double4 dsc, double4 shf, double inv_dt, int lumped, int legacy,
@@ -296,6 +431,48 @@ extern "C" int tp_csr_images(const tp_csr_op* op, const double* x1, const double
   else
     k_csr_images<4, G><<<grid, 256, 0, st>>>(op->n_rows, op->indptr, op->indices, op->K64, dsc,
                                              x1, x2, y1, y2);
+  TP_LAUNCH_CHECK();
+  return TP_OK;
+}
+
+extern "C" size_t tp_guess_project_workspace_doubles(void) {
+  return (size_t)GP_BLOCKS * GP_Q * 4 + 8;
+}
+
+extern "C" int tp_guess_project(const tp_csr_op* op, const double* diag, const uint8_t* bc_mask,
+                                const double* b, const double* U, const double* U_prev,
+                                const double* opU, const double* opDU, const double* d,
+                                double* x, double* work, void* stream) {
+  TP_REQUIRE(op && op->indptr && op->indices && op->K64 && diag && b && U && U_prev && opU &&
+                 opDU && d && x && work,
+             "null pointer");
+  TP_REQUIRE(op->ld == 1 || op->ld == 2 || op->ld == 4, "ld must be 1, 2 or 4");
+  TP_REQUIRE(op->S >= 1 && op->S <= op->ld, "bad S");
+  if (op->n_rows == 0) return TP_OK;
+  cudaStream_t st = as_stream(stream);
+  constexpr int G = 4;
+  const double4 dsc = make_double4(op->S > 0 ? op->dscale[0] : 0.0, op->S > 1 ? op->dscale[1] : 0.0,
+                                   op->S > 2 ? op->dscale[2] : 0.0, op->S > 3 ? op->dscale[3] : 0.0);
+  const int nb = (int)std::min<int64_t>(GP_BLOCKS, (op->n_rows + 63) / 64);
+  double* part = work;
+  double* coef = work + (size_t)GP_BLOCKS * GP_Q * 4;
+  const int64_t n = op->n_rows;
+#define TP_GP(LDV)                                                                          \
+  do {                                                                                      \
+    k_guess_dots<LDV, G><<<nb, 256, 0, st>>>(n, op->S, op->indptr, op->indices, op->K64,    \
+                                             dsc, diag, bc_mask, b, U, U_prev, opU, opDU,   \
+                                             d, part);                                      \
+    k_guess_coeffs<<<1, 256, 0, st>>>(nb, op->S, part, coef);                               \
+    k_guess_update<LDV><<<grid_for(n * LDV, 256, sm_count() * 8), 256, 0, st>>>(           \
+        n, op->S, bc_mask, b, U, U_prev, d, coef, x);                                       \
+  } while (0)
+  if (op->ld == 1)
+    TP_GP(1);
+  else if (op->ld == 2)
+    TP_GP(2);
+  else
+    TP_GP(4);
+#undef TP_GP
   TP_LAUNCH_CHECK();
   return TP_OK;
 }

@@ -7,7 +7,9 @@
 //   0 phi, 1 |grad phi|, 2 u^n, 3 u^{n-1}, 4 u^n - u^{n-1}, 5 log D_s, 6 k_s, 7 1,
 //   8 (D_s K u^n)_v, 9 (D_s K (u^n - u^{n-1}))_v -- the stiffness images give the
 //   network the local curvature that decides how fast each part of the change decays
-// The output y predicts (u^{n+1} - u^n) / sigma; the guess is u^n + sigma y.
+// The output y predicts (u^{n+1} - B) / sigma and the guess is B + sigma y, with the base
+// B = u^n or the linear extrapolation 2 u^n - u^{n-1} (the network learns the correction
+// to the extrapolation: with zero output the guess is the extrapolation itself).
 //
 // Tensor-core fragments are those of mma.sync.m16n8k16 (row.col, bf16 x bf16 -> f32):
 // a warp owns 16 rows; layer outputs stay in registers and are re-packed from the
@@ -47,6 +49,7 @@ struct MlpFeat {
   const double* opU;    // (V, ld) D_s K u^n or NULL
   const double* opDU;   // (V, ld) D_s K (u^n - u^{n-1}) or NULL
   int S, ld;
+  int base;  // the guess the output corrects: 0 u^n, 1 2 u^n - u^{n-1}, 2 none
   float logD[4], k[4];
   float mean[NFEAT], istd[NFEAT];
 };
@@ -236,7 +239,8 @@ __global__ void __launch_bounds__(128) k_mlp_predict(MlpFeat F, int64_t nrows,
       if (r < nrows) {
         if (x_out) {
           const int64_t i = (h ? vv[1] : vv[0]) * F.ld + (h ? ss[1] : ss[0]);
-          x_out[i] = F.U[i] + (double)sigma * (double)y;
+          const double b = F.base == 1 ? 2.0 * F.U[i] - F.Up[i] : (F.base == 0 ? F.U[i] : 0.0);
+          x_out[i] = b + (double)sigma * (double)y;
         } else {
           y_out[r] = y;
         }
@@ -269,13 +273,16 @@ __global__ void k_mlp_features(MlpFeat F, int64_t nrows, __nv_bfloat16* __restri
 
 // training target (u^{n+1} - u^n) / sigma per row
 __global__ void k_mlp_target(int64_t nrows, int S, int ld, const double* __restrict__ Un,
+                             const double* __restrict__ Uprev,
                              const double* __restrict__ Unext, float inv_sigma,
                              float* __restrict__ T) {
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < nrows;
        r += (int64_t)gridDim.x * blockDim.x) {
     const int64_t v = r / S;
     const int s = (int)(r - v * S);
-    T[r] = (float)((Unext[v * ld + s] - Un[v * ld + s]) * inv_sigma);
+    const int64_t i = v * ld + s;
+    const double b = Uprev ? 2.0 * Un[i] - Uprev[i] : Un[i];
+    T[r] = (float)((Unext[i] - b) * inv_sigma);
   }
 }
 
@@ -532,6 +539,7 @@ static MlpFeat make_feat(const tp_mlp_inputs* in) {
   F.opDU = in->opDU;
   F.S = in->S;
   F.ld = in->ld;
+  F.base = in->base;
   for (int s = 0; s < 4; s++) {
     F.logD[s] = (float)in->logD[s];
     F.k[s] = (float)in->k[s];
@@ -549,6 +557,7 @@ extern "C" int tp_mlp_predict(const tp_mlp_inputs* in, const float* params, floa
                               double* x_out, float* y_out, void* stream) {
   TP_REQUIRE(in && in->U && in->U_prev && params && (x_out || y_out), "null pointer");
   TP_REQUIRE(in->S >= 1 && in->S <= 4 && in->ld >= in->S, "bad S/ld");
+  TP_REQUIRE(in->base >= 0 && in->base <= 2, "base must be 0 (u^n), 1 (2 u^n - u^{n-1}) or 2 (none)");
   const int64_t nrows = in->n_verts * in->S;
   if (nrows == 0) return TP_OK;
   const int64_t ntiles = (nrows + 15) / 16;
@@ -570,12 +579,13 @@ extern "C" int tp_mlp_features(const tp_mlp_inputs* in, void* X, void* stream) {
 }
 
 extern "C" int tp_mlp_target(int64_t n_verts, int S, int ld, const double* U_n,
-                             const double* U_next, double sigma, float* T, void* stream) {
+                             const double* U_prev, const double* U_next, double sigma, float* T,
+                             void* stream) {
   TP_REQUIRE(U_n && U_next && T && sigma > 0, "bad argument");
   const int64_t nrows = n_verts * S;
   if (nrows == 0) return TP_OK;
   k_mlp_target<<<grid_for(nrows, 256, 65535), 256, 0, as_stream(stream)>>>(
-      nrows, S, ld, U_n, U_next, (float)(1.0 / sigma), T);
+      nrows, S, ld, U_n, U_prev, U_next, (float)(1.0 / sigma), T);
   TP_LAUNCH_CHECK();
   return TP_OK;
 }

@@ -71,7 +71,7 @@ class TpMlpInputs(ctypes.Structure):
     _fields_ = [("n_verts", _c_i64), ("S", _c_i32), ("ld", _c_i32), ("U", _vp), ("U_prev", _vp),
                 ("phi", _vp), ("normgradphi", _vp), ("opU", _vp), ("opDU", _vp),
                 ("logD", _c_dbl * 4), ("k", _c_dbl * 4), ("mean", _c_dbl * 10),
-                ("istd", _c_dbl * 10)]
+                ("istd", _c_dbl * 10), ("base", _c_i32)]
 
 
 class TpCgResult(ctypes.Structure):
@@ -132,6 +132,9 @@ SIGNATURES = {
                                         ctypes.c_int, _vp, _vp, _vp]),
     "tp_csr_apply": (ctypes.c_int, [_P(TpCsrOp), ctypes.c_int, _vp, _vp, _vp]),
     "tp_csr_images": (ctypes.c_int, [_P(TpCsrOp), _vp, _vp, _vp, _vp, _vp]),
+    "tp_guess_project_workspace_doubles": (ctypes.c_size_t, []),
+    "tp_guess_project": (ctypes.c_int, [_P(TpCsrOp), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                        _vp, _vp, _vp]),
     "tp_cg_workspace_bytes": (ctypes.c_size_t, [_P(TpCsrOp), _P(TpCgConfig)]),
     "tp_cg_create": (ctypes.c_int, [_P(TpCsrOp), _P(TpCgConfig), _vp, _vp, _vp, _vp,
                                     ctypes.c_size_t, _vp, _P(_vp)]),
@@ -154,8 +157,8 @@ SIGNATURES = {
     "tp_mlp_param_count": (ctypes.c_int, []),
     "tp_mlp_predict": (ctypes.c_int, [_P(TpMlpInputs), _vp, ctypes.c_float, _vp, _vp, _vp]),
     "tp_mlp_features": (ctypes.c_int, [_P(TpMlpInputs), _vp, _vp]),
-    "tp_mlp_target": (ctypes.c_int, [_c_i64, ctypes.c_int, ctypes.c_int, _vp, _vp, _c_dbl, _vp,
-                                     _vp]),
+    "tp_mlp_target": (ctypes.c_int, [_c_i64, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _c_dbl,
+                                     _vp, _vp]),
     "tp_mlp_grad_workspace_floats": (ctypes.c_size_t, [ctypes.c_int]),
     "tp_mlp_train_step": (ctypes.c_int, [_vp, _vp, _c_i64, _c_i64, _vp, _vp, _vp, ctypes.c_int,
                                          ctypes.c_float, ctypes.c_float, ctypes.c_float,

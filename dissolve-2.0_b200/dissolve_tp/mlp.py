@@ -2,7 +2,8 @@
 initial guess (kernels in csrc/tp_mlp.cu, C ABI tp_mlp_*).
 
 The network is trained on trajectories the solver itself produces (pairs u^{n-1}, u^n ->
-u^{n+1}), by the project's own forward/backward/AdamW kernels.  The Krylov solve always
+u^{n+1}), by the project's own forward/backward/AdamW kernels.  It predicts the
+correction to a base guess, by default the linear extrapolation 2 u^n - u^{n-1}.  The Krylov solve always
 runs to the same tolerance, so the guess only changes how many iterations it takes: the
 plain method is both the fallback (no predictor -> previous step) and the judge of the
 prediction's error.
@@ -39,7 +40,19 @@ def initial_params(seed: int = 3) -> np.ndarray:
 
 
 class WarmStartMLP:
-    def __init__(self, device, seed: int = 3, capacity_rows: int = 0, grid: int = 0):
+    def __init__(self, device, seed: int = 3, capacity_rows: int = 0, grid: int = 0,
+                 base: str = "extrapolate", project: bool = True):
+        """base: the guess the network corrects, "previous" (u^n) or "extrapolate"
+        (2 u^n - u^{n-1}); the training target is (u^{n+1} - base) / sigma.
+        project: the transport guess is u^n + a (u^n - u^{n-1}) + c sigma y with (a, c) per
+        species from the energy-norm (Galerkin) projection of tp_guess_project, never
+        worse than the previous-step guess in that norm; False: base + sigma y as is."""
+        if base not in ("previous", "extrapolate"):
+            raise ValueError("base must be 'previous' or 'extrapolate'")
+        self.base = base
+        self.project = bool(project)
+        self._d = None
+        self._work = None
         if int(_lib.lib.tp_mlp_param_count()) != P:
             raise RuntimeError("parameter layout mismatch with the library")
         self.device = device
@@ -58,14 +71,17 @@ class WarmStartMLP:
         self.T = torch.empty(max(capacity_rows, 1), dtype=torch.float32, device=device)
         self.rows = 0
         self.rng = np.random.default_rng(seed)
-        self.launches = 2  # per guess: the stiffness images, the network
+        # per guess: the stiffness images, the network (+ dots, coefficients, update)
+        self.launches = 5 if self.project else 2
 
     # ---- inputs -----------------------------------------------------------------
-    def inputs(self, U, Up, S, ld, D, k, phi=None, ngphi=None, ops=None) -> TpMlpInputs:
+    def inputs(self, U, Up, S, ld, D, k, phi=None, ngphi=None, ops=None,
+               base: int | None = None) -> TpMlpInputs:
         st = TpMlpInputs()
         st.n_verts = int(U.shape[0])
         st.S, st.ld = int(S), int(ld)
         st.U, st.U_prev = ptr(U), ptr(Up)
+        st.base = (1 if self.base == "extrapolate" else 0) if base is None else int(base)
         st.phi, st.normgradphi = ptr(phi), ptr(ngphi)
         opU, opDU = ops if ops is not None else (None, None)
         st.opU, st.opDU = ptr(opU), ptr(opDU)
@@ -84,7 +100,8 @@ class WarmStartMLP:
         up = np.concatenate([p[0][:, :S].cpu().numpy().reshape(-1) for p in pairs])
         un = np.concatenate([p[1][:, :S].cpu().numpy().reshape(-1) for p in pairs])
         nx = np.concatenate([p[2][:, :S].cpu().numpy().reshape(-1) for p in pairs])
-        du, tg = un - up, nx - un
+        du = un - up
+        tg = nx - (2.0 * un - up if self.base == "extrapolate" else un)
         raw = [np.zeros(1) if phi is None else phi.cpu().numpy(),
                np.zeros(1) if ngphi is None else ngphi.cpu().numpy(), un, up, du,
                np.log(np.asarray(D, dtype=np.float64)), np.asarray(k, dtype=np.float64),
@@ -116,7 +133,8 @@ class WarmStartMLP:
                               None if ops is None else ops[i])
             r0 = self.rows
             call("tp_mlp_features", ctypes.byref(inp), ptr(self.X) + r0 * IN * 2, st)
-            call("tp_mlp_target", V, S, ld, ptr(Un), ptr(Unx), float(self.sigma),
+            call("tp_mlp_target", V, S, ld, ptr(Un),
+                 ptr(Up) if self.base == "extrapolate" else None, ptr(Unx), float(self.sigma),
                  ptr(self.T) + r0 * 4, st)
             self.rows += V * S
 
@@ -146,8 +164,11 @@ class WarmStartMLP:
         return g, self.loss_dev
 
     # ---- inference --------------------------------------------------------------
-    def predict(self, U, Up, S, ld, D, k, phi=None, ngphi=None, x_out=None, ops=None):
-        inp = self.inputs(U, Up, S, ld, D, k, phi, ngphi, ops)
+    def predict(self, U, Up, S, ld, D, k, phi=None, ngphi=None, x_out=None, ops=None,
+                base: int | None = None):
+        """x_out = base + sigma y (base: 0 u^n, 1 2 u^n - u^{n-1}, 2 none; default from
+        the constructor), or y itself when x_out is None."""
+        inp = self.inputs(U, Up, S, ld, D, k, phi, ngphi, ops, base)
         if x_out is not None:
             call("tp_mlp_predict", ctypes.byref(inp), ptr(self.params), float(self.sigma),
                  ptr(x_out), None, stream_handle())
@@ -158,9 +179,22 @@ class WarmStartMLP:
         return y
 
     def predict_into(self, tr, x):
-        """The transport driver's hook: guess for tr's next step written into x."""
-        self.predict(tr.U, tr.U_prev, tr.S, tr.ld, tr.D, tr.k, getattr(tr, "phi", None),
-                     getattr(tr, "ngphi", None), x_out=x, ops=tr.operator_images())
+        """The transport driver's hook: guess for tr's next step written into x (tr's
+        right-hand side tr.solver.b and diagonal tr.D64 are already assembled)."""
+        ops = tr.operator_images()
+        phi, ngphi = getattr(tr, "phi", None), getattr(tr, "ngphi", None)
+        if not self.project:
+            self.predict(tr.U, tr.U_prev, tr.S, tr.ld, tr.D, tr.k, phi, ngphi, x_out=x, ops=ops)
+            return
+        if self._d is None or self._d.shape != tr.U.shape:
+            self._d = torch.zeros_like(tr.U)  # padding columns stay zero
+            self._work = torch.empty(int(_lib.lib.tp_guess_project_workspace_doubles()),
+                                     dtype=torch.float64, device=self.device)
+        self.predict(tr.U, tr.U_prev, tr.S, tr.ld, tr.D, tr.k, phi, ngphi, x_out=self._d,
+                     ops=ops, base=2)
+        call("tp_guess_project", ctypes.byref(tr.stiff_op.struct), ptr(tr.D64),
+             ptr(tr.bc_mask), ptr(tr.solver.b), ptr(tr.U), ptr(tr.U_prev), ptr(ops[0]),
+             ptr(ops[1]), ptr(self._d), ptr(x), ptr(self._work), stream_handle())
 
 
 def trajectory_pairs(tr, steps):

@@ -302,6 +302,21 @@ TP_API int tp_csr_apply(const tp_csr_op* op, int fp32, const void* x, void* y, v
 TP_API int tp_csr_images(const tp_csr_op* op, const double* x1, const double* x2, double* y1,
                          double* y2, void* stream);
 
+/* The learned initial guess projected in the energy norm (no reference counterpart).
+ * op: the stiffness D K (K64, dscale, S, ld); with A = D K + diag (diag (n_rows, ld); identity
+ * rows where bc_mask), r0 = b - A U and du = U - U_prev, writes
+ *   x = U + a du + c d   (free rows),   x = b   (Dirichlet rows, columns < S),
+ * (a, c) per column solving the 2x2 Galerkin system on span{du, d} (d: the network's
+ * direction, taken as zero on Dirichlet rows) -- the minimum of the A-norm of the error over
+ * that plane, so never above the previous-step guess U in that norm.  opU = D K U and
+ * opDU = D K du (tp_csr_images).  Deterministic.  work: device scratch of
+ * tp_guess_project_workspace_doubles() doubles. */
+TP_API size_t tp_guess_project_workspace_doubles(void);
+TP_API int tp_guess_project(const tp_csr_op* op, const double* diag, const uint8_t* bc_mask,
+                            const double* b, const double* U, const double* U_prev,
+                            const double* opU, const double* opDU, const double* d, double* x,
+                            double* work, void* stream);
+
 /* ------------------------------------------------------------------ Krylov solve */
 /* Jacobi-preconditioned CG on every (system, column) lane at once, captured in a CUDA
  * graph whose device-side while loop runs until every lane converges or max_it.
@@ -440,18 +455,24 @@ typedef struct tp_mlp_inputs {
   const double* opDU;        /* (n_verts, ld) D_s K (u^n - u^{n-1}), or NULL           */
   double logD[4], k[4];      /* per species             */
   double mean[10], istd[10]; /* input normalisation (features 0..9) */
+  int32_t base;              /* the guess the network corrects: 0 u^n, 1 2 u^n - u^{n-1},
+                                2 none (tp_mlp_predict writes sigma y alone)             */
 } tp_mlp_inputs;
 
 TP_API int tp_mlp_param_count(void);
-/* x_out[v, s] = U[v, s] + sigma * y(v, s) (the guess, written into a solver's x), or
+/* x_out[v, s] = B[v, s] + sigma * y(v, s) (the guess, written into a solver's x), with
+ * B = U (base 0), 2 U - U_prev (base 1, linear extrapolation) or 0 (base 2: the scaled
+ * output alone, the direction tp_guess_project takes), or
  * y_out[v * S + s] = y when x_out is NULL */
 TP_API int tp_mlp_predict(const tp_mlp_inputs* in, const float* params, float sigma,
                           double* x_out, float* y_out, void* stream);
 /* the normalised inputs as BF16 rows of 16 (training set) */
 TP_API int tp_mlp_features(const tp_mlp_inputs* in, void* X_bf16, void* stream);
-/* training target (U_next - U_n) / sigma per row */
+/* training target (U_next - B) / sigma per row, B = U_n (U_prev NULL) or
+ * 2 U_n - U_prev (the base of tp_mlp_inputs.base = 1) */
 TP_API int tp_mlp_target(int64_t n_verts, int S, int ld, const double* U_n,
-                         const double* U_next, double sigma, float* T, void* stream);
+                         const double* U_prev, const double* U_next, double sigma, float* T,
+                         void* stream);
 TP_API size_t tp_mlp_grad_workspace_floats(int grid);
 /* one AdamW step on rows [row0, row0 + nrows) of (X, T), loss = mean squared error.
  * grid CTAs write partial gradients into workspace (tp_mlp_grad_workspace_floats(grid)).

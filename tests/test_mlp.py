@@ -94,7 +94,8 @@ def test_gpu_adamw_step_matches_oracle(cuda_device):
 
 
 @pytest.mark.gpu
-def test_gpu_forward_from_fields_matches_oracle(cuda_device):
+@pytest.mark.parametrize("base", ["previous", "extrapolate"])
+def test_gpu_forward_from_fields_matches_oracle(cuda_device, base):
     import torch
 
     from dissolve_tp.mlp import WarmStartMLP
@@ -105,7 +106,7 @@ def test_gpu_forward_from_fields_matches_oracle(cuda_device):
     phi = rng.normal(0, 1, V)
     ng = np.abs(rng.normal(1, 0.2, V))
     D, k = [1.0, 1.0, 2.6], [0.5, 0.0, 0.2]
-    m = WarmStartMLP(cuda_device)
+    m = WarmStartMLP(cuda_device, base=base)
     m.mean = np.array([0.0, 1.0, 0.5, 0.5, 0.0, 0.3, 0.2, 0.0, 0.1, -0.1])
     m.istd = np.array([1.0, 5.0, 3.0, 3.0, 20.0, 2.0, 4.0, 1.0, 0.5, 2.0])
     m.sigma = 0.01
@@ -127,8 +128,16 @@ def test_gpu_forward_from_fields_matches_oracle(cuda_device):
     assert np.abs(y - yo).max() <= 2e-3 * np.abs(yo).max()
     x = torch.zeros_like(Ud)
     m.predict(Ud, Upd, S, ld, D, k, phid, ngd, x_out=x, ops=ops)
-    xo = U + m.sigma * yo.reshape(V, S)
+    b = 2.0 * U - Up if base == "extrapolate" else U
+    xo = b + m.sigma * yo.reshape(V, S)
     assert np.abs(x[:, :S].cpu().numpy() - xo).max() <= 2e-3 * m.sigma * np.abs(yo).max() + 1e-12
+    # training target: (u^{n+1} - base) / sigma, rounded to FP32
+    Un1 = U + rng.normal(0, 0.02, (V, S))
+    Un1d = torch.zeros_like(Ud)
+    Un1d[:, :S] = torch.from_numpy(Un1)
+    m.add_pairs([(Upd, Ud, Un1d)], S, ld, D, k, phid, ngd, ops=[ops])
+    To = ((Un1 - b) / m.sigma).reshape(-1)
+    assert np.abs(m.T[: V * S].cpu().numpy() - To).max() <= 1e-6 * np.abs(To).max()
 
 
 @pytest.mark.gpu
@@ -159,3 +168,72 @@ def test_learned_guess_reduces_iterations(cuda_device):
     assert sum(learned[0][1:]) < sum(prev[0][1:]), (prev[0], learned[0])
     # the guess only changes the iteration count: both solves meet the same tolerance
     assert np.linalg.norm(learned[1] - prev[1]) / np.linalg.norm(prev[1]) < 1e-7
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("with_bc", [False, True])
+def test_guess_projection_matches_galerkin_solve(cuda_device, with_bc):
+    """tp_guess_project against the 2x2 Galerkin solve done with scipy on the same
+    operator; the projected guess is never worse than u^n in the energy norm."""
+    import ctypes
+
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    import torch
+
+    from dissolve_tp import _lib
+    from dissolve_tp._lib import call
+    from dissolve_tp.device import ptr, stream_handle
+    from dissolve_tp.mesh import face_dofs, kuhn_cube
+    from dissolve_tp.transport import BatchedTransport
+    m = kuhn_cube(8, 0.2, seed=0)
+    coef = np.exp(0.3 * np.random.default_rng(1).standard_normal(m.n_cells))
+    D, K, S = (1.0, 1.0, 2.6), (0.5, 0.0, 0.2), 3
+    bcv = [1.0, 0.5, 0.2]
+    bc = face_dofs(m, 0, "min") if with_bc else None
+    tr = BatchedTransport(m, coef, D, K, 0.02, bc_dofs=bc, bc_values=bcv if with_bc else None)
+    rng = np.random.default_rng(3)
+    U = rng.uniform(0, 1, (m.n_verts, S))
+    Up = U + rng.normal(0, 0.05, U.shape)
+    if with_bc:
+        U[bc] = bcv
+        Up[bc] = bcv
+    tr.set_state(U, Up)
+    tr.assemble_operator()
+    tr.assemble_rhs()
+    d = torch.zeros_like(tr.U)
+    dn = rng.normal(0, 0.02, U.shape)
+    d[:, :S] = torch.from_numpy(dn)
+    opU, opDU = tr.operator_images()
+    x = torch.zeros_like(tr.U)
+    work = torch.empty(int(_lib.lib.tp_guess_project_workspace_doubles()), dtype=torch.float64,
+                       device=cuda_device)
+    call("tp_guess_project", ctypes.byref(tr.stiff_op.struct), ptr(tr.D64), ptr(tr.bc_mask),
+         ptr(tr.solver.b), ptr(tr.U), ptr(tr.U_prev), ptr(opU), ptr(opDU), ptr(d), ptr(x),
+         ptr(work), stream_handle())
+    xg = x.cpu().numpy()
+    n = m.n_verts
+    Km = sp.csr_matrix((tr.K64.cpu().numpy(), tr.dm.indices[: tr.dm.nnz].cpu().numpy(),
+                        tr.dm.indptr.cpu().numpy()), shape=(n, n))
+    dg = tr.D64.cpu().numpy()
+    b = tr.solver.b.cpu().numpy()
+    free = np.ones(n, bool)
+    if with_bc:
+        free[bc] = False
+    for s in range(S):
+        A = (D[s] * Km + sp.diags(dg[:, s])).tocsr()
+        AF = A[free][:, free]
+        u, du = U[:, s], U[:, s] - Up[:, s]
+        dd = np.where(free, dn[:, s], 0.0)
+        r0 = (b[:, s] - A @ u)[free]
+        Adu, Ad = (A @ du)[free], (A @ dd)[free]
+        G = np.array([[du[free] @ Adu, du[free] @ Ad], [dd[free] @ Adu, dd[free] @ Ad]])
+        a, c = np.linalg.solve(0.5 * (G + G.T), [du[free] @ r0, dd[free] @ r0])
+        xr = np.where(free, u + a * du + c * dd, b[:, s])
+        assert np.abs(xg[:, s] - xr).max() <= 1e-9 * np.abs(xr).max(), s
+        # energy norm of the free-row error against the exact solution
+        xs = u.copy()
+        xs[free] = spla.spsolve(AF.tocsc(), b[free, s] - (A[free][:, ~free] @ u[~free]
+                                                          if with_bc else 0.0))
+        e_new, e_old = (xg[:, s] - xs)[free], (u - xs)[free]
+        assert e_new @ (AF @ e_new) <= e_old @ (AF @ e_old) * (1 + 1e-12)
