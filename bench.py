@@ -70,17 +70,20 @@ class ClockSampler:
         import pynvml
         h = pynvml.nvmlDeviceGetHandleByIndex(self.idx)
         self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
-        while not self._stop.is_set():
+        while True:
             self.samples.append(float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)))
             mask = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
             for nm, bit in self.REASONS.items():
                 if mask & bit:
                     self.reasons.add(nm)
-            self._stop.wait(self.period)
+            self._ready.set()
+            if self._stop.wait(self.period):
+                break
 
     def __enter__(self):
         import threading
         self._stop = threading.Event()
+        self._ready = threading.Event()
         self._thr = None
         try:
             import pynvml
@@ -90,6 +93,9 @@ class ClockSampler:
                 self.idx = int(dev.split(",")[self.idx].strip())
             self._thr = threading.Thread(target=self._run, daemon=True)
             self._thr.start()
+            # the first sample is taken before the timed region starts (NVML set-up can
+            # take longer than the whole region)
+            self._ready.wait(timeout=5.0)
         except Exception as e:  # no NVML: report no samples
             self.error = str(e)
         return self

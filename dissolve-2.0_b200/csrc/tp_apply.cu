@@ -175,24 +175,26 @@ __global__ void __launch_bounds__(256) k_csr_images(int64_t n, const int32_t* __
 // which minimises the A-norm of the error over that plane: the guess is never worse than
 // u^n in that norm (a = c = 0 is in the plane).  Sums run over the free rows; d is taken
 // as zero on the Dirichlet rows, which keep x = b.
-constexpr int GP_BLOCKS = 512, GP_Q = 5;  // 5 sums per column: du.Adu du.Ad d.Ad du.r0 d.r0
+constexpr int GP_BLOCKS = 592, GP_Q = 5;  // 5 sums per column: du.Adu du.Ad d.Ad du.r0 d.r0
 
-template <int LD, int G>
+// A d by a CSR pass (G = LD lanes per row), then lane s of the row's group takes column s:
+// its loads of the row's fields are contiguous across the group.  Partials: one row of
+// GP_Q * 4 sums per block.
+template <int LD>
 __global__ void __launch_bounds__(256) k_guess_dots(
     int64_t n, int S, const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
     const double* __restrict__ K, double4 dsc, const double* __restrict__ diag,
     const uint8_t* __restrict__ bc, const double* __restrict__ b, const double* __restrict__ U,
     const double* __restrict__ Up, const double* __restrict__ opU,
     const double* __restrict__ opDU, const double* __restrict__ d, double* __restrict__ part) {
+  constexpr int G = LD;
   __shared__ double sh[32];
   const double dscale[4] = {dsc.x, dsc.y, dsc.z, dsc.w};
   const int gl = threadIdx.x % G;
   const int64_t rpb = blockDim.x / G;
-  double acc[GP_Q][LD];
+  double acc[GP_Q];
 #pragma unroll
-  for (int q = 0; q < GP_Q; q++)
-#pragma unroll
-    for (int s = 0; s < LD; s++) acc[q][s] = 0.0;
+  for (int q = 0; q < GP_Q; q++) acc[q] = 0.0;
   for (int64_t base = blockIdx.x * rpb; base < n; base += (int64_t)gridDim.x * rpb) {
     const int64_t row = base + threadIdx.x / G;
     const int64_t rr = row < n ? row : n - 1;
@@ -213,52 +215,67 @@ __global__ void __launch_bounds__(256) k_guess_dots(
     for (int o = G / 2; o > 0; o >>= 1)
 #pragma unroll
       for (int s = 0; s < LD; s++) kd[s] += __shfl_xor_sync(0xffffffffu, kd[s], o, G);
-    if (row < n && gl == 0 && !(bc && bc[row])) {
-      double u[LD], up[LD], dd[LD], dg[LD], bv[LD], iu[LD], idu[LD];
-      ldv<double, LD>(U, row, u);
-      ldv<double, LD>(Up, row, up);
-      ldv<double, LD>(d, row, dd);
-      ldv<double, LD>(diag, row, dg);
-      ldv<double, LD>(b, row, bv);
-      ldv<double, LD>(opU, row, iu);
-      ldv<double, LD>(opDU, row, idu);
+    const int s = gl;
+    if (row < n && s < S && !(bc && bc[row])) {
+      double kds = kd[0], dsc_s = dscale[0];
 #pragma unroll
-      for (int s = 0; s < LD; s++) {
-        if (s >= S) continue;
-        const double du = u[s] - up[s];
-        const double Au = iu[s] + dg[s] * u[s];
-        const double Adu = idu[s] + dg[s] * du;
-        const double Ad = dscale[s] * kd[s] + dg[s] * dd[s];
-        const double r0 = bv[s] - Au;
-        acc[0][s] += du * Adu;
-        acc[1][s] += du * Ad;
-        acc[2][s] += dd[s] * Ad;
-        acc[3][s] += du * r0;
-        acc[4][s] += dd[s] * r0;
-      }
+      for (int c = 1; c < LD; c++)
+        if (c == s) {
+          kds = kd[c];
+          dsc_s = dscale[c];
+        }
+      const int64_t i = row * LD + s;
+      const double u = U[i], du = u - Up[i], dd = d[i], dg = diag[i];
+      const double Au = opU[i] + dg * u;
+      const double Adu = opDU[i] + dg * du;
+      const double Ad = dsc_s * kds + dg * dd;
+      const double r0 = b[i] - Au;
+      acc[0] += du * Adu;
+      acc[1] += du * Ad;
+      acc[2] += dd * Ad;
+      acc[3] += du * r0;
+      acc[4] += dd * r0;
     }
   }
+  // per column: sum the lanes with gl == s (fixed tree over the block)
 #pragma unroll
   for (int q = 0; q < GP_Q; q++)
 #pragma unroll
-    for (int s = 0; s < LD; s++) {
-      const double v = block_sum(acc[q][s], sh);
+    for (int s = 0; s < 4; s++) {
+      const double v = block_sum((s < LD && gl == s) ? acc[q] : 0.0, sh);
       if (threadIdx.x == 0) part[(int64_t)blockIdx.x * GP_Q * 4 + q * 4 + s] = v;
     }
 }
 
-// one block: the sums over the partials in a fixed order, then (a, c) per column into
-// coef[2 s], coef[2 s + 1]
-__global__ void __launch_bounds__(256) k_guess_coeffs(int nparts, int S,
+// Every block sums the nparts partial rows in a fixed order (warp k: slot k), solves the
+// 2x2 system per column and updates its rows: the coefficients are the same bits in
+// every block.
+template <int LD>
+__global__ void __launch_bounds__(512) k_guess_update(int64_t n, int S, int nparts,
                                                       const double* __restrict__ part,
-                                                      double* __restrict__ coef) {
-  __shared__ double sh[32];
+                                                      const uint8_t* __restrict__ bc,
+                                                      const double* __restrict__ b,
+                                                      const double* __restrict__ U,
+                                                      const double* __restrict__ Up,
+                                                      const double* __restrict__ d,
+                                                      double* __restrict__ x) {
   __shared__ double tot[GP_Q * 4];
-  for (int k = 0; k < GP_Q * 4; k++) {
+  __shared__ double coef[8];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int k = w; k < GP_Q * 4; k += nw) {
+    // partials lane, lane + 32, ...: all loads in flight together, summed in order
+    constexpr int QN = (GP_BLOCKS + 31) / 32;
+    double xq[QN];
+#pragma unroll
+    for (int q = 0; q < QN; q++) {
+      const int bl = lane + 32 * q;
+      xq[q] = (bl < nparts) ? part[(int64_t)bl * GP_Q * 4 + k] : 0.0;
+    }
     double v = 0.0;
-    for (int bl = threadIdx.x; bl < nparts; bl += blockDim.x) v += part[(int64_t)bl * GP_Q * 4 + k];
-    v = block_sum(v, sh);
-    if (threadIdx.x == 0) tot[k] = v;
+#pragma unroll
+    for (int q = 0; q < QN; q++) v += xq[q];
+    v = warp_sum(v);
+    if (lane == 0) tot[k] = v;
   }
   __syncthreads();
   if (threadIdx.x < 4) {
@@ -281,13 +298,7 @@ __global__ void __launch_bounds__(256) k_guess_coeffs(int nparts, int S,
     coef[2 * s] = a;
     coef[2 * s + 1] = c;
   }
-}
-
-template <int LD>
-__global__ void k_guess_update(int64_t n, int S, const uint8_t* __restrict__ bc,
-                               const double* __restrict__ b, const double* __restrict__ U,
-                               const double* __restrict__ Up, const double* __restrict__ d,
-                               const double* __restrict__ coef, double* __restrict__ x) {
+  __syncthreads();
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n * LD;
        i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t row = i / LD;
@@ -436,7 +447,7 @@ extern "C" int tp_csr_images(const tp_csr_op* op, const double* x1, const double
 }
 
 extern "C" size_t tp_guess_project_workspace_doubles(void) {
-  return (size_t)GP_BLOCKS * GP_Q * 4 + 8;
+  return (size_t)GP_BLOCKS * GP_Q * 4;
 }
 
 extern "C" int tp_guess_project(const tp_csr_op* op, const double* diag, const uint8_t* bc_mask,
@@ -450,21 +461,17 @@ extern "C" int tp_guess_project(const tp_csr_op* op, const double* diag, const u
   TP_REQUIRE(op->S >= 1 && op->S <= op->ld, "bad S");
   if (op->n_rows == 0) return TP_OK;
   cudaStream_t st = as_stream(stream);
-  constexpr int G = 4;
   const double4 dsc = make_double4(op->S > 0 ? op->dscale[0] : 0.0, op->S > 1 ? op->dscale[1] : 0.0,
                                    op->S > 2 ? op->dscale[2] : 0.0, op->S > 3 ? op->dscale[3] : 0.0);
   const int nb = (int)std::min<int64_t>(GP_BLOCKS, (op->n_rows + 63) / 64);
   double* part = work;
-  double* coef = work + (size_t)GP_BLOCKS * GP_Q * 4;
   const int64_t n = op->n_rows;
 #define TP_GP(LDV)                                                                          \
   do {                                                                                      \
-    k_guess_dots<LDV, G><<<nb, 256, 0, st>>>(n, op->S, op->indptr, op->indices, op->K64,    \
-                                             dsc, diag, bc_mask, b, U, U_prev, opU, opDU,   \
-                                             d, part);                                      \
-    k_guess_coeffs<<<1, 256, 0, st>>>(nb, op->S, part, coef);                               \
-    k_guess_update<LDV><<<grid_for(n * LDV, 256, sm_count() * 8), 256, 0, st>>>(           \
-        n, op->S, bc_mask, b, U, U_prev, d, coef, x);                                       \
+    k_guess_dots<LDV><<<nb, 256, 0, st>>>(n, op->S, op->indptr, op->indices, op->K64, dsc,  \
+                                          diag, bc_mask, b, U, U_prev, opU, opDU, d, part); \
+    k_guess_update<LDV><<<std::min(nb, 148), 512, 0, st>>>(n, op->S, nb, part, bc_mask, b,  \
+                                                           U, U_prev, d, x);                \
   } while (0)
   if (op->ld == 1)
     TP_GP(1);

@@ -188,7 +188,7 @@ __device__ __forceinline__ void mlp_tile_forward(const MlpSmem& sm, const uint32
 // Persistent warps over 16-row tiles.  Every lane of a quad gathers all features of its
 // two rows (the quad's loads hit the same addresses) and keeps the four its A fragment
 // holds: no divergent per-feature branches.
-__global__ void __launch_bounds__(128) k_mlp_predict(MlpFeat F, int64_t nrows,
+__global__ void __launch_bounds__(128, 6) k_mlp_predict(MlpFeat F, int64_t nrows,
                                                      const float* __restrict__ P, float sigma,
                                                      double* __restrict__ x_out,
                                                      float* __restrict__ y_out) {
@@ -561,6 +561,7 @@ extern "C" int tp_mlp_predict(const tp_mlp_inputs* in, const float* params, floa
   const int64_t nrows = in->n_verts * in->S;
   if (nrows == 0) return TP_OK;
   const int64_t ntiles = (nrows + 15) / 16;
+  // one wave: 6 CTAs of 4 warps per SM
   const int grid = (int)std::min<int64_t>((ntiles + 3) / 4, (int64_t)sm_count() * 6);
   k_mlp_predict<<<grid, 128, 0, as_stream(stream)>>>(make_feat(in), nrows, params, sigma, x_out,
                                                       y_out);
