@@ -3,7 +3,9 @@ initial guess (kernels in csrc/tp_mlp.cu, C ABI tp_mlp_*).
 
 The network is trained on trajectories the solver itself produces (pairs u^{n-1}, u^n ->
 u^{n+1}), by the project's own forward/backward/AdamW kernels.  It predicts the
-correction to a base guess, by default the linear extrapolation 2 u^n - u^{n-1}.  The Krylov solve always
+correction to a base guess (u^n by default, or the linear extrapolation 2 u^n - u^{n-1}),
+and the transport guess is the energy-norm projection onto span{u^n - u^{n-1}, that
+correction} around u^n (tp_guess_project).  The Krylov solve always
 runs to the same tolerance, so the guess only changes how many iterations it takes: the
 plain method is both the fallback (no predictor -> previous step) and the judge of the
 prediction's error.
@@ -41,7 +43,7 @@ def initial_params(seed: int = 3) -> np.ndarray:
 
 class WarmStartMLP:
     def __init__(self, device, seed: int = 3, capacity_rows: int = 0, grid: int = 0,
-                 base: str = "extrapolate", project: bool = True):
+                 base: str = "previous", project: bool = True):
         """base: the guess the network corrects, "previous" (u^n) or "extrapolate"
         (2 u^n - u^{n-1}); the training target is (u^{n+1} - base) / sigma.
         project: the transport guess is u^n + a (u^n - u^{n-1}) + c sigma y with (a, c) per
