@@ -167,109 +167,129 @@ __global__ void __launch_bounds__(256) k_csr_images(int64_t n, const int32_t* __
 }
 
 // ---------------------------------------------------------------- guess projection
-// The learned guess projected in the energy norm.  With A = D K + diag (identity rows
-// where bc), u = u^n, du = u^n - u^{n-1} and the network's direction d, the guess is
-// x = u + a du + c d on the free rows, (a, c) per column from the 2x2 Galerkin system
-//   [du.A du  du.A d] [a]   [du.r0]
-//   [ d.A du   d.A d] [c] = [ d.r0],   r0 = b - A u,
-// which minimises the A-norm of the error over that plane: the guess is never worse than
-// u^n in that norm (a = c = 0 is in the plane).  Sums run over the free rows; d is taken
-// as zero on the Dirichlet rows, which keep x = b.
-constexpr int GP_BLOCKS = 592, GP_Q = 5;  // 5 sums per column: du.Adu du.Ad d.Ad du.r0 d.r0
+// The initial guess projected in the energy norm.  With A = D K + diag (identity rows
+// where bc), u = u^n and M <= 4 directions d_k (increments of past steps, the network's
+// correction), the guess is x = u + sum_k c_k d_k on the free rows, c per column from the
+// Galerkin system  G c = h,  G_kl = d_k . A d_l,  h_k = d_k . (b - A u),  which minimises
+// the A-norm of the error over u + span{d_k}: the guess is never worse than u^n in that
+// norm.  Sums run over the free rows; every direction is taken as zero on the Dirichlet
+// rows, which keep x = b.
+constexpr int GP_BLOCKS = 592, GP_SLOTS = 14 * 4;  // per column: 10 of G (upper) + 4 of h
 
-// A d by a CSR pass (G = LD lanes per row), then lane s of the row's group takes column s:
-// its loads of the row's fields are contiguous across the group.  Partials: one row of
-// GP_Q * 4 sums per block.
-template <int LD>
+struct GuessDirs {
+  const double* d[4];
+};
+
+template <int M>
+__device__ __forceinline__ constexpr int gp_nq() {
+  return M * (M + 1) / 2 + M;
+}
+
+// A d_k by one CSR pass over all M directions (G = LD lanes per row), then lane s of the
+// row's group takes column s.  Partials: one row of GP_SLOTS sums per block, slot q * 4 + s.
+template <int LD, int M>
 __global__ void __launch_bounds__(256) k_guess_dots(
     int64_t n, int S, const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
     const double* __restrict__ K, double4 dsc, const double* __restrict__ diag,
     const uint8_t* __restrict__ bc, const double* __restrict__ b, const double* __restrict__ U,
-    const double* __restrict__ Up, const double* __restrict__ opU,
-    const double* __restrict__ opDU, const double* __restrict__ d, double* __restrict__ part) {
-  constexpr int G = LD;
+    const double* __restrict__ opU, GuessDirs dirs, double* __restrict__ part) {
+  constexpr int G = LD, NQ = gp_nq<M>();
   __shared__ double sh[32];
   const double dscale[4] = {dsc.x, dsc.y, dsc.z, dsc.w};
   const int gl = threadIdx.x % G;
   const int64_t rpb = blockDim.x / G;
-  double acc[GP_Q];
+  double acc[NQ];
 #pragma unroll
-  for (int q = 0; q < GP_Q; q++) acc[q] = 0.0;
+  for (int q = 0; q < NQ; q++) acc[q] = 0.0;
   for (int64_t base = blockIdx.x * rpb; base < n; base += (int64_t)gridDim.x * rpb) {
     const int64_t row = base + threadIdx.x / G;
     const int64_t rr = row < n ? row : n - 1;
-    double kd[LD];
+    double kd[M][LD];
 #pragma unroll
-    for (int s = 0; s < LD; s++) kd[s] = 0.0;
+    for (int k = 0; k < M; k++)
+#pragma unroll
+      for (int s = 0; s < LD; s++) kd[k][s] = 0.0;
     const int beg = indptr[rr], end = indptr[rr + 1];
     for (int p = beg + gl; p < end; p += G) {
       const int j = __ldg(indices + p);
       if (bc && bc[j]) continue;
       const double kv = __ldg(K + p);
-      double dv[LD];
-      ldv<double, LD>(d, j, dv);
 #pragma unroll
-      for (int s = 0; s < LD; s++) kd[s] += kv * dv[s];
+      for (int k = 0; k < M; k++) {
+        double dv[LD];
+        ldv<double, LD>(dirs.d[k], j, dv);
+#pragma unroll
+        for (int s = 0; s < LD; s++) kd[k][s] += kv * dv[s];
+      }
     }
 #pragma unroll
     for (int o = G / 2; o > 0; o >>= 1)
 #pragma unroll
-      for (int s = 0; s < LD; s++) kd[s] += __shfl_xor_sync(0xffffffffu, kd[s], o, G);
+      for (int k = 0; k < M; k++)
+#pragma unroll
+        for (int s = 0; s < LD; s++) kd[k][s] += __shfl_xor_sync(0xffffffffu, kd[k][s], o, G);
     const int s = gl;
     if (row < n && s < S && !(bc && bc[row])) {
-      double kds = kd[0], dsc_s = dscale[0];
+      double kds[M], dsc_s = dscale[0];
+#pragma unroll
+      for (int k = 0; k < M; k++) kds[k] = kd[k][0];
 #pragma unroll
       for (int c = 1; c < LD; c++)
         if (c == s) {
-          kds = kd[c];
           dsc_s = dscale[c];
+#pragma unroll
+          for (int k = 0; k < M; k++) kds[k] = kd[k][c];
         }
       const int64_t i = row * LD + s;
-      const double u = U[i], du = u - Up[i], dd = d[i], dg = diag[i];
-      const double Au = opU[i] + dg * u;
-      const double Adu = opDU[i] + dg * du;
-      const double Ad = dsc_s * kds + dg * dd;
-      const double r0 = b[i] - Au;
-      acc[0] += du * Adu;
-      acc[1] += du * Ad;
-      acc[2] += dd * Ad;
-      acc[3] += du * r0;
-      acc[4] += dd * r0;
+      const double u = U[i], dg = diag[i];
+      const double r0 = b[i] - (opU[i] + dg * u);
+      double dv[M], Ad[M];
+#pragma unroll
+      for (int k = 0; k < M; k++) {
+        dv[k] = dirs.d[k][i];
+        Ad[k] = dsc_s * kds[k] + dg * dv[k];
+      }
+      int q = 0;
+#pragma unroll
+      for (int k = 0; k < M; k++)
+#pragma unroll
+        for (int l = k; l < M; l++) acc[q++] += dv[k] * Ad[l];
+#pragma unroll
+      for (int k = 0; k < M; k++) acc[q++] += dv[k] * r0;
     }
   }
   // per column: sum the lanes with gl == s (fixed tree over the block)
 #pragma unroll
-  for (int q = 0; q < GP_Q; q++)
+  for (int q = 0; q < NQ; q++)
 #pragma unroll
     for (int s = 0; s < 4; s++) {
       const double v = block_sum((s < LD && gl == s) ? acc[q] : 0.0, sh);
-      if (threadIdx.x == 0) part[(int64_t)blockIdx.x * GP_Q * 4 + q * 4 + s] = v;
+      if (threadIdx.x == 0) part[(int64_t)blockIdx.x * GP_SLOTS + q * 4 + s] = v;
     }
 }
 
-// Every block sums the nparts partial rows in a fixed order (warp k: slot k), solves the
-// 2x2 system per column and updates its rows: the coefficients are the same bits in
-// every block.
-template <int LD>
+// Every block sums the nparts partial rows in a fixed order (warp w: slots w, w + 16, ...),
+// solves the M x M system per column and updates its rows: the coefficients are the same
+// bits in every block.  The solve is a Cholesky factorisation that drops a direction whose
+// pivot falls below 1e-12 of its diagonal (numerically in the span of the earlier ones).
+template <int LD, int M>
 __global__ void __launch_bounds__(512) k_guess_update(int64_t n, int S, int nparts,
                                                       const double* __restrict__ part,
                                                       const uint8_t* __restrict__ bc,
                                                       const double* __restrict__ b,
                                                       const double* __restrict__ U,
-                                                      const double* __restrict__ Up,
-                                                      const double* __restrict__ d,
-                                                      double* __restrict__ x) {
-  __shared__ double tot[GP_Q * 4];
-  __shared__ double coef[8];
+                                                      GuessDirs dirs, double* __restrict__ x) {
+  constexpr int NQ = gp_nq<M>();
+  __shared__ double tot[NQ * 4];
+  __shared__ double coef[4][4];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int k = w; k < GP_Q * 4; k += nw) {
-    // partials lane, lane + 32, ...: all loads in flight together, summed in order
+  for (int k = w; k < NQ * 4; k += nw) {
     constexpr int QN = (GP_BLOCKS + 31) / 32;
     double xq[QN];
 #pragma unroll
     for (int q = 0; q < QN; q++) {
       const int bl = lane + 32 * q;
-      xq[q] = (bl < nparts) ? part[(int64_t)bl * GP_Q * 4 + k] : 0.0;
+      xq[q] = (bl < nparts) ? part[(int64_t)bl * GP_SLOTS + k] : 0.0;
     }
     double v = 0.0;
 #pragma unroll
@@ -280,23 +300,63 @@ __global__ void __launch_bounds__(512) k_guess_update(int64_t n, int S, int npar
   __syncthreads();
   if (threadIdx.x < 4) {
     const int s = threadIdx.x;
-    double a = 0.0, c = 0.0;
+    double c[M];
+#pragma unroll
+    for (int k = 0; k < M; k++) c[k] = 0.0;
     if (s < S) {
-      const double g11 = tot[0 * 4 + s], g12 = tot[1 * 4 + s], g22 = tot[2 * 4 + s];
-      const double h1 = tot[3 * 4 + s], h2 = tot[4 * 4 + s];
-      const double det = g11 * g22 - g12 * g12;
-      if (g11 > 0.0 && g22 > 0.0 && det > 1e-12 * g11 * g22) {
-        a = (h1 * g22 - h2 * g12) / det;
-        c = (g11 * h2 - g12 * h1) / det;
-      } else if (g11 > 0.0 && (!(g22 > 0.0) || h1 * h1 / g11 >= h2 * h2 / g22)) {
-        a = h1 / g11;  // (nearly) collinear directions: the better single one
-      } else if (g22 > 0.0) {
-        c = h2 / g22;
+      double Gm[M][M], h[M], L[M][M];
+      int q = 0;
+#pragma unroll
+      for (int k = 0; k < M; k++)
+#pragma unroll
+        for (int l = k; l < M; l++) {
+          Gm[k][l] = tot[q * 4 + s];
+          Gm[l][k] = Gm[k][l];
+          q++;
+        }
+#pragma unroll
+      for (int k = 0; k < M; k++) h[k] = tot[(q + k) * 4 + s];
+      bool keep[M];
+#pragma unroll
+      for (int k = 0; k < M; k++) {
+        double p = Gm[k][k];
+#pragma unroll
+        for (int j = 0; j < k; j++) p -= L[k][j] * L[k][j];
+        keep[k] = Gm[k][k] > 0.0 && p > 1e-12 * Gm[k][k] && isfinite(p);
+        const double lk = keep[k] ? sqrt(p) : 0.0;
+        L[k][k] = lk;
+#pragma unroll
+        for (int i = k + 1; i < M; i++) {
+          double v = Gm[i][k];
+#pragma unroll
+          for (int j = 0; j < k; j++) v -= L[i][j] * L[k][j];
+          L[i][k] = keep[k] ? v / lk : 0.0;
+        }
       }
-      if (!isfinite(a) || !isfinite(c)) a = c = 0.0;
+      double y[M];
+#pragma unroll
+      for (int k = 0; k < M; k++) {
+        double v = h[k];
+#pragma unroll
+        for (int j = 0; j < k; j++) v -= L[k][j] * y[j];
+        y[k] = keep[k] ? v / L[k][k] : 0.0;
+      }
+#pragma unroll
+      for (int k = M - 1; k >= 0; k--) {
+        double v = y[k];
+#pragma unroll
+        for (int j = k + 1; j < M; j++) v -= L[j][k] * c[j];
+        c[k] = keep[k] ? v / L[k][k] : 0.0;
+      }
+      bool fin = true;
+#pragma unroll
+      for (int k = 0; k < M; k++) fin = fin && isfinite(c[k]);
+      if (!fin)
+#pragma unroll
+        for (int k = 0; k < M; k++) c[k] = 0.0;
     }
-    coef[2 * s] = a;
-    coef[2 * s + 1] = c;
+#pragma unroll
+    for (int k = 0; k < M; k++) coef[s][k] = c[k];
   }
   __syncthreads();
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n * LD;
@@ -304,10 +364,12 @@ __global__ void __launch_bounds__(512) k_guess_update(int64_t n, int S, int npar
     const int64_t row = i / LD;
     const int s = (int)(i - row * LD);
     double v = U[i];
-    if (bc && bc[row])
+    if (bc && bc[row]) {
       v = (s < S) ? b[i] : v;
-    else if (s < S)
-      v = v + coef[2 * s] * (v - Up[i]) + coef[2 * s + 1] * d[i];
+    } else if (s < S) {
+#pragma unroll
+      for (int k = 0; k < M; k++) v += coef[s][k] * dirs.d[k][i];
+    }
     x[i] = v;
   }
 }
@@ -447,38 +509,58 @@ extern "C" int tp_csr_images(const tp_csr_op* op, const double* x1, const double
 }
 
 extern "C" size_t tp_guess_project_workspace_doubles(void) {
-  return (size_t)GP_BLOCKS * GP_Q * 4;
+  return (size_t)GP_BLOCKS * GP_SLOTS;
 }
 
 extern "C" int tp_guess_project(const tp_csr_op* op, const double* diag, const uint8_t* bc_mask,
-                                const double* b, const double* U, const double* U_prev,
-                                const double* opU, const double* opDU, const double* d,
-                                double* x, double* work, void* stream) {
-  TP_REQUIRE(op && op->indptr && op->indices && op->K64 && diag && b && U && U_prev && opU &&
-                 opDU && d && x && work,
+                                const double* b, const double* U, const double* opU,
+                                int n_dirs, const double* const* dirs, double* x, double* work,
+                                void* stream) {
+  TP_REQUIRE(op && op->indptr && op->indices && op->K64 && diag && b && U && opU && x && work,
              "null pointer");
   TP_REQUIRE(op->ld == 1 || op->ld == 2 || op->ld == 4, "ld must be 1, 2 or 4");
   TP_REQUIRE(op->S >= 1 && op->S <= op->ld, "bad S");
+  TP_REQUIRE(n_dirs >= 0 && n_dirs <= 4 && (n_dirs == 0 || dirs), "1 to 4 directions");
+  GuessDirs gd{};
+  for (int k = 0; k < n_dirs; k++) {
+    TP_REQUIRE(dirs[k], "null direction");
+    gd.d[k] = dirs[k];
+  }
   if (op->n_rows == 0) return TP_OK;
   cudaStream_t st = as_stream(stream);
+  if (n_dirs == 0) {
+    TP_CUDA_TRY(cudaMemcpyAsync(x, U, sizeof(double) * op->n_rows * op->ld,
+                                cudaMemcpyDeviceToDevice, st));
+    return TP_OK;
+  }
   const double4 dsc = make_double4(op->S > 0 ? op->dscale[0] : 0.0, op->S > 1 ? op->dscale[1] : 0.0,
                                    op->S > 2 ? op->dscale[2] : 0.0, op->S > 3 ? op->dscale[3] : 0.0);
   const int nb = (int)std::min<int64_t>(GP_BLOCKS, (op->n_rows + 63) / 64);
   double* part = work;
   const int64_t n = op->n_rows;
-#define TP_GP(LDV)                                                                          \
+#define TP_GP(LDV, MV)                                                                      \
   do {                                                                                      \
-    k_guess_dots<LDV><<<nb, 256, 0, st>>>(n, op->S, op->indptr, op->indices, op->K64, dsc,  \
-                                          diag, bc_mask, b, U, U_prev, opU, opDU, d, part); \
-    k_guess_update<LDV><<<std::min(nb, 148), 512, 0, st>>>(n, op->S, nb, part, bc_mask, b,  \
-                                                           U, U_prev, d, x);                \
+    k_guess_dots<LDV, MV><<<nb, 256, 0, st>>>(n, op->S, op->indptr, op->indices, op->K64,   \
+                                              dsc, diag, bc_mask, b, U, opU, gd, part);     \
+    k_guess_update<LDV, MV><<<std::min(nb, 148), 512, 0, st>>>(n, op->S, nb, part, bc_mask, \
+                                                               b, U, gd, x);                \
+  } while (0)
+#define TP_GP_M(LDV)                 \
+  do {                               \
+    switch (n_dirs) {                \
+      case 1: TP_GP(LDV, 1); break;  \
+      case 2: TP_GP(LDV, 2); break;  \
+      case 3: TP_GP(LDV, 3); break;  \
+      default: TP_GP(LDV, 4); break; \
+    }                                \
   } while (0)
   if (op->ld == 1)
-    TP_GP(1);
+    TP_GP_M(1);
   else if (op->ld == 2)
-    TP_GP(2);
+    TP_GP_M(2);
   else
-    TP_GP(4);
+    TP_GP_M(4);
+#undef TP_GP_M
 #undef TP_GP
   TP_LAUNCH_CHECK();
   return TP_OK;

@@ -133,8 +133,8 @@ SIGNATURES = {
     "tp_csr_apply": (ctypes.c_int, [_P(TpCsrOp), ctypes.c_int, _vp, _vp, _vp]),
     "tp_csr_images": (ctypes.c_int, [_P(TpCsrOp), _vp, _vp, _vp, _vp, _vp]),
     "tp_guess_project_workspace_doubles": (ctypes.c_size_t, []),
-    "tp_guess_project": (ctypes.c_int, [_P(TpCsrOp), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
-                                        _vp, _vp, _vp]),
+    "tp_guess_project": (ctypes.c_int, [_P(TpCsrOp), _vp, _vp, _vp, _vp, _vp, ctypes.c_int,
+                                        _P(ctypes.c_void_p), _vp, _vp, _vp]),
     "tp_cg_workspace_bytes": (ctypes.c_size_t, [_P(TpCsrOp), _P(TpCgConfig)]),
     "tp_cg_create": (ctypes.c_int, [_P(TpCsrOp), _P(TpCgConfig), _vp, _vp, _vp, _vp,
                                     ctypes.c_size_t, _vp, _P(_vp)]),

@@ -95,9 +95,7 @@ class GyroidStep:
         tr.assemble_rhs()
         tr.initial_guess()
         tr.solver.run()
-        tr.U_prev.copy_(tr.U)
-        tr.U.copy_(tr.solver.x)
-        tr.steps_done += 1
+        tr.advance_state()
         self.advance_levelset()
         return tr.solver.result() if sync else None
 
@@ -108,10 +106,11 @@ class GyroidStep:
         return self.tr.state()
 
     def launches_per_step(self) -> int:
-        """gradient, interface terms, cell average, diagonal, RHS, guess, solve, level set"""
+        """gradient, interface terms, cell average, diagonal, RHS, guess, solve, increment,
+        level set"""
         guess = self.tr.predictor.launches if (self.tr.guess == "learned"
                                                and self.tr.predictor is not None) else 0
-        return 7 + guess
+        return 8 + guess
 
     # ---- learned warm start
     def train_predictor(self, steps: int, every: int = 10, epochs: int = 400, seed: int = 3,

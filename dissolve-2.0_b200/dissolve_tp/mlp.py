@@ -46,9 +46,10 @@ class WarmStartMLP:
                  base: str = "previous", project: bool = True):
         """base: the guess the network corrects, "previous" (u^n) or "extrapolate"
         (2 u^n - u^{n-1}); the training target is (u^{n+1} - base) / sigma.
-        project: the transport guess is u^n + a (u^n - u^{n-1}) + c sigma y with (a, c) per
-        species from the energy-norm (Galerkin) projection of tp_guess_project, never
-        worse than the previous-step guess in that norm; False: base + sigma y as is."""
+        project: the transport guess is u^n + sum_k c_k d_k over the directions
+        d = (u^n - u^{n-1}, sigma y, u^{n-1} - u^{n-2}, u^{n-2} - u^{n-3}) (those the history
+        has), c per species from the energy-norm (Galerkin) projection of tp_guess_project,
+        never worse than the previous-step guess in that norm; False: base + sigma y."""
         if base not in ("previous", "extrapolate"):
             raise ValueError("base must be 'previous' or 'extrapolate'")
         self.base = base
@@ -73,8 +74,8 @@ class WarmStartMLP:
         self.T = torch.empty(max(capacity_rows, 1), dtype=torch.float32, device=device)
         self.rows = 0
         self.rng = np.random.default_rng(seed)
-        # per guess: the stiffness images, the network (+ dots, coefficients, update)
-        self.launches = 5 if self.project else 2
+        # per guess: the stiffness images, the network (+ projection dots and update)
+        self.launches = 4 if self.project else 2
 
     # ---- inputs -----------------------------------------------------------------
     def inputs(self, U, Up, S, ld, D, k, phi=None, ngphi=None, ops=None,
@@ -194,9 +195,12 @@ class WarmStartMLP:
                                      dtype=torch.float64, device=self.device)
         self.predict(tr.U, tr.U_prev, tr.S, tr.ld, tr.D, tr.k, phi, ngphi, x_out=self._d,
                      ops=ops, base=2)
+        nh = max(1, int(getattr(tr, "n_hist", 1)))
+        dirs = [tr.dU[0], self._d] + list(tr.dU[1:nh])
+        arr = (ctypes.c_void_p * len(dirs))(*[ptr(d) for d in dirs])
         call("tp_guess_project", ctypes.byref(tr.stiff_op.struct), ptr(tr.D64),
-             ptr(tr.bc_mask), ptr(tr.solver.b), ptr(tr.U), ptr(tr.U_prev), ptr(ops[0]),
-             ptr(ops[1]), ptr(self._d), ptr(x), ptr(self._work), stream_handle())
+             ptr(tr.bc_mask), ptr(tr.solver.b), ptr(tr.U), ptr(ops[0]), len(dirs), arr, ptr(x),
+             ptr(self._work), stream_handle())
 
 
 def trajectory_pairs(tr, steps):

@@ -170,6 +170,10 @@ class BatchedTransport:
                                    delta=delta, **cg)
         self.U = torch.zeros((n, self.ld), dtype=torch.float64, device=dev)
         self.U_prev = torch.zeros_like(self.U)
+        # increments of the last steps, newest first (u^n - u^{n-1}, u^{n-1} - u^{n-2}, ...):
+        # directions of the projected learned guess
+        self.dU = [torch.zeros_like(self.U) for _ in range(3)]
+        self.n_hist = 0
         # D_s K_xi alone (no diagonal): the stiffness images the learned guess reads
         self.stiff_op = CsrOperator(dm.indptr, dm.indices, self.K64, dscale=self.D, S=self.S,
                                     ld=self.ld)
@@ -234,6 +238,11 @@ class BatchedTransport:
         self.U[:, : self.S] = u
         self.U_prev.copy_(self.U if U_prev is None else self._pad(U_prev))
         self.steps_done = 0 if U_prev is None else 1
+        self.n_hist = 0
+        if U_prev is not None:
+            self.dU[0].copy_(self.U)
+            self.dU[0].sub_(self.U_prev)
+            self.n_hist = 1
 
     def _pad(self, U):
         out = torch.zeros_like(self.U)
@@ -255,10 +264,21 @@ class BatchedTransport:
         self.assemble_rhs()
         self.initial_guess()
         self.solver.run()
-        self.U_prev.copy_(self.U)
-        self.U.copy_(self.solver.x)
-        self.steps_done += 1
+        self.advance_state()
         return self.solver.result() if sync else None
+
+    def advance_state(self):
+        """After a solve: the increment x - U joins the history (newest first), then
+        U_prev = U, U = x."""
+        x = self.solver.x
+        d = self.dU.pop()
+        d.copy_(x)
+        call("tp_axpby", d.numel(), -1.0, ptr(self.U), 1.0, ptr(d), stream_handle())
+        self.dU.insert(0, d)
+        self.n_hist = min(self.n_hist + 1, len(self.dU))
+        self.U_prev.copy_(self.U)
+        self.U.copy_(x)
+        self.steps_done += 1
 
     def state(self) -> np.ndarray:
         return self.U[:, : self.S].cpu().numpy()
@@ -271,8 +291,9 @@ class BatchedTransport:
         if self.guess == "learned" and self.predictor is not None:
             guess = self.predictor.launches
         if self.engine == "persistent":
-            return 3 + 1 + guess + 1  # assembly, diagonal, RHS, SELL scatter, guess, solve
-        return 3 + guess + 4 + 3 * int(res["iterations"]) + 2 * int(res["n_reliable"])
+            # assembly, diagonal, RHS, SELL scatter, guess, solve, increment
+            return 3 + 1 + guess + 1 + 1
+        return 3 + guess + 4 + 3 * int(res["iterations"]) + 2 * int(res["n_reliable"]) + 1
 
     def step_host(self, u_host: torch.Tensor, out_host: torch.Tensor):
         """End-to-end step through host buffers: (V, S) float64 pinned in -> out (V, S).

@@ -302,20 +302,21 @@ TP_API int tp_csr_apply(const tp_csr_op* op, int fp32, const void* x, void* y, v
 TP_API int tp_csr_images(const tp_csr_op* op, const double* x1, const double* x2, double* y1,
                          double* y2, void* stream);
 
-/* The learned initial guess projected in the energy norm (no reference counterpart).
- * op: the stiffness D K (K64, dscale, S, ld); with A = D K + diag (diag (n_rows, ld); identity
- * rows where bc_mask), r0 = b - A U and du = U - U_prev, writes
- *   x = U + a du + c d   (free rows),   x = b   (Dirichlet rows, columns < S),
- * (a, c) per column solving the 2x2 Galerkin system on span{du, d} (d: the network's
- * direction, taken as zero on Dirichlet rows) -- the minimum of the A-norm of the error over
- * that plane, so never above the previous-step guess U in that norm.  opU = D K U and
- * opDU = D K du (tp_csr_images).  Deterministic.  work: device scratch of
- * tp_guess_project_workspace_doubles() doubles. */
+/* The initial guess projected in the energy norm (no reference counterpart; the learned
+ * guess's last stage).  op: the stiffness D K (K64, dscale, S, ld); A = D K + diag (diag
+ * (n_rows, ld); identity rows where bc_mask); opU = D K U (tp_csr_images).  With n_dirs
+ * (0..4) directions dirs[k] ((n_rows, ld) device arrays: increments of past steps, the
+ * network's correction), writes
+ *   x = U + sum_k c_k dirs[k]   (free rows),   x = b   (Dirichlet rows, columns < S),
+ * c per column solving the Galerkin system G c = h, G_kl = d_k . A d_l,
+ * h_k = d_k . (b - A U) over the free rows (directions taken as zero on Dirichlet rows;
+ * a direction numerically in the span of the earlier ones gets c_k = 0): the minimum of
+ * the A-norm of the error over U + span{d_k}, so never above U in that norm.
+ * Deterministic.  work: device scratch of tp_guess_project_workspace_doubles() doubles. */
 TP_API size_t tp_guess_project_workspace_doubles(void);
 TP_API int tp_guess_project(const tp_csr_op* op, const double* diag, const uint8_t* bc_mask,
-                            const double* b, const double* U, const double* U_prev,
-                            const double* opU, const double* opDU, const double* d, double* x,
-                            double* work, void* stream);
+                            const double* b, const double* U, const double* opU, int n_dirs,
+                            const double* const* dirs, double* x, double* work, void* stream);
 
 /* ------------------------------------------------------------------ Krylov solve */
 /* Jacobi-preconditioned CG on every (system, column) lane at once, captured in a CUDA

@@ -171,10 +171,10 @@ def test_learned_guess_reduces_iterations(cuda_device):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("with_bc", [False, True])
-def test_guess_projection_matches_galerkin_solve(cuda_device, with_bc):
-    """tp_guess_project against the 2x2 Galerkin solve done with scipy on the same
-    operator; the projected guess is never worse than u^n in the energy norm."""
+@pytest.mark.parametrize("with_bc,n_dirs", [(False, 2), (False, 4), (True, 3)])
+def test_guess_projection_matches_galerkin_solve(cuda_device, with_bc, n_dirs):
+    """tp_guess_project against the Galerkin solve done with scipy on the same operator;
+    the projected guess is never worse than u^n in the energy norm."""
     import ctypes
 
     import scipy.sparse as sp
@@ -194,23 +194,25 @@ def test_guess_projection_matches_galerkin_solve(cuda_device, with_bc):
     tr = BatchedTransport(m, coef, D, K, 0.02, bc_dofs=bc, bc_values=bcv if with_bc else None)
     rng = np.random.default_rng(3)
     U = rng.uniform(0, 1, (m.n_verts, S))
-    Up = U + rng.normal(0, 0.05, U.shape)
     if with_bc:
         U[bc] = bcv
-        Up[bc] = bcv
-    tr.set_state(U, Up)
+    tr.set_state(U)
     tr.assemble_operator()
     tr.assemble_rhs()
-    d = torch.zeros_like(tr.U)
-    dn = rng.normal(0, 0.02, U.shape)
-    d[:, :S] = torch.from_numpy(dn)
-    opU, opDU = tr.operator_images()
+    dn = [rng.normal(0, 0.02 * (k + 1), U.shape) for k in range(n_dirs)]
+    dirs = []
+    for a in dn:
+        t = torch.zeros_like(tr.U)
+        t[:, :S] = torch.from_numpy(a)
+        dirs.append(t)
+    opU, _ = tr.operator_images(tr.U, tr.U)
     x = torch.zeros_like(tr.U)
     work = torch.empty(int(_lib.lib.tp_guess_project_workspace_doubles()), dtype=torch.float64,
                        device=cuda_device)
+    arr = (ctypes.c_void_p * n_dirs)(*[ptr(d) for d in dirs])
     call("tp_guess_project", ctypes.byref(tr.stiff_op.struct), ptr(tr.D64), ptr(tr.bc_mask),
-         ptr(tr.solver.b), ptr(tr.U), ptr(tr.U_prev), ptr(opU), ptr(opDU), ptr(d), ptr(x),
-         ptr(work), stream_handle())
+         ptr(tr.solver.b), ptr(tr.U), ptr(opU), n_dirs, arr, ptr(x), ptr(work),
+         stream_handle())
     xg = x.cpu().numpy()
     n = m.n_verts
     Km = sp.csr_matrix((tr.K64.cpu().numpy(), tr.dm.indices[: tr.dm.nnz].cpu().numpy(),
@@ -223,13 +225,13 @@ def test_guess_projection_matches_galerkin_solve(cuda_device, with_bc):
     for s in range(S):
         A = (D[s] * Km + sp.diags(dg[:, s])).tocsr()
         AF = A[free][:, free]
-        u, du = U[:, s], U[:, s] - Up[:, s]
-        dd = np.where(free, dn[:, s], 0.0)
+        u = U[:, s]
+        ds = [np.where(free, a[:, s], 0.0) for a in dn]
         r0 = (b[:, s] - A @ u)[free]
-        Adu, Ad = (A @ du)[free], (A @ dd)[free]
-        G = np.array([[du[free] @ Adu, du[free] @ Ad], [dd[free] @ Adu, dd[free] @ Ad]])
-        a, c = np.linalg.solve(0.5 * (G + G.T), [du[free] @ r0, dd[free] @ r0])
-        xr = np.where(free, u + a * du + c * dd, b[:, s])
+        Ad = [(A @ d)[free] for d in ds]
+        G = np.array([[di[free] @ Aj for Aj in Ad] for di in ds])
+        c = np.linalg.solve(0.5 * (G + G.T), [di[free] @ r0 for di in ds])
+        xr = np.where(free, u + sum(ci * di for ci, di in zip(c, ds)), b[:, s])
         assert np.abs(xg[:, s] - xr).max() <= 1e-9 * np.abs(xr).max(), s
         # energy norm of the free-row error against the exact solution
         xs = u.copy()
@@ -237,3 +239,12 @@ def test_guess_projection_matches_galerkin_solve(cuda_device, with_bc):
                                                           if with_bc else 0.0))
         e_new, e_old = (xg[:, s] - xs)[free], (u - xs)[free]
         assert e_new @ (AF @ e_new) <= e_old @ (AF @ e_old) * (1 + 1e-12)
+    # a repeated direction is dropped (its pivot vanishes), the result is unchanged
+    arr2 = (ctypes.c_void_p * 2)(ptr(dirs[0]), ptr(dirs[0]))
+    x1, x2 = torch.zeros_like(x), torch.zeros_like(x)
+    arr1 = (ctypes.c_void_p * 1)(ptr(dirs[0]))
+    call("tp_guess_project", ctypes.byref(tr.stiff_op.struct), ptr(tr.D64), ptr(tr.bc_mask),
+         ptr(tr.solver.b), ptr(tr.U), ptr(opU), 1, arr1, ptr(x1), ptr(work), stream_handle())
+    call("tp_guess_project", ctypes.byref(tr.stiff_op.struct), ptr(tr.D64), ptr(tr.bc_mask),
+         ptr(tr.solver.b), ptr(tr.U), ptr(opU), 2, arr2, ptr(x2), ptr(work), stream_handle())
+    assert torch.equal(x1, x2)
