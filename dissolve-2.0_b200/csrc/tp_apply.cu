@@ -168,134 +168,117 @@ __global__ void __launch_bounds__(256) k_csr_images(int64_t n, const int32_t* __
 
 // ---------------------------------------------------------------- guess projection
 // The initial guess projected in the energy norm.  With A = D K + diag (identity rows
-// where bc), u = u^n and M <= 4 directions d_k (increments of past steps, the network's
-// correction), the guess is x = u + sum_k c_k d_k on the free rows, c per column from the
-// Galerkin system  G c = h,  G_kl = d_k . A d_l,  h_k = d_k . (b - A u),  which minimises
-// the A-norm of the error over u + span{d_k}: the guess is never worse than u^n in that
-// norm.  Sums run over the free rows; every direction is taken as zero on the Dirichlet
-// rows, which keep x = b.
-constexpr int GP_BLOCKS = 592, GP_SLOTS = 14 * 4;  // per column: 10 of G (upper) + 4 of h
+// where bc), u = u^n and M <= GP_MAXD directions d_k (increments of past steps, the
+// network's correction), the guess is x = u + sum_k c_k d_k on the free rows, c per column
+// from the Galerkin system  G c = h,  G_kl = d_k . A d_l,  h_k = d_k . (b - A u),  which
+// minimises the A-norm of the error over u + span{d_k}: the guess is never worse than u^n
+// in that norm.  Sums run over the free rows; every direction is taken as zero on the
+// Dirichlet rows, which keep x = b.
+constexpr int GP_MAXD = 6;
+constexpr int GP_BLOCKS = 592;
 
 struct GuessDirs {
-  const double* d[4];
+  const double* d[GP_MAXD];
 };
 
 template <int M>
-__device__ __forceinline__ constexpr int gp_nq() {
-  return M * (M + 1) / 2 + M;
+__host__ __device__ constexpr int gp_nq() {
+  return M * (M + 1) / 2 + M;  // upper triangle of G, then h
 }
+constexpr int GP_SLOTS = gp_nq<GP_MAXD>() * 4;
 
-// A d_k by one CSR pass over all M directions (G = LD lanes per row), then lane s of the
-// row's group takes column s.  Partials: one row of GP_SLOTS sums per block, slot q * 4 + s.
+// A d_k for all M directions by one CSR walk per row: a group of LD lanes per row, lane s
+// reads column s of every gathered row (the group's loads are one contiguous run).  The
+// sums of lane s feed column s; one row of GP_SLOTS partials per block (slot q * 4 + s),
+// summed over the warps in a fixed order.
 template <int LD, int M>
 __global__ void __launch_bounds__(256) k_guess_dots(
     int64_t n, int S, const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
     const double* __restrict__ K, double4 dsc, const double* __restrict__ diag,
     const uint8_t* __restrict__ bc, const double* __restrict__ b, const double* __restrict__ U,
     const double* __restrict__ opU, GuessDirs dirs, double* __restrict__ part) {
-  constexpr int G = LD, NQ = gp_nq<M>();
-  __shared__ double sh[32];
+  constexpr int NQ = gp_nq<M>();
+  __shared__ double red[8][NQ * 4];  // blockDim 256: 8 warps
   const double dscale[4] = {dsc.x, dsc.y, dsc.z, dsc.w};
-  const int gl = threadIdx.x % G;
-  const int64_t rpb = blockDim.x / G;
+  const int s = threadIdx.x % LD;
+  double dsc_s = dscale[0];
+#pragma unroll
+  for (int c = 1; c < LD; c++)
+    if (c == s) dsc_s = dscale[c];
+  const int64_t rpb = blockDim.x / LD;
   double acc[NQ];
 #pragma unroll
   for (int q = 0; q < NQ; q++) acc[q] = 0.0;
   for (int64_t base = blockIdx.x * rpb; base < n; base += (int64_t)gridDim.x * rpb) {
-    const int64_t row = base + threadIdx.x / G;
-    const int64_t rr = row < n ? row : n - 1;
-    double kd[M][LD];
+    const int64_t row = base + threadIdx.x / LD;
+    if (row >= n || s >= S || (bc && bc[row])) continue;
+    double kd[M];
 #pragma unroll
-    for (int k = 0; k < M; k++)
-#pragma unroll
-      for (int s = 0; s < LD; s++) kd[k][s] = 0.0;
-    const int beg = indptr[rr], end = indptr[rr + 1];
-    for (int p = beg + gl; p < end; p += G) {
+    for (int k = 0; k < M; k++) kd[k] = 0.0;
+    const int beg = indptr[row], end = indptr[row + 1];
+    for (int p = beg; p < end; p++) {
       const int j = __ldg(indices + p);
       if (bc && bc[j]) continue;
       const double kv = __ldg(K + p);
+      const int64_t jj = (int64_t)j * LD + s;
 #pragma unroll
-      for (int k = 0; k < M; k++) {
-        double dv[LD];
-        ldv<double, LD>(dirs.d[k], j, dv);
-#pragma unroll
-        for (int s = 0; s < LD; s++) kd[k][s] += kv * dv[s];
-      }
+      for (int k = 0; k < M; k++) kd[k] += kv * __ldg(dirs.d[k] + jj);
     }
+    const int64_t i = row * LD + s;
+    const double u = U[i], dg = diag[i];
+    const double r0 = b[i] - (opU[i] + dg * u);
+    double dv[M], Ad[M];
 #pragma unroll
-    for (int o = G / 2; o > 0; o >>= 1)
-#pragma unroll
-      for (int k = 0; k < M; k++)
-#pragma unroll
-        for (int s = 0; s < LD; s++) kd[k][s] += __shfl_xor_sync(0xffffffffu, kd[k][s], o, G);
-    const int s = gl;
-    if (row < n && s < S && !(bc && bc[row])) {
-      double kds[M], dsc_s = dscale[0];
-#pragma unroll
-      for (int k = 0; k < M; k++) kds[k] = kd[k][0];
-#pragma unroll
-      for (int c = 1; c < LD; c++)
-        if (c == s) {
-          dsc_s = dscale[c];
-#pragma unroll
-          for (int k = 0; k < M; k++) kds[k] = kd[k][c];
-        }
-      const int64_t i = row * LD + s;
-      const double u = U[i], dg = diag[i];
-      const double r0 = b[i] - (opU[i] + dg * u);
-      double dv[M], Ad[M];
-#pragma unroll
-      for (int k = 0; k < M; k++) {
-        dv[k] = dirs.d[k][i];
-        Ad[k] = dsc_s * kds[k] + dg * dv[k];
-      }
-      int q = 0;
-#pragma unroll
-      for (int k = 0; k < M; k++)
-#pragma unroll
-        for (int l = k; l < M; l++) acc[q++] += dv[k] * Ad[l];
-#pragma unroll
-      for (int k = 0; k < M; k++) acc[q++] += dv[k] * r0;
+    for (int k = 0; k < M; k++) {
+      dv[k] = dirs.d[k][i];
+      Ad[k] = dsc_s * kd[k] + dg * dv[k];
     }
+    int q = 0;
+#pragma unroll
+    for (int k = 0; k < M; k++)
+#pragma unroll
+      for (int l = k; l < M; l++) acc[q++] += dv[k] * Ad[l];
+#pragma unroll
+    for (int k = 0; k < M; k++) acc[q++] += dv[k] * r0;
   }
-  // per column: sum the lanes with gl == s (fixed tree over the block)
+  // lanes of one column within the warp, then the warps in order
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
-  for (int q = 0; q < NQ; q++)
+  for (int q = 0; q < NQ; q++) {
+    double v = acc[q];
 #pragma unroll
-    for (int s = 0; s < 4; s++) {
-      const double v = block_sum((s < LD && gl == s) ? acc[q] : 0.0, sh);
-      if (threadIdx.x == 0) part[(int64_t)blockIdx.x * GP_SLOTS + q * 4 + s] = v;
-    }
+    for (int o = LD; o < 32; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane < 4) red[w][q * 4 + lane] = (lane < LD) ? v : 0.0;
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < NQ * 4; k += blockDim.x) {
+    double v = 0.0;
+    for (int ww = 0; ww < (int)(blockDim.x >> 5); ww++) v += red[ww][k];
+    part[(int64_t)blockIdx.x * GP_SLOTS + k] = v;
+  }
 }
 
-// Every block sums the nparts partial rows in a fixed order (warp w: slots w, w + 16, ...),
-// solves the M x M system per column and updates its rows: the coefficients are the same
-// bits in every block.  The solve is a Cholesky factorisation that drops a direction whose
-// pivot falls below 1e-12 of its diagonal (numerically in the span of the earlier ones).
-template <int LD, int M>
-__global__ void __launch_bounds__(512) k_guess_update(int64_t n, int S, int nparts,
+// One block: the sums over the partial rows in a fixed order, then per column the M x M
+// solve by a Cholesky factorisation that drops a direction whose pivot falls below 1e-12
+// of its diagonal (numerically in the span of the earlier ones): coef[s * GP_MAXD + k].
+template <int M>
+__global__ void __launch_bounds__(128) k_guess_coeffs(int nparts, int S,
                                                       const double* __restrict__ part,
-                                                      const uint8_t* __restrict__ bc,
-                                                      const double* __restrict__ b,
-                                                      const double* __restrict__ U,
-                                                      GuessDirs dirs, double* __restrict__ x) {
+                                                      double* __restrict__ coef) {
   constexpr int NQ = gp_nq<M>();
   __shared__ double tot[NQ * 4];
-  __shared__ double coef[4][4];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int k = w; k < NQ * 4; k += nw) {
-    constexpr int QN = (GP_BLOCKS + 31) / 32;
-    double xq[QN];
-#pragma unroll
-    for (int q = 0; q < QN; q++) {
-      const int bl = lane + 32 * q;
-      xq[q] = (bl < nparts) ? part[(int64_t)bl * GP_SLOTS + k] : 0.0;
-    }
+  for (int k = threadIdx.x; k < NQ * 4; k += blockDim.x) {
     double v = 0.0;
+    int bl = 0;
+    for (; bl + 8 <= nparts; bl += 8) {
+      double xq[8];
 #pragma unroll
-    for (int q = 0; q < QN; q++) v += xq[q];
-    v = warp_sum(v);
-    if (lane == 0) tot[k] = v;
+      for (int u = 0; u < 8; u++) xq[u] = part[(int64_t)(bl + u) * GP_SLOTS + k];
+#pragma unroll
+      for (int u = 0; u < 8; u++) v += xq[u];
+    }
+    for (; bl < nparts; bl++) v += part[(int64_t)bl * GP_SLOTS + k];
+    tot[k] = v;
   }
   __syncthreads();
   if (threadIdx.x < 4) {
@@ -356,8 +339,17 @@ __global__ void __launch_bounds__(512) k_guess_update(int64_t n, int S, int npar
         for (int k = 0; k < M; k++) c[k] = 0.0;
     }
 #pragma unroll
-    for (int k = 0; k < M; k++) coef[s][k] = c[k];
+    for (int k = 0; k < M; k++) coef[s * GP_MAXD + k] = c[k];
   }
+}
+
+template <int LD, int M>
+__global__ void k_guess_update(int64_t n, int S, const double* __restrict__ coef,
+                               const uint8_t* __restrict__ bc, const double* __restrict__ b,
+                               const double* __restrict__ U, GuessDirs dirs,
+                               double* __restrict__ x) {
+  __shared__ double cs[4 * GP_MAXD];
+  if (threadIdx.x < 4 * GP_MAXD) cs[threadIdx.x] = coef[threadIdx.x];
   __syncthreads();
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n * LD;
        i += (int64_t)gridDim.x * blockDim.x) {
@@ -368,7 +360,7 @@ __global__ void __launch_bounds__(512) k_guess_update(int64_t n, int S, int npar
       v = (s < S) ? b[i] : v;
     } else if (s < S) {
 #pragma unroll
-      for (int k = 0; k < M; k++) v += coef[s][k] * dirs.d[k][i];
+      for (int k = 0; k < M; k++) v += cs[s * GP_MAXD + k] * dirs.d[k][i];
     }
     x[i] = v;
   }
@@ -509,7 +501,7 @@ extern "C" int tp_csr_images(const tp_csr_op* op, const double* x1, const double
 }
 
 extern "C" size_t tp_guess_project_workspace_doubles(void) {
-  return (size_t)GP_BLOCKS * GP_SLOTS;
+  return (size_t)GP_BLOCKS * GP_SLOTS + 4 * GP_MAXD;
 }
 
 extern "C" int tp_guess_project(const tp_csr_op* op, const double* diag, const uint8_t* bc_mask,
@@ -520,7 +512,7 @@ extern "C" int tp_guess_project(const tp_csr_op* op, const double* diag, const u
              "null pointer");
   TP_REQUIRE(op->ld == 1 || op->ld == 2 || op->ld == 4, "ld must be 1, 2 or 4");
   TP_REQUIRE(op->S >= 1 && op->S <= op->ld, "bad S");
-  TP_REQUIRE(n_dirs >= 0 && n_dirs <= 4 && (n_dirs == 0 || dirs), "1 to 4 directions");
+  TP_REQUIRE(n_dirs >= 0 && n_dirs <= GP_MAXD && (n_dirs == 0 || dirs), "0 to 6 directions");
   GuessDirs gd{};
   for (int k = 0; k < n_dirs; k++) {
     TP_REQUIRE(dirs[k], "null direction");
@@ -535,15 +527,17 @@ extern "C" int tp_guess_project(const tp_csr_op* op, const double* diag, const u
   }
   const double4 dsc = make_double4(op->S > 0 ? op->dscale[0] : 0.0, op->S > 1 ? op->dscale[1] : 0.0,
                                    op->S > 2 ? op->dscale[2] : 0.0, op->S > 3 ? op->dscale[3] : 0.0);
-  const int nb = (int)std::min<int64_t>(GP_BLOCKS, (op->n_rows + 63) / 64);
-  double* part = work;
   const int64_t n = op->n_rows;
-#define TP_GP(LDV, MV)                                                                      \
-  do {                                                                                      \
-    k_guess_dots<LDV, MV><<<nb, 256, 0, st>>>(n, op->S, op->indptr, op->indices, op->K64,   \
-                                              dsc, diag, bc_mask, b, U, opU, gd, part);     \
-    k_guess_update<LDV, MV><<<std::min(nb, 148), 512, 0, st>>>(n, op->S, nb, part, bc_mask, \
-                                                               b, U, gd, x);                \
+  double* part = work;
+  double* coef = work + (size_t)GP_BLOCKS * GP_SLOTS;
+#define TP_GP(LDV, MV)                                                                       \
+  do {                                                                                       \
+    const int nb = (int)std::min<int64_t>(GP_BLOCKS, (n + 256 / LDV - 1) / (256 / LDV));     \
+    k_guess_dots<LDV, MV><<<nb, 256, 0, st>>>(n, op->S, op->indptr, op->indices, op->K64,    \
+                                              dsc, diag, bc_mask, b, U, opU, gd, part);      \
+    k_guess_coeffs<MV><<<1, 128, 0, st>>>(nb, op->S, part, coef);                            \
+    k_guess_update<LDV, MV><<<grid_for(n * LDV, 256, sm_count() * 8), 256, 0, st>>>(         \
+        n, op->S, coef, bc_mask, b, U, gd, x);                                               \
   } while (0)
 #define TP_GP_M(LDV)                 \
   do {                               \
@@ -551,7 +545,9 @@ extern "C" int tp_guess_project(const tp_csr_op* op, const double* diag, const u
       case 1: TP_GP(LDV, 1); break;  \
       case 2: TP_GP(LDV, 2); break;  \
       case 3: TP_GP(LDV, 3); break;  \
-      default: TP_GP(LDV, 4); break; \
+      case 4: TP_GP(LDV, 4); break;  \
+      case 5: TP_GP(LDV, 5); break;  \
+      default: TP_GP(LDV, 6); break; \
     }                                \
   } while (0)
   if (op->ld == 1)

@@ -47,8 +47,8 @@ class WarmStartMLP:
         """base: the guess the network corrects, "previous" (u^n) or "extrapolate"
         (2 u^n - u^{n-1}); the training target is (u^{n+1} - base) / sigma.
         project: the transport guess is u^n + sum_k c_k d_k over the directions
-        d = (u^n - u^{n-1}, sigma y, u^{n-1} - u^{n-2}, u^{n-2} - u^{n-3}) (those the history
-        has), c per species from the energy-norm (Galerkin) projection of tp_guess_project,
+        d = (u^n - u^{n-1}, sigma y, u^{n-1} - u^{n-2}, ..., u^{n-4} - u^{n-5}) (those the
+        history has, at most six), c per species from the energy-norm (Galerkin) projection of tp_guess_project,
         never worse than the previous-step guess in that norm; False: base + sigma y."""
         if base not in ("previous", "extrapolate"):
             raise ValueError("base must be 'previous' or 'extrapolate'")

@@ -172,7 +172,7 @@ class BatchedTransport:
         self.U_prev = torch.zeros_like(self.U)
         # increments of the last steps, newest first (u^n - u^{n-1}, u^{n-1} - u^{n-2}, ...):
         # directions of the projected learned guess
-        self.dU = [torch.zeros_like(self.U) for _ in range(3)]
+        self.dU = [torch.zeros_like(self.U) for _ in range(5)]
         self.n_hist = 0
         # D_s K_xi alone (no diagonal): the stiffness images the learned guess reads
         self.stiff_op = CsrOperator(dm.indptr, dm.indices, self.K64, dscale=self.D, S=self.S,

@@ -305,7 +305,7 @@ TP_API int tp_csr_images(const tp_csr_op* op, const double* x1, const double* x2
 /* The initial guess projected in the energy norm (no reference counterpart; the learned
  * guess's last stage).  op: the stiffness D K (K64, dscale, S, ld); A = D K + diag (diag
  * (n_rows, ld); identity rows where bc_mask); opU = D K U (tp_csr_images).  With n_dirs
- * (0..4) directions dirs[k] ((n_rows, ld) device arrays: increments of past steps, the
+ * (0..6) directions dirs[k] ((n_rows, ld) device arrays: increments of past steps, the
  * network's correction), writes
  *   x = U + sum_k c_k dirs[k]   (free rows),   x = b   (Dirichlet rows, columns < S),
  * c per column solving the Galerkin system G c = h, G_kl = d_k . A d_l,

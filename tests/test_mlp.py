@@ -171,7 +171,7 @@ def test_learned_guess_reduces_iterations(cuda_device):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("with_bc,n_dirs", [(False, 2), (False, 4), (True, 3)])
+@pytest.mark.parametrize("with_bc,n_dirs", [(False, 2), (False, 6), (True, 3), (True, 5)])
 def test_guess_projection_matches_galerkin_solve(cuda_device, with_bc, n_dirs):
     """tp_guess_project against the Galerkin solve done with scipy on the same operator;
     the projected guess is never worse than u^n in the energy norm."""
