@@ -216,13 +216,29 @@ __global__ void __launch_bounds__(256) k_guess_dots(
 #pragma unroll
     for (int k = 0; k < M; k++) kd[k] = 0.0;
     const int beg = indptr[row], end = indptr[row + 1];
-    for (int p = beg; p < end; p++) {
-      const int j = __ldg(indices + p);
-      if (bc && bc[j]) continue;
-      const double kv = __ldg(K + p);
-      const int64_t jj = (int64_t)j * LD + s;
+    // four entries at a time: their index, value and gathers in flight together; the
+    // sums still run entry by entry in CSR order
+    constexpr int RP = 4;
+    for (int p0 = beg; p0 < end; p0 += RP) {
+      int64_t jj[RP];
+      double kv[RP], dvv[RP][M];
 #pragma unroll
-      for (int k = 0; k < M; k++) kd[k] += kv * __ldg(dirs.d[k] + jj);
+      for (int u = 0; u < RP; u++) {
+        const bool in = p0 + u < end;
+        const int j = in ? __ldg(indices + p0 + u) : 0;
+        kv[u] = (in && !(bc && bc[j])) ? __ldg(K + p0 + u) : 0.0;
+        jj[u] = (int64_t)j * LD + s;
+      }
+#pragma unroll
+      for (int u = 0; u < RP; u++)
+#pragma unroll
+        for (int k = 0; k < M; k++) dvv[u][k] = __ldg(dirs.d[k] + jj[u]);
+#pragma unroll
+      for (int u = 0; u < RP; u++) {
+        if (p0 + u >= end) break;
+#pragma unroll
+        for (int k = 0; k < M; k++) kd[k] += kv[u] * dvv[u][k];
+      }
     }
     const int64_t i = row * LD + s;
     const double u = U[i], dg = diag[i];
@@ -262,23 +278,27 @@ __global__ void __launch_bounds__(256) k_guess_dots(
 // solve by a Cholesky factorisation that drops a direction whose pivot falls below 1e-12
 // of its diagonal (numerically in the span of the earlier ones): coef[s * GP_MAXD + k].
 template <int M>
-__global__ void __launch_bounds__(128) k_guess_coeffs(int nparts, int S,
-                                                      const double* __restrict__ part,
-                                                      double* __restrict__ coef) {
+__global__ void __launch_bounds__(1024) k_guess_coeffs(int nparts, int S,
+                                                       const double* __restrict__ part,
+                                                       double* __restrict__ coef) {
   constexpr int NQ = gp_nq<M>();
   __shared__ double tot[NQ * 4];
-  for (int k = threadIdx.x; k < NQ * 4; k += blockDim.x) {
-    double v = 0.0;
-    int bl = 0;
-    for (; bl + 8 <= nparts; bl += 8) {
-      double xq[8];
+  // warp w sums slots w, w + 32, ...: lane l adds partial rows l, l + 32, ... (all loads
+  // in flight together), then a fixed shuffle tree
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int k = w; k < NQ * 4; k += nw) {
+    constexpr int QN = (GP_BLOCKS + 31) / 32;
+    double xq[QN];
 #pragma unroll
-      for (int u = 0; u < 8; u++) xq[u] = part[(int64_t)(bl + u) * GP_SLOTS + k];
-#pragma unroll
-      for (int u = 0; u < 8; u++) v += xq[u];
+    for (int q = 0; q < QN; q++) {
+      const int bl = lane + 32 * q;
+      xq[q] = (bl < nparts) ? part[(int64_t)bl * GP_SLOTS + k] : 0.0;
     }
-    for (; bl < nparts; bl++) v += part[(int64_t)bl * GP_SLOTS + k];
-    tot[k] = v;
+    double v = 0.0;
+#pragma unroll
+    for (int q = 0; q < QN; q++) v += xq[q];
+    v = warp_sum(v);
+    if (lane == 0) tot[k] = v;
   }
   __syncthreads();
   if (threadIdx.x < 4) {
@@ -535,7 +555,7 @@ extern "C" int tp_guess_project(const tp_csr_op* op, const double* diag, const u
     const int nb = (int)std::min<int64_t>(GP_BLOCKS, (n + 256 / LDV - 1) / (256 / LDV));     \
     k_guess_dots<LDV, MV><<<nb, 256, 0, st>>>(n, op->S, op->indptr, op->indices, op->K64,    \
                                               dsc, diag, bc_mask, b, U, opU, gd, part);      \
-    k_guess_coeffs<MV><<<1, 128, 0, st>>>(nb, op->S, part, coef);                            \
+    k_guess_coeffs<MV><<<1, 1024, 0, st>>>(nb, op->S, part, coef);                           \
     k_guess_update<LDV, MV><<<grid_for(n * LDV, 256, sm_count() * 8), 256, 0, st>>>(         \
         n, op->S, coef, bc_mask, b, U, gd, x);                                               \
   } while (0)

@@ -46,15 +46,28 @@ __device__ __forceinline__ void kref_row(int li, const GeoRec& g, double k[4]) {
 }
 
 // ----------------------------------------------------------------- CSR assembly
+// Optional extras of the same row walk (the stiffness of the batched step): the per-column
+// lumped diagonal of tp_lumped_diag, and the FP32 values in SELL order for the solver.
+struct RowExtras {
+  int S, ld;
+  const double* alpha;  // (n_cells, ld) or NULL
+  double4 shift;
+  double* d64;
+  float* d32;
+  const int32_t* csr2sell;  // with sell32: SELL position of every CSR entry
+  float* sell32;
+};
+
 // One thread per row; the block's rows are written back coalesced from shared memory.
-template <int MODE>
+// DIAG: the row also sums its lumped diagonal, in the order of k_lumped_diag.
+template <int MODE, bool DIAG>
 __global__ void __launch_bounds__(128) k_assemble_rows(
     int64_t nv, const int32_t* __restrict__ v2c_ptr, const int32_t* __restrict__ v2c,
     const uint32_t* __restrict__ slots, const double* __restrict__ geo,
     const double* __restrict__ De, const double* __restrict__ alpha, double inv_dt, int lumped,
     const uint8_t* __restrict__ bc_mask, const int32_t* __restrict__ indptr,
     const int32_t* __restrict__ indices, double* __restrict__ out64,
-    float* __restrict__ out32) {
+    float* __restrict__ out32, RowExtras ex) {
   constexpr int B = 128;
   extern __shared__ double acc[];  // [max_row_len][B]
   __shared__ int32_t s_ptr[B + 1];
@@ -70,6 +83,8 @@ __global__ void __launch_bounds__(128) k_assemble_rows(
   const int len = valid ? s_ptr[tid + 1] - s_ptr[tid] : 0;
   for (int s = 0; s < len; s++) acc[s * B + tid] = 0.0;
   const bool is_bc = valid && bc_mask && bc_mask[r];
+  double dacc[4] = {0.0, 0.0, 0.0, 0.0};
+  const double dsh[4] = {ex.shift.x, ex.shift.y, ex.shift.z, ex.shift.w};
   if (valid && !is_bc) {
     // incident cells in ascending order, fetched PF at a time so their loads overlap;
     // accumulation stays in cell order
@@ -98,6 +113,17 @@ __global__ void __launch_bounds__(128) k_assemble_rows(
         if (k0 + u >= kend) break;
         const int li = ev[u] & 3;
         const GeoRec& g = gv[u];
+        if constexpr (DIAG) {
+          const int64_t c = ev[u] >> 2;
+          const double Ld = __dmul_rn(__ddiv_rn(g.dJ, 120.0), 5.0);
+#pragma unroll
+          for (int s = 0; s < 4; s++) {
+            if (s < ex.S) {
+              const double w = __dadd_rn(dsh[s], ex.alpha ? ex.alpha[c * ex.ld + s] : 0.0);
+              dacc[s] = __dadd_rn(dacc[s], __dmul_rn(w, Ld));
+            }
+          }
+        }
         double kr[4];
         kref_row(li, g, kr);
         const double kscale = (MODE == TP_ASM_MASS) ? 0.0
@@ -121,6 +147,18 @@ __global__ void __launch_bounds__(128) k_assemble_rows(
       }
     }
   }
+  if constexpr (DIAG) {
+    if (valid) {
+#pragma unroll
+      for (int s = 0; s < 4; s++) {
+        if (s < ex.ld) {
+          const double v = is_bc ? 1.0 : (s < ex.S ? dacc[s] : 0.0);
+          if (ex.d64) ex.d64[r * ex.ld + s] = v;
+          if (ex.d32) ex.d32[r * ex.ld + s] = (float)v;
+        }
+      }
+    }
+  }
   __syncthreads();
   const int pbeg = s_ptr[0], pend = s_ptr[nrows];
   for (int p = pbeg + tid; p < pend; p += B) {
@@ -137,6 +175,7 @@ __global__ void __launch_bounds__(128) k_assemble_rows(
     if (bc_mask && bc_mask[r0 + lo]) v = (indices[p] == r0 + lo) ? 1.0 : 0.0;
     if (out64) out64[p] = v;
     if (out32) out32[p] = (float)v;
+    if (ex.sell32) ex.sell32[ex.csr2sell[p]] = (float)v;
   }
 }
 
@@ -667,16 +706,16 @@ extern "C" int tp_assemble_csr(const tp_mesh* m, const double* De_cell, const do
   cudaStream_t st = as_stream(stream);
   const size_t smem = sizeof(double) * 128 * (size_t)m->max_row_len;
   const int grid = grid_for(m->n_verts, 128);
+  const RowExtras ex{};
 #define TP_ASM_LAUNCH(MD)                                                                 \
   do {                                                                                    \
     if (smem > 48 * 1024)                                                                 \
-      TP_CUDA_TRY(cudaFuncSetAttribute(k_assemble_rows<MD>,                               \
+      TP_CUDA_TRY(cudaFuncSetAttribute(k_assemble_rows<MD, false>,                        \
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,       \
                                        (int)smem));                                       \
-    k_assemble_rows<MD><<<grid, 128, smem, st>>>(m->n_verts, m->v2c_ptr, m->v2c,          \
-                                                 m->v2c_slots, m->geo, De_cell, alpha_cell, \
-                                                 inv_dt, lumped, bc_mask, m->indptr,      \
-                                                 m->indices, out64, out32);               \
+    k_assemble_rows<MD, false><<<grid, 128, smem, st>>>(                                  \
+        m->n_verts, m->v2c_ptr, m->v2c, m->v2c_slots, m->geo, De_cell, alpha_cell, inv_dt, \
+        lumped, bc_mask, m->indptr, m->indices, out64, out32, ex);                        \
   } while (0)
   switch (mode) {
     case TP_ASM_FULL:
@@ -720,6 +759,35 @@ extern "C" int tp_lumped_diag(const tp_mesh* m, int S, int ld, const double* alp
   k_lumped_diag<<<grid_for(m->n_verts, 128, 65535), 128, 0, as_stream(stream)>>>(
       m->n_verts, S, ld, m->v2c_ptr, m->v2c, m->geo, alpha, make_double4(sh[0], sh[1], sh[2], sh[3]),
       bc_mask, diag64, diag32);
+  TP_LAUNCH_CHECK();
+  return TP_OK;
+}
+
+extern "C" int tp_assemble_stiffness_diag(const tp_mesh* m, const double* De_cell, int S,
+                                          int ld, const double* alpha, const double* shift,
+                                          const uint8_t* bc_mask, double* out64, float* out32,
+                                          const int32_t* csr2sell, float* sell32,
+                                          double* diag64, float* diag32, void* stream) {
+  TP_REQUIRE(mesh_ok(m) && m->v2c_slots && m->indices && De_cell, "incomplete mesh or De");
+  TP_REQUIRE(S >= 1 && S <= TP_MAX_COLS && ld >= S && ld <= TP_MAX_COLS, "bad S/ld");
+  TP_REQUIRE(out64 || out32 || sell32, "no operator output");
+  TP_REQUIRE(diag64 || diag32, "no diagonal output");
+  TP_REQUIRE(!sell32 || csr2sell, "sell32 needs csr2sell");
+  TP_REQUIRE(m->max_row_len >= 1 && m->max_row_len <= 255, "bad max_row_len");
+  if (m->n_verts == 0) return TP_OK;
+  cudaStream_t st = as_stream(stream);
+  double sh[4] = {0, 0, 0, 0};
+  for (int s = 0; s < S; s++) sh[s] = shift ? shift[s] : 0.0;
+  RowExtras ex{S, ld, alpha, make_double4(sh[0], sh[1], sh[2], sh[3]), diag64, diag32,
+               csr2sell, sell32};
+  const size_t smem = sizeof(double) * 128 * (size_t)m->max_row_len;
+  const int grid = grid_for(m->n_verts, 128);
+  if (smem > 48 * 1024)
+    TP_CUDA_TRY(cudaFuncSetAttribute(k_assemble_rows<TP_ASM_STIFF, true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_assemble_rows<TP_ASM_STIFF, true><<<grid, 128, smem, st>>>(
+      m->n_verts, m->v2c_ptr, m->v2c, m->v2c_slots, m->geo, De_cell, nullptr, 0.0, 1, bc_mask,
+      m->indptr, m->indices, out64, out32, ex);
   TP_LAUNCH_CHECK();
   return TP_OK;
 }

@@ -74,8 +74,9 @@ class WarmStartMLP:
         self.T = torch.empty(max(capacity_rows, 1), dtype=torch.float32, device=device)
         self.rows = 0
         self.rng = np.random.default_rng(seed)
-        # per guess: the stiffness images, the network (+ projection dots and update)
-        self.launches = 4 if self.project else 2
+        # per guess: the stiffness images, the network (+ projection dots, coefficients and
+        # update)
+        self.launches = 5 if self.project else 2
 
     # ---- inputs -----------------------------------------------------------------
     def inputs(self, U, Up, S, ld, D, k, phi=None, ngphi=None, ops=None,

@@ -184,8 +184,21 @@ class BatchedTransport:
 
     # -- per-step pieces -------------------------------------------------------------
     def assemble_operator(self):
-        self.assemble_stiffness()
-        self.assemble_diagonal()
+        """Shared stiffness K_xi (FP64, FP32) and the per-column lumped diagonal in one row
+        walk (tp_assemble_stiffness_diag); with the persistent FP32 engine the same launch
+        writes the solver's FP32 SELL values (no separate scatter)."""
+        sol = getattr(self, "solver", None)
+        direct = (self.engine == "persistent" and sol is not None and sol.inner_fp32
+                  and sol.sM is None)
+        call("tp_assemble_stiffness_diag", ctypes.byref(self.dm.tpm), ptr(self.coef), self.S,
+             self.ld, ptr(self.alpha), self._shift(), ptr(self.bc_mask), ptr(self.K64),
+             ptr(self.K32), ptr(sol.sell.csr2sell) if direct else None,
+             ptr(sol.sK) if direct else None, ptr(self.D64), ptr(self.D32), stream_handle())
+        self._sell_fresh = direct
+
+    def _shift(self):
+        return (ctypes.c_double * 4)(*([self.inv_dt + kk for kk in self.k] +
+                                       [0.0] * (4 - self.S)))
 
     def assemble_stiffness(self):
         """Shared stiffness K_xi (FP64 and FP32 values)."""
@@ -194,10 +207,8 @@ class BatchedTransport:
 
     def assemble_diagonal(self):
         """Per-column lumped (1/dt + k_s + alpha_s) m."""
-        shift = (ctypes.c_double * 4)(*([self.inv_dt + kk for kk in self.k] +
-                                        [0.0] * (4 - self.S)))
         call("tp_lumped_diag", ctypes.byref(self.dm.tpm), self.S, self.ld, ptr(self.alpha),
-             shift, ptr(self.bc_mask), ptr(self.D64), ptr(self.D32), stream_handle())
+             self._shift(), ptr(self.bc_mask), ptr(self.D64), ptr(self.D32), stream_handle())
 
     def assemble_rhs(self):
         """b = M (U/dt + f) per column; f (V, ld) when a source is set (self.f)."""
@@ -256,7 +267,7 @@ class BatchedTransport:
     def step_operator(self):
         """The part of a step that does not read the state: the operator."""
         self.assemble_operator()
-        if self.engine == "persistent":
+        if self.engine == "persistent" and not self._sell_fresh:
             self.solver.refresh_values()
 
     def step_state(self, sync=True):
@@ -291,8 +302,8 @@ class BatchedTransport:
         if self.guess == "learned" and self.predictor is not None:
             guess = self.predictor.launches
         if self.engine == "persistent":
-            # assembly, diagonal, RHS, SELL scatter, guess, solve, increment
-            return 3 + 1 + guess + 1 + 1
+            # operator (+ SELL scatter for the FP64 engine), RHS, guess, solve, increment
+            return 1 + (0 if getattr(self, "_sell_fresh", False) else 1) + 1 + guess + 1 + 1
         return 3 + guess + 4 + 3 * int(res["iterations"]) + 2 * int(res["n_reliable"]) + 1
 
     def step_host(self, u_host: torch.Tensor, out_host: torch.Tensor):

@@ -148,6 +148,18 @@ TP_API int tp_dirichlet_rows(int64_t n_bc, const int32_t* bc_dofs, int64_t n_row
 TP_API int tp_lumped_diag(const tp_mesh* m, int S, int ld, const double* alpha, const double* shift,
                    const uint8_t* bc_mask, double* diag64, float* diag32, void* stream);
 
+/* The shared stiffness of the batched step and its per-column lumped diagonal in one row
+ * walk (no reference counterpart as one call: gpu_assembler.py:60-139 in TP_ASM_STIFF mode
+ * plus tp_lumped_diag): out64 / out32 (CSR order) as tp_assemble_csr(mode TP_ASM_STIFF,
+ * lumped) and diag64 / diag32 as tp_lumped_diag, both bit-identical to those calls;
+ * optionally sell32[csr2sell[p]] = (float) value p (the FP32 SELL values of tp_sell_build's
+ * csr2sell map, as tp_sell_scatter writes them). */
+TP_API int tp_assemble_stiffness_diag(const tp_mesh* m, const double* De_cell, int S, int ld,
+                                      const double* alpha, const double* shift,
+                                      const uint8_t* bc_mask, double* out64, float* out32,
+                                      const int32_t* csr2sell, float* sell32, double* diag64,
+                                      float* diag32, void* stream);
+
 /* gpu_assembler.py:176-221 + :228-239 for S columns (interleaved, leading dim ld):
  * b = M (inv_dt u_old + f) lumped or consistent, then b[bc_dofs, s] = bc_value[s]
  * (host array of S values; bc_dofs may be NULL).  f may be NULL (zero source). */

@@ -51,3 +51,48 @@ def test_batch_matches_one_at_a_time_plain(cuda_device):
         assert r1["converged"] and all(r["converged"] for r in r2)
     a, b = mb.state(), pl.state()
     assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-7
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("with_alpha_bc", [False, True])
+def test_fused_stiffness_diag_equals_separate_calls(cuda_device, with_alpha_bc):
+    """tp_assemble_stiffness_diag = tp_assemble_csr(STIFF) + tp_lumped_diag + the FP32 SELL
+    scatter, bit for bit."""
+    import ctypes
+
+    import torch
+
+    from dissolve_tp import _lib
+    from dissolve_tp.assembler import DeviceMesh
+    from dissolve_tp.device import ptr, stream_handle
+    from dissolve_tp.krylov import SellPattern
+    from dissolve_tp.mesh import face_dofs, kuhn_cube
+    m = kuhn_cube(10, 0.2, seed=4)
+    rng = np.random.default_rng(9)
+    dm = DeviceMesh(m.coords, m.cells)
+    dev = torch.device("cuda")
+    S, ld, nnz, V = 3, 4, dm.nnz, dm.n_verts
+    De = torch.from_numpy(np.exp(0.3 * rng.standard_normal(m.n_cells))).to(dev)
+    alpha = bc = None
+    if with_alpha_bc:
+        alpha = torch.zeros((m.n_cells, ld), dtype=torch.float64, device=dev)
+        alpha[:, :S] = torch.from_numpy(rng.uniform(0, 2, (m.n_cells, S)))
+        bc = dm.bc_mask(face_dofs(m, 1, "max"))
+    shift = (ctypes.c_double * 4)(50.5, 50.0, 50.2, 0.0)
+    st = stream_handle()
+    K64a, K64b = (torch.zeros(nnz, dtype=torch.float64, device=dev) for _ in range(2))
+    K32a, K32b = (torch.zeros(nnz, dtype=torch.float32, device=dev) for _ in range(2))
+    D64a, D64b = (torch.zeros((V, ld), dtype=torch.float64, device=dev) for _ in range(2))
+    D32a, D32b = (torch.zeros((V, ld), dtype=torch.float32, device=dev) for _ in range(2))
+    sell = SellPattern(dm.indptr, dm.indices[:nnz])
+    Sa, Sb = sell.values(torch.float32), sell.values(torch.float32)
+    _lib.call("tp_assemble_csr", ctypes.byref(dm.tpm), ptr(De), None, 0.0, 1, _lib.TP_ASM_STIFF,
+              ptr(bc), ptr(K64a), ptr(K32a), st)
+    _lib.call("tp_lumped_diag", ctypes.byref(dm.tpm), S, ld, ptr(alpha), shift, ptr(bc),
+              ptr(D64a), ptr(D32a), st)
+    sell.scatter(K64a, out32=Sa)
+    _lib.call("tp_assemble_stiffness_diag", ctypes.byref(dm.tpm), ptr(De), S, ld, ptr(alpha),
+              shift, ptr(bc), ptr(K64b), ptr(K32b), ptr(sell.csr2sell), ptr(Sb), ptr(D64b),
+              ptr(D32b), st)
+    for a, b in ((K64a, K64b), (K32a, K32b), (D64a, D64b), (D32a, D32b), (Sa, Sb)):
+        assert torch.equal(a, b)
