@@ -325,6 +325,20 @@ __global__ void k_rhs_rows(int64_t nv, int S, int ld, const int32_t* __restrict_
   }
 }
 
+// lumped right-hand side from the per-vertex lumped mass: b = m (inv_dt u + f) per column
+__global__ void k_lumped_rhs(int64_t nv, int S, int ld, const double* __restrict__ mass,
+                             const double* __restrict__ u, const double* __restrict__ f,
+                             double inv_dt, double* __restrict__ b) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv * ld;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t v = i / ld;
+    const int s = (int)(i - v * ld);
+    double r = 0.0;
+    if (s < S) r = __dmul_rn(mass[v], __dadd_rn(__dmul_rn(inv_dt, u[i]), f ? f[i] : 0.0));
+    b[i] = r;
+  }
+}
+
 // gpu_assembler.py:228-239
 __global__ void k_rhs_bc(int64_t n_bc, const int32_t* __restrict__ bc, int64_t nv, int S,
                          int ld, double4 val, double* __restrict__ b) {
@@ -808,6 +822,28 @@ extern "C" int tp_assemble_rhs(const tp_mesh* m, int S, int ld, const double* u_
     double v[4] = {0, 0, 0, 0};
     for (int s = 0; s < S; s++) v[s] = bc_value ? bc_value[s] : 0.0;
     k_rhs_bc<<<grid_for(n_bc, 128), 128, 0, st>>>(n_bc, bc_dofs, m->n_verts, S, ld,
+                                                  make_double4(v[0], v[1], v[2], v[3]), b);
+    TP_LAUNCH_CHECK();
+  }
+  return TP_OK;
+}
+
+extern "C" int tp_lumped_rhs(int64_t n_verts, int S, int ld, const double* mass,
+                             const double* u_old, const double* f, double inv_dt, int64_t n_bc,
+                             const int32_t* bc_dofs, const double* bc_value, double* b,
+                             void* stream) {
+  TP_REQUIRE(mass && u_old && b, "null pointer");
+  TP_REQUIRE(S >= 1 && S <= TP_MAX_COLS && ld >= S && ld <= TP_MAX_COLS, "bad S/ld");
+  cudaStream_t st = as_stream(stream);
+  if (n_verts > 0) {
+    k_lumped_rhs<<<grid_for(n_verts * ld, 256, sm_count() * 8), 256, 0, st>>>(
+        n_verts, S, ld, mass, u_old, f, inv_dt, b);
+    TP_LAUNCH_CHECK();
+  }
+  if (n_bc > 0 && bc_dofs) {
+    double v[4] = {0, 0, 0, 0};
+    for (int s = 0; s < S; s++) v[s] = bc_value ? bc_value[s] : 0.0;
+    k_rhs_bc<<<grid_for(n_bc, 128), 128, 0, st>>>(n_bc, bc_dofs, n_verts, S, ld,
                                                   make_double4(v[0], v[1], v[2], v[3]), b);
     TP_LAUNCH_CHECK();
   }

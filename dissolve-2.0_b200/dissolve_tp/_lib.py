@@ -106,6 +106,8 @@ SIGNATURES = {
     "tp_assemble_stiffness_diag": (ctypes.c_int, [_P(TpMesh), _vp, ctypes.c_int, ctypes.c_int,
                                                   _vp, _P(_c_dbl), _vp, _vp, _vp, _vp, _vp, _vp,
                                                   _vp, _vp]),
+    "tp_lumped_rhs": (ctypes.c_int, [_c_i64, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _c_dbl,
+                                     _c_i64, _vp, _P(_c_dbl), _vp, _vp]),
     "tp_assemble_rhs": (ctypes.c_int, [_P(TpMesh), ctypes.c_int, ctypes.c_int, _vp, _vp, _c_dbl,
                                        ctypes.c_int, _c_i64, _vp, _P(_c_dbl), _vp, _vp]),
     "tp_nodal_gradient": (ctypes.c_int, [_P(TpMesh), _vp, _vp, _vp, _vp]),

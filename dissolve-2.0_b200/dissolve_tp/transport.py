@@ -170,6 +170,11 @@ class BatchedTransport:
                                    delta=delta, **cg)
         self.U = torch.zeros((n, self.ld), dtype=torch.float64, device=dev)
         self.U_prev = torch.zeros_like(self.U)
+        # lumped mass per vertex (the cell-order sums of tp_lumped_diag with shift 1): the
+        # right-hand side becomes one element-wise pass
+        self.mass = torch.zeros(n, dtype=torch.float64, device=dev)
+        call("tp_lumped_diag", ctypes.byref(dm.tpm), 1, 1, None, (ctypes.c_double * 4)(1.0),
+             None, ptr(self.mass), None, stream_handle())
         # increments of the last steps, newest first (u^n - u^{n-1}, u^{n-1} - u^{n-2}, ...):
         # directions of the projected learned guess
         self.dU = [torch.zeros_like(self.U) for _ in range(5)]
@@ -211,10 +216,11 @@ class BatchedTransport:
              self._shift(), ptr(self.bc_mask), ptr(self.D64), ptr(self.D32), stream_handle())
 
     def assemble_rhs(self):
-        """b = M (U/dt + f) per column; f (V, ld) when a source is set (self.f)."""
+        """b = M (U/dt + f) per column (lumped M, tp_lumped_rhs); f (V, ld) when a source is
+        set (self.f)."""
         n_bc = 0 if self.bc_dofs is None else int(self.bc_dofs.numel())
-        call("tp_assemble_rhs", ctypes.byref(self.dm.tpm), self.S, self.ld, ptr(self.U),
-             ptr(getattr(self, "f", None)), self.inv_dt, 1, n_bc, ptr(self.bc_dofs),
+        call("tp_lumped_rhs", self.dm.n_verts, self.S, self.ld, ptr(self.mass), ptr(self.U),
+             ptr(getattr(self, "f", None)), self.inv_dt, n_bc, ptr(self.bc_dofs),
              self.bc_values, ptr(self.solver.b), stream_handle())
 
     def initial_guess(self):

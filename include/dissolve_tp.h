@@ -167,6 +167,14 @@ TP_API int tp_assemble_rhs(const tp_mesh* m, int S, int ld, const double* u_old,
                     double inv_dt, int lumped, int64_t n_bc, const int32_t* bc_dofs,
                     const double* bc_value, double* b, void* stream);
 
+/* The lumped right-hand side of tp_assemble_rhs (lumped = 1) from a precomputed lumped
+ * mass per vertex (mass = tp_lumped_diag with S = 1, shift 1, no alpha): b = mass (inv_dt
+ * u_old + f) per column, one element-wise pass (no reference counterpart as such; it
+ * differs from the cell-order sums of tp_assemble_rhs by rounding only, ~1e-16 relative). */
+TP_API int tp_lumped_rhs(int64_t n_verts, int S, int ld, const double* mass, const double* u_old,
+                         const double* f, double inv_dt, int64_t n_bc, const int32_t* bc_dofs,
+                         const double* bc_value, double* b, void* stream);
+
 /* gpu_assembler.py:251-304, 646-673: volume-weighted vertex average of the cellwise
  * gradient.  JinvT (n_cells, 9) as the reference stores it, or NULL to recompute J^-T
  * from coords4.  grad (n_verts, 3). */

@@ -96,3 +96,40 @@ def test_fused_stiffness_diag_equals_separate_calls(cuda_device, with_alpha_bc):
               ptr(D32b), st)
     for a, b in ((K64a, K64b), (K32a, K32b), (D64a, D64b), (D32a, D32b), (Sa, Sb)):
         assert torch.equal(a, b)
+
+
+@pytest.mark.gpu
+def test_lumped_rhs_matches_cell_order_rhs(cuda_device):
+    """tp_lumped_rhs (mass per vertex x (u/dt + f)) against tp_assemble_rhs (cell-order sums),
+    with a source and Dirichlet rows: equal to rounding."""
+    import ctypes
+
+    import torch
+
+    from dissolve_tp import _lib
+    from dissolve_tp.assembler import DeviceMesh
+    from dissolve_tp.device import ptr, stream_handle
+    from dissolve_tp.mesh import face_dofs, kuhn_cube
+    m = kuhn_cube(9, 0.2, seed=2)
+    dm = DeviceMesh(m.coords, m.cells)
+    rng = np.random.default_rng(4)
+    V, S, ld = dm.n_verts, 3, 4
+    dev = torch.device("cuda")
+    U = torch.zeros((V, ld), dtype=torch.float64, device=dev)
+    F = torch.zeros_like(U)
+    U[:, :S] = torch.from_numpy(rng.uniform(0, 1, (V, S)))
+    F[:, :S] = torch.from_numpy(rng.normal(0, 1, (V, S)))
+    bc = torch.from_numpy(face_dofs(m, 2, "min")).to(dev)
+    bcv = (ctypes.c_double * 4)(1.0, 0.5, 0.25, 0.0)
+    st = stream_handle()
+    mass = torch.zeros(V, dtype=torch.float64, device=dev)
+    _lib.call("tp_lumped_diag", ctypes.byref(dm.tpm), 1, 1, None, (ctypes.c_double * 4)(1.0), None,
+              ptr(mass), None, st)
+    b1, b2 = torch.zeros_like(U), torch.full_like(U, 7.0)
+    _lib.call("tp_assemble_rhs", ctypes.byref(dm.tpm), S, ld, ptr(U), ptr(F), 50.0, 1,
+              int(bc.numel()), ptr(bc), bcv, ptr(b1), st)
+    _lib.call("tp_lumped_rhs", V, S, ld, ptr(mass), ptr(U), ptr(F), 50.0, int(bc.numel()),
+              ptr(bc), bcv, ptr(b2), st)
+    assert (b1 - b2).abs().max().item() <= 1e-14 * b1.abs().max().item()
+    assert torch.equal(b1[bc.long()], b2[bc.long()])
+    assert torch.equal(b2[:, S:], torch.zeros_like(b2[:, S:]))
