@@ -179,6 +179,7 @@ constexpr int GP_BLOCKS = 592;
 
 struct GuessDirs {
   const double* d[GP_MAXD];
+  const double* img0;  // D K d[0] precomputed (no Dirichlet rows), or NULL
 };
 
 template <int M>
@@ -232,7 +233,8 @@ __global__ void __launch_bounds__(256) k_guess_dots(
 #pragma unroll
       for (int u = 0; u < RP; u++)
 #pragma unroll
-        for (int k = 0; k < M; k++) dvv[u][k] = __ldg(dirs.d[k] + jj[u]);
+        for (int k = 0; k < M; k++)
+          dvv[u][k] = (k == 0 && dirs.img0) ? 0.0 : __ldg(dirs.d[k] + jj[u]);
 #pragma unroll
       for (int u = 0; u < RP; u++) {
         if (p0 + u >= end) break;
@@ -247,7 +249,7 @@ __global__ void __launch_bounds__(256) k_guess_dots(
 #pragma unroll
     for (int k = 0; k < M; k++) {
       dv[k] = dirs.d[k][i];
-      Ad[k] = dsc_s * kd[k] + dg * dv[k];
+      Ad[k] = ((k == 0 && dirs.img0) ? dirs.img0[i] : dsc_s * kd[k]) + dg * dv[k];
     }
     int q = 0;
 #pragma unroll
@@ -526,8 +528,8 @@ extern "C" size_t tp_guess_project_workspace_doubles(void) {
 
 extern "C" int tp_guess_project(const tp_csr_op* op, const double* diag, const uint8_t* bc_mask,
                                 const double* b, const double* U, const double* opU,
-                                int n_dirs, const double* const* dirs, double* x, double* work,
-                                void* stream) {
+                                int n_dirs, const double* const* dirs, const double* img0,
+                                double* x, double* work, void* stream) {
   TP_REQUIRE(op && op->indptr && op->indices && op->K64 && diag && b && U && opU && x && work,
              "null pointer");
   TP_REQUIRE(op->ld == 1 || op->ld == 2 || op->ld == 4, "ld must be 1, 2 or 4");
@@ -538,6 +540,7 @@ extern "C" int tp_guess_project(const tp_csr_op* op, const double* diag, const u
     TP_REQUIRE(dirs[k], "null direction");
     gd.d[k] = dirs[k];
   }
+  gd.img0 = bc_mask ? nullptr : img0;
   if (op->n_rows == 0) return TP_OK;
   cudaStream_t st = as_stream(stream);
   if (n_dirs == 0) {

@@ -632,6 +632,18 @@ __global__ void k_axpby(int64_t n, double a, const double* __restrict__ x, doubl
     y[i] = a * x[i] + b * y[i];
 }
 
+// state advance after a solve: d = x - u, u_prev = u, u = x (one pass)
+__global__ void k_advance(int64_t n, const double* __restrict__ x, double* __restrict__ u,
+                          double* __restrict__ u_prev, double* __restrict__ d) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double xv = x[i], uv = u[i];
+    d[i] = xv - uv;
+    u_prev[i] = uv;
+    u[i] = xv;
+  }
+}
+
 // (n, S) contiguous <-> (n, ld) interleaved with zero padding
 __global__ void k_pack(int64_t n, int S, int ld, const double* __restrict__ src,
                        double* __restrict__ dst) {
@@ -1062,6 +1074,15 @@ extern "C" int tp_mean_cell_diameter(const tp_mesh* m, double* out_dev, void* sc
                                         reinterpret_cast<const double4*>(m->coords4), part);
   TP_LAUNCH_CHECK();
   k_sum_parts<<<1, 256, 0, st>>>(grid, part, out_dev);  // the sum; the caller divides by n
+  TP_LAUNCH_CHECK();
+  return TP_OK;
+}
+
+extern "C" int tp_advance_state(int64_t n, const double* x, double* u, double* u_prev,
+                                double* d, void* stream) {
+  TP_REQUIRE(x && u && u_prev && d, "null pointer");
+  if (n == 0) return TP_OK;
+  k_advance<<<grid_for(n, 256, sm_count() * 8), 256, 0, as_stream(stream)>>>(n, x, u, u_prev, d);
   TP_LAUNCH_CHECK();
   return TP_OK;
 }

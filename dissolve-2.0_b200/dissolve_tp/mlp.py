@@ -199,9 +199,10 @@ class WarmStartMLP:
         nh = max(1, int(getattr(tr, "n_hist", 1)))
         dirs = [tr.dU[0], self._d] + list(tr.dU[1:nh])
         arr = (ctypes.c_void_p * len(dirs))(*[ptr(d) for d in dirs])
+        # ops[1] = D K (u^n - u^{n-1}) is the image of the first direction
         call("tp_guess_project", ctypes.byref(tr.stiff_op.struct), ptr(tr.D64),
-             ptr(tr.bc_mask), ptr(tr.solver.b), ptr(tr.U), ptr(ops[0]), len(dirs), arr, ptr(x),
-             ptr(self._work), stream_handle())
+             ptr(tr.bc_mask), ptr(tr.solver.b), ptr(tr.U), ptr(ops[0]), len(dirs), arr,
+             ptr(ops[1]), ptr(x), ptr(self._work), stream_handle())
 
 
 def trajectory_pairs(tr, steps):

@@ -287,14 +287,11 @@ class BatchedTransport:
     def advance_state(self):
         """After a solve: the increment x - U joins the history (newest first), then
         U_prev = U, U = x."""
-        x = self.solver.x
         d = self.dU.pop()
-        d.copy_(x)
-        call("tp_axpby", d.numel(), -1.0, ptr(self.U), 1.0, ptr(d), stream_handle())
+        call("tp_advance_state", self.U.numel(), ptr(self.solver.x), ptr(self.U),
+             ptr(self.U_prev), ptr(d), stream_handle())
         self.dU.insert(0, d)
         self.n_hist = min(self.n_hist + 1, len(self.dU))
-        self.U_prev.copy_(self.U)
-        self.U.copy_(x)
         self.steps_done += 1
 
     def state(self) -> np.ndarray:

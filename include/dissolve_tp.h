@@ -268,6 +268,10 @@ TP_API int tp_levelset_advance(int64_t n, double* phi, int ld, const double* U, 
 
 /* y = a x + b y (n doubles): numerics/solvers.py:278-279 under-relaxation */
 TP_API int tp_axpby(int64_t n, double a, const double* x, double b, double* y, void* stream);
+/* After a solve, in one pass over n values: d = x - u, u_prev = u, u = x (the step
+ * increment for the projected guess and the state update; no reference counterpart) */
+TP_API int tp_advance_state(int64_t n, const double* x, double* u, double* u_prev, double* d,
+                            void* stream);
 
 /* (n, S) row-major columns -> (n, ld) interleaved, padding columns zero, and back.
  * Plumbing for host arrays of S species (no reference counterpart). */
@@ -332,11 +336,14 @@ TP_API int tp_csr_images(const tp_csr_op* op, const double* x1, const double* x2
  * h_k = d_k . (b - A U) over the free rows (directions taken as zero on Dirichlet rows;
  * a direction numerically in the span of the earlier ones gets c_k = 0): the minimum of
  * the A-norm of the error over U + span{d_k}, so never above U in that norm.
- * Deterministic.  work: device scratch of tp_guess_project_workspace_doubles() doubles. */
+ * img0: D K dirs[0] when already computed (tp_csr_images' second output), else NULL; it
+ * is used only without Dirichlet rows.  Deterministic.  work: device scratch of
+ * tp_guess_project_workspace_doubles() doubles. */
 TP_API size_t tp_guess_project_workspace_doubles(void);
 TP_API int tp_guess_project(const tp_csr_op* op, const double* diag, const uint8_t* bc_mask,
                             const double* b, const double* U, const double* opU, int n_dirs,
-                            const double* const* dirs, double* x, double* work, void* stream);
+                            const double* const* dirs, const double* img0, double* x,
+                            double* work, void* stream);
 
 /* ------------------------------------------------------------------ Krylov solve */
 /* Jacobi-preconditioned CG on every (system, column) lane at once, captured in a CUDA

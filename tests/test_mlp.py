@@ -211,7 +211,7 @@ def test_guess_projection_matches_galerkin_solve(cuda_device, with_bc, n_dirs):
                        device=cuda_device)
     arr = (ctypes.c_void_p * n_dirs)(*[ptr(d) for d in dirs])
     call("tp_guess_project", ctypes.byref(tr.stiff_op.struct), ptr(tr.D64), ptr(tr.bc_mask),
-         ptr(tr.solver.b), ptr(tr.U), ptr(opU), n_dirs, arr, ptr(x), ptr(work),
+         ptr(tr.solver.b), ptr(tr.U), ptr(opU), n_dirs, arr, None, ptr(x), ptr(work),
          stream_handle())
     xg = x.cpu().numpy()
     n = m.n_verts
@@ -244,7 +244,17 @@ def test_guess_projection_matches_galerkin_solve(cuda_device, with_bc, n_dirs):
     x1, x2 = torch.zeros_like(x), torch.zeros_like(x)
     arr1 = (ctypes.c_void_p * 1)(ptr(dirs[0]))
     call("tp_guess_project", ctypes.byref(tr.stiff_op.struct), ptr(tr.D64), ptr(tr.bc_mask),
-         ptr(tr.solver.b), ptr(tr.U), ptr(opU), 1, arr1, ptr(x1), ptr(work), stream_handle())
+         ptr(tr.solver.b), ptr(tr.U), ptr(opU), 1, arr1, None, ptr(x1), ptr(work),
+         stream_handle())
     call("tp_guess_project", ctypes.byref(tr.stiff_op.struct), ptr(tr.D64), ptr(tr.bc_mask),
-         ptr(tr.solver.b), ptr(tr.U), ptr(opU), 2, arr2, ptr(x2), ptr(work), stream_handle())
+         ptr(tr.solver.b), ptr(tr.U), ptr(opU), 2, arr2, None, ptr(x2), ptr(work),
+         stream_handle())
     assert torch.equal(x1, x2)
+    if not with_bc:
+        # the first direction's image supplied precomputed: same guess to rounding
+        x3 = torch.zeros_like(x)
+        _, img = tr.operator_images(tr.U + dirs[0], tr.U, fresh=True)
+        call("tp_guess_project", ctypes.byref(tr.stiff_op.struct), ptr(tr.D64), None,
+             ptr(tr.solver.b), ptr(tr.U), ptr(opU), n_dirs, arr, ptr(img), ptr(x3), ptr(work),
+             stream_handle())
+        assert (x3 - x).abs().max().item() <= 1e-9 * x.abs().max().item()
