@@ -994,14 +994,12 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
     cp_async_wait_all();
     __syncthreads();
     const int e0 = s_sp[0];
-    auto row_done = [&](int sl, const VT ak[LD], const VT am[LD]) {
+    // dr: the row's diagonal (loaded by the caller)
+    auto row_done = [&](int sl, const VT ak[LD], const VT am[LD], const VT dr[LD]) {
       const int64_t row = (int64_t)sl * 32 + lane;
       if (row < a.n) {
-        VT ur[LD], dr[LD], wv[LD];
+        VT ur[LD], wv[LD];
         ld_win<VT, LD>(s_win, (int)(row - r0), ur);
-#pragma unroll
-        for (int s = 0; s < LD; s++) dr[s] = VT(0);
-        if (a.diag) ldv<VT, LD>(a.diag, row, dr);
         const bool bcr = a.bc && a.bc[row];
 #pragma unroll
         for (int s = 0; s < LD; s++) {
@@ -1027,6 +1025,20 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
             if constexpr (HASM) mvals[j][k] = (k < w) ? ld_na(a.sM + base + k * 32 + lane) : VT(0);
           }
         }
+        // the slab rows' diagonals: issued with the values for rows of at most 8 bytes
+        // (wider rows have no registers to spare and load them per slice)
+        constexpr bool DPRE = RB <= 8;
+        VT dgs[MAXS][LD];
+        auto load_diag = [&](int j) {
+          const int64_t row = (int64_t)(slb + j * nwarps) * 32 + lane;
+#pragma unroll
+          for (int s = 0; s < LD; s++) dgs[j][s] = VT(0);
+          if (a.diag && slb + j * nwarps < se && row < a.n) ldv<VT, LD>(a.diag, row, dgs[j]);
+        };
+        if constexpr (DPRE) {
+#pragma unroll
+          for (int j = 0; j < MAXS; j++) load_diag(j);
+        }
 #pragma unroll
         for (int j = 0; j < MAXS; j++) {
           const int sl = slb + j * nwarps;
@@ -1048,7 +1060,8 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
                 }
               }
             }
-            row_done(sl, ak, am);
+            if constexpr (!DPRE) load_diag(j);
+            row_done(sl, ak, am, dgs[j]);
           }
         }
       }
@@ -1082,7 +1095,11 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
             if constexpr (HASM) mm[u] = mn[u];
           }
         }
-        row_done(sl, ak, am);
+        VT dr[LD];
+#pragma unroll
+        for (int s = 0; s < LD; s++) dr[s] = VT(0);
+        if (a.diag && (int64_t)sl * 32 + lane < a.n) ldv<VT, LD>(a.diag, (int64_t)sl * 32 + lane, dr);
+        row_done(sl, ak, am, dr);
       }
     }
   };
