@@ -555,7 +555,7 @@ extern "C" int tp_guess_project(const tp_csr_op* op, const double* diag, const u
   double* coef = work + (size_t)GP_BLOCKS * GP_SLOTS;
 #define TP_GP(LDV, MV)                                                                       \
   do {                                                                                       \
-    const int nb = (int)std::min<int64_t>(GP_BLOCKS, (n + 256 / LDV - 1) / (256 / LDV));     \
+    const int nb = (int)std::min<int64_t>(GP_BLOCKS / 2, (n + 256 / LDV - 1) / (256 / LDV)); \
     k_guess_dots<LDV, MV><<<nb, 256, 0, st>>>(n, op->S, op->indptr, op->indices, op->K64,    \
                                               dsc, diag, bc_mask, b, U, opU, gd, part);      \
     k_guess_coeffs<MV><<<1, 1024, 0, st>>>(nb, op->S, part, coef);                           \

@@ -1463,14 +1463,29 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
       }
       ok = grid_sync(a.bar, target);
       if (!ok) break;
-      {
+      // the FP64 residual sums first: when no triggered lane goes on (all converged or
+      // failed) the product is skipped.  Every CTA reads the same totals, so every CTA
+      // takes the same branch and the barrier counts stay equal.
+      grid_totals<8, 0>(a.part, s_tot, s_buf);
+      if (threadIdx.x == 0) {
+        int cont = 0;
+        for (int s = 0; s < S; s++)
+          if (L.trigger[s] && isfinite(s_tot[s]) && isfinite(s_tot[4 + s]) &&
+              s_tot[4 + s] > L.tol2[s])
+            cont = 1;
+        s_anytrig = cont;
+        if (!cont)
+          for (int s = 0; s < 4; s++) s_tot[8 + s] = 0.0;  // w.u not needed
+      }
+      __syncthreads();
+      if (s_anytrig) {
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
         product(acc, false);
         block_partial<4>(acc, a.part + 8, sh);
+        ok = grid_sync(a.bar, target);
+        if (!ok) break;
+        grid_totals<4, 8>(a.part, s_tot, s_buf);
       }
-      ok = grid_sync(a.bar, target);
-      if (!ok) break;
-      grid_totals<12>(a.part, s_tot, s_buf);
       if (threadIdx.x == 0) {
         n_rel++;
         for (int s = 0; s < S; s++) {

@@ -117,7 +117,7 @@ class BatchedTransport:
     """All species in one multi-column solve (shared stiffness, per-column diagonal)."""
 
     def __init__(self, mesh, coef_cell, D, k, dt, rtol=1e-8, max_it=5000, lumped=True,
-                 inner_fp32=True, delta=0.01, guess="previous", bc_dofs=None, bc_values=None,
+                 inner_fp32=True, delta=0.001, guess="previous", bc_dofs=None, bc_values=None,
                  alpha_cells=None, autotune=True, cg=None, asm=None, engine="persistent"):
         if not lumped:
             raise ValueError("the batched form splits the operator into a shared stiffness "
