@@ -644,6 +644,24 @@ __global__ void k_advance(int64_t n, const double* __restrict__ x, double* __res
   }
 }
 
+// the same with a history of step increments in fixed buffers, shifted in place (newest
+// first): hist[k] = hist[k - 1] for k = H - 1 .. 1, hist[0] = x - u (graph-replayable)
+struct HistPtrs {
+  double* h[8];
+};
+__global__ void k_advance_hist(int64_t n, int H, const double* __restrict__ x,
+                               double* __restrict__ u, double* __restrict__ u_prev,
+                               HistPtrs hp) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const double xv = x[i], uv = u[i];
+    for (int k = H - 1; k >= 1; k--) hp.h[k][i] = hp.h[k - 1][i];
+    hp.h[0][i] = xv - uv;
+    u_prev[i] = uv;
+    u[i] = xv;
+  }
+}
+
 // (n, S) contiguous <-> (n, ld) interleaved with zero padding
 __global__ void k_pack(int64_t n, int S, int ld, const double* __restrict__ src,
                        double* __restrict__ dst) {
@@ -1083,6 +1101,21 @@ extern "C" int tp_advance_state(int64_t n, const double* x, double* u, double* u
   TP_REQUIRE(x && u && u_prev && d, "null pointer");
   if (n == 0) return TP_OK;
   k_advance<<<grid_for(n, 256, sm_count() * 8), 256, 0, as_stream(stream)>>>(n, x, u, u_prev, d);
+  TP_LAUNCH_CHECK();
+  return TP_OK;
+}
+
+extern "C" int tp_advance_history(int64_t n, const double* x, double* u, double* u_prev,
+                                  int n_hist, double* const* hist, void* stream) {
+  TP_REQUIRE(x && u && u_prev && hist && n_hist >= 1 && n_hist <= 8, "bad arguments");
+  HistPtrs hp{};
+  for (int k = 0; k < n_hist; k++) {
+    TP_REQUIRE(hist[k], "null history buffer");
+    hp.h[k] = hist[k];
+  }
+  if (n == 0) return TP_OK;
+  k_advance_hist<<<grid_for(n, 256, sm_count() * 8), 256, 0, as_stream(stream)>>>(
+      n, n_hist, x, u, u_prev, hp);
   TP_LAUNCH_CHECK();
   return TP_OK;
 }

@@ -130,6 +130,8 @@ SIGNATURES = {
                                      _vp]),
     "tp_mean_cell_diameter": (ctypes.c_int, [_P(TpMesh), _vp, _vp, _vp]),
     "tp_advance_state": (ctypes.c_int, [_c_i64, _vp, _vp, _vp, _vp, _vp]),
+    "tp_advance_history": (ctypes.c_int, [_c_i64, _vp, _vp, _vp, ctypes.c_int,
+                                          _P(ctypes.c_void_p), _vp]),
     "tp_axpby": (ctypes.c_int, [_c_i64, _c_dbl, _vp, _c_dbl, _vp, _vp]),
     "tp_pack_columns": (ctypes.c_int, [_c_i64, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
     "tp_unpack_columns": (ctypes.c_int, [_c_i64, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),

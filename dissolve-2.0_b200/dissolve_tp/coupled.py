@@ -58,6 +58,7 @@ class GyroidStep:
                                    inner_fp32=inner_fp32, guess=guess,
                                    alpha_cells=np.zeros((mesh.n_cells, 3)))
         tr = self.tr
+        tr.history_shift = True  # the step is meant to be captured in a CUDA graph
         dev = tr.device
         self.device = dev
         nv = tr.dm.n_verts

@@ -179,6 +179,9 @@ class BatchedTransport:
         # directions of the projected learned guess
         self.dU = [torch.zeros_like(self.U) for _ in range(5)]
         self.n_hist = 0
+        # False: the history rotates by pointer (cheapest); True: the buffers stay fixed and
+        # their contents shift (a captured CUDA graph of the step replays correctly)
+        self.history_shift = False
         # D_s K_xi alone (no diagonal): the stiffness images the learned guess reads
         self.stiff_op = CsrOperator(dm.indptr, dm.indices, self.K64, dscale=self.D, S=self.S,
                                     ld=self.ld)
@@ -287,10 +290,15 @@ class BatchedTransport:
     def advance_state(self):
         """After a solve: the increment x - U joins the history (newest first), then
         U_prev = U, U = x."""
-        d = self.dU.pop()
-        call("tp_advance_state", self.U.numel(), ptr(self.solver.x), ptr(self.U),
-             ptr(self.U_prev), ptr(d), stream_handle())
-        self.dU.insert(0, d)
+        if self.history_shift:
+            arr = (ctypes.c_void_p * len(self.dU))(*[ptr(d) for d in self.dU])
+            call("tp_advance_history", self.U.numel(), ptr(self.solver.x), ptr(self.U),
+                 ptr(self.U_prev), len(self.dU), arr, stream_handle())
+        else:
+            d = self.dU.pop()
+            call("tp_advance_state", self.U.numel(), ptr(self.solver.x), ptr(self.U),
+                 ptr(self.U_prev), ptr(d), stream_handle())
+            self.dU.insert(0, d)
         self.n_hist = min(self.n_hist + 1, len(self.dU))
         self.steps_done += 1
 

@@ -272,6 +272,10 @@ TP_API int tp_axpby(int64_t n, double a, const double* x, double b, double* y, v
  * increment for the projected guess and the state update; no reference counterpart) */
 TP_API int tp_advance_state(int64_t n, const double* x, double* u, double* u_prev, double* d,
                             void* stream);
+/* The same with n_hist (1..8) increment buffers shifted in place, newest first:
+ * hist[k] = hist[k-1], hist[0] = x - u (fixed pointers: replayable in a CUDA graph) */
+TP_API int tp_advance_history(int64_t n, const double* x, double* u, double* u_prev,
+                              int n_hist, double* const* hist, void* stream);
 
 /* (n, S) row-major columns -> (n, ld) interleaved, padding columns zero, and back.
  * Plumbing for host arrays of S species (no reference counterpart). */
