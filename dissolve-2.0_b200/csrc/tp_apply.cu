@@ -179,7 +179,7 @@ constexpr int GP_BLOCKS = 592;
 
 struct GuessDirs {
   const double* d[GP_MAXD];
-  const double* img0;  // D K d[0] precomputed (no Dirichlet rows), or NULL
+  const double* img[GP_MAXD];  // D K d[k] precomputed (no Dirichlet rows), or NULL
 };
 
 template <int M>
@@ -188,11 +188,12 @@ __host__ __device__ constexpr int gp_nq() {
 }
 constexpr int GP_SLOTS = gp_nq<GP_MAXD>() * 4;
 
-// A d_k for all M directions by one CSR walk per row: a group of LD lanes per row, lane s
-// reads column s of every gathered row (the group's loads are one contiguous run).  The
-// sums of lane s feed column s; one row of GP_SLOTS partials per block (slot q * 4 + s),
-// summed over the warps in a fixed order.
-template <int LD, int M>
+// A d_k for the first NG directions by one CSR walk per row (the others come with their
+// images d.img[k]): a group of LD lanes per row, lane s reads column s of every gathered
+// row (the group's loads are one contiguous run).  The sums of lane s feed column s; one
+// row of GP_SLOTS partials per block (slot q * 4 + s), summed over the warps in a fixed
+// order.
+template <int LD, int M, int NG>
 __global__ void __launch_bounds__(256) k_guess_dots(
     int64_t n, int S, const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
     const double* __restrict__ K, double4 dsc, const double* __restrict__ diag,
@@ -213,16 +214,16 @@ __global__ void __launch_bounds__(256) k_guess_dots(
   for (int64_t base = blockIdx.x * rpb; base < n; base += (int64_t)gridDim.x * rpb) {
     const int64_t row = base + threadIdx.x / LD;
     if (row >= n || s >= S || (bc && bc[row])) continue;
-    double kd[M];
+    double kd[NG > 0 ? NG : 1];
 #pragma unroll
-    for (int k = 0; k < M; k++) kd[k] = 0.0;
+    for (int k = 0; k < NG; k++) kd[k] = 0.0;
     const int beg = indptr[row], end = indptr[row + 1];
     // four entries at a time: their index, value and gathers in flight together; the
     // sums still run entry by entry in CSR order
     constexpr int RP = 4;
     for (int p0 = beg; p0 < end; p0 += RP) {
       int64_t jj[RP];
-      double kv[RP], dvv[RP][M];
+      double kv[RP], dvv[RP][NG > 0 ? NG : 1];
 #pragma unroll
       for (int u = 0; u < RP; u++) {
         const bool in = p0 + u < end;
@@ -233,13 +234,12 @@ __global__ void __launch_bounds__(256) k_guess_dots(
 #pragma unroll
       for (int u = 0; u < RP; u++)
 #pragma unroll
-        for (int k = 0; k < M; k++)
-          dvv[u][k] = (k == 0 && dirs.img0) ? 0.0 : __ldg(dirs.d[k] + jj[u]);
+        for (int k = 0; k < NG; k++) dvv[u][k] = __ldg(dirs.d[k] + jj[u]);
 #pragma unroll
       for (int u = 0; u < RP; u++) {
         if (p0 + u >= end) break;
 #pragma unroll
-        for (int k = 0; k < M; k++) kd[k] += kv[u] * dvv[u][k];
+        for (int k = 0; k < NG; k++) kd[k] += kv[u] * dvv[u][k];
       }
     }
     const int64_t i = row * LD + s;
@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(256) k_guess_dots(
 #pragma unroll
     for (int k = 0; k < M; k++) {
       dv[k] = dirs.d[k][i];
-      Ad[k] = ((k == 0 && dirs.img0) ? dirs.img0[i] : dsc_s * kd[k]) + dg * dv[k];
+      Ad[k] = (k < NG ? dsc_s * kd[k < NG ? k : 0] : dirs.img[k][i]) + dg * dv[k];
     }
     int q = 0;
 #pragma unroll
@@ -528,19 +528,37 @@ extern "C" size_t tp_guess_project_workspace_doubles(void) {
 
 extern "C" int tp_guess_project(const tp_csr_op* op, const double* diag, const uint8_t* bc_mask,
                                 const double* b, const double* U, const double* opU,
-                                int n_dirs, const double* const* dirs, const double* img0,
-                                double* x, double* work, void* stream) {
+                                int n_dirs, const double* const* dirs,
+                                const double* const* imgs, double* x, double* work,
+                                void* stream) {
   TP_REQUIRE(op && op->indptr && op->indices && op->K64 && diag && b && U && opU && x && work,
              "null pointer");
   TP_REQUIRE(op->ld == 1 || op->ld == 2 || op->ld == 4, "ld must be 1, 2 or 4");
   TP_REQUIRE(op->S >= 1 && op->S <= op->ld, "bad S");
   TP_REQUIRE(n_dirs >= 0 && n_dirs <= GP_MAXD && (n_dirs == 0 || dirs), "0 to 6 directions");
-  GuessDirs gd{};
-  for (int k = 0; k < n_dirs; k++) {
-    TP_REQUIRE(dirs[k], "null direction");
-    gd.d[k] = dirs[k];
+  for (int k = 0; k < n_dirs; k++) TP_REQUIRE(dirs[k], "null direction");
+  // directions without an image first (gathered), then those with one; other counts of
+  // gathered directions than 1, 2 or all gather everything
+  int ng = n_dirs;
+  bool split = false;
+  if (imgs && !bc_mask) {
+    int cnt = 0;
+    for (int k = 0; k < n_dirs; k++) cnt += imgs[k] ? 0 : 1;
+    split = (cnt == 1 || cnt == 2) && cnt < n_dirs;
+    if (split) ng = cnt;
   }
-  gd.img0 = bc_mask ? nullptr : img0;
+  GuessDirs gd{};
+  {
+    int q = 0;
+    for (int k = 0; k < n_dirs; k++)
+      if (!split || !imgs[k]) gd.d[q++] = dirs[k];
+    if (split)
+      for (int k = 0; k < n_dirs; k++)
+        if (imgs[k]) {
+          gd.img[q] = imgs[k];
+          gd.d[q++] = dirs[k];
+        }
+  }
   if (op->n_rows == 0) return TP_OK;
   cudaStream_t st = as_stream(stream);
   if (n_dirs == 0) {
@@ -556,8 +574,16 @@ extern "C" int tp_guess_project(const tp_csr_op* op, const double* diag, const u
 #define TP_GP(LDV, MV)                                                                       \
   do {                                                                                       \
     const int nb = (int)std::min<int64_t>(GP_BLOCKS / 2, (n + 256 / LDV - 1) / (256 / LDV)); \
-    k_guess_dots<LDV, MV><<<nb, 256, 0, st>>>(n, op->S, op->indptr, op->indices, op->K64,    \
-                                              dsc, diag, bc_mask, b, U, opU, gd, part);      \
+    if (ng == 1)                                                                             \
+      k_guess_dots<LDV, MV, (MV < 1 ? MV : 1)><<<nb, 256, 0, st>>>(                          \
+          n, op->S, op->indptr, op->indices, op->K64, dsc, diag, bc_mask, b, U, opU, gd, part); \
+    else if (ng == 2)                                                                        \
+      k_guess_dots<LDV, MV, (MV < 2 ? MV : 2)><<<nb, 256, 0, st>>>(                          \
+          n, op->S, op->indptr, op->indices, op->K64, dsc, diag, bc_mask, b, U, opU, gd, part); \
+    else                                                                                     \
+      k_guess_dots<LDV, MV, MV><<<nb, 256, 0, st>>>(n, op->S, op->indptr, op->indices,       \
+                                                    op->K64, dsc, diag, bc_mask, b, U, opU,  \
+                                                    gd, part);                               \
     k_guess_coeffs<MV><<<1, 1024, 0, st>>>(nb, op->S, part, coef);                           \
     k_guess_update<LDV, MV><<<grid_for(n * LDV, 256, sm_count() * 8), 256, 0, st>>>(         \
         n, op->S, coef, bc_mask, b, U, gd, x);                                               \

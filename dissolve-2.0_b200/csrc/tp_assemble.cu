@@ -648,6 +648,7 @@ __global__ void k_advance(int64_t n, const double* __restrict__ x, double* __res
 // first): hist[k] = hist[k - 1] for k = H - 1 .. 1, hist[0] = x - u (graph-replayable)
 struct HistPtrs {
   double* h[8];
+  double* g[8];  // optional second ring shifted alongside (slot 0 left as it is)
 };
 __global__ void k_advance_hist(int64_t n, int H, const double* __restrict__ x,
                                double* __restrict__ u, double* __restrict__ u_prev,
@@ -656,6 +657,8 @@ __global__ void k_advance_hist(int64_t n, int H, const double* __restrict__ x,
        i += (int64_t)gridDim.x * blockDim.x) {
     const double xv = x[i], uv = u[i];
     for (int k = H - 1; k >= 1; k--) hp.h[k][i] = hp.h[k - 1][i];
+    if (hp.g[0])
+      for (int k = H - 1; k >= 1; k--) hp.g[k][i] = hp.g[k - 1][i];
     hp.h[0][i] = xv - uv;
     u_prev[i] = uv;
     u[i] = xv;
@@ -1106,12 +1109,14 @@ extern "C" int tp_advance_state(int64_t n, const double* x, double* u, double* u
 }
 
 extern "C" int tp_advance_history(int64_t n, const double* x, double* u, double* u_prev,
-                                  int n_hist, double* const* hist, void* stream) {
+                                  int n_hist, double* const* hist, double* const* ring2,
+                                  void* stream) {
   TP_REQUIRE(x && u && u_prev && hist && n_hist >= 1 && n_hist <= 8, "bad arguments");
   HistPtrs hp{};
   for (int k = 0; k < n_hist; k++) {
-    TP_REQUIRE(hist[k], "null history buffer");
+    TP_REQUIRE(hist[k] && (!ring2 || ring2[k]), "null history buffer");
     hp.h[k] = hist[k];
+    hp.g[k] = ring2 ? ring2[k] : nullptr;
   }
   if (n == 0) return TP_OK;
   k_advance_hist<<<grid_for(n, 256, sm_count() * 8), 256, 0, as_stream(stream)>>>(

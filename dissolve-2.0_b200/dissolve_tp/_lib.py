@@ -131,7 +131,7 @@ SIGNATURES = {
     "tp_mean_cell_diameter": (ctypes.c_int, [_P(TpMesh), _vp, _vp, _vp]),
     "tp_advance_state": (ctypes.c_int, [_c_i64, _vp, _vp, _vp, _vp, _vp]),
     "tp_advance_history": (ctypes.c_int, [_c_i64, _vp, _vp, _vp, ctypes.c_int,
-                                          _P(ctypes.c_void_p), _vp]),
+                                          _P(ctypes.c_void_p), _P(ctypes.c_void_p), _vp]),
     "tp_axpby": (ctypes.c_int, [_c_i64, _c_dbl, _vp, _c_dbl, _vp, _vp]),
     "tp_pack_columns": (ctypes.c_int, [_c_i64, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
     "tp_unpack_columns": (ctypes.c_int, [_c_i64, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]),
@@ -142,7 +142,8 @@ SIGNATURES = {
     "tp_csr_images": (ctypes.c_int, [_P(TpCsrOp), _vp, _vp, _vp, _vp, _vp]),
     "tp_guess_project_workspace_doubles": (ctypes.c_size_t, []),
     "tp_guess_project": (ctypes.c_int, [_P(TpCsrOp), _vp, _vp, _vp, _vp, _vp, ctypes.c_int,
-                                        _P(ctypes.c_void_p), _vp, _vp, _vp, _vp]),
+                                        _P(ctypes.c_void_p), _P(ctypes.c_void_p), _vp, _vp,
+                                        _vp]),
     "tp_cg_workspace_bytes": (ctypes.c_size_t, [_P(TpCsrOp), _P(TpCgConfig)]),
     "tp_cg_create": (ctypes.c_int, [_P(TpCsrOp), _P(TpCgConfig), _vp, _vp, _vp, _vp,
                                     ctypes.c_size_t, _vp, _P(_vp)]),

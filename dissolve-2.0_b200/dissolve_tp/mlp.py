@@ -198,11 +198,14 @@ class WarmStartMLP:
                      ops=ops, base=2)
         nh = max(1, int(getattr(tr, "n_hist", 1)))
         dirs = [tr.dU[0], self._d] + list(tr.dU[1:nh])
+        # stiffness images known already: ops[1] for the newest increment, earlier steps'
+        # for the older ones (the network's direction is gathered)
+        imgs = [ops[1], None] + [tr.dimg[k] if tr.img_ok[k] else None for k in range(1, nh)]
         arr = (ctypes.c_void_p * len(dirs))(*[ptr(d) for d in dirs])
-        # ops[1] = D K (u^n - u^{n-1}) is the image of the first direction
+        iarr = (ctypes.c_void_p * len(dirs))(*[ptr(d) for d in imgs])
         call("tp_guess_project", ctypes.byref(tr.stiff_op.struct), ptr(tr.D64),
-             ptr(tr.bc_mask), ptr(tr.solver.b), ptr(tr.U), ptr(ops[0]), len(dirs), arr,
-             ptr(ops[1]), ptr(x), ptr(self._work), stream_handle())
+             ptr(tr.bc_mask), ptr(tr.solver.b), ptr(tr.U), ptr(ops[0]), len(dirs), arr, iarr,
+             ptr(x), ptr(self._work), stream_handle())
 
 
 def trajectory_pairs(tr, steps):

@@ -179,13 +179,17 @@ class BatchedTransport:
         # directions of the projected learned guess
         self.dU = [torch.zeros_like(self.U) for _ in range(5)]
         self.n_hist = 0
+        # their stiffness images D_s K dU[k] (written by operator_images when it images the
+        # newest increment; kept while the stiffness is unchanged), and which are current
+        self.dimg = [torch.zeros_like(self.U) for _ in range(5)]
+        self.img_ok = [False] * 5
+        self._opU = None
         # False: the history rotates by pointer (cheapest); True: the buffers stay fixed and
         # their contents shift (a captured CUDA graph of the step replays correctly)
         self.history_shift = False
         # D_s K_xi alone (no diagonal): the stiffness images the learned guess reads
         self.stiff_op = CsrOperator(dm.indptr, dm.indices, self.K64, dscale=self.D, S=self.S,
                                     ld=self.ld)
-        self._op_bufs = None
         self.guess = guess
         self.predictor = None
         self.steps_done = 0
@@ -238,16 +242,18 @@ class BatchedTransport:
 
     def operator_images(self, U=None, U_prev=None, fresh=False):
         """(D_s K U, D_s K (U - U_prev)) with the current stiffness, one launch
-        (tp_csr_images); defaults to the state.  Reuses two buffers unless fresh=True."""
+        (tp_csr_images).  Defaults to the state: then the second image is that of the newest
+        increment dU[0] and is kept in dimg[0].  fresh=True: new buffers."""
+        state = U is None and U_prev is None and not fresh
         U = self.U if U is None else U
         Up = self.U_prev if U_prev is None else U_prev
-        if fresh or self._op_bufs is None:
-            bufs = tuple(torch.empty_like(self.U) for _ in range(2))
-            if not fresh:
-                self._op_bufs = bufs
+        if state:
+            if self._opU is None:
+                self._opU = torch.empty_like(self.U)
+            opU, opDU = self._opU, self.dimg[0]
+            self.img_ok[0] = True
         else:
-            bufs = self._op_bufs
-        opU, opDU = bufs
+            opU, opDU = torch.empty_like(self.U), torch.empty_like(self.U)
         call("tp_csr_images", ctypes.byref(self.stiff_op.struct), ptr(U), ptr(Up), ptr(opU),
              ptr(opDU), stream_handle())
         return opU, opDU
@@ -259,6 +265,7 @@ class BatchedTransport:
         self.U_prev.copy_(self.U if U_prev is None else self._pad(U_prev))
         self.steps_done = 0 if U_prev is None else 1
         self.n_hist = 0
+        self.img_ok = [False] * len(self.dimg)
         if U_prev is not None:
             self.dU[0].copy_(self.U)
             self.dU[0].sub_(self.U_prev)
@@ -292,13 +299,16 @@ class BatchedTransport:
         U_prev = U, U = x."""
         if self.history_shift:
             arr = (ctypes.c_void_p * len(self.dU))(*[ptr(d) for d in self.dU])
+            arr2 = (ctypes.c_void_p * len(self.dimg))(*[ptr(d) for d in self.dimg])
             call("tp_advance_history", self.U.numel(), ptr(self.solver.x), ptr(self.U),
-                 ptr(self.U_prev), len(self.dU), arr, stream_handle())
+                 ptr(self.U_prev), len(self.dU), arr, arr2, stream_handle())
         else:
             d = self.dU.pop()
             call("tp_advance_state", self.U.numel(), ptr(self.solver.x), ptr(self.U),
                  ptr(self.U_prev), ptr(d), stream_handle())
             self.dU.insert(0, d)
+            self.dimg.insert(0, self.dimg.pop())
+        self.img_ok = [False] + self.img_ok[:-1]
         self.n_hist = min(self.n_hist + 1, len(self.dU))
         self.steps_done += 1
 

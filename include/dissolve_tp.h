@@ -273,9 +273,12 @@ TP_API int tp_axpby(int64_t n, double a, const double* x, double b, double* y, v
 TP_API int tp_advance_state(int64_t n, const double* x, double* u, double* u_prev, double* d,
                             void* stream);
 /* The same with n_hist (1..8) increment buffers shifted in place, newest first:
- * hist[k] = hist[k-1], hist[0] = x - u (fixed pointers: replayable in a CUDA graph) */
+ * hist[k] = hist[k-1], hist[0] = x - u (fixed pointers: replayable in a CUDA graph);
+ * ring2 (NULL or n_hist buffers, e.g. the increments' stiffness images) is shifted the
+ * same way with its slot 0 left unchanged */
 TP_API int tp_advance_history(int64_t n, const double* x, double* u, double* u_prev,
-                              int n_hist, double* const* hist, void* stream);
+                              int n_hist, double* const* hist, double* const* ring2,
+                              void* stream);
 
 /* (n, S) row-major columns -> (n, ld) interleaved, padding columns zero, and back.
  * Plumbing for host arrays of S species (no reference counterpart). */
@@ -340,13 +343,14 @@ TP_API int tp_csr_images(const tp_csr_op* op, const double* x1, const double* x2
  * h_k = d_k . (b - A U) over the free rows (directions taken as zero on Dirichlet rows;
  * a direction numerically in the span of the earlier ones gets c_k = 0): the minimum of
  * the A-norm of the error over U + span{d_k}, so never above U in that norm.
- * img0: D K dirs[0] when already computed (tp_csr_images' second output), else NULL; it
- * is used only without Dirichlet rows.  Deterministic.  work: device scratch of
+ * imgs: NULL, or n_dirs pointers with D K dirs[k] where already computed (tp_csr_images'
+ * second output, kept from earlier steps while K is unchanged) and NULL where the kernel
+ * gathers it; used only without Dirichlet rows.  Deterministic.  work: device scratch of
  * tp_guess_project_workspace_doubles() doubles. */
 TP_API size_t tp_guess_project_workspace_doubles(void);
 TP_API int tp_guess_project(const tp_csr_op* op, const double* diag, const uint8_t* bc_mask,
                             const double* b, const double* U, const double* opU, int n_dirs,
-                            const double* const* dirs, const double* img0, double* x,
+                            const double* const* dirs, const double* const* imgs, double* x,
                             double* work, void* stream);
 
 /* ------------------------------------------------------------------ Krylov solve */

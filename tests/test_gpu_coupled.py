@@ -133,5 +133,8 @@ def test_graph_replay_matches_eager_steps(cuda_device):
                 its.append(g.step()["iterations"])
         runs[mode] = (its, g.state())
     assert runs["graph"][0] == runs["eager"][0], runs
+    # the captured step keeps the set of directions whose stiffness images were known at
+    # capture (the eager steps gain more as they go): the guesses differ by rounding and
+    # both solves stop at rtol 1e-8
     a, b = runs["graph"][1], runs["eager"][1]
-    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-12
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-8

@@ -251,10 +251,12 @@ def test_guess_projection_matches_galerkin_solve(cuda_device, with_bc, n_dirs):
          stream_handle())
     assert torch.equal(x1, x2)
     if not with_bc:
-        # the first direction's image supplied precomputed: same guess to rounding
+        # every other direction's image supplied precomputed: same guess to rounding
         x3 = torch.zeros_like(x)
-        _, img = tr.operator_images(tr.U + dirs[0], tr.U, fresh=True)
+        imgs = [tr.operator_images(tr.U + d, tr.U, fresh=True)[1] for d in dirs]
+        iarr = (ctypes.c_void_p * n_dirs)(*[ptr(im) if k % 2 == 0 else None
+                                            for k, im in enumerate(imgs)])
         call("tp_guess_project", ctypes.byref(tr.stiff_op.struct), ptr(tr.D64), None,
-             ptr(tr.solver.b), ptr(tr.U), ptr(opU), n_dirs, arr, ptr(img), ptr(x3), ptr(work),
+             ptr(tr.solver.b), ptr(tr.U), ptr(opU), n_dirs, arr, iarr, ptr(x3), ptr(work),
              stream_handle())
         assert (x3 - x).abs().max().item() <= 1e-9 * x.abs().max().item()
