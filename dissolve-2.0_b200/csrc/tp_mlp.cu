@@ -11,9 +11,11 @@
 // B = u^n or the linear extrapolation 2 u^n - u^{n-1} (the network learns the correction
 // to the extrapolation: with zero output the guess is the extrapolation itself).
 //
-// Tensor-core fragments are those of mma.sync.m16n8k16 (row.col, bf16 x bf16 -> f32):
-// a warp owns 16 rows; layer outputs stay in registers and are re-packed from the
-// accumulator layout into the next layer's A layout.  Backward: the weight gradients
+// Inference (k_mlp_predict) runs layers 1 and 2 as tcgen05.mma on 128-row tiles with the
+// accumulators in tensor memory.  Training uses mma.sync.m16n8k16 fragments (row.col,
+// bf16 x bf16 -> f32): a warp owns 16 rows; layer outputs stay in registers and are
+// re-packed from the accumulator layout into the next layer's A layout.  Backward: the
+// weight gradients
 // are GEMMs over the row dimension (dW2 = dZ2^T H1, dW1 = dZ1^T X) fed from transposed
 // tiles staged in shared memory; every CTA writes its partial gradient, and the AdamW
 // kernel sums the partials in CTA order (training is deterministic for a given grid).
@@ -184,69 +186,238 @@ __device__ __forceinline__ void mlp_tile_forward(const MlpSmem& sm, const uint32
 }
 
 // ----------------------------------------------------------------- inference
-// x_out[v, s] = U[v, s] + sigma * y(v, s)  (or y_out[r] = y when x_out is NULL).
-// Persistent warps over 16-row tiles.  Every lane of a quad gathers all features of its
-// two rows (the quad's loads hit the same addresses) and keeps the four its A fragment
-// holds: no divergent per-feature branches.
-__global__ void __launch_bounds__(128, 6) k_mlp_predict(MlpFeat F, int64_t nrows,
-                                                     const float* __restrict__ P, float sigma,
-                                                     double* __restrict__ x_out,
-                                                     float* __restrict__ y_out) {
-  __shared__ MlpSmem sm;
-  load_weights(sm, P);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int g = lane >> 2, t = lane & 3;
-  const int64_t ntiles = (nrows + 15) / 16;
-  for (int64_t tile = (int64_t)blockIdx.x * 4 + warp; tile < ntiles;
-       tile += (int64_t)gridDim.x * 4) {
-    const int64_t r0 = tile * 16;
-    uint32_t xa[4];
-    int64_t vv[2];
-    int ss[2];
-    float fa[2][4];
+// 5th-generation tensor cores: 128-row tiles, one row per thread of a 128-thread CTA.
+// Layer 1 (128 x 64, K = 16) and layer 2 (128 x 64, K = 64 as four K = 16 steps) are
+// tcgen05.mma from shared-memory operands into tensor memory (z1 in columns 0..63, z2 in
+// columns 64..127 of a 128-column allocation), issued by one thread and completed through
+// an mbarrier (tcgen05.commit); every thread reads its own row back with tcgen05.ld (warp w
+// owns TMEM lanes 32w..32w+31).  Operands are K-major without swizzle: 8-row x 16-byte
+// core matrices, the two 8-element K halves 128 bytes apart, 8-row groups 256 bytes apart.
+// Every mbarrier wait is bounded; a wait that runs out sets g_mlp_tc_timeout, ends the
+// CTA's tiles and still releases its tensor memory.
+constexpr int TC_M = 128, TC_COLS = 128;
+constexpr uint32_t TC_WAIT_LIMIT = 1u << 24;  // polls of one mbarrier phase (~0.1 s)
+
+__device__ int g_mlp_tc_timeout;
+
+struct TcSmem {
+  __nv_bfloat16 A1[TC_M * 16];     // features of the tile, 4 KB
+  __nv_bfloat16 A2[4][TC_M * 16];  // h1 of the tile, one 4 KB block per K step
+  __nv_bfloat16 W1[MLP_H * 16];    // 2 KB
+  __nv_bfloat16 W2[4][MLP_H * 16]; // 8 KB
+  float b1[MLP_H], b2[MLP_H], w3[MLP_H];
+  float b3;
+  uint64_t bar;
+  uint32_t taddr;
+};
+
+// element offset of (row, k) in a K-major no-swizzle block of 16 K columns
+__device__ __forceinline__ int tc_off(int row, int k) {
+  return (row >> 3) * 128 + (k >> 3) * 64 + (row & 7) * 8 + (k & 7);
+}
+
+__device__ __forceinline__ uint64_t tc_desc(const void* smem) {
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(smem);
+  uint64_t d = (uint64_t)((a >> 4) & 0x3FFFu);  // start address
+  d |= (uint64_t)(128 >> 4) << 16;              // leading byte offset: the K halves
+  d |= (uint64_t)(256 >> 4) << 32;              // stride byte offset: 8-row groups
+  d |= (uint64_t)1 << 46;                       // descriptor version of sm_100
+  return d;                                     // base offset 0, no swizzle
+}
+
+// kind::f16 instruction descriptor: F32 accumulate, BF16 A and B (K-major), N = 64, M = 128
+constexpr uint32_t TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(MLP_H >> 3) << 17) |
+                              ((uint32_t)(TC_M >> 4) << 24);
+
+__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t a, uint64_t b, int accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(TC_IDESC), "r"(accumulate));
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+  const uint32_t ba = (uint32_t)__cvta_generic_to_shared(bar);
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(ba)
+               : "memory");
+}
+
+// bounded wait for the given phase of the mbarrier; false when the limit ran out
+__device__ __forceinline__ bool tc_wait(uint64_t* bar, uint32_t phase) {
+  const uint32_t ba = (uint32_t)__cvta_generic_to_shared(bar);
+  for (uint32_t it = 0; it < TC_WAIT_LIMIT; it++) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}"
+        : "=r"(done)
+        : "r"(ba), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void proxy_fence() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// 16 consecutive FP32 columns of this thread's TMEM lane
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float v[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
+      "%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-    for (int h = 0; h < 2; h++) {
-      const int64_t r = r0 + g + 8 * h;
-      const bool in = r < nrows;
-      // 32-bit division while the row index fits
-      const int64_t v = !in ? 0
-                            : (r < (int64_t)UINT32_MAX ? (int64_t)((uint32_t)r / (uint32_t)F.S)
-                                                       : r / F.S);
-      const int s = in ? (int)(r - v * F.S) : 0;
-      vv[h] = v;
-      ss[h] = s;
+  for (int k = 0; k < 16; k++) v[k] = __uint_as_float(r[k]);
+}
+
+// x_out[v, s] = B[v, s] + sigma * y(v, s)  (or y_out[r] = y when x_out is NULL).
+// Every thread gathers all features of its row (no divergent per-feature branches).
+__global__ void __launch_bounds__(TC_M) k_mlp_predict(MlpFeat F, int64_t nrows,
+                                                      const float* __restrict__ P, float sigma,
+                                                      double* __restrict__ x_out,
+                                                      float* __restrict__ y_out) {
+  __shared__ __align__(128) TcSmem sm;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  // weights in the operand layout (BF16), biases and w3 (w3 rounded to BF16 as in training)
+  for (int i = tid; i < MLP_H * 16; i += blockDim.x) {
+    const int n = i >> 4, k = i & 15;
+    sm.W1[tc_off(n, k)] = __float2bfloat16_rn(P[OFF_W1 + i]);
+  }
+  for (int i = tid; i < MLP_H * MLP_H; i += blockDim.x) {
+    const int n = i >> 6, k = i & 63;
+    sm.W2[k >> 4][tc_off(n, k & 15)] = __float2bfloat16_rn(P[OFF_W2 + i]);
+  }
+  for (int i = tid; i < MLP_H; i += blockDim.x) {
+    sm.b1[i] = P[OFF_B1 + i];
+    sm.b2[i] = P[OFF_B2 + i];
+    sm.w3[i] = __bfloat162float(__float2bfloat16_rn(P[OFF_W3 + i]));
+  }
+  if (tid == 0) sm.b3 = P[OFF_B3];
+  if (warp == 0) {
+    const uint32_t slot = (uint32_t)__cvta_generic_to_shared(&sm.taddr);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(slot),
+                 "r"(TC_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (tid == 0) {
+    const uint32_t ba = (uint32_t)__cvta_generic_to_shared(&sm.bar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(ba), "r"(1));
+  }
+  proxy_fence();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t taddr = sm.taddr;
+  const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+  uint32_t phase = 0;
+  const int64_t ntiles = (nrows + TC_M - 1) / TC_M;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t r = tile * TC_M + tid;
+    const bool in = r < nrows;
+    // 32-bit division while the row index fits
+    const int64_t v = !in ? 0
+                          : (r < (int64_t)UINT32_MAX ? (int64_t)((uint32_t)r / (uint32_t)F.S)
+                                                     : r / F.S);
+    const int s = in ? (int)(r - v * F.S) : 0;
+    {
       float f[NFEAT];
       row_features(F, v, s, f);
-      // this lane's features 2t, 2t+1, 2t+8, 2t+9 (10..15 are zero)
-      const float lo = (t == 0) ? f[0] : (t == 1) ? f[2] : (t == 2) ? f[4] : f[6];
-      const float hi = (t == 0) ? f[1] : (t == 1) ? f[3] : (t == 2) ? f[5] : f[7];
-      fa[h][0] = in ? lo : 0.f;
-      fa[h][1] = in ? hi : 0.f;
-      fa[h][2] = (in && t == 0) ? f[8] : 0.f;
-      fa[h][3] = (in && t == 0) ? f[9] : 0.f;
+      uint32_t w[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        const float lo = (in && 2 * k < NFEAT) ? f[2 * k] : 0.f;
+        const float hi = (in && 2 * k + 1 < NFEAT) ? f[2 * k + 1] : 0.f;
+        w[k] = pack_bf16(lo, hi);
+      }
+      *reinterpret_cast<uint4*>(&sm.A1[tc_off(tid, 0)]) = make_uint4(w[0], w[1], w[2], w[3]);
+      *reinterpret_cast<uint4*>(&sm.A1[tc_off(tid, 8)]) = make_uint4(w[4], w[5], w[6], w[7]);
     }
-    xa[0] = pack_bf16(fa[0][0], fa[0][1]);
-    xa[1] = pack_bf16(fa[1][0], fa[1][1]);
-    xa[2] = pack_bf16(fa[0][2], fa[0][3]);
-    xa[3] = pack_bf16(fa[1][2], fa[1][3]);
-    float z1[8][4], z2[8][4], y0, y1;
-    mlp_tile_forward(sm, xa, g, t, z1, z2, y0, y1);
-    // lane t < 2 of each quad writes row g + 8t
-    if (t < 2) {
-      const int h = t;
-      const int64_t r = r0 + g + 8 * h;
-      const float y = h ? y1 : y0;
-      if (r < nrows) {
-        if (x_out) {
-          const int64_t i = (h ? vv[1] : vv[0]) * F.ld + (h ? ss[1] : ss[0]);
-          const double b = F.base == 1 ? 2.0 * F.U[i] - F.Up[i] : (F.base == 0 ? F.U[i] : 0.0);
-          x_out[i] = b + (double)sigma * (double)y;
-        } else {
-          y_out[r] = y;
-        }
+    proxy_fence();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (tid == 0) {
+      tc_mma(taddr, tc_desc(sm.A1), tc_desc(sm.W1), 0);
+      tc_commit(&sm.bar);
+    }
+    bool ok = tc_wait(&sm.bar, phase);
+    phase ^= 1u;
+    tc_fence_after();
+    // h1 = relu(z1 + b1), BF16, into the layer-2 operand
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      float z[16];
+      tc_ld16(taddr + lane_base + 16 * j, z);
+      uint32_t w[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++)
+        w[k] = pack_bf16(fmaxf(z[2 * k] + sm.b1[16 * j + 2 * k], 0.f),
+                         fmaxf(z[2 * k + 1] + sm.b1[16 * j + 2 * k + 1], 0.f));
+      *reinterpret_cast<uint4*>(&sm.A2[j][tc_off(tid, 0)]) = make_uint4(w[0], w[1], w[2], w[3]);
+      *reinterpret_cast<uint4*>(&sm.A2[j][tc_off(tid, 8)]) = make_uint4(w[4], w[5], w[6], w[7]);
+    }
+    proxy_fence();
+    tc_fence_before();
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) atomicExch(&g_mlp_tc_timeout, 1);
+      break;
+    }
+    tc_fence_after();
+    if (tid == 0) {
+#pragma unroll
+      for (int j = 0; j < 4; j++) tc_mma(taddr + MLP_H, tc_desc(sm.A2[j]), tc_desc(sm.W2[j]), j > 0);
+      tc_commit(&sm.bar);
+    }
+    ok = tc_wait(&sm.bar, phase);
+    phase ^= 1u;
+    tc_fence_after();
+    // layer 3 on the CUDA cores: BF16-rounded h2 . w3 + b3
+    float y = 0.f;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      float z[16];
+      tc_ld16(taddr + lane_base + MLP_H + 16 * j, z);
+#pragma unroll
+      for (int k = 0; k < 16; k++)
+        y += __bfloat162float(__float2bfloat16_rn(fmaxf(z[k] + sm.b2[16 * j + k], 0.f))) *
+             sm.w3[16 * j + k];
+    }
+    y += sm.b3;
+    if (in && ok) {
+      if (x_out) {
+        const int64_t i = v * F.ld + s;
+        const double b = F.base == 1 ? 2.0 * F.U[i] - F.Up[i] : (F.base == 0 ? F.U[i] : 0.0);
+        x_out[i] = b + (double)sigma * (double)y;
+      } else {
+        y_out[r] = y;
       }
     }
+    // the tile's tensor-memory reads and operand reads are done before the next tile
+    tc_fence_before();
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) atomicExch(&g_mlp_tc_timeout, 1);
+      break;
+    }
   }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr),
+                 "r"(TC_COLS));
 }
 
 // features of every row, materialised (training set), BF16 (nrows, 16): one thread per
@@ -560,12 +731,21 @@ extern "C" int tp_mlp_predict(const tp_mlp_inputs* in, const float* params, floa
   TP_REQUIRE(in->base >= 0 && in->base <= 2, "base must be 0 (u^n), 1 (2 u^n - u^{n-1}) or 2 (none)");
   const int64_t nrows = in->n_verts * in->S;
   if (nrows == 0) return TP_OK;
-  const int64_t ntiles = (nrows + 15) / 16;
-  // one wave: 6 CTAs of 4 warps per SM
-  const int grid = (int)std::min<int64_t>((ntiles + 3) / 4, (int64_t)sm_count() * 6);
-  k_mlp_predict<<<grid, 128, 0, as_stream(stream)>>>(make_feat(in), nrows, params, sigma, x_out,
-                                                      y_out);
+  const int64_t ntiles = (nrows + TC_M - 1) / TC_M;
+  // persistent CTAs, 4 per SM (4 x 128 tensor-memory columns = the SM's 512)
+  const int grid = (int)std::min<int64_t>(ntiles, (int64_t)sm_count() * 4);
+  k_mlp_predict<<<grid, TC_M, 0, as_stream(stream)>>>(make_feat(in), nrows, params, sigma, x_out,
+                                                       y_out);
   TP_LAUNCH_CHECK();
+  return TP_OK;
+}
+
+extern "C" int tp_mlp_tensor_status(int* timed_out, void* stream) {
+  TP_REQUIRE(timed_out, "null pointer");
+  cudaStream_t st = as_stream(stream);
+  TP_CUDA_TRY(cudaMemcpyFromSymbolAsync(timed_out, g_mlp_tc_timeout, sizeof(int), 0,
+                                        cudaMemcpyDeviceToHost, st));
+  TP_CUDA_TRY(cudaStreamSynchronize(st));
   return TP_OK;
 }
 

@@ -164,6 +164,7 @@ SIGNATURES = {
     "tp_pcg_set_profile": (ctypes.c_int, [_vp, _vp]),
     "tp_pcg_destroy": (ctypes.c_int, [_vp]),
     "tp_mlp_param_count": (ctypes.c_int, []),
+    "tp_mlp_tensor_status": (ctypes.c_int, [_P(ctypes.c_int), _vp]),
     "tp_mlp_predict": (ctypes.c_int, [_P(TpMlpInputs), _vp, ctypes.c_float, _vp, _vp, _vp]),
     "tp_mlp_features": (ctypes.c_int, [_P(TpMlpInputs), _vp, _vp]),
     "tp_mlp_target": (ctypes.c_int, [_c_i64, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _c_dbl,

@@ -502,6 +502,9 @@ TP_API int tp_mlp_param_count(void);
  * y_out[v * S + s] = y when x_out is NULL */
 TP_API int tp_mlp_predict(const tp_mlp_inputs* in, const float* params, float sigma,
                           double* x_out, float* y_out, void* stream);
+/* [sync] *timed_out = 1 if an inference launch of this library gave up waiting for its
+ * tensor-core operations (bounded waits; its rows were then not written), else 0 */
+TP_API int tp_mlp_tensor_status(int* timed_out, void* stream);
 /* the normalised inputs as BF16 rows of 16 (training set) */
 TP_API int tp_mlp_features(const tp_mlp_inputs* in, void* X_bf16, void* stream);
 /* training target (U_next - B) / sigma per row, B = U_n (U_prev NULL) or

@@ -131,6 +131,13 @@ def test_gpu_forward_from_fields_matches_oracle(cuda_device, base):
     b = 2.0 * U - Up if base == "extrapolate" else U
     xo = b + m.sigma * yo.reshape(V, S)
     assert np.abs(x[:, :S].cpu().numpy() - xo).max() <= 2e-3 * m.sigma * np.abs(yo).max() + 1e-12
+    # the tensor-core inference never gave up waiting
+    import ctypes
+
+    from dissolve_tp import _lib
+    flag = ctypes.c_int(-1)
+    _lib.call("tp_mlp_tensor_status", ctypes.byref(flag), None)
+    assert flag.value == 0
     # training target: (u^{n+1} - base) / sigma, rounded to FP32
     Un1 = U + rng.normal(0, 0.02, (V, S))
     Un1d = torch.zeros_like(Ud)
