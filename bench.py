@@ -142,6 +142,12 @@ def run_ours(args, rank, world, local_rank):
     def flush():
         flush_buf.zero_()
 
+    if args.kernels_only:
+        if rank == 0:
+            print(json.dumps({"workload": WORKLOAD, "kernels": kernel_table(m, coef, u0, flush)}),
+                  flush=True)
+        return
+
     def barrier():
         if world > 1:
             dist.barrier()
@@ -618,6 +624,8 @@ def main():
                     help="skip the assembly / RHS / apply bandwidth table")
     ap.add_argument("--no-configs", dest="configs", action="store_false",
                     help="skip the multi-mesh batch and gyroid coupled-step workloads")
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="print only the assembly / RHS / apply bandwidth table (no step)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

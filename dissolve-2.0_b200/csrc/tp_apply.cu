@@ -8,23 +8,47 @@
 // with scale = De/(6|det J|) (exact P1 stiffness) or 4 De/det^2 (legacy: the reference
 // QFunction drops wdetJ), and consistent (|det|/120 (1+d_ij)) or lumped (|det|/24) mass.
 // Contributions land with hardware atomics (FP32 columns as one 16-byte vector atomic),
-// so the result's last bits depend on arrival order, as in the reference.
+// so the result's last bits depend on arrival order, as in the reference.  A warp takes
+// 32 consecutive cells.  Scalar atomics (FP64, FP32 rows narrower than 16 bytes) are
+// grouped: for each local vertex slot, a run of consecutive lanes whose cells have the
+// same vertex in that slot sums its contributions through shared memory and the run's
+// first lane issues the atomics.  The six cells of a Kuhn cube share their first and last
+// vertex (runs of six) and pairs of them their second (runs of two): 11 atomics per cube
+// instead of 24; on any other ordering the runs are single lanes.  A 16-byte FP32 row
+// goes out as one vector atomic per lane, where the grouping does not pay.
 #include "tp_ops.cuh"
 
 namespace tp {
 
-template <typename T, int LD>
-__global__ void __launch_bounds__(256) k_matfree(
+// CS columns of LD are used (compile time, so the column loops carry no predicates).
+template <typename T, int LD, int CS>
+__global__ void __launch_bounds__(256, sizeof(T) == 8 ? 3 : 4) k_matfree(
     int64_t n, const int4* __restrict__ cells, const double4* __restrict__ X,
     const double* __restrict__ De, const double* __restrict__ alpha, double4 dsc, double4 shf,
-    double inv_dt, int S, int lumped, int legacy, const T* __restrict__ x, T* __restrict__ y) {
+    double inv_dt, int lumped, int legacy, const T* __restrict__ x, T* __restrict__ y) {
+  constexpr bool VEC = sizeof(T) == 4 && LD == 4;  // one 16-byte vector atomic per row
+  constexpr int WPB = 256 / 32;
+  __shared__ T s_val[VEC ? 1 : WPB][32][CS];  // one contribution per lane, for the run head
   const double dscale[4] = {dsc.x, dsc.y, dsc.z, dsc.w};
   const double shift[4] = {shf.x, shf.y, shf.z, shf.w};
-  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
-       c += (int64_t)gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int64_t wstride = (int64_t)gridDim.x * WPB * 32;
+  // the loop trip count is uniform over the warp: lanes past n compute a copy of the
+  // last cell and add nothing
+  for (int64_t base = ((int64_t)blockIdx.x * WPB + wib) * 32; base < n; base += wstride) {
+    const int64_t c0 = base + lane;
+    const bool valid = c0 < n;
+    const int64_t c = valid ? c0 : n - 1;
     const int4 v = cells[c];
     const double4 x0 = ldg_d4(X + v.x), x1 = ldg_d4(X + v.y), x2 = ldg_d4(X + v.z),
                   x3 = ldg_d4(X + v.w);
+    T xv[4][LD];
+    ldv<T, LD>(x, v.x, xv[0]);
+    ldv<T, LD>(x, v.y, xv[1]);
+    ldv<T, LD>(x, v.z, xv[2]);
+    ldv<T, LD>(x, v.w, xv[3]);
+    const double De_c = De[c];
+    const double al = alpha ? alpha[c] : 0.0;
     const double e[3][3] = {{x1.x - x0.x, x1.y - x0.y, x1.z - x0.z},
                             {x2.x - x0.x, x2.y - x0.y, x2.z - x0.z},
                             {x3.x - x0.x, x3.y - x0.y, x3.z - x0.z}};
@@ -40,28 +64,17 @@ __global__ void __launch_bounds__(256) k_matfree(
     cr[2][2] = e[0][0] * e[1][1] - e[0][1] * e[1][0];
     const double det = e[0][0] * cr[0][0] + e[0][1] * cr[0][1] + e[0][2] * cr[0][2];
     const double adet = fabs(det);
-    const double De_c = De[c];
-    const double kbase = legacy ? 4.0 * De_c / (det * det) : De_c / (6.0 * adet);
-    const double mbase = lumped ? adet / 24.0 : adet / 120.0;
-    const double al = alpha ? alpha[c] : 0.0;
+    // one division: De/(6|det|), or 4 De/det^2 for the legacy QFunction
+    const double kbase = legacy ? (4.0 * De_c) / (det * det) : De_c / (6.0 * adet);
+    const double mbase = adet * (lumped ? 1.0 / 24.0 : 1.0 / 120.0);
     T c_[3][3];
 #pragma unroll
     for (int a = 0; a < 3; a++)
 #pragma unroll
       for (int b = 0; b < 3; b++) c_[a][b] = (T)cr[a][b];
-    T xv[4][LD];
-    ldv<T, LD>(x, v.x, xv[0]);
-    ldv<T, LD>(x, v.y, xv[1]);
-    ldv<T, LD>(x, v.z, xv[2]);
-    ldv<T, LD>(x, v.w, xv[3]);
-    T out[4][LD];
+    T out[4][CS];
 #pragma unroll
-    for (int s = 0; s < LD; s++) {
-      if (s >= S) {
-#pragma unroll
-        for (int i = 0; i < 4; i++) out[i][s] = T(0);
-        continue;
-      }
+    for (int s = 0; s < CS; s++) {
       const T ks = (T)(kbase * dscale[s]);
       const T ms = (T)(mbase * (inv_dt + al + shift[s]));
       const T d1 = xv[1][s] - xv[0][s], d2 = xv[2][s] - xv[0][s], d3 = xv[3][s] - xv[0][s];
@@ -86,14 +99,40 @@ __global__ void __launch_bounds__(256) k_matfree(
 #pragma unroll
     for (int i = 0; i < 4; i++) {
       T* dst = y + (int64_t)vid[i] * LD;
-      if constexpr (sizeof(T) == 4 && LD == 4) {
-        atomicAdd(reinterpret_cast<float4*>(dst),
-                  make_float4(out[i][0], out[i][1], out[i][2], out[i][3]));
-      } else {
-#pragma unroll
-        for (int s = 0; s < LD; s++)
-          if (s < S) atomicAdd(dst + s, out[i][s]);
+      if constexpr (VEC) {
+        if (valid) {
+          float4 o;
+          o.x = out[i][0];
+          o.y = CS > 1 ? out[i][CS > 1 ? 1 : 0] : 0.f;
+          o.z = CS > 2 ? out[i][CS > 2 ? 2 : 0] : 0.f;
+          o.w = CS > 3 ? out[i][CS > 3 ? 3 : 0] : 0.f;
+          atomicAdd(reinterpret_cast<float4*>(dst), o);
+        }
+        continue;
       }
+      // vertex ids are >= 0, so the keys of lanes past n are unique (runs of one)
+      const int key = valid ? vid[i] : -1 - lane;
+      const int prev = __shfl_up_sync(0xffffffffu, key, 1);
+      const bool head = lane == 0 || prev != key;
+      const unsigned above = (__ballot_sync(0xffffffffu, head) >> lane) >> 1;
+      const int end = above ? lane + __ffs(above) : 32;  // run = lanes [lane, end)
+      if (!head) {
+#pragma unroll
+        for (int s = 0; s < CS; s++) s_val[wib][lane][s] = out[i][s];
+      }
+      __syncwarp();
+      if (head && valid) {
+        T acc[CS];
+#pragma unroll
+        for (int s = 0; s < CS; s++) acc[s] = out[i][s];
+        for (int l = lane + 1; l < end; l++) {
+#pragma unroll
+          for (int s = 0; s < CS; s++) acc[s] += s_val[wib][l][s];
+        }
+#pragma unroll
+        for (int s = 0; s < CS; s++) atomicAdd(dst + s, acc[s]);
+      }
+      __syncwarp();
     }
   }
 }
@@ -388,32 +427,37 @@ __global__ void k_guess_update(int64_t n, int S, const double* __restrict__ coef
   }
 }
 
+template <typename T, int LD, int CS>
+static void launch_matfree_cs(const tp_mesh* m, const double* De, const double* al, double4 dsc,
+                              double4 shf, double inv_dt, int lumped, int legacy, const void* x,
+                              void* y, cudaStream_t st) {
+  const int grid = grid_for(m->n_cells, 256, sm_count() * 8);
+  k_matfree<T, LD, CS><<<grid, 256, 0, st>>>(
+      m->n_cells, reinterpret_cast<const int4*>(m->cells),
+      reinterpret_cast<const double4*>(m->coords4), De, al, dsc, shf, inv_dt, lumped, legacy,
+      static_cast<const T*>(x), static_cast<T*>(y));
+}
+
 template <typename T>
 static int launch_matfree(const tp_mesh* m, int S, int ld, const double* De, const double* al,
                           double4 dsc, double4 shf, double inv_dt, int lumped, int legacy,
                           const void* x, void* y, cudaStream_t st) {
-  const int grid = grid_for(m->n_cells, 256, sm_count() * 8);
-  const int4* cells = reinterpret_cast<const int4*>(m->cells);
-  const double4* X = reinterpret_cast<const double4*>(m->coords4);
-  const T* xx = static_cast<const T*>(x);
-  T* yy = static_cast<T*>(y);
-  switch (ld) {
-    case 1:
-      k_matfree<T, 1><<<grid, 256, 0, st>>>(m->n_cells, cells, X, De, al, dsc, shf, inv_dt, S,
-                                            lumped, legacy, xx, yy);
-      break;
-    case 2:
-      k_matfree<T, 2><<<grid, 256, 0, st>>>(m->n_cells, cells, X, De, al, dsc, shf, inv_dt, S,
-                                            lumped, legacy, xx, yy);
-      break;
-    case 4:
-      k_matfree<T, 4><<<grid, 256, 0, st>>>(m->n_cells, cells, X, De, al, dsc, shf, inv_dt, S,
-                                            lumped, legacy, xx, yy);
-      break;
-    default:
-      set_error("ld must be 1, 2 or 4");
-      return TP_ERR_ARG;
+#define TP_MF(LD_, CS_) \
+  launch_matfree_cs<T, LD_, CS_>(m, De, al, dsc, shf, inv_dt, lumped, legacy, x, y, st)
+  if (ld == 1) {
+    TP_MF(1, 1);
+  } else if (ld == 2) {
+    if (S == 1) TP_MF(2, 1); else TP_MF(2, 2);
+  } else if (ld == 4) {
+    if (S == 1) TP_MF(4, 1);
+    else if (S == 2) TP_MF(4, 2);
+    else if (S == 3) TP_MF(4, 3);
+    else TP_MF(4, 4);
+  } else {
+    set_error("ld must be 1, 2 or 4");
+    return TP_ERR_ARG;
   }
+#undef TP_MF
   TP_LAUNCH_CHECK();
   return TP_OK;
 }
@@ -459,6 +503,7 @@ extern "C" int tp_matfree_apply(const tp_mesh* m, int S, int ld, int fp32, const
                                 const double* shift, double inv_dt, int lumped, int legacy,
                                 const void* x, void* y, void* stream) {
   TP_REQUIRE(m && m->cells && m->coords4 && De_cell && x && y, "null pointer");
+  TP_REQUIRE((reinterpret_cast<uintptr_t>(m->coords4) & 31) == 0, "coords4 not 32-byte aligned");
   TP_REQUIRE(S >= 1 && S <= TP_MAX_COLS && (ld == 1 || ld == 2 || ld == 4) && ld >= S,
              "bad S/ld");
   cudaStream_t st = as_stream(stream);

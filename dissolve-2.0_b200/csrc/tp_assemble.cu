@@ -69,7 +69,12 @@ __global__ void __launch_bounds__(128) k_assemble_rows(
     const int32_t* __restrict__ indices, double* __restrict__ out64,
     float* __restrict__ out32, RowExtras ex) {
   constexpr int B = 128;
-  extern __shared__ double acc[];  // [max_row_len][B]
+  // [max_row_len][B + 1]: the odd row stride puts consecutive slots of one row in
+  // different banks (the write-back reads them with consecutive lanes); the walk's
+  // accesses (one row per lane, the same slot on every lane of a structured mesh) stay
+  // conflict-free
+  constexpr int BS = B + 1;
+  extern __shared__ double acc[];
   __shared__ int32_t s_ptr[B + 1];
   const int tid = threadIdx.x;
   const int64_t r0 = (int64_t)blockIdx.x * B;
@@ -81,7 +86,7 @@ __global__ void __launch_bounds__(128) k_assemble_rows(
   if (tid == 0) s_ptr[nrows] = indptr[rend];
   __syncthreads();
   const int len = valid ? s_ptr[tid + 1] - s_ptr[tid] : 0;
-  for (int s = 0; s < len; s++) acc[s * B + tid] = 0.0;
+  for (int s = 0; s < len; s++) acc[s * BS + tid] = 0.0;
   const bool is_bc = valid && bc_mask && bc_mask[r];
   double dacc[4] = {0.0, 0.0, 0.0, 0.0};
   const double dsh[4] = {ex.shift.x, ex.shift.y, ex.shift.z, ex.shift.w};
@@ -142,7 +147,7 @@ __global__ void __launch_bounds__(128) k_assemble_rows(
             a = (MODE == TP_ASM_FULL) ? __dadd_rn(a, __dmul_rn(react, M)) : M;
           }
           const int slot = (sv[u] >> (8 * j)) & 0xff;
-          if (slot < len) acc[slot * B + tid] = __dadd_rn(acc[slot * B + tid], a);
+          if (slot < len) acc[slot * BS + tid] = __dadd_rn(acc[slot * BS + tid], a);
         }
       }
     }
@@ -171,7 +176,7 @@ __global__ void __launch_bounds__(128) k_assemble_rows(
         hi = mid;
     }
     const int slot = p - s_ptr[lo];
-    double v = acc[slot * B + lo];
+    double v = acc[slot * BS + lo];
     if (bc_mask && bc_mask[r0 + lo]) v = (indices[p] == r0 + lo) ? 1.0 : 0.0;
     if (out64) out64[p] = v;
     if (out32) out32[p] = (float)v;
@@ -708,8 +713,11 @@ extern "C" int tp_unpack_columns(int64_t n, int S, int ld, const double* src, do
   return TP_OK;
 }
 
+// geo and coords4 rows are read with 32-byte loads
 static bool mesh_ok(const tp_mesh* m) {
-  return m && m->cells && m->geo && m->v2c_ptr && m->v2c && m->indptr;
+  return m && m->cells && m->geo && m->v2c_ptr && m->v2c && m->indptr &&
+         (reinterpret_cast<uintptr_t>(m->geo) & 31) == 0 &&
+         (reinterpret_cast<uintptr_t>(m->coords4) & 31) == 0;
 }
 
 extern "C" int tp_cell_average(int64_t n_cells, const int32_t* cells, const double* vert_vals,
@@ -751,7 +759,7 @@ extern "C" int tp_assemble_csr(const tp_mesh* m, const double* De_cell, const do
   TP_REQUIRE(m->max_row_len >= 1 && m->max_row_len <= 255, "bad max_row_len");
   if (m->n_verts == 0) return TP_OK;
   cudaStream_t st = as_stream(stream);
-  const size_t smem = sizeof(double) * 128 * (size_t)m->max_row_len;
+  const size_t smem = sizeof(double) * 129 * (size_t)m->max_row_len;
   const int grid = grid_for(m->n_verts, 128);
   const RowExtras ex{};
 #define TP_ASM_LAUNCH(MD)                                                                 \
@@ -827,7 +835,7 @@ extern "C" int tp_assemble_stiffness_diag(const tp_mesh* m, const double* De_cel
   for (int s = 0; s < S; s++) sh[s] = shift ? shift[s] : 0.0;
   RowExtras ex{S, ld, alpha, make_double4(sh[0], sh[1], sh[2], sh[3]), diag64, diag32,
                csr2sell, sell32};
-  const size_t smem = sizeof(double) * 128 * (size_t)m->max_row_len;
+  const size_t smem = sizeof(double) * 129 * (size_t)m->max_row_len;
   const int grid = grid_for(m->n_verts, 128);
   if (smem > 48 * 1024)
     TP_CUDA_TRY(cudaFuncSetAttribute(k_assemble_rows<TP_ASM_STIFF, true>,

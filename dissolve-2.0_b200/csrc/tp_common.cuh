@@ -82,10 +82,14 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
 }
 
 // 32-byte read-only load as two 128-bit loads
+// One 256-bit read-only load (sm_100): p must be 32-byte aligned (coords4 and geo rows;
+// the entry points that read them check the base pointers).
 __device__ __forceinline__ double4 ldg_d4(const double4* p) {
-  const double2* q = reinterpret_cast<const double2*>(p);
-  const double2 a = __ldg(q), b = __ldg(q + 1);
-  return make_double4(a.x, a.y, b.x, b.y);
+  double4 v;
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+      : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w)
+      : "l"(p));
+  return v;
 }
 
 template <typename T>

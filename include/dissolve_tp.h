@@ -67,8 +67,8 @@ typedef struct tp_mesh {
   int32_t max_row_len;        /* longest CSR row (<= 255)                            */
   int32_t max_degree;         /* most cells sharing one vertex                       */
   const int32_t* cells;       /* (n_cells, 4) vertex ids = P1 dofs                   */
-  const double* coords4;      /* (n_verts, 4) x, y, z, 0 (32-byte rows)              */
-  const double* geo;          /* (n_cells, 8) G00 G01 G02 G11 G12 G22 |detJ| 0       */
+  const double* coords4;      /* (n_verts, 4) x, y, z, 0 (32-byte rows, 32-byte base) */
+  const double* geo;          /* (n_cells, 8) G00 G01 G02 G11 G12 G22 |detJ| 0, 32-byte base */
   const int32_t* v2c_ptr;     /* (n_verts + 1) incidence offsets                     */
   const int32_t* v2c;         /* (4 n_cells) cell*4 + local index, ascending cell    */
   const uint32_t* v2c_slots;  /* (4 n_cells) row-local CSR slot of the cell's 4 vertices,
