@@ -1045,6 +1045,10 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
           if (sl < se) {
             const int base = s_sp[sl - sb], w = (s_sp[sl - sb + 1] - base) >> 5;
             const int lb = base - e0;
+            // wider FP32 rows without a mass matrix: the slice's diagonal is issued before
+            // its gathers, which hide the load (the other forms have no registers left)
+            constexpr bool DEARLY = !DPRE && !HASM && sizeof(VT) == 4;
+            if constexpr (DEARLY) load_diag(j);
             VT ak[LD], am[LD];
 #pragma unroll
             for (int s = 0; s < LD; s++) ak[s] = am[s] = VT(0);
@@ -1060,7 +1064,7 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
                 }
               }
             }
-            if constexpr (!DPRE) load_diag(j);
+            if constexpr (!DPRE && !DEARLY) load_diag(j);
             row_done(sl, ak, am, dgs[j]);
           }
         }
