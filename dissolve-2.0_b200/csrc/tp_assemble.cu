@@ -47,14 +47,14 @@ __device__ __forceinline__ void kref_row(int li, const GeoRec& g, double k[4]) {
 
 // ----------------------------------------------------------------- CSR assembly
 // Optional extras of the same row walk (the stiffness of the batched step): the per-column
-// lumped diagonal of tp_lumped_diag, and the FP32 values in SELL order for the solver.
+// lumped diagonal of tp_lumped_diag, and the FP32 values in SELL-32 order for the solver.
 struct RowExtras {
   int S, ld;
   const double* alpha;  // (n_cells, ld) or NULL
   double4 shift;
   double* d64;
   float* d32;
-  const int32_t* csr2sell;  // with sell32: SELL position of every CSR entry
+  const int32_t* slice_ptr;  // with sell32: SELL-32 slice offsets (rows in CSR order)
   float* sell32;
 };
 
@@ -180,7 +180,29 @@ __global__ void __launch_bounds__(128) k_assemble_rows(
     if (bc_mask && bc_mask[r0 + lo]) v = (indices[p] == r0 + lo) ? 1.0 : 0.0;
     if (out64) out64[p] = v;
     if (out32) out32[p] = (float)v;
-    if (ex.sell32) ex.sell32[ex.csr2sell[p]] = (float)v;
+  }
+  if (ex.sell32) {
+    // SELL-32: the block's 128 rows are four whole slices; warp w writes slice r0/32 + w,
+    // entry k of its lane's row at slice_ptr[slice] + 32 k + lane (padding entries 0), so
+    // every store is one coalesced 128-byte line
+    const int wsl = tid >> 5, ln = tid & 31;
+    if (r0 + wsl * 32 < nv) {
+      const int64_t sl = (r0 >> 5) + wsl;
+      const int base = ex.slice_ptr[sl], width = (ex.slice_ptr[sl + 1] - base) >> 5;
+      const int lr = wsl * 32 + ln;
+      const bool rv = lr < nrows;
+      const int rlen = rv ? s_ptr[lr + 1] - s_ptr[lr] : 0;
+      const bool rbc = rv && bc_mask && bc_mask[r0 + lr];
+      for (int k = 0; k < width; k++) {
+        float f = 0.f;
+        if (k < rlen) {
+          double v = acc[k * BS + lr];
+          if (rbc) v = (indices[s_ptr[lr] + k] == r0 + lr) ? 1.0 : 0.0;
+          f = (float)v;
+        }
+        ex.sell32[base + k * 32 + ln] = f;
+      }
+    }
   }
 }
 
@@ -821,20 +843,20 @@ extern "C" int tp_lumped_diag(const tp_mesh* m, int S, int ld, const double* alp
 extern "C" int tp_assemble_stiffness_diag(const tp_mesh* m, const double* De_cell, int S,
                                           int ld, const double* alpha, const double* shift,
                                           const uint8_t* bc_mask, double* out64, float* out32,
-                                          const int32_t* csr2sell, float* sell32,
+                                          const int32_t* slice_ptr, float* sell32,
                                           double* diag64, float* diag32, void* stream) {
   TP_REQUIRE(mesh_ok(m) && m->v2c_slots && m->indices && De_cell, "incomplete mesh or De");
   TP_REQUIRE(S >= 1 && S <= TP_MAX_COLS && ld >= S && ld <= TP_MAX_COLS, "bad S/ld");
   TP_REQUIRE(out64 || out32 || sell32, "no operator output");
   TP_REQUIRE(diag64 || diag32, "no diagonal output");
-  TP_REQUIRE(!sell32 || csr2sell, "sell32 needs csr2sell");
+  TP_REQUIRE(!sell32 || slice_ptr, "sell32 needs slice_ptr");
   TP_REQUIRE(m->max_row_len >= 1 && m->max_row_len <= 255, "bad max_row_len");
   if (m->n_verts == 0) return TP_OK;
   cudaStream_t st = as_stream(stream);
   double sh[4] = {0, 0, 0, 0};
   for (int s = 0; s < S; s++) sh[s] = shift ? shift[s] : 0.0;
   RowExtras ex{S, ld, alpha, make_double4(sh[0], sh[1], sh[2], sh[3]), diag64, diag32,
-               csr2sell, sell32};
+               slice_ptr, sell32};
   const size_t smem = sizeof(double) * 129 * (size_t)m->max_row_len;
   const int grid = grid_for(m->n_verts, 128);
   if (smem > 48 * 1024)

@@ -204,7 +204,7 @@ class BatchedTransport:
                   and sol.sM is None)
         call("tp_assemble_stiffness_diag", ctypes.byref(self.dm.tpm), ptr(self.coef), self.S,
              self.ld, ptr(self.alpha), self._shift(), ptr(self.bc_mask), ptr(self.K64),
-             ptr(self.K32), ptr(sol.sell.csr2sell) if direct else None,
+             ptr(self.K32), ptr(sol.sell.slice_ptr) if direct else None,
              ptr(sol.sK) if direct else None, ptr(self.D64), ptr(self.D32), stream_handle())
         self._sell_fresh = direct
 

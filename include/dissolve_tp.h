@@ -152,12 +152,13 @@ TP_API int tp_lumped_diag(const tp_mesh* m, int S, int ld, const double* alpha, 
  * walk (no reference counterpart as one call: gpu_assembler.py:60-139 in TP_ASM_STIFF mode
  * plus tp_lumped_diag): out64 / out32 (CSR order) as tp_assemble_csr(mode TP_ASM_STIFF,
  * lumped) and diag64 / diag32 as tp_lumped_diag, both bit-identical to those calls;
- * optionally sell32[csr2sell[p]] = (float) value p (the FP32 SELL values of tp_sell_build's
- * csr2sell map, as tp_sell_scatter writes them). */
+ * optionally the FP32 values in the SELL-32 order of tp_sell_build (slice_ptr: its slice
+ * offsets; entry k of row r at slice_ptr[r / 32] + 32 k + r % 32, padding entries 0), the
+ * values tp_sell_scatter writes from out64. */
 TP_API int tp_assemble_stiffness_diag(const tp_mesh* m, const double* De_cell, int S, int ld,
                                       const double* alpha, const double* shift,
                                       const uint8_t* bc_mask, double* out64, float* out32,
-                                      const int32_t* csr2sell, float* sell32, double* diag64,
+                                      const int32_t* slice_ptr, float* sell32, double* diag64,
                                       float* diag32, void* stream);
 
 /* gpu_assembler.py:176-221 + :228-239 for S columns (interleaved, leading dim ld):

@@ -91,8 +91,9 @@ def test_fused_stiffness_diag_equals_separate_calls(cuda_device, with_alpha_bc):
     _lib.call("tp_lumped_diag", ctypes.byref(dm.tpm), S, ld, ptr(alpha), shift, ptr(bc),
               ptr(D64a), ptr(D32a), st)
     sell.scatter(K64a, out32=Sa)
+    Sb.fill_(7.0)  # every SELL entry, padding included, must be written
     _lib.call("tp_assemble_stiffness_diag", ctypes.byref(dm.tpm), ptr(De), S, ld, ptr(alpha),
-              shift, ptr(bc), ptr(K64b), ptr(K32b), ptr(sell.csr2sell), ptr(Sb), ptr(D64b),
+              shift, ptr(bc), ptr(K64b), ptr(K32b), ptr(sell.slice_ptr), ptr(Sb), ptr(D64b),
               ptr(D32b), st)
     for a, b in ((K64a, K64b), (K32a, K32b), (D64a, D64b), (D32a, D32b), (Sa, Sb)):
         assert torch.equal(a, b)
