@@ -247,7 +247,9 @@ __device__ __forceinline__ void block_partial(double v[NV], double* part, double
 
 struct LaneState {
   double rz[4], alpha[4], beta[4], rr[4], rmax2[4], tol2[4], bb[4], rtrue[4];
-  int active[4], trigger[4], status[4], iters[4];
+  // frozen (window engine): the lane's recurrence residual reached the tolerance; it takes
+  // no further steps and is confirmed by the next FP64 sweep
+  int active[4], trigger[4], status[4], iters[4], frozen[4];
 };
 
 // z and p of row j from a [z | p] record buffer (plain loads: written by this kernel)
@@ -883,15 +885,17 @@ __device__ __forceinline__ void cg_coefficients(LaneState& L, int s, double gm, 
 }
 
 // lane results and status (block 0, thread 0); s_tot holds the final true r.r
+// have_final: s_tot holds the final FP64 residual norms of every lane (else each lane's
+// rtrue is the one of the sweep that confirmed it)
 template <typename VT>
 __device__ void write_result(const PArgs<VT>& a, LaneState& L, bool ok2, const double* s_tot,
-                             int it, int n_rel) {
+                             int it, int n_rel, bool have_final = true) {
   // a CTA that gave up at the last barrier leaves only the flag behind
   if (ld_acquire(&a.bar->abort)) ok2 = false;
   int status = TP_OK;
   for (int s = 0; s < 4; s++) {
     if (s < a.S) {
-      if (ok2) L.rtrue[s] = s_tot[s];
+      if (ok2 && have_final) L.rtrue[s] = s_tot[s];
       if (L.status[s] == -1) {
         L.status[s] = (ok2 && L.rtrue[s] <= L.tol2[s]) ? TP_OK : TP_ERR_NOT_CONVERGED;
         L.iters[s] = it;
@@ -1297,6 +1301,7 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
       L.alpha[s] = 0.0;
       L.beta[s] = 0.0;
       L.trigger[s] = 0;
+      L.frozen[s] = 0;
       L.iters[s] = 0;
       const bool fin = isfinite(rr) && isfinite(rz);
       const bool act = use && fin && rr > L.tol2[s];
@@ -1342,7 +1347,7 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
       VT al[LD], be[LD];
 #pragma unroll
       for (int s = 0; s < LD; s++) {
-        const bool act = (s < S) && L.active[s];
+        const bool act = (s < S) && L.active[s] && !L.frozen[s];  // frozen lanes stand still
         al[s] = act ? (VT)L.alpha[s] : VT(0);
         be[s] = act ? (VT)L.beta[s] : VT(0);
       }
@@ -1407,12 +1412,15 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
     if (!ok) break;
     grid_totals<4, 8>(a.part, s_tot, s_buf);
     it++;
-    // lanes in parallel: thread s owns lane s
+    // lanes in parallel: thread s owns lane s.  A lane whose recurrence residual reaches
+    // the tolerance freezes (its columns of the next steps are no-ops) instead of asking for
+    // a sweep at once: the lanes converge at different iterations, and one sweep then
+    // confirms them together.
     int trig = 0;
     if (threadIdx.x < S) {
       const int s = threadIdx.x;
       L.trigger[s] = 0;
-      if (L.active[s]) {
+      if (L.active[s] && !L.frozen[s]) {
         const double gm = s_tot[s], rr = s_tot[4 + s], dl = s_tot[8 + s];
         if (!isfinite(gm) || !isfinite(rr) || !isfinite(dl)) {
           L.active[s] = 0;
@@ -1420,17 +1428,29 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
           L.iters[s] = it;
         } else {
           L.rr[s] = rr;
-          trig = (rr <= L.tol2[s]) || (a.delta2 > 0.0 && rr < a.delta2 * L.rmax2[s]);
+          if (rr <= L.tol2[s])
+            L.frozen[s] = 1;
+          else
+            trig = a.delta2 > 0.0 && rr < a.delta2 * L.rmax2[s];
         }
       }
     }
-    // one FP64 sweep refreshes every active lane when any lane asks for it
-    const int any = __syncthreads_or(trig);
+    // one FP64 sweep refreshes every active lane when any lane asks for it, or when every
+    // lane still active is frozen (the same decision in every CTA: same totals)
+    int any = __syncthreads_or(trig);
+    if (!any) {
+      int running = 0, pending = 0;
+      for (int s = 0; s < S; s++) {
+        running |= L.active[s] && !L.frozen[s];
+        pending |= L.active[s] && L.frozen[s];
+      }
+      any = pending && !running;
+    }
     if (threadIdx.x < S && L.active[threadIdx.x]) {
       const int s = threadIdx.x;
       if (any)
         L.trigger[s] = 1;
-      else
+      else if (!L.frozen[s])
         cg_coefficients(L, s, s_tot[s], s_tot[8 + s], it);
     }
     if (threadIdx.x == 0) s_anytrig = any;
@@ -1495,6 +1515,7 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
         for (int s = 0; s < S; s++) {
           if (!L.trigger[s]) continue;
           L.trigger[s] = 0;
+          L.frozen[s] = 0;
           const double gm = s_tot[s], rr = s_tot[4 + s], dl = s_tot[8 + s];
           L.rtrue[s] = rr;
           if (!isfinite(rr) || !isfinite(gm) || !isfinite(dl)) {
@@ -1517,7 +1538,21 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
     }
   }
 
-  // ---- final: x += xi, true residual norms
+  // ---- final: x += xi, true residual norms.  When every lane was confirmed by a sweep
+  // (converged there, or before the first iteration), x holds its solution already (xi
+  // was added and zeroed then, and the lane took no step after) and rtrue its FP64
+  // residual: the pass is skipped (the same decision in every CTA).
+  bool all_confirmed = true;
+  for (int s = 0; s < S; s++) all_confirmed &= !L.active[s] && L.status[s] == TP_OK;
+  if (ok && all_confirmed) {
+    if (clk.on) {
+      clk.lap(6);
+#pragma unroll
+      for (int k = 0; k < 8; k++) a.prof[blockIdx.x * 8 + k] = clk.acc[k];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) write_result(a, L, true, s_tot, it, n_rel, false);
+    return;
+  }
   FOR_OWN_ROWS {
     VT xv[LD];
     ldv_cg<VT, LD>(a.xi, row, xv);
