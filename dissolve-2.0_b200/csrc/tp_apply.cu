@@ -253,6 +253,16 @@ __global__ void __launch_bounds__(256) k_guess_dots(
   for (int64_t base = blockIdx.x * rpb; base < n; base += (int64_t)gridDim.x * rpb) {
     const int64_t row = base + threadIdx.x / LD;
     if (row >= n || s >= S || (bc && bc[row])) continue;
+    // the row's vector entries first: they do not depend on the CSR walk, so their loads
+    // are in flight during it
+    const int64_t i = row * LD + s;
+    const double u = U[i], dg = diag[i], bi = b[i], ou = opU[i];
+    double dv[M], im[M];
+#pragma unroll
+    for (int k = 0; k < M; k++) {
+      dv[k] = dirs.d[k][i];
+      im[k] = k < NG ? 0.0 : dirs.img[k][i];
+    }
     double kd[NG > 0 ? NG : 1];
 #pragma unroll
     for (int k = 0; k < NG; k++) kd[k] = 0.0;
@@ -281,15 +291,10 @@ __global__ void __launch_bounds__(256) k_guess_dots(
         for (int k = 0; k < NG; k++) kd[k] += kv[u] * dvv[u][k];
       }
     }
-    const int64_t i = row * LD + s;
-    const double u = U[i], dg = diag[i];
-    const double r0 = b[i] - (opU[i] + dg * u);
-    double dv[M], Ad[M];
+    const double r0 = bi - (ou + dg * u);
+    double Ad[M];
 #pragma unroll
-    for (int k = 0; k < M; k++) {
-      dv[k] = dirs.d[k][i];
-      Ad[k] = (k < NG ? dsc_s * kd[k < NG ? k : 0] : dirs.img[k][i]) + dg * dv[k];
-    }
+    for (int k = 0; k < M; k++) Ad[k] = (k < NG ? dsc_s * kd[k < NG ? k : 0] : im[k]) + dg * dv[k];
     int q = 0;
 #pragma unroll
     for (int k = 0; k < M; k++)
