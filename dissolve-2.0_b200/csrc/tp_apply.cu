@@ -153,8 +153,9 @@ __global__ void __launch_bounds__(256) k_csr_apply(int64_t n, CsrView<T> A,
 
 // y1 = D K x1 and y2 = D K (x1 - x2) in one pass over the CSR operator (no mass, no
 // diagonal, no identity rows): the stiffness images of u^n and of the last increment.
-// G lanes per row, FP64.
-template <int LD, int G>
+// G lanes per row, FP64.  W256: 4-column rows of x1 and x2 are gathered with one 256-bit
+// load each (both bases 32-byte aligned, checked by the caller).
+template <int LD, int G, bool W256 = false>
 __global__ void __launch_bounds__(256) k_csr_images(int64_t n, const int32_t* __restrict__ indptr,
                                                     const int32_t* __restrict__ indices,
                                                     const double* __restrict__ K, double4 dsc,
@@ -176,8 +177,15 @@ __global__ void __launch_bounds__(256) k_csr_images(int64_t n, const int32_t* __
       const int j = __ldg(indices + p);
       const double kv = __ldg(K + p);
       double u[LD], up[LD];
-      ldv<double, LD>(x1, j, u);
-      ldv<double, LD>(x2, j, up);
+      if constexpr (W256 && LD == 4) {
+        const double4 a = ldg_d4(reinterpret_cast<const double4*>(x1) + j);
+        const double4 c = ldg_d4(reinterpret_cast<const double4*>(x2) + j);
+        u[0] = a.x, u[1] = a.y, u[2] = a.z, u[3] = a.w;
+        up[0] = c.x, up[1] = c.y, up[2] = c.z, up[3] = c.w;
+      } else {
+        ldv<double, LD>(x1, j, u);
+        ldv<double, LD>(x2, j, up);
+      }
 #pragma unroll
       for (int s = 0; s < LD; s++) {
         a1[s] += kv * u[s];
@@ -565,6 +573,9 @@ extern "C" int tp_csr_images(const tp_csr_op* op, const double* x1, const double
   else if (op->ld == 2)
     k_csr_images<2, G><<<grid, 256, 0, st>>>(op->n_rows, op->indptr, op->indices, op->K64, dsc,
                                              x1, x2, y1, y2);
+  else if (((reinterpret_cast<uintptr_t>(x1) | reinterpret_cast<uintptr_t>(x2)) & 31) == 0)
+    k_csr_images<4, G, true><<<grid, 256, 0, st>>>(op->n_rows, op->indptr, op->indices, op->K64,
+                                                   dsc, x1, x2, y1, y2);
   else
     k_csr_images<4, G><<<grid, 256, 0, st>>>(op->n_rows, op->indptr, op->indices, op->K64, dsc,
                                              x1, x2, y1, y2);
