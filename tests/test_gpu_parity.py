@@ -383,3 +383,33 @@ def test_bad_mesh_inputs_raise(tp):
     asm = A.GPUSparseAssembler((coords, np.array([[0, 1, 2, 3]], dtype=np.int32)))
     with pytest.raises(ValueError, match="index"):
         asm.assemble(np.ones(1), 1.0, bc_dofs=np.array([9], dtype=np.int32))
+
+
+def test_zero_size_inputs_are_no_ops(tp):
+    """Entry points given zero rows / cells / values return TP_OK and write nothing (a
+    sentinel buffer stays as it was)."""
+    _lib, _, _ = tp
+    import torch
+
+    from dissolve_tp.device import ptr, stream_handle
+    st = stream_handle()
+    a = torch.full((8,), 7.0, dtype=torch.float64, device="cuda")
+    b = torch.full((8,), 7.0, dtype=torch.float64, device="cuda")
+    c = torch.full((8,), 7.0, dtype=torch.float64, device="cuda")
+    d = torch.full((8,), 7.0, dtype=torch.float64, device="cuda")
+    cells = torch.zeros((2, 4), dtype=torch.int32, device="cuda")
+    one = (ctypes.c_double * 4)(1.0, 1.0, 1.0, 1.0)
+    calls = [
+        ("tp_cell_average", 0, ptr(cells), ptr(a), ptr(b), st),
+        ("tp_axpby", 0, 2.0, ptr(a), 3.0, ptr(b), st),
+        ("tp_advance_state", 0, ptr(a), ptr(b), ptr(c), ptr(d), st),
+        ("tp_pack_columns", 0, 3, 4, ptr(a), ptr(b), st),
+        ("tp_unpack_columns", 0, 3, 4, ptr(a), ptr(b), st),
+        ("tp_o2_alpha", 0, ptr(a), ptr(b), 0.1, 2.0, ptr(c), st),
+        ("tp_lumped_rhs", 0, 3, 4, ptr(a), ptr(b), None, 50.0, 0, None, one, ptr(c), st),
+    ]
+    for name, *args in calls:
+        assert _lib.call(name, *args) == 0, name
+    torch.cuda.synchronize()
+    for t in (a, b, c, d):
+        assert torch.all(t == 7.0)
