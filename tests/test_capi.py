@@ -54,3 +54,35 @@ def test_no_cpu_fallback_when_library_missing(tmp_path, monkeypatch):
         assert "no CPU fallback" in str(e)
     else:
         raise AssertionError("loaded a missing library")
+
+
+def test_zero_size_and_null_arguments_need_no_device():
+    """Zero-length calls return TP_OK and null operands are rejected with ValueError, both
+    before any device work: nothing here needs a GPU, so the placeholder addresses are
+    never dereferenced."""
+    import pytest
+
+    from dissolve_tp import _lib
+
+    one = (ctypes.c_double * 4)(1.0, 1.0, 1.0, 1.0)
+    P = 4096  # placeholder address, never read
+    zero_calls = [
+        ("tp_cell_average", 0, P, P, P, None),
+        ("tp_axpby", 0, 2.0, P, 3.0, P, None),
+        ("tp_advance_state", 0, P, P, P, P, None),
+        ("tp_pack_columns", 0, 3, 4, P, P, None),
+        ("tp_unpack_columns", 0, 3, 4, P, P, None),
+        ("tp_o2_alpha", 0, P, P, 0.1, 2.0, P, None),
+        ("tp_lumped_rhs", 0, 3, 4, P, P, None, 50.0, 0, None, one, P, None),
+    ]
+    for name, *args in zero_calls:
+        assert _lib.call(name, *args) == _lib.TP_OK, name
+    null_calls = [
+        ("tp_axpby", 8, 2.0, None, 3.0, P, None),
+        ("tp_cell_average", 8, P, None, P, None),
+        ("tp_pack_columns", 8, 3, 2, P, P, None),  # ld < S
+        ("tp_lumped_rhs", 8, 5, 5, P, P, None, 50.0, 0, None, one, P, None),  # S > 4
+    ]
+    for name, *args in null_calls:
+        with pytest.raises(ValueError):
+            _lib.call(name, *args)
