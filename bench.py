@@ -39,6 +39,11 @@ import numpy as np  # noqa: E402
 METRIC = "3-species BE steps/s at 1.57M P1 tets, rtol 1e-8: mixed+learned vs plain FP64"
 N_SIDE, JITTER = 64, 0.2
 D_S, K_S, DT, RTOL = (1.0, 1.0, 2.6), (0.5, 0.0, 0.2), 0.02, 1e-8
+# steps from u_prev after which both GPU forms are compared with the oracle (and the number
+# of steps of the CPU baseline sample)
+PARITY_STEPS = 3
+# relative residual of the oracle's Jacobi-PCG solves that stand in for exact solutions
+ORACLE_RTOL = 1e-12
 # measured with ncu on this workload (see profiles/); None until captured
 DRAM_BYTES_PER_ITERATION = 11.30e6  # 3.040 GB over a 269-iteration launch of k_cgw
 WORKLOAD = ("3-species backward-Euler step, 64^3 Kuhn cube (1,572,864 P1 tets, 274,625 "
@@ -280,6 +285,7 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- the plain FP64 GPU form on the same steps
     forms = {}
+    plain = None
     if args.forms:
         plain = PlainTransport(m, coef, D_S, K_S, DT, rtol=RTOL)
         plain.set_state(u0)
@@ -348,12 +354,28 @@ def run_ours(args, rank, world, local_rank):
         "e2e": e2e,
         "forms": forms,
     }
+    # states of both forms after PARITY_STEPS steps from u0, compared with the oracle in the
+    # CPU leg below
+    gpu_states = {}
+    if args.cpu_baseline and world == 1:
+        if plain is None:
+            plain = PlainTransport(m, coef, D_S, K_S, DT, rtol=RTOL)
+        for name, tr in (("fast", fast), ("plain_fp64", plain)):
+            tr.set_state(u0)
+            for _ in range(PARITY_STEPS):
+                tr.step(sync=True)
+            gpu_states[name] = tr.state()
+    del plain
     if args.kernels and world == 1:
         line["kernels"] = kernel_table(m, coef, u0, flush)
+        line["setup"] = setup_times(m)
+    parity_inputs = {}
     if args.configs and world == 1:
-        line["other_configs"] = other_configs(flush)
+        line["other_configs"] = other_configs(flush, parity_inputs)
     if rank == 0 and world == 1 and args.cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(m, coef, u0, sample_steps=args.cpu_sample_steps)
+        line["cpu_baseline"], line["parity"] = cpu_baseline(
+            m, coef, u0, sample_steps=args.cpu_sample_steps, gpu_states=gpu_states,
+            gyroid=parity_inputs.get("gyroid_48"))
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -426,6 +448,85 @@ def kernel_table(m, coef, u0, flush):
                      "GB_s": round(gbs, 1), "frac_hbm": round(gbs / hbm, 3)}
     out["peak_gbs"] = {"value": hbm, "source": "measured" if "hbm_gbs" in _peaks() else
                        "fallback (MEASURED_PEAKS.json absent)"}
+    rows["assemble_full_fp64"][0]()  # o64 = the full operator again (the rows reuse it)
+    out["reference_assemble_p1_tet"] = reference_kernel_baseline(dm, De, al, o64, flush, hbm)
+    return out
+
+
+def reference_kernel_baseline(dm, De, alpha, ours64, flush, hbm):
+    """Baseline leg (not the product): the reference's own GPU assembly kernel,
+    assemble_p1_tet of gpu/gpu_assembler.py:60-139, compiled from its source string for
+    sm_100a into oracle/_ref/ and launched as the reference launches it (:494-508: the CSR
+    values zeroed, then one thread per cell, 128 per block, 16 FP64 atomicAdds through the
+    scatter map), on the same mesh and coefficients as the full FP64 row above.  Its
+    algorithmic bytes are the scope table's n (16 + 64 + 16) + V 24 + nnz 8; what it reads
+    is the reference layout (detJ 8 B + Gflat 72 B per cell)."""
+    import ctypes
+
+    import torch
+
+    from dissolve_tp.device import ptr, stream_handle
+    path = os.path.join(REPO, "oracle", "_ref", "libref_kernels_gpu.so")
+    if not os.path.exists(path):
+        return {"unavailable": "oracle/_ref/libref_kernels_gpu.so not built"}
+    lib = ctypes.CDLL(path)
+    fn = lib.ref_gpu_assemble_p1_tet
+    fn.restype = ctypes.c_int
+    detJ, G, _ = dm.ref_geometry
+    sm = dm.scatter_map
+    n, V, nnz = dm.n_cells, dm.n_verts, dm.nnz
+    out = torch.empty(nnz, dtype=torch.float64, device=De.device)
+    st = stream_handle()
+    grid = (n + 127) // 128
+
+    def launch():
+        rc = fn(ctypes.c_uint(grid), ctypes.c_uint(128), ctypes.c_void_p(st), ctypes.c_int(n),
+                ctypes.c_void_p(ptr(dm.cells)), ctypes.c_void_p(ptr(detJ)),
+                ctypes.c_void_p(ptr(G)), ctypes.c_void_p(ptr(De)), ctypes.c_void_p(ptr(alpha)),
+                ctypes.c_double(50.0), ctypes.c_int(1), ctypes.c_void_p(ptr(sm)),
+                ctypes.c_void_p(ptr(out)))
+        if rc != 0:
+            raise RuntimeError(f"reference kernel launch failed ({rc})")
+
+    def with_fill():
+        out.zero_()
+        launch()
+
+    nbytes = n * (16 + 64 + 16) + V * 24 + nnz * 8
+    res = {"source": "gpu/gpu_assembler.py:60-139 compiled for sm_100a (oracle/_ref)"}
+    for name, fn_ in (("kernel", launch), ("fill_and_kernel", with_fill)):
+        ms = _event_ms(fn_, 10, flush, torch)
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        res[name] = {"us": round(ms * 1e3, 1), "GB_s": round(gbs, 1),
+                     "frac_hbm": round(gbs / hbm, 3)}
+    with_fill()
+    a, b = out.cpu().numpy(), ours64.cpu().numpy()
+    # the atomics add in no fixed order: equal up to rounding
+    res["max_rel_diff_vs_ours"] = float(np.abs(a - b).max() / np.abs(b).max())
+    return res
+
+
+def setup_times(m):
+    """Mesh setup on the GPU at this workload: geometry, incidence, CSR pattern and the
+    element-to-nonzero slots (DeviceMesh), then the reference-layout scatter map on
+    request; host wall time around each (the setup calls synchronise)."""
+    import torch
+
+    from dissolve_tp.assembler import DeviceMesh
+    out = {}
+    for rep in range(2):  # the first run pays one-time module loading
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        dm = DeviceMesh(m.coords, m.cells)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        _ = dm.scatter_map
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        out = {"device_mesh_s": round(t1 - t, 4), "scatter_map_s": round(t2 - t1, 4),
+               "includes": "H2D of coords and cells, geometry, incidence, pattern (two "
+                           "passes), slots; scatter map built only on request"}
+        del dm
     return out
 
 
@@ -436,12 +537,14 @@ def _peaks():
         return {}
 
 
-def other_configs(flush):
+def other_configs(flush, parity_inputs):
     """The other workloads at their own shapes, each timed with CUDA events after warm-up:
     256 uneven meshes as one batch vs one mesh at a time; the gyroid coupled step with the
     learned guess trained on 300 steps and evaluated on 100 (N=48) against the
     previous-step guess; the gyroid step at N=96 with the learned guess, eager and
-    CUDA-graph captured, against the plain FP64 step."""
+    CUDA-graph captured, against the plain FP64 step.  parity_inputs receives the gyroid
+    run's start state and its GPU states after the first evaluated steps (compared with
+    the oracle in the CPU leg)."""
     import torch
     out = {}
 
@@ -486,6 +589,12 @@ def other_configs(flush):
         p = GyroidStep(mesh, phi, coef)
         p.tr.set_state(g.state(), g.tr.U_prev[:, :3].cpu().numpy())
         p.phi.copy_(g.phi)
+        # the state the evaluation starts from, for the oracle's run of its first steps
+        n_or = 10
+        start = {"coords": mesh.coords, "cells": mesh.cells, "phi": g.phi.cpu().numpy(),
+                 "coef": coef, "U": g.state(), "steps": n_or, "dt": g.dt, "eps": g.eps,
+                 "workload": f"gyroid 48^3, the first {n_or} evaluated steps after the 300 "
+                             "training steps", "gpu": {}}
         res = {}
         for name, obj in (("learned", g), ("previous", p)):
             its = []
@@ -493,12 +602,15 @@ def other_configs(flush):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
-            for _ in range(100):
+            for i in range(100):
                 its.append(obj.step()["iterations"])
+                if i == n_or - 1:
+                    start["gpu"][name] = obj.state()
             e1.record()
             e1.synchronize()
             res[name] = {"ms_per_step": round(e0.elapsed_time(e1) / 100, 3),
                          "mean_iterations": round(float(np.mean(its)), 1)}
+        parity_inputs["gyroid_48"] = start
         a, b_ = g.state(), p.state()
         res["rel_l2_learned_vs_previous"] = float(np.linalg.norm(a - b_) / np.linalg.norm(b_))
         res["workload"] = ("gyroid 48^3 (663,552 tets), k_ORR H_eps interface reaction, 300 "
@@ -565,15 +677,50 @@ def cpu_step_runner(m, coef, u0):
     return step, nt, state
 
 
-def cpu_baseline(m, coef, u0, sample_steps=3):
+def cpu_baseline(m, coef, u0, sample_steps=PARITY_STEPS, gpu_states=None, gyroid=None):
+    """The timed CPU sample (oracle port of the reference's CPU path: GMRES(50) + block
+    Jacobi ILU(0) to rtol 1e-8, one block per host thread), then the parity of the GPU
+    forms: the oracle's states after the same steps from u0 with every species solved by
+    Jacobi-PCG to ORACLE_RTOL (standing in for the exact solution), against the GPU states
+    after those steps; and the gyroid coupled step's first evaluated steps the same way."""
     step, nt, state = cpu_step_runner(m, coef, u0)
     t = time.perf_counter()
     for _ in range(sample_steps):
         step()
     dt = time.perf_counter() - t
-    return {"value": sample_steps / dt, "unit": "steps/s", "cores": nt, "kind": "port",
+    base = {"value": sample_steps / dt, "unit": "steps/s", "cores": nt, "kind": "port",
             "sample": f"{sample_steps} full 3-species steps from u_prev ~ U(0,1) "
                       f"(GMRES iterations per species {state['iters'][-1]})"}
+    parity = {}
+    if gpu_states:
+        from oracle import oracle as orc
+        t = time.perf_counter()
+        want = orc.transport_steps(m.coords, m.cells, coef, D_S, K_S, DT, u0, PARITY_STEPS,
+                                   rtol=ORACLE_RTOL)[-1]
+        parity["headline"] = {
+            "workload": f"{WORKLOAD}; {PARITY_STEPS} steps from u_prev",
+            "oracle": f"per-species FP64 assembly + Jacobi-PCG to {ORACLE_RTOL:g} (CPU port, "
+                      f"{nt} threads, {time.perf_counter() - t:.1f} s)",
+            "bar": 1e-7}
+        for name, U in gpu_states.items():
+            parity["headline"][f"rel_l2_vs_oracle_{name}"] = float(
+                np.linalg.norm(U - want) / np.linalg.norm(want))
+    if gyroid:
+        from oracle import oracle as orc
+        g = gyroid
+        t = time.perf_counter()
+        want, _ = orc.gyroid_steps(g["coords"], g["cells"], g["phi"], g["coef"], g["U"],
+                                   g["steps"], g["dt"], g["eps"], rtol=ORACLE_RTOL)
+        parity["gyroid_48"] = {
+            "workload": g["workload"],
+            "oracle": f"coupled step, per-species FP64 assembly + Jacobi-PCG to "
+                      f"{ORACLE_RTOL:g} (CPU port, {time.perf_counter() - t:.1f} s)",
+            "bar": 1e-7}
+        for name in ("learned", "previous"):
+            U = g["gpu"][name]
+            parity["gyroid_48"][f"rel_l2_vs_oracle_{name}"] = float(
+                np.linalg.norm(U - want) / np.linalg.norm(want))
+    return base, parity
 
 
 def run_reference(args, rank, world):

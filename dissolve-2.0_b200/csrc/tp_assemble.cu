@@ -942,30 +942,38 @@ extern "C" int tp_scaffold_volume(const tp_mesh* m, const double* phi, double ep
 
 // ----------------------------------------------------------------- scaffold volume, fixed scratch
 // tp_scaffold_volume_static keeps its block partials in this module-resident array instead
-// of a caller buffer.  The launch uses at most kSvMaxParts blocks (the same cap as
-// tp_scaffold_volume), so every mesh size fits; nothing in the array has to start at zero
-// because every partial is written before the second kernel reads it.  One array per
-// device, shared by all callers: calls that overlap on one device (two streams, two host
-// threads) race on it.
+// of a caller buffer.  The launch uses at most kSvMaxParts blocks (grid_for caps the grid;
+// the kernel strides over the cells), so every mesh size fits; nothing in the array has to
+// start at zero because every partial is written before the second kernel reads it.  One
+// array per device, shared by all callers: calls that overlap on one device (two streams,
+// two host threads) race on it.
 static constexpr int kSvMaxParts = 1024;  // 8 KiB of doubles
 static constexpr int kSvMaxDevices = 64;
 static __device__ __align__(256) double g_sv_parts[kSvMaxParts];
 static std::mutex g_sv_mu;
 static double* g_sv_ptr[kSvMaxDevices] = {};
 
-// device address of g_sv_parts on the current device, looked up on the first call there
-static int sv_parts_on_current_device(double** out) {
+// Device address of g_sv_parts on the current device.  Outside a stream capture it is
+// looked up on every call (cheap after the first), so a device reset or another context
+// never leaves a stale address behind; inside a capture the address kept by an earlier
+// call on this device is used (no lookup while a graph is being recorded).
+static int sv_parts_on_current_device(cudaStream_t st, double** out) {
   int dev = -1;
   TP_CUDA_TRY(cudaGetDevice(&dev));
   TP_REQUIRE(dev >= 0 && dev < kSvMaxDevices,
              "tp_scaffold_volume_static: device ordinal %d beyond the %d supported", dev,
              kSvMaxDevices);
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  TP_CUDA_TRY(cudaStreamIsCapturing(st, &cs));
   std::lock_guard<std::mutex> lock(g_sv_mu);
-  if (g_sv_ptr[dev] == nullptr) {
+  if (cs == cudaStreamCaptureStatusNone) {
     void* p = nullptr;
     TP_CUDA_TRY(cudaGetSymbolAddress(&p, g_sv_parts));
     g_sv_ptr[dev] = static_cast<double*>(p);
   }
+  TP_REQUIRE(g_sv_ptr[dev] != nullptr,
+             "tp_scaffold_volume_static: the first call on device %d was inside a stream "
+             "capture; call it once on that device before capturing", dev);
   *out = g_sv_ptr[dev];
   return TP_OK;
 }
@@ -974,14 +982,11 @@ extern "C" int tp_scaffold_volume_static(const tp_mesh* m, const double* phi, do
                                          double* out_dev, void* stream) {
   TP_REQUIRE(mesh_ok(m) && phi && out_dev, "null pointer");
   TP_REQUIRE(eps > 0.0, "epsilon must be positive");
-  const int grid = grid_for(m->n_cells, 256, kSvMaxParts);
-  TP_REQUIRE(grid <= kSvMaxParts,
-             "tp_scaffold_volume_static: %d block partials exceed the fixed scratch of %d",
-             grid, kSvMaxParts);
-  double* part = nullptr;
-  const int rc = sv_parts_on_current_device(&part);
-  if (rc != TP_OK) return rc;
   cudaStream_t st = as_stream(stream);
+  const int grid = grid_for(m->n_cells, 256, kSvMaxParts);  // at most kSvMaxParts partials
+  double* part = nullptr;
+  const int rc = sv_parts_on_current_device(st, &part);
+  if (rc != TP_OK) return rc;
   const double qa = (5.0 + 3.0 * sqrt(5.0)) / 20.0, qb = (5.0 - sqrt(5.0)) / 20.0;
   k_scaffold_volume<<<grid, 256, 0, st>>>(m->n_cells, reinterpret_cast<const int4*>(m->cells),
                                           m->geo, phi, eps, qa, qb, part);

@@ -23,6 +23,8 @@
 
 #include <algorithm>
 
+#include <atomic>
+
 #include "tp_common.cuh"
 
 namespace tp {
@@ -193,12 +195,19 @@ __device__ __forceinline__ void mlp_tile_forward(const MlpSmem& sm, const uint32
 // an mbarrier (tcgen05.commit); every thread reads its own row back with tcgen05.ld (warp w
 // owns TMEM lanes 32w..32w+31).  Operands are K-major without swizzle: 8-row x 16-byte
 // core matrices, the two 8-element K halves 128 bytes apart, 8-row groups 256 bytes apart.
-// Every mbarrier wait is bounded; a wait that runs out sets g_mlp_tc_timeout, ends the
-// CTA's tiles and still releases its tensor memory.
+// Every mbarrier wait is bounded; a wait that runs out sets the call's status word and
+// g_mlp_tc_timeout, ends the CTA's tiles and still releases its tensor memory.
 constexpr int TC_M = 128, TC_COLS = 128;
-constexpr uint32_t TC_WAIT_LIMIT = 1u << 24;  // polls of one mbarrier phase (~0.1 s)
+constexpr uint32_t TC_WAIT_LIMIT = 1u << 24;  // default polls of one mbarrier phase (~0.1 s)
 
 __device__ int g_mlp_tc_timeout;
+
+// wait bound and failure-path test switch of the next launches (tp_mlp_set_wait_limit)
+struct TcWait {
+  uint32_t polls;
+  int skip_issue;
+  int32_t* status;
+};
 
 struct TcSmem {
   __nv_bfloat16 A1[TC_M * 16];     // features of the tile, 4 KB
@@ -243,9 +252,9 @@ __device__ __forceinline__ void tc_commit(uint64_t* bar) {
 }
 
 // bounded wait for the given phase of the mbarrier; false when the limit ran out
-__device__ __forceinline__ bool tc_wait(uint64_t* bar, uint32_t phase) {
+__device__ __forceinline__ bool tc_wait(uint64_t* bar, uint32_t phase, uint32_t polls) {
   const uint32_t ba = (uint32_t)__cvta_generic_to_shared(bar);
-  for (uint32_t it = 0; it < TC_WAIT_LIMIT; it++) {
+  for (uint32_t it = 0; it < polls; it++) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
@@ -256,6 +265,11 @@ __device__ __forceinline__ bool tc_wait(uint64_t* bar, uint32_t phase) {
     if (done) return true;
   }
   return false;
+}
+
+__device__ __forceinline__ void tc_timed_out(const TcWait& tw) {
+  atomicExch(&g_mlp_tc_timeout, 1);
+  if (tw.status) atomicExch(tw.status, 1);
 }
 
 __device__ __forceinline__ void tc_fence_before() {
@@ -288,7 +302,7 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, float v[16]) {
 __global__ void __launch_bounds__(TC_M) k_mlp_predict(MlpFeat F, int64_t nrows,
                                                       const float* __restrict__ P, float sigma,
                                                       double* __restrict__ x_out,
-                                                      float* __restrict__ y_out) {
+                                                      float* __restrict__ y_out, TcWait tw) {
   __shared__ __align__(128) TcSmem sm;
   const int tid = threadIdx.x, warp = tid >> 5;
   // weights in the operand layout (BF16), biases and w3 (w3 rounded to BF16 as in training)
@@ -349,11 +363,11 @@ __global__ void __launch_bounds__(TC_M) k_mlp_predict(MlpFeat F, int64_t nrows,
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    if (tid == 0) {
+    if (tid == 0 && !tw.skip_issue) {
       tc_mma(taddr, tc_desc(sm.A1), tc_desc(sm.W1), 0);
       tc_commit(&sm.bar);
     }
-    bool ok = tc_wait(&sm.bar, phase);
+    bool ok = tc_wait(&sm.bar, phase, tw.polls);
     phase ^= 1u;
     tc_fence_after();
     // h1 = relu(z1 + b1), BF16, into the layer-2 operand
@@ -372,16 +386,16 @@ __global__ void __launch_bounds__(TC_M) k_mlp_predict(MlpFeat F, int64_t nrows,
     proxy_fence();
     tc_fence_before();
     if (__syncthreads_or(!ok)) {
-      if (tid == 0) atomicExch(&g_mlp_tc_timeout, 1);
+      if (tid == 0) tc_timed_out(tw);
       break;
     }
     tc_fence_after();
-    if (tid == 0) {
+    if (tid == 0 && !tw.skip_issue) {
 #pragma unroll
       for (int j = 0; j < 4; j++) tc_mma(taddr + MLP_H, tc_desc(sm.A2[j]), tc_desc(sm.W2[j]), j > 0);
       tc_commit(&sm.bar);
     }
-    ok = tc_wait(&sm.bar, phase);
+    ok = tc_wait(&sm.bar, phase, tw.polls);
     phase ^= 1u;
     tc_fence_after();
     // layer 3 on the CUDA cores: BF16-rounded h2 . w3 + b3
@@ -408,7 +422,7 @@ __global__ void __launch_bounds__(TC_M) k_mlp_predict(MlpFeat F, int64_t nrows,
     // the tile's tensor-memory reads and operand reads are done before the next tile
     tc_fence_before();
     if (__syncthreads_or(!ok)) {
-      if (tid == 0) atomicExch(&g_mlp_tc_timeout, 1);
+      if (tid == 0) tc_timed_out(tw);
       break;
     }
   }
@@ -722,6 +736,9 @@ static MlpFeat make_feat(const tp_mlp_inputs* in) {
   return F;
 }
 
+static std::atomic<uint32_t> g_tc_polls{TC_WAIT_LIMIT};
+static std::atomic<int> g_tc_skip{0};
+
 extern "C" int tp_mlp_param_count(void) { return MLP_P; }
 
 extern "C" int tp_mlp_predict(const tp_mlp_inputs* in, const float* params, float sigma,
@@ -734,9 +751,17 @@ extern "C" int tp_mlp_predict(const tp_mlp_inputs* in, const float* params, floa
   const int64_t ntiles = (nrows + TC_M - 1) / TC_M;
   // persistent CTAs, 4 per SM (4 x 128 tensor-memory columns = the SM's 512)
   const int grid = (int)std::min<int64_t>(ntiles, (int64_t)sm_count() * 4);
-  k_mlp_predict<<<grid, TC_M, 0, as_stream(stream)>>>(make_feat(in), nrows, params, sigma, x_out,
-                                                       y_out);
+  cudaStream_t st = as_stream(stream);
+  TcWait tw{g_tc_polls.load(), g_tc_skip.load(), in->tc_status};
+  if (tw.status) TP_CUDA_TRY(cudaMemsetAsync(tw.status, 0, sizeof(int32_t), st));
+  k_mlp_predict<<<grid, TC_M, 0, st>>>(make_feat(in), nrows, params, sigma, x_out, y_out, tw);
   TP_LAUNCH_CHECK();
+  return TP_OK;
+}
+
+extern "C" int tp_mlp_set_wait_limit(unsigned int polls, int skip_issue) {
+  g_tc_polls.store(polls ? polls : TC_WAIT_LIMIT);
+  g_tc_skip.store(skip_issue ? 1 : 0);
   return TP_OK;
 }
 

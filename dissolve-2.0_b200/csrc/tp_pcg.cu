@@ -32,8 +32,9 @@
 //
 // Barrier.  A monotonic arrival counter: each CTA adds 1 (release) and waits until the
 // counter reaches (barriers so far) x gridDim.  The wait is bounded in time (2 s of
-// %globaltimer); a CTA that gives up raises an abort flag that every other wait also
-// watches, so a lost CTA ends the kernel with TP_ERR_TIMEOUT instead of a hang.
+// %globaltimer by default, tp_pcg_set_wait_limit); a CTA that gives up raises an abort
+// flag that every other wait also watches, so a lost CTA ends the kernel with
+// TP_ERR_TIMEOUT instead of a hang.
 //
 // Reliable updates (FP32 inner solve).  When any lane's recurrence residual has dropped
 // by delta since its last refresh (or reached the tolerance), every active lane is
@@ -95,9 +96,14 @@ struct PArgs {
   PBar* bar;
   POut* out;
   unsigned long long* prof;  // optional: gridDim.x * 8 phase times (ns)
+  // barrier wait bound, and arrivals every barrier waits for beyond the grid's own (0 in
+  // production; > 0 only to make the waits run out on purpose, which exercises the
+  // timeout path).  Kernel arguments: reading them costs no memory access per barrier.
+  unsigned long long wait_limit_ns;
+  unsigned int wait_missing;
 };
 
-constexpr unsigned long long WAIT_LIMIT_NS = 2000000000ull;  // one barrier wait: 2 s
+constexpr unsigned long long WAIT_LIMIT_NS = 2000000000ull;  // default barrier bound: 2 s
 
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
   unsigned int v;
@@ -159,12 +165,13 @@ struct PhaseClock {
 // `target` (thread 0 only) counts the arrivals this CTA has waited for so far.  The CTA's
 // writes are ordered by __syncthreads and published by thread 0's gpu-scope release add;
 // the acquire poll and the closing __syncthreads make the other CTAs' writes visible.
-__device__ __forceinline__ bool grid_sync(PBar* bar, unsigned int& target) {
+__device__ __forceinline__ bool grid_sync(PBar* bar, unsigned int& target,
+                                          unsigned long long limit_ns, unsigned int missing) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
-    target += gridDim.x;
+    target += gridDim.x + missing;
     red_release_add(&bar->count, 1u);
     unsigned int spins = 0;
     unsigned long long t0 = 0;
@@ -177,7 +184,7 @@ __device__ __forceinline__ bool grid_sync(PBar* bar, unsigned int& target) {
         const unsigned long long t = gtime();
         if (t0 == 0) {
           t0 = t;
-        } else if (t - t0 > WAIT_LIMIT_NS) {
+        } else if (t - t0 > limit_ns) {
           atomicExch(&bar->abort, 1u);
           ok = 0;
           break;
@@ -448,7 +455,7 @@ __global__ void __launch_bounds__(512, MINB) k_pcg(PArgs<VT> a) {
     }
     stv<VT, LD>(a.dinv, row, dv);
   }
-  bool ok = grid_sync(a.bar, target);
+  bool ok = grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
 
   // ---- I2: r = b - A x, z = D^-1 r, record 0 = [z | z], xi = 0; rr, rz, bb
   {
@@ -480,7 +487,7 @@ __global__ void __launch_bounds__(512, MINB) k_pcg(PArgs<VT> a) {
     }
     block_partial<12>(acc, a.part, sh);
   }
-  ok = ok && grid_sync(a.bar, target);
+  ok = ok && grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
   if (ok) grid_totals<12>(a.part, s_tot, s_buf);
   if (threadIdx.x == 0) {
     for (int s = 0; s < 4; s++) {
@@ -604,7 +611,7 @@ __global__ void __launch_bounds__(512, MINB) k_pcg(PArgs<VT> a) {
       block_partial<4>(acc, a.part, sh);
     }
     clk.lap(0);
-    ok = grid_sync(a.bar, target);
+    ok = grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
     clk.lap(1);
     if (!ok) break;
     grid_totals<4>(a.part, s_tot, s_buf);
@@ -671,7 +678,7 @@ __global__ void __launch_bounds__(512, MINB) k_pcg(PArgs<VT> a) {
       block_partial<8>(acc, a.part, sh);
     }
     clk.lap(2);
-    ok = grid_sync(a.bar, target);
+    ok = grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
     clk.lap(3);
     if (!ok) break;
     grid_totals<8>(a.part, s_tot, s_buf);
@@ -722,7 +729,7 @@ __global__ void __launch_bounds__(512, MINB) k_pcg(PArgs<VT> a) {
         }
         stv<VT, LD>(a.xi, row, xv);
       }
-      ok = grid_sync(a.bar, target);
+      ok = grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
       if (!ok) break;
       // ---- RU2: FP64 residual on trigger lanes, replace r and z (z of the next record)
       double acc[8];
@@ -748,7 +755,7 @@ __global__ void __launch_bounds__(512, MINB) k_pcg(PArgs<VT> a) {
         stv<VT, LD>(rec_n, 2 * row, zv);
       }
       block_partial<8>(acc, a.part, sh);
-      ok = grid_sync(a.bar, target);
+      ok = grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
       if (!ok) break;
       grid_totals<8>(a.part, s_tot, s_buf);
       if (threadIdx.x == 0) {
@@ -790,7 +797,7 @@ __global__ void __launch_bounds__(512, MINB) k_pcg(PArgs<VT> a) {
     }
     stv<VT, LD>(a.xi, row, xv);
   }
-  bool ok2 = ok && grid_sync(a.bar, target);
+  bool ok2 = ok && grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
   {
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     if (ok2) {
@@ -803,7 +810,7 @@ __global__ void __launch_bounds__(512, MINB) k_pcg(PArgs<VT> a) {
     }
     block_partial<4>(acc, a.part, sh);
   }
-  ok2 = ok2 && grid_sync(a.bar, target);
+  ok2 = ok2 && grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
   if (ok2) grid_totals<4>(a.part, s_tot, s_buf);
   if (clk.on) {
     clk.lap(6);
@@ -1266,7 +1273,7 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
     stv<VT, LD>(a.r, row, rz);
     stv<VT, LD>(a.u, row, rz);
   }
-  bool ok = grid_sync(a.bar, target);
+  bool ok = grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
 
   // ---- I2: r = b - A x, u = D^-1 r; r.u, r.r, b.b
   {
@@ -1284,7 +1291,7 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
     }
     block_partial<12>(acc, a.part, sh);
   }
-  ok = ok && grid_sync(a.bar, target);
+  ok = ok && grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
   if (ok) grid_totals<12>(a.part, s_tot, s_buf);
   if (threadIdx.x == 0) {
     for (int s = 0; s < 4; s++) {
@@ -1315,7 +1322,7 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
     if (ok) product(acc, false);
     block_partial<4>(acc, a.part, sh);
   }
-  ok = ok && grid_sync(a.bar, target);
+  ok = ok && grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
   if (ok) grid_totals<4>(a.part, s_tot, s_buf);
   if (threadIdx.x == 0 && ok) {
     for (int s = 0; s < S; s++) {
@@ -1395,7 +1402,7 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
       block_partial<8>(acc, a.part, sh);
     }
     clk.lap(2);
-    ok = grid_sync(a.bar, target);  // u published
+    ok = grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);  // u published
     clk.lap(3);
     if (!ok) break;
     // ---- W: w = A u; w.u into slots 8..11.  The three sums are read together below.
@@ -1407,7 +1414,7 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
       block_partial<4>(acc, a.part + 8, sh);
     }
     clk.lap(0);
-    ok = grid_sync(a.bar, target);
+    ok = grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
     clk.lap(1);
     if (!ok) break;
     grid_totals<4, 8>(a.part, s_tot, s_buf);
@@ -1473,7 +1480,7 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
         }
         stv<VT, LD>(a.xi, row, xv);
       }
-      ok = grid_sync(a.bar, target);
+      ok = grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
       if (!ok) break;
       {
         double acc[12];
@@ -1485,7 +1492,7 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
           refresh(tr, acc);
         block_partial<12>(acc, a.part, sh);  // slots 8..11 (b.b) are replaced by w.u
       }
-      ok = grid_sync(a.bar, target);
+      ok = grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
       if (!ok) break;
       // the FP64 residual sums first: when no triggered lane goes on (all converged or
       // failed) the product is skipped.  Every CTA reads the same totals, so every CTA
@@ -1506,7 +1513,7 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
         product(acc, false);
         block_partial<4>(acc, a.part + 8, sh);
-        ok = grid_sync(a.bar, target);
+        ok = grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
         if (!ok) break;
         grid_totals<4, 8>(a.part, s_tot, s_buf);
       }
@@ -1563,7 +1570,7 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
     }
     stv<VT, LD>(a.xi, row, xv);
   }
-  bool ok2 = ok && grid_sync(a.bar, target);
+  bool ok2 = ok && grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
   {
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     if (ok2) {
@@ -1583,7 +1590,7 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
     }
     block_partial<4>(acc, a.part, sh);
   }
-  ok2 = ok2 && grid_sync(a.bar, target);
+  ok2 = ok2 && grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
   if (ok2) grid_totals<4>(a.part, s_tot, s_buf);
   if (clk.on) {
     clk.lap(6);
@@ -1797,6 +1804,8 @@ static void fill_pargs(PArgs<VT>& a, const tp_csr_op* op, const tp_sell* sl, con
   a.loc_col = nullptr;
   a.sp_cap = a.halo_cap = a.col_cap = a.win_cap = 0;
   a.reg_values = 0;
+  a.wait_limit_ns = WAIT_LIMIT_NS;
+  a.wait_missing = 0;
   a.part = reinterpret_cast<double*>(p);
   p += a256(sizeof(double) * 16 * grid);
   a.bar = reinterpret_cast<PBar*>(p);
@@ -2097,6 +2106,16 @@ extern "C" int tp_pcg_set_profile(tp_pcg_handle* h, unsigned long long* prof) {
   TP_REQUIRE(h, "null handle");
   h->af.prof = prof;
   h->ad.prof = prof;
+  return TP_OK;
+}
+
+extern "C" int tp_pcg_set_wait_limit(tp_pcg_handle* h, unsigned long long limit_ns,
+                                     unsigned int missing_arrivals) {
+  TP_REQUIRE(h, "null handle");
+  TP_REQUIRE(missing_arrivals <= 1024, "missing_arrivals above 1024");
+  const unsigned long long lim = limit_ns ? limit_ns : WAIT_LIMIT_NS;
+  h->af.wait_limit_ns = h->ad.wait_limit_ns = lim;
+  h->af.wait_missing = h->ad.wait_missing = missing_arrivals;
   return TP_OK;
 }
 

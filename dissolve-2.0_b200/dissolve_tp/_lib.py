@@ -71,7 +71,7 @@ class TpMlpInputs(ctypes.Structure):
     _fields_ = [("n_verts", _c_i64), ("S", _c_i32), ("ld", _c_i32), ("U", _vp), ("U_prev", _vp),
                 ("phi", _vp), ("normgradphi", _vp), ("opU", _vp), ("opDU", _vp),
                 ("logD", _c_dbl * 4), ("k", _c_dbl * 4), ("mean", _c_dbl * 10),
-                ("istd", _c_dbl * 10), ("base", _c_i32)]
+                ("istd", _c_dbl * 10), ("base", _c_i32), ("tc_status", _vp)]
 
 
 class TpCgResult(ctypes.Structure):
@@ -162,9 +162,11 @@ SIGNATURES = {
     "tp_pcg_grid": (ctypes.c_int, [_vp, _P(ctypes.c_int), _P(ctypes.c_int)]),
     "tp_pcg_engine": (ctypes.c_int, [_vp, _P(ctypes.c_int), _P(ctypes.c_size_t)]),
     "tp_pcg_set_profile": (ctypes.c_int, [_vp, _vp]),
+    "tp_pcg_set_wait_limit": (ctypes.c_int, [_vp, ctypes.c_ulonglong, ctypes.c_uint]),
     "tp_pcg_destroy": (ctypes.c_int, [_vp]),
     "tp_mlp_param_count": (ctypes.c_int, []),
     "tp_mlp_tensor_status": (ctypes.c_int, [_P(ctypes.c_int), _vp]),
+    "tp_mlp_set_wait_limit": (ctypes.c_int, [ctypes.c_uint, ctypes.c_int]),
     "tp_mlp_predict": (ctypes.c_int, [_P(TpMlpInputs), _vp, ctypes.c_float, _vp, _vp, _vp]),
     "tp_mlp_features": (ctypes.c_int, [_P(TpMlpInputs), _vp, _vp]),
     "tp_mlp_target": (ctypes.c_int, [_c_i64, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _c_dbl,

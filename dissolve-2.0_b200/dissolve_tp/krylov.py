@@ -242,6 +242,13 @@ class PersistentCG:
                 "max_us": dict(zip(names, p.max(0).round(1).tolist())),
                 "min_us": dict(zip(names, p.min(0).round(1).tolist()))}
 
+    def set_wait_limit(self, limit_s: float = 0.0, missing_arrivals: int = 0):
+        """Bound of every grid-barrier wait of the next solves (0: the 2 s default).
+        missing_arrivals > 0 is for tests of the failure path: every barrier then waits for
+        that many CTAs that do not exist, so the solve ends with TP_ERR_TIMEOUT after
+        limit_s; set it back to 0 for normal solves (the handle stays usable)."""
+        call("tp_pcg_set_wait_limit", self._h, int(round(limit_s * 1e9)), int(missing_arrivals))
+
     def grid(self):
         g, b = ctypes.c_int(0), ctypes.c_int(0)
         call("tp_pcg_grid", self._h, ctypes.byref(g), ctypes.byref(b))

@@ -70,6 +70,10 @@ class WarmStartMLP:
         self.ws = torch.empty(int(_lib.lib.tp_mlp_grad_workspace_floats(self.grid)),
                               dtype=torch.float32, device=device)
         self.loss_dev = torch.zeros(1, dtype=torch.float32, device=device)
+        # per-call status of the tensor-core inference (1: a bounded wait ran out and the
+        # tile's rows kept what they held -- u^n in the solver's x, the previous direction in
+        # the projection -- so the solve still starts from a valid guess)
+        self.tc_status = torch.zeros(1, dtype=torch.int32, device=device)
         self.X = torch.empty((max(capacity_rows, 1), IN), dtype=torch.bfloat16, device=device)
         self.T = torch.empty(max(capacity_rows, 1), dtype=torch.float32, device=device)
         self.rows = 0
@@ -89,6 +93,7 @@ class WarmStartMLP:
         st.phi, st.normgradphi = ptr(phi), ptr(ngphi)
         opU, opDU = ops if ops is not None else (None, None)
         st.opU, st.opDU = ptr(opU), ptr(opDU)
+        st.tc_status = ptr(self.tc_status)
         for s in range(S):
             st.logD[s] = math.log(float(D[s]))
             st.k[s] = float(k[s])
@@ -181,6 +186,10 @@ class WarmStartMLP:
         call("tp_mlp_predict", ctypes.byref(inp), ptr(self.params), float(self.sigma), None,
              ptr(y), stream_handle())
         return y
+
+    def timed_out(self) -> bool:
+        """Whether the last inference gave up on a tensor-core wait (reads the device word)."""
+        return bool(int(self.tc_status.item()))
 
     def predict_into(self, tr, x):
         """The transport driver's hook: guess for tr's next step written into x (tr's

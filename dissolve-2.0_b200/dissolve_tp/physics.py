@@ -1,6 +1,7 @@
 """Per-vertex builders around the transport step, on the GPU (the CuPy/numpy element-wise
-code of the reference's time loop): effective film diffusivity, Zn transport
-coefficients, Sussman redistancing of the level set and the mean cell diameter."""
+code of the reference's time loop): the O2 reaction and OH- source coefficients, effective
+film diffusivity, Zn transport coefficients, Sussman redistancing of the level set and the
+mean cell diameter."""
 from __future__ import annotations
 
 import ctypes
@@ -17,6 +18,30 @@ def film_floor(porosity: float = 0.25, constrictivity: float = 1.0,
                tortuosity: float = 2.0) -> float:
     """eps delta / tau^2 (physics/interface_velocity.py:118-127; parameters.py:119-121)."""
     return porosity * constrictivity / (tortuosity * tortuosity)
+
+
+def o2_alpha(phi, normgradphi, epsilon, k_orr):
+    """alpha_O2 = delta_eps(phi) |grad phi| k_ORR per vertex (dissolve.py:866-875, with
+    delta_eps of physics/weak_forms.py:18-24): the O2 consumption at the interface band."""
+    phi_d = to_device(phi, torch.float64, torch.device("cuda"))
+    dev = phi_d.device
+    ng_d = to_device(normgradphi, torch.float64, dev)
+    out = torch.empty_like(phi_d)
+    call("tp_o2_alpha", int(phi_d.numel()), ptr(phi_d), ptr(ng_d), float(epsilon), float(k_orr),
+         ptr(out), stream_handle())
+    return out
+
+
+def oh_source(phi, normgradphi, F, Cl, O2, epsilon, kd, k_orr, orr_factor=4.0):
+    """f_OH = [phi <= 0] kd F Cl^2 + orr_factor delta_eps(phi) |grad phi| k_ORR O2 per vertex
+    (dissolve.py:923-936): film dissolution plus the ORR production of OH-."""
+    phi_d = to_device(phi, torch.float64, torch.device("cuda"))
+    dev = phi_d.device
+    ins = [to_device(a, torch.float64, dev) for a in (normgradphi, F, Cl, O2)]
+    out = torch.empty_like(phi_d)
+    call("tp_oh_source", int(phi_d.numel()), ptr(phi_d), *(ptr(a) for a in ins),
+         float(epsilon), float(kd), float(k_orr), float(orr_factor), ptr(out), stream_handle())
+    return out
 
 
 def effective_diffusion(phi, F, Fmax, D0=(2.72, 7.78, 20.16, 9.36), floor=None):

@@ -292,7 +292,13 @@ class BatchedTransport:
         self.initial_guess()
         self.solver.run()
         self.advance_state()
-        return self.solver.result() if sync else None
+        if not sync:
+            return None
+        res = self.solver.result()
+        if self.guess == "learned" and self.predictor is not None and self.steps_done > 1:
+            # a timed-out inference left a valid (older) guess; the solve is unaffected
+            res["guess_timed_out"] = self.predictor.timed_out()
+        return res
 
     def advance_state(self):
         """After a solve: the increment x - U joins the history (newest first), then

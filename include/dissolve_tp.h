@@ -193,13 +193,15 @@ TP_API int tp_scaffold_volume(const tp_mesh* m, const double* phi, double eps, d
  * that bind plain pointers and own no device allocator (a cgo/JNI/FFI embedding that only
  * passes the mesh and phi it already holds), and per-step loops that must not call
  * cudaMalloc/cudaFree, which synchronise the device.
- * Scratch: a fixed 8 KiB array compiled into this library, one per device, holding the at
- * most 1024 block partials; any mesh size fits, and a launch that would need more partials
- * is rejected with TP_ERR_ARG.  Nothing in it has to start at zero.  The first call on each
- * device looks up the array's address (cudaGetSymbolAddress) with that device current and
- * keeps it; a caller that records calls into a stream capture makes one call on that device
- * before the capture begins.  Calls that overlap on one device (two streams, or two host
- * threads) share the array and race: serialise them.  Result as tp_scaffold_volume. */
+ * Scratch: a fixed 8 KiB array compiled into this library, one per device, holding the
+ * block partials; the launch is capped at 1024 blocks (grid-stride over the cells), so
+ * every mesh size fits.  Nothing in it has to start at zero.  Outside a stream capture
+ * every call looks up the array's address (cudaGetSymbolAddress) with the calling device
+ * current and keeps it for that device; inside a capture the kept address is used, so a
+ * caller that records calls into a stream capture makes one call on that device before the
+ * capture begins (a call in a capture without one is rejected with TP_ERR_ARG).  Calls
+ * that overlap on one device (two streams, or two host threads) share the array and race:
+ * serialise them.  Result as tp_scaffold_volume. */
 TP_API int tp_scaffold_volume_static(const tp_mesh* m, const double* phi, double eps,
                               double* out_dev, void* stream);
 
@@ -472,6 +474,15 @@ TP_API int tp_pcg_engine(tp_pcg_handle* h, int* window, size_t* smem_bytes);
  * [A work, A barrier wait, B work, B barrier wait, scalar updates, reliable updates,
  * final, init]; NULL switches it off */
 TP_API int tp_pcg_set_profile(tp_pcg_handle* h, unsigned long long* prof);
+/* Bound of every grid-barrier wait of the next runs (limit_ns; 0 restores the default of
+ * 2 s) and, for tests of the failure path only, missing_arrivals (<= 1024) arrivals that
+ * every barrier waits for beyond the grid's own: with missing_arrivals > 0 the first wait
+ * runs out after limit_ns, the run ends with TP_ERR_TIMEOUT in its status and every
+ * lane status, and the handle stays usable (set 0 again for normal runs).  The failure
+ * it stands for is a CTA that never arrives; the caller's contract on any error is the
+ * reference's fallback (numerics/solvers.py:264-271: catch, then solve another way). */
+TP_API int tp_pcg_set_wait_limit(tp_pcg_handle* h, unsigned long long limit_ns,
+                                 unsigned int missing_arrivals);
 TP_API int tp_pcg_destroy(tp_pcg_handle* h);
 
 /* ------------------------------------------------------------------ learned guess */
@@ -494,6 +505,10 @@ typedef struct tp_mlp_inputs {
   double mean[10], istd[10]; /* input normalisation (features 0..9) */
   int32_t base;              /* the guess the network corrects: 0 u^n, 1 2 u^n - u^{n-1},
                                 2 none (tp_mlp_predict writes sigma y alone)             */
+  int32_t* tc_status;        /* device int32 or NULL: tp_mlp_predict sets it to 0 before its
+                                launch (on the stream) and the launch sets it to 1 when a
+                                bounded tensor-core wait ran out; the rows of such a tile
+                                are then not written (x_out keeps what it held)          */
 } tp_mlp_inputs;
 
 TP_API int tp_mlp_param_count(void);
@@ -503,9 +518,15 @@ TP_API int tp_mlp_param_count(void);
  * y_out[v * S + s] = y when x_out is NULL */
 TP_API int tp_mlp_predict(const tp_mlp_inputs* in, const float* params, float sigma,
                           double* x_out, float* y_out, void* stream);
-/* [sync] *timed_out = 1 if an inference launch of this library gave up waiting for its
- * tensor-core operations (bounded waits; its rows were then not written), else 0 */
+/* [sync] *timed_out = 1 if any inference launch of this library since it was loaded gave
+ * up waiting for its tensor-core operations (sticky; the per-call word is
+ * tp_mlp_inputs.tc_status), else 0 */
 TP_API int tp_mlp_tensor_status(int* timed_out, void* stream);
+/* Polls of one mbarrier phase before an inference wait gives up (0 restores the default,
+ * 2^24, about 0.1 s), for the launches that follow on any thread.  skip_issue != 0 is for
+ * tests of the failure path only: the issuing thread then launches no tensor-core
+ * operation and commits nothing, so every wait runs out with nothing in flight. */
+TP_API int tp_mlp_set_wait_limit(unsigned int polls, int skip_issue);
 /* the normalised inputs as BF16 rows of 16 (training set) */
 TP_API int tp_mlp_features(const tp_mlp_inputs* in, void* X_bf16, void* stream);
 /* training target (U_next - B) / sigma per row, B = U_n (U_prev NULL) or

@@ -321,3 +321,63 @@ def direct_solve(indptr, indices, data, b):
     n = b.shape[0]
     A = sp.csr_matrix((data, indices, indptr), shape=(n, n))
     return spla.spsolve(A.tocsc(), b)
+
+
+def transport_steps(coords, cells, coef, D, k, dt, U, steps, rtol=1e-12, lumped=1):
+    """Backward-Euler steps of the multi-species transport (numerics/solvers.py:322-372 per
+    species, dissolve.py:780-954 species by species): per species the FP64 assembly of
+    (1/dt + k_s) M + D_s coef K (gpu_assembler.py:60-139), the RHS M u/dt
+    (:176-221) and a Jacobi-PCG solve to ||b - A x|| <= rtol ||b|| from the previous
+    state (a tight rtol stands in for the exact solution).  Returns the state after each
+    step."""
+    detJ, G, _ = geometry(coords, cells)
+    ip, ix, sm = csr_pattern(cells, coords.shape[0])
+    n = cells.shape[0]
+    As = [assemble(detJ, G, D[s] * coef, np.full(n, float(k[s])), 1.0 / dt, lumped, sm,
+                   ix.size) for s in range(len(D))]
+    U = np.array(U, dtype=np.float64)
+    out = []
+    for _ in range(steps):
+        new = np.empty_like(U)
+        for s in range(len(D)):
+            b = assemble_rhs(cells, detJ, U[:, s], None, 1.0 / dt, lumped)
+            x, _, st, _ = pcg_jacobi(ip, ix, As[s], b, U[:, s], rtol)
+            if st != 0:
+                raise RuntimeError(f"oracle PCG did not converge (species {s})")
+            new[:, s] = x
+        U = new
+        out.append(U.copy())
+    return out
+
+
+def gyroid_steps(coords, cells, phi, coef, U, steps, dt, eps, D=(1.0, 1.0, 2.6),
+                 k=(0.5, 0.0, 0.2), k_orr=2.0, orr=2.0, rate=0.01, gain=0.5, rtol=None):
+    """Coupled gyroid-scaffold steps: interface reaction from phi (hv = k_orr H_eps(phi),
+    O2 consumption alpha = cell mean of hv, OH- source orr hv c_O2), the three species
+    solved one at a time (FP64 assembly, RHS, direct solve, or Jacobi-PCG to rtol when
+    given), then phi -= dt rate (1 + gain c_Cl).  Returns (U, phi) after the steps."""
+    detJ, G, JT = geometry(coords, cells)
+    ip, ix, sm = csr_pattern(cells, coords.shape[0])
+    phi, U = np.array(phi, dtype=np.float64), np.array(U, dtype=np.float64)
+    n = cells.shape[0]
+    for _ in range(steps):
+        grad = nodal_gradient(cells, detJ, JT, phi)
+        hv, _, f = interface_terms(phi, grad, eps, k_orr, orr, U)
+        hv_cell = hv[cells].sum(axis=1) / 4.0
+        new = np.empty_like(U)
+        for s in range(3):
+            alpha = k[s] + (hv_cell if s == 0 else 0.0)
+            A = assemble(detJ, G, D[s] * coef, np.broadcast_to(alpha, (n,)), 1.0 / dt, 1, sm,
+                         ix.size)
+            b = assemble_rhs(cells, detJ, U[:, s], f[:, s] if s == 2 else None, 1.0 / dt, 1)
+            if rtol is None:
+                new[:, s] = direct_solve(ip, ix, A, b)
+            else:
+                x, _, st, _ = pcg_jacobi(ip, ix, A, b, U[:, s], rtol)
+                if st != 0:
+                    raise RuntimeError(f"oracle PCG did not converge (species {s})")
+                new[:, s] = x
+        U = new
+        phi = levelset_advance(phi, U, 1, dt, rate, gain)
+    return U, phi
+

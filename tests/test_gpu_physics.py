@@ -1,4 +1,5 @@
-"""Builders around the transport step on the GPU against the oracle: effective film
+"""Builders around the transport step on the GPU against the oracle: the O2 reaction and
+OH- source coefficients (dissolve.py:866-875, 923-936), effective film
 diffusivity (interface_velocity.py:90-155), Zn transport coefficients and the Zn solve with
 the scaffold as its Dirichlet set (dissolve.py:740-778, through the solvers drop-in),
 Sussman redistancing (mesh_utils.py:450-542) and the mean cell diameter.
@@ -19,6 +20,53 @@ pytestmark = pytest.mark.gpu
 def _gyroid(n=8, jitter=0.15):
     from dissolve_tp.coupled import gyroid_inputs
     return gyroid_inputs(n, jitter)
+
+
+def _species_fields(n=20000, eps=0.1):
+    """phi spread over the band |phi| < eps, its edges, both sides of it and exact zeros."""
+    rng = np.random.default_rng(11)
+    phi = np.concatenate([rng.uniform(-eps, eps, n // 2), rng.uniform(-1.0, 1.0, n // 2)])
+    phi[:8] = [0.0, eps, -eps, np.nextafter(eps, 0.0), -np.nextafter(eps, 0.0), 1e-300,
+               -1e-300, 0.5 * eps]
+    ng = np.abs(rng.normal(1.0, 0.3, n))
+    F, Cl, O2 = rng.uniform(0, 2, n), rng.uniform(0, 1, n), rng.uniform(0, 1, n)
+    return phi, ng, F, Cl, O2
+
+
+def _close(got, want, rel=1e-14):
+    scale = np.maximum(np.abs(want), 1e-300)
+    return np.all((got == want) | (np.abs(got - want) <= rel * scale))
+
+
+def test_o2_alpha_matches_oracle(cuda_device):
+    from dissolve_tp import physics
+    eps, k_orr = 0.1, 2.0
+    phi, ng, _, _, _ = _species_fields(eps=eps)
+    got = physics.o2_alpha(phi, ng, eps, k_orr).cpu().numpy()
+    want = orc.o2_alpha(phi, ng, eps, k_orr)
+    inside = np.abs(phi) < eps
+    assert inside.sum() > 1000 and (~inside).sum() > 1000
+    assert np.all(got[~inside] == 0.0) and np.all(want[~inside] == 0.0)
+    # just inside the band edges 1 + cos(pi phi / eps) rounds to 0: non-negative, and
+    # positive almost everywhere
+    assert np.all(got[inside] >= 0.0) and (got[inside] > 0.0).mean() > 0.99
+    assert _close(got, want)
+
+
+def test_oh_source_matches_oracle(cuda_device):
+    from dissolve_tp import physics
+    eps, kd, k_orr = 0.1, 0.05, 2.0
+    phi, ng, F, Cl, O2 = _species_fields(eps=eps)
+    for fac in (4.0, 2.0):
+        got = physics.oh_source(phi, ng, F, Cl, O2, eps, kd, k_orr, fac).cpu().numpy()
+        want = orc.oh_source(phi, ng, F, Cl, O2, eps, kd, k_orr, fac)
+        assert _close(got, want)
+    # outside the band and outside the medium (phi > eps) nothing is produced
+    dry = phi >= eps
+    assert dry.sum() > 1000 and np.all(got[dry] == 0.0)
+    # inside the medium and outside the band: the film term alone
+    wet = phi <= -eps
+    assert np.allclose(got[wet], kd * F[wet] * Cl[wet] ** 2, rtol=1e-15, atol=0)
 
 
 def test_effective_diffusion_and_bounds(cuda_device):
