@@ -409,7 +409,11 @@ def kernel_table(m, coef, u0, flush):
     dev = torch.device("cuda", torch.cuda.current_device())
     dm = DeviceMesh(m.coords, m.cells)
     n, V, nnz = m.n_cells, m.n_verts, dm.nnz
-    st, tpm = stream_handle(), ctypes.byref(dm.tpm)
+    st = stream_handle()
+
+    class _Tpm:  # the mesh struct as it is at call time (set_tiles replaces it)
+        _as_parameter_ = property(lambda self: ctypes.byref(dm.tpm))
+    tpm = _Tpm()
     hbm = _peaks().get("hbm_gbs", 6650.0)
     De = torch.from_numpy(coef).to(dev)
     al = torch.full((n,), 0.5, dtype=torch.float64, device=dev)
@@ -441,6 +445,18 @@ def kernel_table(m, coef, u0, flush):
                               n * 28 + V * 48),
     }
     out = {}
+    # the row walk the tiled kernels replaced (same results), for comparison
+    rows_walk = {"assemble_full_fp64_row_walk": rows["assemble_full_fp64"],
+                 "assemble_stiffness_fp64_fp32_row_walk": rows["assemble_stiffness_fp64_fp32"]}
+    tile_rows = dm.tile_rows
+    dm.set_tiles(0)
+    for name, (fn, nbytes) in rows_walk.items():
+        ms = _event_ms(fn, 10, flush, torch)
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        out[name] = {"us": round(ms * 1e3, 1), "algorithmic_MB": round(nbytes / 1e6, 1),
+                     "GB_s": round(gbs, 1), "frac_hbm": round(gbs / hbm, 3)}
+    dm.set_tiles(tile_rows)
+    out["tiles"] = dm.tiles_info()
     for name, (fn, nbytes) in rows.items():
         ms = _event_ms(fn, 10, flush, torch)
         gbs = nbytes / (ms * 1e-3) / 1e9

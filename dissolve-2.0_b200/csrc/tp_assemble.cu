@@ -8,42 +8,13 @@
 // and -- because the walk follows cell order and every product/sum is rounded
 // separately (__dmul_rn/__dadd_rn, no FMA contraction) in the reference's operation
 // order -- equal to the reference kernel executed in cell order.
+#include <algorithm>
 #include <mutex>
 
-#include "tp_common.cuh"
+#include "tp_elem.cuh"
+#include "tp_tiles.cuh"
 
 namespace tp {
-
-struct GeoRec {
-  double G00, G01, G02, G11, G12, G22, dJ;
-};
-
-__device__ __forceinline__ GeoRec load_geo(const double* __restrict__ geo, int64_t c) {
-  const double4* g = reinterpret_cast<const double4*>(geo) + 2 * c;
-  const double4 a = ldg_d4(g), b = ldg_d4(g + 1);
-  return GeoRec{a.x, a.y, a.z, a.w, b.x, b.y, b.z};
-}
-
-// Row li of K / ((dJ De)/6), K_li,j for j = 0..3, in the reference's order
-// (gpu_assembler.py:108-119): with reference gradients g_0 = (-1,-1,-1), g_k = e_{k-1},
-// every product is exact and
-//   Gg_j[a] = -((G[a][0] + G[a][1]) + G[a][2])  (j = 0),   G[a][j-1]  (j > 0)
-//   K_ij    = -((Gg_j[0] + Gg_j[1]) + Gg_j[2])  (i = 0),   Gg_j[i-1]  (i > 0)
-// G is symmetric, so the column sums of the first row are the row sums
-// S[a] = (G[a][0] + G[a][1]) + G[a][2] (same operands, same order).  li is a runtime
-// value: the row comes from selects, not from an indexed array (which would live in
-// local memory).
-__device__ __forceinline__ void kref_row(int li, const GeoRec& g, double k[4]) {
-  const double S0 = __dadd_rn(__dadd_rn(g.G00, g.G01), g.G02);
-  const double S1 = __dadd_rn(__dadd_rn(g.G01, g.G11), g.G12);
-  const double S2 = __dadd_rn(__dadd_rn(g.G02, g.G12), g.G22);
-  const double T = __dadd_rn(__dadd_rn(S0, S1), S2);
-  const bool l0 = li == 0, l1 = li == 1, l2 = li == 2;
-  k[0] = l0 ? T : -(l1 ? S0 : (l2 ? S1 : S2));
-  k[1] = l0 ? -S0 : (l1 ? g.G00 : (l2 ? g.G01 : g.G02));
-  k[2] = l0 ? -S1 : (l1 ? g.G01 : (l2 ? g.G11 : g.G12));
-  k[3] = l0 ? -S2 : (l1 ? g.G02 : (l2 ? g.G12 : g.G22));
-}
 
 // ----------------------------------------------------------------- CSR assembly
 // Optional extras of the same row walk (the stiffness of the batched step): the per-column
@@ -136,16 +107,7 @@ __global__ void __launch_bounds__(128) k_assemble_rows(
         const double react = (MODE == TP_ASM_FULL) ? __dadd_rn(inv_dt, alv[u]) : 1.0;
 #pragma unroll
         for (int j = 0; j < 4; j++) {
-          double a = 0.0;
-          if (MODE != TP_ASM_MASS) a = __dmul_rn(kr[j], kscale);
-          if (MODE != TP_ASM_STIFF) {
-            double M;
-            if (lumped)
-              M = (li == j) ? __ddiv_rn(__dmul_rn(g.dJ, 5.0), 120.0) : 0.0;
-            else
-              M = __ddiv_rn(__dmul_rn(g.dJ, (li == j) ? 2.0 : 1.0), 120.0);
-            a = (MODE == TP_ASM_FULL) ? __dadd_rn(a, __dmul_rn(react, M)) : M;
-          }
+          const double a = elem_entry<MODE>(kr, li, j, g.dJ, kscale, react, lumped);
           const int slot = (sv[u] >> (8 * j)) & 0xff;
           if (slot < len) acc[slot * BS + tid] = __dadd_rn(acc[slot * BS + tid], a);
         }
@@ -203,6 +165,284 @@ __global__ void __launch_bounds__(128) k_assemble_rows(
         ex.sell32[base + k * 32 + ln] = f;
       }
     }
+  }
+}
+
+// ----------------------------------------------------------------- tiled CSR assembly
+// One CTA per row tile (tp_tiles.cu).  Phase A: the records of the tile's distinct cells
+// are copied into shared memory with asynchronous copies, all in flight together; each
+// cell's 10 upper-triangle entries (elem_entry, the reference's rounding) and, with DIAG,
+// its S lumped-diagonal terms replace its record in place (odd slot stride: the cells the
+// lanes of a warp read fall in different banks).  Phase B: each
+// tile row sums its diagonal over its cells in ascending order, each owned edge sums its
+// cells in ascending order, in registers, and writes (r, v) and (v, r) -- the same
+// ordered sums as the row walk of k_assemble_rows, bit for bit.
+constexpr int TILE_BLOCK = 256;
+
+// Shared-memory slot of one cell: ew doubles, ew = 10 or 14 (80 or 112 bytes: 5 or 7
+// sixteen-byte units, so 16-byte accesses of 8 consecutive slots fall in 8 different
+// bank groups).  First the raw record as copied -- the 64-byte geometry record
+// (G00 G01 G02 G11 G12 G22 |detJ| 0) at 0..7, De at 8, alpha at 9 or the DIAG alpha
+// columns at 9..9+ld-1 -- then, computed in place by one thread, the 10 upper-triangle
+// entries at 0..9 and, with DIAG, the S lumped-diagonal column terms at 10..10+S-1.
+__device__ __forceinline__ void lds2(const double* p, double& a, double& b) {
+  const double2 v = *reinterpret_cast<const double2*>(p);
+  a = v.x;
+  b = v.y;
+}
+__device__ __forceinline__ void sts2(double* p, double a, double b) {
+  *reinterpret_cast<double2*>(p) = make_double2(a, b);
+}
+
+template <int MODE, bool DIAG>
+__device__ __forceinline__ void tile_cell_entries(double* slot, bool has_alpha, double inv_dt,
+                                                  int lumped, const RowExtras& ex,
+                                                  const double dsh[4]) {
+  // the whole raw record first (the entries overwrite it)
+  double r[10];
+#pragma unroll
+  for (int k = 0; k < 5; k++) lds2(slot + 2 * k, r[2 * k], r[2 * k + 1]);
+  double alc[4] = {0.0, 0.0, 0.0, 0.0};
+  if constexpr (DIAG) {
+    if (ex.alpha) {
+      alc[0] = r[9];
+#pragma unroll
+      for (int s = 1; s < 4; s++)
+        if (s < ex.ld) alc[s] = slot[9 + s];
+    }
+  }
+  const GeoRec g{r[0], r[1], r[2], r[3], r[4], r[5], r[6]};
+  const double de = (MODE == TP_ASM_MASS) ? 0.0 : r[8];
+  const double al = (MODE == TP_ASM_FULL && has_alpha) ? r[9] : 0.0;
+  const double ks = (MODE == TP_ASM_MASS) ? 0.0 : __ddiv_rn(__dmul_rn(g.dJ, de), 6.0);
+  const double react = (MODE == TP_ASM_FULL) ? __dadd_rn(inv_dt, al) : 1.0;
+  double e[10];
+#pragma unroll
+  for (int li = 0; li < 4; li++) {
+    double kr[4];
+    kref_row(li, g, kr);
+#pragma unroll
+    for (int j = li; j < 4; j++)
+      e[tri_index(li, j)] = elem_entry<MODE>(kr, li, j, g.dJ, ks, react, lumped);
+  }
+#pragma unroll
+  for (int k = 0; k < 5; k++) sts2(slot + 2 * k, e[2 * k], e[2 * k + 1]);
+  if constexpr (DIAG) {
+    const double Ld = __dmul_rn(__ddiv_rn(g.dJ, 120.0), 5.0);
+    double dt[4];
+#pragma unroll
+    for (int s = 0; s < 4; s++)
+      dt[s] = (s < ex.S) ? __dmul_rn(__dadd_rn(dsh[s], alc[s]), Ld) : 0.0;
+    sts2(slot + 10, dt[0], dt[1]);
+    sts2(slot + 12, dt[2], dt[3]);
+  }
+}
+
+__device__ __forceinline__ void sell_put(const RowExtras& ex, int64_t row, int slot, float v) {
+  const int64_t sl = row >> 5;
+  ex.sell32[ex.slice_ptr[sl] + (int64_t)slot * 32 + (row & 31)] = v;
+}
+
+// term k (0..7) of 8 packed 16-bit terms
+__device__ __forceinline__ uint32_t term_of(const uint4& v, int k) {
+  const uint32_t w = (k < 2) ? v.x : (k < 4) ? v.y : (k < 6) ? v.z : v.w;
+  return (k & 1) ? (w >> 16) : (w & 0xffffu);
+}
+
+template <int MODE, bool DIAG>
+__global__ void __launch_bounds__(TILE_BLOCK, 3) k_assemble_tiles(
+    TileView tv, const double* __restrict__ geo, const double* __restrict__ De,
+    const double* __restrict__ alpha, double inv_dt, int lumped,
+    const uint8_t* __restrict__ bc_mask, const int32_t* __restrict__ indptr,
+    double* __restrict__ out64, float* __restrict__ out32, RowExtras ex, int ew, int64_t nv) {
+  extern __shared__ double sm_tiles[];
+  const int R = tv.R, T = blockDim.x;
+  const int t = blockIdx.x, tid = threadIdx.x;
+  const int c0 = __ldg(tv.cell_ptr + t), m = __ldg(tv.cell_ptr + t + 1) - c0;
+  double* E = sm_tiles;
+  const double dsh[4] = {ex.shift.x, ex.shift.y, ex.shift.z, ex.shift.w};
+  const uint4 none4 = make_uint4(0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu);
+
+  // ---- phase A: every record of the tile copied into shared memory at once: the ids
+  // first, then the 64-byte geometry records as 16-byte chunks (four lanes per record,
+  // consecutive records on consecutive lanes), De and alpha as 8-byte copies ...
+  {
+    constexpr int MAXC = 4;
+    const int lane = tid & 31;
+    int64_t cid[MAXC];
+#pragma unroll
+    for (int u = 0; u < MAXC; u++) {
+      const int i = tid + u * T;
+      cid[u] = (i < m) ? (int64_t)__ldg(tv.cells + c0 + i) : -1;
+    }
+#pragma unroll
+    for (int u = 0; u < MAXC; u++) {
+      const int ib = (tid & ~31) + u * T;  // the warp's first cell of this round
+      if (ib >= m) break;
+      const int h = lane & 3;
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const int j = (lane >> 2) + 8 * k;
+        const int64_t c = __shfl_sync(0xffffffffu, cid[u], j);
+        if (ib + j < m) cp_async<16>(E + (size_t)(ib + j) * ew + 2 * h, geo + 8 * c + 2 * h);
+      }
+      if (cid[u] >= 0) {
+        double* slot = E + (size_t)(ib + lane) * ew;
+        const int64_t c = cid[u];
+        if (MODE != TP_ASM_MASS) cp_async<8>(slot + 8, De + c);
+        if (MODE == TP_ASM_FULL && alpha) cp_async<8>(slot + 9, alpha + c);
+        if constexpr (DIAG) {
+          if (ex.alpha)
+            for (int s = 0; s < ex.ld; s++) cp_async<8>(slot + 9 + s, ex.alpha + c * ex.ld + s);
+        }
+      }
+    }
+    for (int i = tid + MAXC * T; i < m; i += T) {  // tiles of more than MAXC * T cells
+      const int64_t c = __ldg(tv.cells + c0 + i);
+      double* slot = E + (size_t)i * ew;
+#pragma unroll
+      for (int h = 0; h < 4; h++) cp_async<16>(slot + 2 * h, geo + 8 * c + 2 * h);
+      if (MODE != TP_ASM_MASS) cp_async<8>(slot + 8, De + c);
+      if (MODE == TP_ASM_FULL && alpha) cp_async<8>(slot + 9, alpha + c);
+      if constexpr (DIAG) {
+        if (ex.alpha)
+          for (int s = 0; s < ex.ld; s++) cp_async<8>(slot + 9 + s, ex.alpha + c * ex.ld + s);
+      }
+    }
+  }
+  // ... while they fly, the phase-B inputs of this thread: its row's first 24 diagonal
+  // terms and its first two edges with their first 8 terms ...
+  int64_t r = -1;
+  int pd = 0, KD = 0;
+  const uint4* dv = nullptr;
+  uint4 dq[3] = {none4, none4, none4};
+  if (tid < R) {
+    r = __ldg(tv.rows + (int64_t)t * R + tid);
+    pd = __ldg(tv.diag_pos + (int64_t)t * R + tid);
+    const int d0 = __ldg(tv.dterm_ptr + t);
+    KD = (__ldg(tv.dterm_ptr + t + 1) - d0) / R;
+    dv = reinterpret_cast<const uint4*>(tv.dterms + d0 + (int64_t)tid * KD);
+#pragma unroll
+    for (int u = 0; u < 3; u++)
+      if (8 * u < KD) dq[u] = __ldg(dv + u);
+  }
+  const int eb = __ldg(tv.edge_ptr + t), ne = __ldg(tv.edge_ptr + t + 1) - eb;
+  const int tb = __ldg(tv.eterm_ptr + t);
+  const int KE = ne ? (__ldg(tv.eterm_ptr + t + 1) - tb) / ne : 0;
+  // the diagonal threads take the last edges of a round, the others the first
+  const int q0 = (tid >= R) ? tid - R : T - R + tid;
+  int2 ep[2];
+  uint4 eq[2] = {none4, none4};
+#pragma unroll
+  for (int u = 0; u < 2; u++) {
+    const int q = q0 + u * T;
+    if (q < ne) {
+      ep[u] = __ldg(tv.edge_pos + eb + q);
+      eq[u] = __ldg(reinterpret_cast<const uint4*>(tv.eterms + tb + (int64_t)q * KE));
+    }
+  }
+  // ... and each thread turns the records it copied into element entries in place
+  cp_async_wait_all();
+  for (int i = tid; i < m; i += T)
+    tile_cell_entries<MODE, DIAG>(E + (size_t)i * ew, alpha != nullptr, inv_dt, lumped, ex, dsh);
+  __syncthreads();
+
+  // ---- phase B1: the diagonal of each tile row
+  if (tid < R && r >= 0) {
+    const bool is_bc = bc_mask && bc_mask[r];
+    double dacc = 0.0, dg[4] = {0.0, 0.0, 0.0, 0.0};
+    if (!is_bc) {
+      auto group = [&](const uint4& g8) -> bool {
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          const uint32_t tm = term_of(g8, k);
+          if (tm == TILE_TERM_NONE) return false;
+          const int loc = tm & ((1 << TILE_LOC_BITS) - 1), li = tm >> TILE_LOC_BITS;
+          const double* e = E + (size_t)loc * ew;
+          dacc = __dadd_rn(dacc, e[tri_index(li, li)]);
+          if constexpr (DIAG) {
+#pragma unroll
+            for (int s = 0; s < 4; s++)
+              if (s < ex.S) dg[s] = __dadd_rn(dg[s], e[10 + s]);
+          }
+        }
+        return true;
+      };
+      bool more = group(dq[0]) && group(dq[1]) && group(dq[2]);
+      for (int g = 3; more && 8 * g < KD; g++) more = group(__ldg(dv + g));
+    }
+    const double v = is_bc ? 1.0 : dacc;
+    if (out64) out64[pd] = v;
+    if (out32) out32[pd] = (float)v;
+    if (ex.sell32) {
+      // the diagonal, then the row's padding entries of its SELL-32 slice
+      const int p0 = __ldg(indptr + r), len = __ldg(indptr + r + 1) - p0;
+      const int64_t sl = r >> 5;
+      const int base = ex.slice_ptr[sl], width = (ex.slice_ptr[sl + 1] - base) >> 5;
+      float* col = ex.sell32 + base + (r & 31);
+      col[(int64_t)(pd - p0) * 32] = (float)v;
+      for (int k = len; k < width; k++) col[(int64_t)k * 32] = 0.f;
+    }
+    if constexpr (DIAG) {
+#pragma unroll
+      for (int s = 0; s < 4; s++) {
+        if (s < ex.ld) {
+          const double dv2 = is_bc ? 1.0 : (s < ex.S ? dg[s] : 0.0);
+          if (ex.d64) ex.d64[r * ex.ld + s] = dv2;
+          if (ex.d32) ex.d32[r * ex.ld + s] = (float)dv2;
+        }
+      }
+    }
+  }
+
+  // ---- phase B2: the tile's edges, (r, v) and (v, r) from one ordered sum
+  auto edge = [&](int q, int2 pp, const uint4& g0) {
+    double acc = 0.0;
+    auto group = [&](const uint4& g8) -> bool {
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        const uint32_t tm = term_of(g8, k);
+        if (tm == TILE_TERM_NONE) return false;
+        const int loc = tm & ((1 << TILE_LOC_BITS) - 1), tq = tm >> TILE_LOC_BITS;
+        acc = __dadd_rn(acc, E[(size_t)loc * ew + tq]);
+      }
+      return true;
+    };
+    bool more = group(g0);
+    for (int g = 1; more && 8 * g < KE; g++)
+      more = group(__ldg(reinterpret_cast<const uint4*>(tv.eterms + tb + (int64_t)q * KE) + g));
+    double a_rv = acc, a_vr = acc;
+    if (bc_mask || ex.sell32) {
+      const int2 rv = __ldg(tv.edge_rv + eb + q);
+      if (bc_mask) {
+        if (bc_mask[rv.x]) a_rv = 0.0;
+        if (bc_mask[rv.y]) a_vr = 0.0;
+      }
+      if (ex.sell32) {
+        sell_put(ex, rv.x, pp.x - __ldg(indptr + rv.x), (float)a_rv);
+        sell_put(ex, rv.y, pp.y - __ldg(indptr + rv.y), (float)a_vr);
+      }
+    }
+    if (out64) {
+      out64[pp.x] = a_rv;
+      out64[pp.y] = a_vr;
+    }
+    if (out32) {
+      out32[pp.x] = (float)a_rv;
+      out32[pp.y] = (float)a_vr;
+    }
+  };
+  if (q0 < ne) edge(q0, ep[0], eq[0]);
+  if (q0 + T < ne) edge(q0 + T, ep[1], eq[1]);
+  for (int q = q0 + 2 * T; q < ne; q += T)
+    edge(q, __ldg(tv.edge_pos + eb + q),
+         __ldg(reinterpret_cast<const uint4*>(tv.eterms + tb + (int64_t)q * KE)));
+  if (ex.sell32 && t == 0 && (nv & 31)) {
+    // the lanes of the last slice past the last row: padding, 0
+    const int64_t sl = nv >> 5;
+    const int base = ex.slice_ptr[sl], width = (ex.slice_ptr[sl + 1] - base) >> 5;
+    for (int q = tid; q < width * 32; q += T)
+      if ((q & 31) >= (nv & 31)) ex.sell32[base + q] = 0.f;
   }
 }
 
@@ -772,6 +1012,30 @@ extern "C" int tp_bc_mask(int64_t n_bc, const int32_t* bc_dofs, int64_t n_verts,
   return TP_OK;
 }
 
+template <int MODE, bool DIAG>
+static int launch_tiles(const tp_mesh* m, const double* De, const double* alpha, double inv_dt,
+                        int lumped, const uint8_t* bc_mask, double* out64, float* out32,
+                        const RowExtras& ex, cudaStream_t st, bool* used) {
+  *used = false;
+  if (!m->tiles) return TP_OK;
+  const TileView& tv = m->tiles->v;
+  // slot of 5 or 7 sixteen-byte units (tile_cell_entries)
+  const int ew = DIAG ? 14 : 10;
+  const size_t smem = sizeof(double) * (size_t)tv.max_cells * ew;
+  int dev = 0, optin = 0;
+  TP_CUDA_TRY(cudaGetDevice(&dev));
+  TP_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  if (smem > (size_t)optin || tv.R > TILE_BLOCK || tv.n_tiles == 0) return TP_OK;
+  auto fn = k_assemble_tiles<MODE, DIAG>;
+  if (smem > 48 * 1024)
+    TP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  fn<<<tv.n_tiles, TILE_BLOCK, smem, st>>>(tv, m->geo, De, alpha, inv_dt, lumped, bc_mask,
+                                           m->indptr, out64, out32, ex, ew, m->n_verts);
+  TP_LAUNCH_CHECK();
+  *used = true;
+  return TP_OK;
+}
+
 extern "C" int tp_assemble_csr(const tp_mesh* m, const double* De_cell, const double* alpha_cell,
                                double inv_dt, int lumped, int mode, const uint8_t* bc_mask,
                                double* out64, float* out32, void* stream) {
@@ -784,6 +1048,20 @@ extern "C" int tp_assemble_csr(const tp_mesh* m, const double* De_cell, const do
   const size_t smem = sizeof(double) * 129 * (size_t)m->max_row_len;
   const int grid = grid_for(m->n_verts, 128);
   const RowExtras ex{};
+  {
+    bool used = false;
+    int rc = TP_OK;
+    if (mode == TP_ASM_FULL)
+      rc = launch_tiles<TP_ASM_FULL, false>(m, De_cell, alpha_cell, inv_dt, lumped, bc_mask,
+                                            out64, out32, ex, st, &used);
+    else if (mode == TP_ASM_STIFF)
+      rc = launch_tiles<TP_ASM_STIFF, false>(m, De_cell, alpha_cell, inv_dt, lumped, bc_mask,
+                                             out64, out32, ex, st, &used);
+    else if (mode == TP_ASM_MASS)
+      rc = launch_tiles<TP_ASM_MASS, false>(m, De_cell, alpha_cell, inv_dt, lumped, bc_mask,
+                                            out64, out32, ex, st, &used);
+    if (rc != TP_OK || used) return rc;
+  }
 #define TP_ASM_LAUNCH(MD)                                                                 \
   do {                                                                                    \
     if (smem > 48 * 1024)                                                                 \
@@ -857,6 +1135,12 @@ extern "C" int tp_assemble_stiffness_diag(const tp_mesh* m, const double* De_cel
   for (int s = 0; s < S; s++) sh[s] = shift ? shift[s] : 0.0;
   RowExtras ex{S, ld, alpha, make_double4(sh[0], sh[1], sh[2], sh[3]), diag64, diag32,
                slice_ptr, sell32};
+  {
+    bool used = false;
+    const int rc = launch_tiles<TP_ASM_STIFF, true>(m, De_cell, nullptr, 0.0, 1, bc_mask, out64,
+                                                    out32, ex, st, &used);
+    if (rc != TP_OK || used) return rc;
+  }
   const size_t smem = sizeof(double) * 129 * (size_t)m->max_row_len;
   const int grid = grid_for(m->n_verts, 128);
   if (smem > 48 * 1024)

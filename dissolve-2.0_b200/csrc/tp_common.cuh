@@ -92,6 +92,21 @@ __device__ __forceinline__ double4 ldg_d4(const double4* p) {
   return v;
 }
 
+// asynchronous global -> shared copy of NB bytes (4, 8 or 16; both addresses NB-aligned)
+template <int NB>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  if constexpr (NB == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(sa), "l"(gmem), "n"(NB)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 template <typename T>
 struct vec_of;
 template <>

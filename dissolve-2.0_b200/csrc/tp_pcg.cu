@@ -921,20 +921,6 @@ __device__ void write_result(const PArgs<VT>& a, LaneState& L, bool ok2, const d
   a.out->timeouts = ok2 ? 0 : 1;
 }
 
-template <int NB>
-__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  if constexpr (NB == 16)
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
-  else
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(sa), "l"(gmem), "n"(NB)
-                 : "memory");
-}
-
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
-}
-
 template <typename VT, int LD, int U, bool HASM>
 __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
   // dynamic shared memory: slice offsets (sp_cap), halo list (halo_cap), window-local

@@ -45,7 +45,8 @@ class TpMesh(ctypes.Structure):
     _fields_ = [("n_cells", _c_i64), ("n_verts", _c_i64), ("nnz", _c_i64),
                 ("max_row_len", _c_i32), ("max_degree", _c_i32),
                 ("cells", _vp), ("coords4", _vp), ("geo", _vp), ("v2c_ptr", _vp),
-                ("v2c", _vp), ("v2c_slots", _vp), ("indptr", _vp), ("indices", _vp)]
+                ("v2c", _vp), ("v2c_slots", _vp), ("indptr", _vp), ("indices", _vp),
+                ("tiles", _vp)]
 
 
 class TpCsrOp(ctypes.Structure):
@@ -162,6 +163,10 @@ SIGNATURES = {
     "tp_pcg_grid": (ctypes.c_int, [_vp, _P(ctypes.c_int), _P(ctypes.c_int)]),
     "tp_pcg_engine": (ctypes.c_int, [_vp, _P(ctypes.c_int), _P(ctypes.c_size_t)]),
     "tp_pcg_set_profile": (ctypes.c_int, [_vp, _vp]),
+    "tp_tiles_create": (ctypes.c_int, [_P(TpMesh), ctypes.c_int, _vp, _P(_vp)]),
+    "tp_tiles_info": (ctypes.c_int, [_vp, _P(_c_i32), _P(_c_i32), _P(_c_i32), _P(_c_i64),
+                                     _P(ctypes.c_size_t)]),
+    "tp_tiles_destroy": (ctypes.c_int, [_vp]),
     "tp_pcg_set_wait_limit": (ctypes.c_int, [_vp, ctypes.c_ulonglong, ctypes.c_uint]),
     "tp_pcg_destroy": (ctypes.c_int, [_vp]),
     "tp_mlp_param_count": (ctypes.c_int, []),

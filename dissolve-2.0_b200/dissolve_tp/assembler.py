@@ -53,10 +53,15 @@ def extract_mesh(domain, V=None):
     return np.ascontiguousarray(coords, dtype=np.float64), np.ascontiguousarray(elem)
 
 
+# rows per tile of the tiled kernels (tp_tiles_create); 0 keeps the row walk
+TILE_ROWS = int(os.environ.get("DISSOLVE_TILE_ROWS", "64"))
+
+
 class DeviceMesh:
     """Mesh state resident on the GPU, built by the setup kernels."""
 
-    def __init__(self, coords: np.ndarray, cells: np.ndarray, device=None):
+    def __init__(self, coords: np.ndarray, cells: np.ndarray, device=None,
+                 tile_rows: int | None = None):
         self.device = device or require_cuda()
         dev = self.device
         coords = np.ascontiguousarray(coords, dtype=np.float64)
@@ -96,9 +101,46 @@ class DeviceMesh:
         self.slots = torch.empty(max(4 * self.n_cells, 1), dtype=torch.int32, device=dev)
         self.tpm = self._struct()
         call("tp_incidence_slots", _lib.ctypes.byref(self.tpm), ptr(self.slots), ptr(self.flags), st)
+        self._tiles = None
+        self.tile_rows = TILE_ROWS if tile_rows is None else int(tile_rows)
         self.tpm = self._struct()
+        if self.tile_rows > 0 and self.n_verts > 0:
+            self.set_tiles(self.tile_rows)
         self._ref_geom = None
         self._scatter_map = None
+
+    def set_tiles(self, rows_per_tile: int):
+        """Row tiles for the tiled kernels (0: none, the kernels walk rows); same results."""
+        self._free_tiles()
+        self.tile_rows = int(rows_per_tile)
+        if self.tile_rows > 0:
+            h = _lib.ctypes.c_void_p()
+            call("tp_tiles_create", _lib.ctypes.byref(self.tpm), self.tile_rows, stream_handle(),
+                 _lib.ctypes.byref(h))
+            self._tiles = h
+        self.tpm = self._struct()
+
+    def tiles_info(self) -> dict:
+        if self._tiles is None:
+            return {}
+        c = _lib.ctypes
+        nt, r, mc = _lib._c_i32(0), _lib._c_i32(0), _lib._c_i32(0)
+        ne, nb = _lib._c_i64(0), c.c_size_t(0)
+        call("tp_tiles_info", self._tiles, c.byref(nt), c.byref(r), c.byref(mc), c.byref(ne),
+             c.byref(nb))
+        return {"n_tiles": nt.value, "rows_per_tile": r.value, "max_cells": mc.value,
+                "entries": ne.value, "bytes": nb.value}
+
+    def _free_tiles(self):
+        if getattr(self, "_tiles", None) is not None:
+            _lib.lib.tp_tiles_destroy(self._tiles)
+            self._tiles = None
+
+    def __del__(self):
+        try:
+            self._free_tiles()
+        except Exception:
+            pass
 
     def _struct(self) -> TpMesh:
         return TpMesh(self.n_cells, self.n_verts, getattr(self, "nnz", 0),
@@ -106,7 +148,8 @@ class DeviceMesh:
                       ptr(self.cells), ptr(self.coords4), ptr(self.geo),
                       ptr(self.v2c_ptr), ptr(self.v2c),
                       ptr(getattr(self, "slots", None)), ptr(self.indptr),
-                      ptr(getattr(self, "indices", None)))
+                      ptr(getattr(self, "indices", None)),
+                      getattr(getattr(self, "_tiles", None), "value", None))
 
     @property
     def ref_geometry(self):

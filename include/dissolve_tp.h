@@ -58,6 +58,10 @@ TP_API const char* tp_last_error(void);
 TP_API int tp_device_sm_count(void);
 
 /* ------------------------------------------------------------------ mesh on device */
+/* Row tiles of a mesh (opaque; tp_tiles_create).  No reference counterpart: the tables
+ * that let the row-owned kernels load every cell record of a group of nearby rows once. */
+typedef struct tp_tiles tp_tiles;
+
 /* Device-resident mesh: the state GPUSparseAssembler keeps between calls
  * (gpu_assembler.py:323-326, 350-367).  Built once by the setup calls below. */
 typedef struct tp_mesh {
@@ -75,6 +79,8 @@ typedef struct tp_mesh {
                                  byte j = slot of vertex j in the incidence row      */
   const int32_t* indptr;      /* (n_verts + 1) CSR row offsets                       */
   const int32_t* indices;     /* (nnz) sorted column ids                             */
+  const tp_tiles* tiles;      /* row tiles (tp_tiles_create) or NULL: the kernels that
+                                 have a tiled form use it when set (same results)     */
 } tp_mesh;
 
 /* [sync] Per-cell geometry of gpu_assembler.py:380-393: J = [x1-x0 | x2-x0 | x3-x0],
@@ -117,6 +123,19 @@ TP_API int tp_scatter_map(int64_t n_cells, const int32_t* cells, const int32_t* 
  * the element-to-nonzero map the atomics-free row assembly reads instead of the
  * reference's scatter_map + atomicAdd). */
 TP_API int tp_incidence_slots(const tp_mesh* m, uint32_t* slots, int32_t* flags_dev, void* stream);
+
+/* [sync] Row tiles for the tiled kernels (no reference counterpart): the rows are cut by
+ * recursive coordinate bisection into tiles of rows_per_tile (64) nearby rows; per tile
+ * the ascending list of the distinct cells its rows touch and, per incidence entry of its
+ * rows (row-major [entry k][row]), the cell's tile-local index, the row's local vertex
+ * and the four CSR slots of tp_incidence_slots.  Needs a complete mesh (coords4, v2c,
+ * v2c_slots, indptr); built on the host from copies of those arrays, device tables owned
+ * by the returned handle.  TP_ERR_CAPACITY if a tile touches more than 16383 cells. */
+TP_API int tp_tiles_create(const tp_mesh* m, int rows_per_tile, void* stream, tp_tiles** out);
+/* size of the tiling (any pointer may be NULL) */
+TP_API int tp_tiles_info(const tp_tiles* t, int32_t* n_tiles, int32_t* rows_per_tile,
+                         int32_t* max_cells, int64_t* n_entries, size_t* device_bytes);
+TP_API int tp_tiles_destroy(tp_tiles* t);
 
 /* ------------------------------------------------------------------ per-step kernels */
 /* gpu_assembler.py:452-470 (_to_cell_avg, per-vertex branch): mean of 4 vertex values */

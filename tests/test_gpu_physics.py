@@ -34,8 +34,9 @@ def _species_fields(n=20000, eps=0.1):
 
 
 def _close(got, want, rel=1e-14):
-    scale = np.maximum(np.abs(want), 1e-300)
-    return np.all((got == want) | (np.abs(got - want) <= rel * scale))
+    """Within rel of each value, or of the largest value where 1 + cos(pi phi / eps)
+    cancels near the band edges (there one ulp of cos is a large relative change)."""
+    return np.all(np.abs(got - want) <= rel * (np.abs(want) + 0.1 * np.abs(want).max()))
 
 
 def test_o2_alpha_matches_oracle(cuda_device):
