@@ -592,6 +592,79 @@ __global__ void k_rhs_rows(int64_t nv, int S, int ld, const int32_t* __restrict_
   }
 }
 
+// Lumped right-hand side on row tiles: the tile's cells' lumped-mass factors
+// Ld = (|detJ| / 120) 5 in shared memory, then each tile row sums Ld (inv_dt u + f) over its
+// cells in ascending order -- the same ordered sums as k_rhs_rows (lumped branch).
+__global__ void __launch_bounds__(256) k_rhs_tiles(TileView tv, int S, int ld,
+                                                   const double* __restrict__ geo,
+                                                   const double* __restrict__ u,
+                                                   const double* __restrict__ f, double inv_dt,
+                                                   double* __restrict__ b) {
+  extern __shared__ double sm_ld[];
+  const int R = tv.R, T = blockDim.x, t = blockIdx.x, tid = threadIdx.x;
+  const int c0 = __ldg(tv.cell_ptr + t), m = __ldg(tv.cell_ptr + t + 1) - c0;
+  {
+    constexpr int MAXC = 4;
+    int64_t cid[MAXC];
+    double dj[MAXC];
+#pragma unroll
+    for (int k = 0; k < MAXC; k++) {
+      const int i = tid + k * T;
+      cid[k] = (i < m) ? (int64_t)__ldg(tv.cells + c0 + i) : -1;
+    }
+#pragma unroll
+    for (int k = 0; k < MAXC; k++) dj[k] = (cid[k] >= 0) ? __ldg(geo + 8 * cid[k] + 6) : 0.0;
+#pragma unroll
+    for (int k = 0; k < MAXC; k++)
+      if (cid[k] >= 0) sm_ld[tid + k * T] = __dmul_rn(__ddiv_rn(dj[k], 120.0), 5.0);
+    for (int i = tid + MAXC * T; i < m; i += T)
+      sm_ld[i] = __dmul_rn(__ddiv_rn(__ldg(geo + 8 * (int64_t)__ldg(tv.cells + c0 + i) + 6), 120.0), 5.0);
+  }
+  // the row's first 24 terms and its u, f are loaded before the barrier (in flight with
+  // the loads above)
+  int64_t r = -1;
+  double w[4] = {0.0, 0.0, 0.0, 0.0};
+  const uint4* dv = nullptr;
+  int KD = 0;
+  const uint4 none4 = make_uint4(0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu);
+  uint4 dq[3] = {none4, none4, none4};
+  if (tid < R) {
+    r = __ldg(tv.rows + (int64_t)t * R + tid);
+    const int d0 = __ldg(tv.dterm_ptr + t);
+    KD = (__ldg(tv.dterm_ptr + t + 1) - d0) / R;
+    dv = reinterpret_cast<const uint4*>(tv.dterms + d0 + (int64_t)tid * KD);
+#pragma unroll
+    for (int g = 0; g < 3; g++)
+      if (8 * g < KD) dq[g] = __ldg(dv + g);
+    if (r >= 0) {
+#pragma unroll
+      for (int s = 0; s < 4; s++)
+        if (s < S)
+          w[s] = __dadd_rn(__dmul_rn(inv_dt, u[r * ld + s]), f ? f[r * ld + s] : 0.0);
+    }
+  }
+  __syncthreads();
+  if (r < 0) return;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  auto group = [&](const uint4& g8) -> bool {
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const uint32_t tm = term_of(g8, k);
+      if (tm == TILE_TERM_NONE) return false;
+      const double Ld = sm_ld[tm & ((1 << TILE_LOC_BITS) - 1)];
+#pragma unroll
+      for (int s = 0; s < 4; s++)
+        if (s < S) acc[s] = __dadd_rn(acc[s], __dmul_rn(Ld, w[s]));
+    }
+    return true;
+  };
+  bool more = group(dq[0]) && group(dq[1]) && group(dq[2]);
+  for (int g = 3; more && 8 * g < KD; g++) more = group(__ldg(dv + g));
+#pragma unroll
+  for (int s = 0; s < 4; s++)
+    if (s < ld) b[r * ld + s] = (s < S) ? acc[s] : 0.0;
+}
+
 // lumped right-hand side from the per-vertex lumped mass: b = m (inv_dt u + f) per column
 __global__ void k_lumped_rhs(int64_t nv, int S, int ld, const double* __restrict__ mass,
                              const double* __restrict__ u, const double* __restrict__ f,
@@ -1160,7 +1233,16 @@ extern "C" int tp_assemble_rhs(const tp_mesh* m, int S, int ld, const double* u_
   TP_REQUIRE(mesh_ok(m) && u_old && b, "null pointer");
   TP_REQUIRE(S >= 1 && S <= TP_MAX_COLS && ld >= S && ld <= TP_MAX_COLS, "bad S/ld");
   cudaStream_t st = as_stream(stream);
-  if (m->n_verts > 0) {
+  if (m->n_verts > 0 && lumped && m->tiles && m->tiles->v.n_tiles > 0 &&
+      m->tiles->v.R <= 256) {
+    const TileView& tv = m->tiles->v;
+    const size_t smem = sizeof(double) * (size_t)std::max(tv.max_cells, 1);
+    if (smem > 48 * 1024)
+      TP_CUDA_TRY(cudaFuncSetAttribute(k_rhs_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+    k_rhs_tiles<<<tv.n_tiles, 256, smem, st>>>(tv, S, ld, m->geo, u_old, f, inv_dt, b);
+    TP_LAUNCH_CHECK();
+  } else if (m->n_verts > 0) {
     k_rhs_rows<<<grid_for(m->n_verts, 128, 65535), 128, 0, st>>>(
         m->n_verts, S, ld, m->cells, m->v2c_ptr, m->v2c, m->geo, u_old, f, inv_dt, lumped, b);
     TP_LAUNCH_CHECK();

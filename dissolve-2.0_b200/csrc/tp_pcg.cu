@@ -92,6 +92,7 @@ struct PArgs {
   int sp_cap, halo_cap, col_cap;  // shared-memory capacities (entries)
   int win_cap;                    // window entries (own rows + halo) of the largest CTA
   int reg_values;                 // every slice at most 16 wide: values via registers
+  int tmem_values;                // FP32 values resident in tensor memory for the solve
   double* part;  // gridDim.x * 16
   PBar* bar;
   POut* out;
@@ -921,6 +922,56 @@ __device__ void write_result(const PArgs<VT>& a, LaneState& L, bool ok2, const d
   a.out->timeouts = ok2 ? 0 : 1;
 }
 
+// Tensor memory (256 KB per SM) as an on-chip home for the operator values of a solve:
+// one warp allocates, every warp stores the values of its slices into its own lane
+// quarter (warp w reaches lanes 32 (w % 4) .. 32 (w % 4) + 31: one lane per row of a
+// 32-row slice) and reads them back with one 16-column load per slice per product.
+__device__ __forceinline__ void tm_alloc(uint32_t* slot, uint32_t ncols) {
+  const uint32_t sa = (uint32_t)__cvta_generic_to_shared(slot);
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sa),
+               "r"(ncols));
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+}
+__device__ __forceinline__ void tm_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols));
+}
+__device__ __forceinline__ void tm_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tm_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tm_st16(uint32_t taddr, const uint32_t v[16]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
+      "%13,%14,%15,%16};" ::"r"(taddr),
+      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]),
+      "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]),
+      "r"(v[15])
+      : "memory");
+}
+__device__ __forceinline__ void tm_wait_st() {
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+// 16 consecutive 32-bit columns of this thread's lane; complete after tm_wait_ld()
+__device__ __forceinline__ void tm_ld16(uint32_t taddr, float v[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+#pragma unroll
+  for (int k = 0; k < 16; k++) v[k] = __uint_as_float(r[k]);
+}
+__device__ __forceinline__ void tm_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+constexpr uint32_t TM_COLS = 256;  // 4 column blocks of 64: warps w and w + 4k share lanes
+
 template <typename VT, int LD, int U, bool HASM>
 __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
   // dynamic shared memory: slice offsets (sp_cap), halo list (halo_cap), window-local
@@ -964,6 +1015,38 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
       for (int i = threadIdx.x; i < ne / 8; i += blockDim.x) dst[i] = src[i];
     }
   }
+  // FP32 values into tensor memory (the host enables this only for 16 warps, slices of at
+  // most 16 entries and at most MAXS slices per warp): warp w, its j-th slice sb + w + 16 j
+  // at lanes 32 (w % 4).., columns 64 (w / 4) + 16 j
+  __shared__ uint32_t s_taddr;
+  uint32_t tm_warp = 0;
+  const bool use_tm = sizeof(VT) == 4 && !HASM && a.tmem_values;
+  if (use_tm) {
+    if (warp == 0) tm_alloc(&s_taddr, TM_COLS);
+    tm_fence_before();
+    __syncthreads();
+    tm_fence_after();
+    tm_warp = s_taddr + ((uint32_t)(32 * (warp & 3)) << 16) + 64u * (uint32_t)(warp >> 2);
+#pragma unroll
+    for (int j = 0; j < MAXS; j++) {
+      const int sl = sb + warp + j * nwarps;
+      uint32_t v[16];
+      const int base = (sl < se) ? a.slice_ptr[sl] : 0;
+      const int w = (sl < se) ? (a.slice_ptr[sl + 1] - base) >> 5 : 0;
+#pragma unroll
+      for (int k = 0; k < 16; k++)
+        v[k] = (k < w) ? __float_as_uint((float)ld_na(a.sK + base + k * 32 + lane)) : 0u;
+      tm_st16(tm_warp + 16u * (uint32_t)j, v);
+    }
+    tm_wait_st();
+  }
+  auto tm_release = [&]() {
+    if (use_tm) {
+      tm_fence_before();
+      __syncthreads();
+      if (warp == 0) tm_dealloc(s_taddr, TM_COLS);
+    }
+  };
 
 #define FOR_OWN_ROWS                                              \
   for (int sl = sb + warp; sl < se; sl += nwarps)                 \
@@ -1011,8 +1094,18 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
       for (int slb = sb + warp; slb < se; slb += MAXS * nwarps) {
         VT vals[MAXS][WMAX];
         VT mvals[HASM ? MAXS : 1][HASM ? WMAX : 1];
+        if constexpr (sizeof(VT) == 4 && !HASM && WMAX == 16) {
+          if (use_tm) {
+            // one round per warp (slb == sb + warp): the values of its slices, on chip
+#pragma unroll
+            for (int j = 0; j < MAXS; j++)
+              tm_ld16(tm_warp + 16u * (uint32_t)j, reinterpret_cast<float*>(vals[j]));
+            tm_wait_ld();
+          }
+        }
 #pragma unroll
         for (int j = 0; j < MAXS; j++) {
+          if (use_tm) break;
           const int sl = slb + j * nwarps;
           const int base = (sl < se) ? s_sp[sl - sb] : 0;
           const int w = (sl < se) ? (s_sp[sl - sb + 1] - base) >> 5 : 0;
@@ -1544,6 +1637,7 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
       for (int k = 0; k < 8; k++) a.prof[blockIdx.x * 8 + k] = clk.acc[k];
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) write_result(a, L, true, s_tot, it, n_rel, false);
+    tm_release();
     return;
   }
   FOR_OWN_ROWS {
@@ -1584,6 +1678,7 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
     for (int k = 0; k < 8; k++) a.prof[blockIdx.x * 8 + k] = clk.acc[k];
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) write_result(a, L, ok2, s_tot, it, n_rel);
+  tm_release();
 #undef FOR_OWN_ROWS
 }
 
@@ -1790,6 +1885,7 @@ static void fill_pargs(PArgs<VT>& a, const tp_csr_op* op, const tp_sell* sl, con
   a.loc_col = nullptr;
   a.sp_cap = a.halo_cap = a.col_cap = a.win_cap = 0;
   a.reg_values = 0;
+  a.tmem_values = 0;
   a.wait_limit_ns = WAIT_LIMIT_NS;
   a.wait_missing = 0;
   a.part = reinterpret_cast<double*>(p);
@@ -1921,6 +2017,11 @@ extern "C" size_t tp_pcg_workspace_bytes(const tp_csr_op* op, int inner_fp32) {
          a256(sizeof(PBar)) + a256(sizeof(POut));
 }
 
+static int getenv_flag(const char* name, int dflt) {
+  const char* v = getenv(name);
+  return v ? atoi(v) : dflt;
+}
+
 // Window engine for a one-CTA-per-SM grid when its tables and window fit in shared
 // memory; leaves h on the streaming engine otherwise.  DISSOLVE_PCG_ENGINE=stream at
 // create keeps the streaming engine.
@@ -1968,6 +2069,14 @@ static int try_window(tp_pcg_handle* h, const tp_sell* sell, bool hasM, cudaStre
     a.col_cap = w.col_cap;
     a.win_cap = w.win_cap;
     a.reg_values = w.max_width <= 16 ? 1 : 0;  // the kernel's register-staging width
+    // FP32 values in tensor memory: 16 warps, one round of at most 4 slices per warp
+    // (k_cgw's MAXS for FP32 without a mass matrix), slices of at most 16 entries
+    const int ns = (int)((sell->n_rows + 31) / 32);
+    const int max_sl = (ns + h->grid - 1) / h->grid;
+    a.tmem_values = (h->fp32 && !hasM && h->block == 512 && a.reg_values && max_sl <= 64 &&
+                     getenv_flag("DISSOLVE_PCG_TMEM", 1))
+                        ? 1
+                        : 0;
   };
   if (h->fp32)
     set(h->af);

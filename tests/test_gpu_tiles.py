@@ -101,3 +101,28 @@ def test_tiled_stiffness_diag_equals_row_walk(mesh, S):
         outs.append([t.cpu().numpy() for t in (o64, o32, s32, d64, d32)])
     for a, b in zip(*outs):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("S,ld,with_f", [(1, 1, False), (3, 4, True), (2, 2, True)])
+def test_tiled_lumped_rhs_equals_row_walk(mesh, S, ld, with_f):
+    import torch
+
+    from dissolve_tp import _lib
+    from dissolve_tp.assembler import DeviceMesh
+    from dissolve_tp.device import ptr, stream_handle
+    dev = torch.device("cuda")
+    dm = DeviceMesh(mesh.coords, mesh.cells, tile_rows=0)
+    rng = np.random.default_rng(6)
+    u = torch.from_numpy(rng.uniform(0, 1, (dm.n_verts, ld))).to(dev)
+    f = torch.from_numpy(rng.normal(0, 1, (dm.n_verts, ld))).to(dev) if with_f else None
+    bc = np.arange(0, dm.n_verts, 13, dtype=np.int32)
+    bcd = torch.from_numpy(bc).to(dev)
+    vals = (ctypes.c_double * 4)(0.5, 1.5, 2.5, 3.5)
+    outs = []
+    for tiles in (0, 64):
+        dm.set_tiles(tiles)
+        b = torch.full((dm.n_verts, ld), -7.0, dtype=torch.float64, device=dev)
+        _lib.call("tp_assemble_rhs", ctypes.byref(dm.tpm), S, ld, ptr(u), ptr(f), 50.0, 1,
+                  bc.size, ptr(bcd), vals, ptr(b), stream_handle())
+        outs.append(b.cpu().numpy())
+    assert np.array_equal(outs[0], outs[1])
