@@ -317,6 +317,7 @@ def run_ours(args, rank, world, local_rank):
         uf = fast.state()
         rel = float(np.linalg.norm(uf - up) / np.linalg.norm(up))
         forms = {
+            "guess_ablation": guess_ablation(fast, u0, args, flush, torch) if learned else None,
             "plain_fp64": {"steps_per_s": args.steps / (sum(p_ms) / 1e3),
                            "ms_per_step": sum(p_ms) / args.steps,
                            "iterations_per_species": p_it[-1]},
@@ -378,6 +379,46 @@ def run_ours(args, rank, world, local_rank):
             gyroid=parity_inputs.get("gyroid_48"))
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def guess_ablation(fast, u0, args, flush, torch):
+    """The same W + K steps from u0 with each initial guess of the fast form: the previous
+    step u^n (the reference's, numerics/solvers.py:367), linear extrapolation
+    2 u^n - u^{n-1}, the energy-norm projection over the last five step increments alone,
+    that projection with the network's correction added as one more direction (the
+    shipped learned guess) and the network alone (u^n + sigma y).  CG iterations and
+    CUDA-event time per step over the K timed steps."""
+    pred = fast.predictor
+    modes = [("previous", "previous", True), ("extrapolate", "extrapolate", True),
+             ("projection_only", "project", True), ("projection_and_network", "learned", True),
+             ("network_only", "learned", False)]
+    out = {}
+    saved = (fast.guess, pred.project, pred.launches)
+    try:
+        for name, guess, proj in modes:
+            fast.guess = guess
+            pred.project = proj
+            fast.set_state(u0)
+            for _ in range(args.warmup):
+                fast.step(sync=True)
+            its, ms = [], []
+            for _ in range(args.steps):
+                flush()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                fast.step(sync=False)
+                e1.record()
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+                its.append(int(fast.solver.result()["iterations"]))
+            out[name] = {"iterations": int(sum(its)), "per_step": its,
+                         "ms_per_step": round(sum(ms) / len(ms), 3)}
+    finally:
+        fast.guess, pred.project, pred.launches = saved
+    b = out["projection_only"]["iterations"]
+    out["network_gain_over_projection"] = round(1.0 - out["projection_and_network"]["iterations"] / b, 3) if b else None
+    return out
 
 
 # ------------------------------------------------------------------ other kernels / configs
@@ -605,6 +646,10 @@ def other_configs(flush, parity_inputs):
         p = GyroidStep(mesh, phi, coef)
         p.tr.set_state(g.state(), g.tr.U_prev[:, :3].cpu().numpy())
         p.phi.copy_(g.phi)
+        # the same start with the increment-history projection alone (no network)
+        q = GyroidStep(mesh, phi, coef, guess="project")
+        q.tr.set_state(g.state(), g.tr.U_prev[:, :3].cpu().numpy())
+        q.phi.copy_(g.phi)
         # the state the evaluation starts from, for the oracle's run of its first steps
         n_or = 10
         start = {"coords": mesh.coords, "cells": mesh.cells, "phi": g.phi.cpu().numpy(),
@@ -612,7 +657,7 @@ def other_configs(flush, parity_inputs):
                  "workload": f"gyroid 48^3, the first {n_or} evaluated steps after the 300 "
                              "training steps", "gpu": {}}
         res = {}
-        for name, obj in (("learned", g), ("previous", p)):
+        for name, obj in (("learned", g), ("previous", p), ("projection_only", q)):
             its = []
             torch.cuda.synchronize()
             e0 = torch.cuda.Event(enable_timing=True)
@@ -620,7 +665,7 @@ def other_configs(flush, parity_inputs):
             e0.record()
             for i in range(100):
                 its.append(obj.step()["iterations"])
-                if i == n_or - 1:
+                if i == n_or - 1 and name != "projection_only":
                     start["gpu"][name] = obj.state()
             e1.record()
             e1.synchronize()

@@ -201,20 +201,11 @@ class WarmStartMLP:
             return
         if self._d is None or self._d.shape != tr.U.shape:
             self._d = torch.zeros_like(tr.U)  # padding columns stay zero
-            self._work = torch.empty(int(_lib.lib.tp_guess_project_workspace_doubles()),
-                                     dtype=torch.float64, device=self.device)
         self.predict(tr.U, tr.U_prev, tr.S, tr.ld, tr.D, tr.k, phi, ngphi, x_out=self._d,
                      ops=ops, base=2)
-        nh = max(1, int(getattr(tr, "n_hist", 1)))
-        dirs = [tr.dU[0], self._d] + list(tr.dU[1:nh])
-        # stiffness images known already: ops[1] for the newest increment, earlier steps'
-        # for the older ones (the network's direction is gathered)
-        imgs = [ops[1], None] + [tr.dimg[k] if tr.img_ok[k] else None for k in range(1, nh)]
-        arr = (ctypes.c_void_p * len(dirs))(*[ptr(d) for d in dirs])
-        iarr = (ctypes.c_void_p * len(dirs))(*[ptr(d) for d in imgs])
-        call("tp_guess_project", ctypes.byref(tr.stiff_op.struct), ptr(tr.D64),
-             ptr(tr.bc_mask), ptr(tr.solver.b), ptr(tr.U), ptr(ops[0]), len(dirs), arr, iarr,
-             ptr(x), ptr(self._work), stream_handle())
+        # the projection over the increment history plus the network's direction (its
+        # stiffness image is gathered; the images of past increments are kept)
+        tr.project_history(x, extra=self._d, ops=ops)
 
 
 def trajectory_pairs(tr, steps):

@@ -234,11 +234,34 @@ class BatchedTransport:
         x = self.solver.x
         if self.guess == "learned" and self.predictor is not None and self.steps_done > 0:
             self.predictor.predict_into(self, x)
+        elif self.guess == "project" and self.steps_done > 0 and self.n_hist > 0:
+            self.project_history(x)
         elif self.guess == "extrapolate" and self.steps_done > 0:
             x.copy_(self.U)  # x = 2 u^n - u^{n-1}
             call("tp_axpby", x.numel(), -1.0, ptr(self.U_prev), 2.0, ptr(x), stream_handle())
         else:
             x.copy_(self.U)
+
+    def project_history(self, x, extra=None, extra_img=None, ops=None):
+        """x = u^n + sum_k c_k d_k, the energy-norm (Galerkin) projection over the step
+        increments d = (u^n - u^{n-1}, ..., at most five) and, when given, one more
+        direction `extra` (the learned correction) -- tp_guess_project; ops: the state's
+        stiffness images when already computed (operator_images()).  Without `extra`
+        this is the projected guess with no network at all (the ablation baseline of the
+        learned guess)."""
+        if getattr(self, "_gp_work", None) is None:
+            self._gp_work = torch.empty(int(_lib.lib.tp_guess_project_workspace_doubles()),
+                                        dtype=torch.float64, device=self.device)
+        ops = self.operator_images() if ops is None else ops
+        nh = max(1, int(self.n_hist))
+        dirs = [self.dU[0]] + ([extra] if extra is not None else []) + list(self.dU[1:nh])
+        imgs = [ops[1]] + ([extra_img] if extra is not None else []) + \
+            [self.dimg[k] if self.img_ok[k] else None for k in range(1, nh)]
+        arr = (ctypes.c_void_p * len(dirs))(*[ptr(d) for d in dirs])
+        iarr = (ctypes.c_void_p * len(dirs))(*[ptr(d) for d in imgs])
+        call("tp_guess_project", ctypes.byref(self.stiff_op.struct), ptr(self.D64),
+             ptr(self.bc_mask), ptr(self.solver.b), ptr(self.U), ptr(ops[0]), len(dirs), arr,
+             iarr, ptr(x), ptr(self._gp_work), stream_handle())
 
     def operator_images(self, U=None, U_prev=None, fresh=False):
         """(D_s K U, D_s K (U - U_prev)) with the current stiffness, one launch
@@ -328,6 +351,8 @@ class BatchedTransport:
         guess = 1 if (self.guess != "previous" and self.steps_done > 1) else 0
         if self.guess == "learned" and self.predictor is not None:
             guess = self.predictor.launches
+        elif self.guess == "project":
+            guess = 4  # stiffness images, projection dots, coefficients, update
         if self.engine == "persistent":
             # operator (+ SELL scatter for the FP64 engine), RHS, guess, solve, increment
             return 1 + (0 if getattr(self, "_sell_fresh", False) else 1) + 1 + guess + 1 + 1
