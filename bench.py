@@ -505,9 +505,37 @@ def kernel_table(m, coef, u0, flush):
                      "GB_s": round(gbs, 1), "frac_hbm": round(gbs / hbm, 3)}
     out["peak_gbs"] = {"value": hbm, "source": "measured" if "hbm_gbs" in _peaks() else
                        "fallback (MEASURED_PEAKS.json absent)"}
+    out["matrix_free_cg_3col_fp64"] = matrix_free_solve(dm, De, U, flush, torch)
     rows["assemble_full_fp64"][0]()  # o64 = the full operator again (the rows reuse it)
     out["reference_assemble_p1_tet"] = reference_kernel_baseline(dm, De, al, o64, flush, hbm)
     return out
+
+
+def matrix_free_solve(dm, De, U, flush, torch):
+    """The three species solved matrix-free (tp_mfcg_solve: Jacobi-PCG whose product is
+    the fused matrix-free apply, FP64, lumped mass, rtol 1e-8) from u_prev, for comparison
+    with the assembled-operator engines per iteration."""
+    import ctypes
+
+    from dissolve_tp import _lib
+    from dissolve_tp.device import ptr, stream_handle
+    from dissolve_tp.krylov import MatrixFreeCG
+    sol = MatrixFreeCG(dm, 3, 4, rtol=RTOL, max_it=5000, lumped=1)
+    _lib.call("tp_assemble_rhs", ctypes.byref(dm.tpm), 3, 4, ptr(U), None, 1.0 / DT, 1, 0, None,
+              None, ptr(sol.b), stream_handle())
+    res = {}
+
+    def run():
+        sol.x.copy_(U)
+        res.update(sol.solve(De, 1.0 / DT, dscale=D_S, shift=K_S))
+
+    ms = _event_ms(run, 3, flush, torch)
+    its = max(int(res["iterations"]), 1)
+    return {"ms": round(ms, 3), "iterations": its, "us_per_iteration": round(ms * 1e3 / its, 2),
+            "converged": bool(res["converged"]),
+            "note": "FP64, 3 lanes, previous-step guess; every product recomputes the "
+                    "gradients (tp_matfree_apply), iterations in batches of 8 between host "
+                    "checks"}
 
 
 def reference_kernel_baseline(dm, De, alpha, ours64, flush, hbm):

@@ -671,3 +671,430 @@ extern "C" int tp_guess_project(const tp_csr_op* op, const double* diag, const u
   TP_LAUNCH_CHECK();
   return TP_OK;
 }
+
+// ================================================================= matrix-free Krylov solve
+// Jacobi-preconditioned CG whose product is the matrix-free apply above (k_matfree): the
+// operator is never assembled, every product recomputes the P1 gradients from the
+// coordinates.  This is the solve of the reference's MatShell branch
+// (numerics/solvers.py:172-203, 375-404: PETSc KSP around CeedDiffusionMassOp) on the GPU.
+// FP64, S columns of LD; Dirichlet rows are identity rows (x = b there, the
+// preconditioner zero), as in the CSR engines.  Reductions are one FP64 partial per block
+// summed in block order by the last block to finish (atomic ticket): deterministic for a
+// given grid.
+namespace tp {
+
+struct MfState {
+  double rz[4], alpha[4], beta[4], rr[4], bb[4], tol2[4], rtrue[4];
+  int32_t active[4], iters[4], status[4];
+  int32_t it, max_it, done, pad;
+  uint32_t ticket;
+};
+
+constexpr int MF_BLOCK = 256;
+
+// The operator's diagonal, per cell from the same arithmetic as k_matfree: stiffness
+// ks |c_{i-1}|^2 (|c_0 + c_1 + c_2|^2 for local vertex 0), mass ms (lumped) or 2 ms.
+template <int LD>
+__global__ void __launch_bounds__(256) k_mf_diag(int64_t n, const int4* __restrict__ cells,
+                                                 const double4* __restrict__ X,
+                                                 const double* __restrict__ De,
+                                                 const double* __restrict__ alpha, double4 dsc,
+                                                 double4 shf, double inv_dt, int lumped,
+                                                 int legacy, int S, double* __restrict__ diag) {
+  const double dscale[4] = {dsc.x, dsc.y, dsc.z, dsc.w};
+  const double shift[4] = {shf.x, shf.y, shf.z, shf.w};
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    const int4 v = cells[c];
+    const double4 x0 = ldg_d4(X + v.x), x1 = ldg_d4(X + v.y), x2 = ldg_d4(X + v.z),
+                  x3 = ldg_d4(X + v.w);
+    const double e[3][3] = {{x1.x - x0.x, x1.y - x0.y, x1.z - x0.z},
+                            {x2.x - x0.x, x2.y - x0.y, x2.z - x0.z},
+                            {x3.x - x0.x, x3.y - x0.y, x3.z - x0.z}};
+    double cr[3][3];
+    cr[0][0] = e[1][1] * e[2][2] - e[1][2] * e[2][1];
+    cr[0][1] = e[1][2] * e[2][0] - e[1][0] * e[2][2];
+    cr[0][2] = e[1][0] * e[2][1] - e[1][1] * e[2][0];
+    cr[1][0] = e[2][1] * e[0][2] - e[2][2] * e[0][1];
+    cr[1][1] = e[2][2] * e[0][0] - e[2][0] * e[0][2];
+    cr[1][2] = e[2][0] * e[0][1] - e[2][1] * e[0][0];
+    cr[2][0] = e[0][1] * e[1][2] - e[0][2] * e[1][1];
+    cr[2][1] = e[0][2] * e[1][0] - e[0][0] * e[1][2];
+    cr[2][2] = e[0][0] * e[1][1] - e[0][1] * e[1][0];
+    const double det = e[0][0] * cr[0][0] + e[0][1] * cr[0][1] + e[0][2] * cr[0][2];
+    const double adet = fabs(det);
+    const double De_c = De[c];
+    const double al = alpha ? alpha[c] : 0.0;
+    const double kbase = legacy ? (4.0 * De_c) / (det * det) : De_c / (6.0 * adet);
+    const double mbase = adet * (lumped ? 1.0 / 24.0 : 1.0 / 120.0);
+    double kd[4];
+    const double g[3] = {cr[0][0] + cr[1][0] + cr[2][0], cr[0][1] + cr[1][1] + cr[2][1],
+                         cr[0][2] + cr[1][2] + cr[2][2]};
+    kd[0] = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
+#pragma unroll
+    for (int i = 1; i < 4; i++)
+      kd[i] = cr[i - 1][0] * cr[i - 1][0] + cr[i - 1][1] * cr[i - 1][1] +
+              cr[i - 1][2] * cr[i - 1][2];
+    const int vid[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+      if (s >= S) break;
+      const double ks = kbase * dscale[s];
+      const double ms = mbase * (inv_dt + al + shift[s]);
+      const double md = lumped ? ms : 2.0 * ms;
+#pragma unroll
+      for (int i = 0; i < 4; i++) atomicAdd(diag + (int64_t)vid[i] * LD + s, ks * kd[i] + md);
+    }
+  }
+}
+
+// per-block partial sums of NQ quantities, then the last block sums them in block order
+template <int NQ>
+__device__ __forceinline__ bool mf_reduce(double v[NQ], double* part, uint32_t* ticket,
+                                          double out[NQ]) {
+  __shared__ double sh[32];
+  __shared__ bool s_last;
+#pragma unroll
+  for (int q = 0; q < NQ; q++) {
+    const double t = block_sum(v[q], sh);
+    if (threadIdx.x == 0) part[blockIdx.x * 16 + q] = t;
+  }
+  __threadfence();
+  if (threadIdx.x == 0) s_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!s_last) return false;
+  __threadfence();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < NQ; q++) out[q] = 0.0;
+    for (unsigned b = 0; b < gridDim.x; b++) {
+#pragma unroll
+      for (int q = 0; q < NQ; q++) out[q] += __ldcg(part + b * 16 + q);
+    }
+    *ticket = 0;
+  }
+  return true;
+}
+
+#define MF_ROWS for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; \
+                     i += (int64_t)gridDim.x * blockDim.x)
+
+// dinv = 1 / diag on free rows (0 on Dirichlet rows and zero diagonals); x = b on
+// Dirichlet rows
+template <int LD>
+__global__ void k_mf_prep(int64_t n, int S, const uint8_t* __restrict__ bc,
+                          const double* __restrict__ b, double* __restrict__ x,
+                          double* __restrict__ dinv) {
+  MF_ROWS {
+    const bool br = bc && bc[i];
+#pragma unroll
+    for (int s = 0; s < LD; s++) {
+      const double d = dinv[i * LD + s];
+      dinv[i * LD + s] = (br || s >= S || d == 0.0) ? 0.0 : 1.0 / d;
+      if (br && s < S) x[i * LD + s] = b[i * LD + s];
+    }
+  }
+}
+
+// r = b - q (q = A x; r = 0 on Dirichlet rows), z = D^-1 r, p = z; r.z, r.r, b.b
+template <int LD>
+__global__ void __launch_bounds__(MF_BLOCK) k_mf_start(int64_t n, int S, const uint8_t* bc,
+                                                       const double* b, const double* q,
+                                                       const double* dinv, double* r,
+                                                       double* z, double* p, double* part,
+                                                       MfState* st, double4 rtol) {
+  double acc[12];
+#pragma unroll
+  for (int k = 0; k < 12; k++) acc[k] = 0.0;
+  MF_ROWS {
+    const bool br = bc && bc[i];
+#pragma unroll
+    for (int s = 0; s < LD; s++) {
+      const int64_t k = i * LD + s;
+      const double bv = (s < S) ? b[k] : 0.0;
+      const double rv = (br || s >= S) ? 0.0 : bv - q[k];
+      const double zv = dinv[k] * rv;
+      r[k] = rv;
+      z[k] = zv;
+      p[k] = zv;
+      acc[s] += rv * zv;
+      acc[4 + s] += rv * rv;
+      acc[8 + s] += bv * bv;
+    }
+  }
+  double tot[12];
+  if (!mf_reduce<12>(acc, part, &st->ticket, tot) || threadIdx.x != 0) return;
+  const double rt[4] = {rtol.x, rtol.y, rtol.z, rtol.w};
+  for (int s = 0; s < 4; s++) {
+    st->rz[s] = tot[s];
+    st->rr[s] = tot[4 + s];
+    st->bb[s] = tot[8 + s];
+    st->tol2[s] = rt[s] * rt[s] * tot[8 + s];
+    st->alpha[s] = st->beta[s] = 0.0;
+    st->iters[s] = 0;
+    const bool fin = isfinite(tot[s]) && isfinite(tot[4 + s]);
+    const bool act = s < S && fin && tot[4 + s] > st->tol2[s];
+    st->active[s] = act;
+    st->status[s] = (s < S && !fin) ? TP_ERR_NONFINITE : (act ? -1 : TP_OK);
+  }
+  st->it = 0;
+  st->done = 0;
+  for (int s = 0; s < S; s++) st->done |= st->active[s];
+  st->done = !st->done;
+}
+
+// q = A p with Dirichlet rows as identity rows (p = 0 there); p.q -> alpha
+template <int LD>
+__global__ void __launch_bounds__(MF_BLOCK) k_mf_alpha(int64_t n, int S, const uint8_t* bc,
+                                                       const double* p, double* q,
+                                                       double* part, MfState* st) {
+  if (st->done) return;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  MF_ROWS {
+    const bool br = bc && bc[i];
+#pragma unroll
+    for (int s = 0; s < LD; s++) {
+      const int64_t k = i * LD + s;
+      const double qv = br ? p[k] : q[k];
+      if (br) q[k] = qv;
+      acc[s] += p[k] * qv;
+    }
+  }
+  double tot[4];
+  if (!mf_reduce<4>(acc, part, &st->ticket, tot) || threadIdx.x != 0) return;
+  for (int s = 0; s < 4; s++) {
+    st->alpha[s] = 0.0;
+    if (!st->active[s]) continue;
+    if (!(tot[s] > 0.0)) {
+      st->active[s] = 0;
+      st->status[s] = isfinite(tot[s]) ? TP_ERR_BREAKDOWN : TP_ERR_NONFINITE;
+      st->iters[s] = st->it;
+      continue;
+    }
+    st->alpha[s] = st->rz[s] / tot[s];
+  }
+}
+
+// x += alpha p, r -= alpha q, z = D^-1 r; r.z, r.r -> beta, convergence of each lane
+template <int LD>
+__global__ void __launch_bounds__(MF_BLOCK) k_mf_update(int64_t n, int S, const double* p,
+                                                        const double* q, const double* dinv,
+                                                        double* x, double* r, double* z,
+                                                        double* part, MfState* st) {
+  if (st->done) return;
+  double al[LD];
+#pragma unroll
+  for (int s = 0; s < LD; s++) al[s] = st->alpha[s];
+  double acc[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) acc[k] = 0.0;
+  MF_ROWS {
+#pragma unroll
+    for (int s = 0; s < LD; s++) {
+      const int64_t k = i * LD + s;
+      if (al[s] != 0.0) {
+        x[k] += al[s] * p[k];
+        r[k] -= al[s] * q[k];
+      }
+      const double rv = r[k], zv = dinv[k] * rv;
+      z[k] = zv;
+      acc[s] += rv * zv;
+      acc[4 + s] += rv * rv;
+    }
+  }
+  double tot[8];
+  if (!mf_reduce<8>(acc, part, &st->ticket, tot) || threadIdx.x != 0) return;
+  st->it++;
+  int any = 0;
+  for (int s = 0; s < S; s++) {
+    st->beta[s] = 0.0;
+    if (!st->active[s]) continue;
+    const double rz = tot[s], rr = tot[4 + s];
+    if (!isfinite(rz) || !isfinite(rr)) {
+      st->active[s] = 0;
+      st->status[s] = TP_ERR_NONFINITE;
+      st->iters[s] = st->it;
+      continue;
+    }
+    st->rr[s] = rr;
+    if (rr <= st->tol2[s]) {
+      st->active[s] = 0;
+      st->status[s] = TP_OK;
+      st->iters[s] = st->it;
+      continue;
+    }
+    st->beta[s] = (st->rz[s] != 0.0) ? rz / st->rz[s] : 0.0;
+    st->rz[s] = rz;
+    any = 1;
+  }
+  if (any && st->it >= st->max_it) {
+    for (int s = 0; s < S; s++) {
+      if (st->active[s]) {
+        st->active[s] = 0;
+        st->status[s] = TP_ERR_NOT_CONVERGED;
+        st->iters[s] = st->it;
+      }
+    }
+    any = 0;
+  }
+  st->done = !any;
+}
+
+// p = z + beta p (the lanes still active; a converged lane's p is left as it is)
+template <int LD>
+__global__ void k_mf_dir(int64_t n, const double* z, double* p, const MfState* st) {
+  double be[LD];
+  int act[LD];
+#pragma unroll
+  for (int s = 0; s < LD; s++) {
+    be[s] = st->beta[s];
+    act[s] = st->active[s];
+  }
+  MF_ROWS {
+#pragma unroll
+    for (int s = 0; s < LD; s++) {
+      const int64_t k = i * LD + s;
+      if (act[s]) p[k] = z[k] + be[s] * p[k];
+    }
+  }
+}
+
+// true residual ||b - A x||^2 per lane (q = A x; Dirichlet rows contribute b - x = 0)
+template <int LD>
+__global__ void __launch_bounds__(MF_BLOCK) k_mf_true(int64_t n, int S, const uint8_t* bc,
+                                                      const double* b, const double* q,
+                                                      double* part, MfState* st) {
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  MF_ROWS {
+    if (bc && bc[i]) continue;
+#pragma unroll
+    for (int s = 0; s < LD; s++) {
+      const int64_t k = i * LD + s;
+      const double d = (s < S) ? b[k] - q[k] : 0.0;
+      acc[s] += d * d;
+    }
+  }
+  double tot[4];
+  if (!mf_reduce<4>(acc, part, &st->ticket, tot) || threadIdx.x != 0) return;
+  for (int s = 0; s < 4; s++) st->rtrue[s] = tot[s];
+}
+#undef MF_ROWS
+
+template <int LD>
+static int mf_solve(const tp_mesh* m, int S, const double* De, const double* alpha,
+                    const double* dscale, const double* shift, double inv_dt, int lumped,
+                    int legacy, const uint8_t* bc, const double* b, double* x, double4 rtol,
+                    int max_it, char* ws, tp_mfcg_result* res, cudaStream_t st) {
+  const int64_t n = m->n_verts;
+  const size_t vec = ((sizeof(double) * LD * (size_t)n) + 255) & ~(size_t)255;
+  double* r = reinterpret_cast<double*>(ws);
+  double* z = reinterpret_cast<double*>(ws + vec);
+  double* p = reinterpret_cast<double*>(ws + 2 * vec);
+  double* q = reinterpret_cast<double*>(ws + 3 * vec);
+  double* dinv = reinterpret_cast<double*>(ws + 4 * vec);
+  const int G = 2 * sm_count();
+  double* part = reinterpret_cast<double*>(ws + 5 * vec);
+  MfState* sd = reinterpret_cast<MfState*>(ws + 5 * vec + ((sizeof(double) * 16 * G + 255) & ~(size_t)255));
+  double d4[4] = {1, 1, 1, 1}, s4[4] = {0, 0, 0, 0};
+  for (int i = 0; i < S; i++) {
+    if (dscale) d4[i] = dscale[i];
+    if (shift) s4[i] = shift[i];
+  }
+  // Jacobi diagonal, Dirichlet values into x
+  TP_CUDA_TRY(cudaMemsetAsync(dinv, 0, sizeof(double) * LD * n, st));
+  TP_CUDA_TRY(cudaMemsetAsync(sd, 0, sizeof(MfState), st));
+  MfState h{};
+  h.max_it = max_it;
+  TP_CUDA_TRY(cudaMemcpyAsync(&sd->max_it, &h.max_it, sizeof(int32_t), cudaMemcpyHostToDevice, st));
+  k_mf_diag<LD><<<grid_for(m->n_cells, 256, sm_count() * 8), 256, 0, st>>>(
+      m->n_cells, reinterpret_cast<const int4*>(m->cells),
+      reinterpret_cast<const double4*>(m->coords4), De, alpha,
+      make_double4(d4[0], d4[1], d4[2], d4[3]), make_double4(s4[0], s4[1], s4[2], s4[3]),
+      inv_dt, lumped, legacy, S, dinv);
+  TP_LAUNCH_CHECK();
+  k_mf_prep<LD><<<G, MF_BLOCK, 0, st>>>(n, S, bc, b, x, dinv);
+  TP_LAUNCH_CHECK();
+  auto apply = [&](const double* in, double* out) -> int {
+    return tp_matfree_apply(m, S, LD, 0, De, alpha, d4, s4, inv_dt, lumped, legacy, in, out,
+                            st);
+  };
+  int rc = apply(x, q);
+  if (rc != TP_OK) return rc;
+  k_mf_start<LD><<<G, MF_BLOCK, 0, st>>>(n, S, bc, b, q, dinv, r, z, p, part, sd, rtol);
+  TP_LAUNCH_CHECK();
+  // iterations in batches, the done flag read between batches (a batch past convergence
+  // is a string of no-op launches)
+  constexpr int BATCH = 8;
+  int32_t done = 0;
+  for (int it = 0; it < max_it && !done; it += BATCH) {
+    for (int k = 0; k < BATCH; k++) {
+      rc = apply(p, q);
+      if (rc != TP_OK) return rc;
+      k_mf_alpha<LD><<<G, MF_BLOCK, 0, st>>>(n, S, bc, p, q, part, sd);
+      k_mf_update<LD><<<G, MF_BLOCK, 0, st>>>(n, S, p, q, dinv, x, r, z, part, sd);
+      k_mf_dir<LD><<<G, MF_BLOCK, 0, st>>>(n, z, p, sd);
+      TP_LAUNCH_CHECK();
+    }
+    TP_CUDA_TRY(cudaMemcpyAsync(&done, &sd->done, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    TP_CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  rc = apply(x, q);
+  if (rc != TP_OK) return rc;
+  k_mf_true<LD><<<G, MF_BLOCK, 0, st>>>(n, S, bc, b, q, part, sd);
+  TP_LAUNCH_CHECK();
+  TP_CUDA_TRY(cudaMemcpyAsync(&h, sd, sizeof(MfState), cudaMemcpyDeviceToHost, st));
+  TP_CUDA_TRY(cudaStreamSynchronize(st));
+  int status = TP_OK;
+  for (int s = 0; s < S; s++) {
+    int ls = h.status[s];
+    if (ls == -1) ls = TP_ERR_NOT_CONVERGED;
+    // the recurrence residual stopped the lane; the true residual confirms it
+    if (ls == TP_OK && !(h.rtrue[s] <= h.tol2[s] * 1.0000001)) ls = TP_ERR_NOT_CONVERGED;
+    res->lane_status[s] = ls;
+    res->lane_iters[s] = h.iters[s];
+    res->lane_rnorm[s] = sqrt(std::max(h.rtrue[s], 0.0));
+    res->lane_bnorm[s] = sqrt(std::max(h.bb[s], 0.0));
+    if (ls != TP_OK && status == TP_OK) status = ls;
+  }
+  res->status = status;
+  res->iterations = h.it;
+  return TP_OK;
+}
+
+}  // namespace tp
+
+extern "C" size_t tp_mfcg_workspace_bytes(int64_t n_verts, int ld) {
+  const size_t vec = ((sizeof(double) * (size_t)ld * (size_t)n_verts) + 255) & ~(size_t)255;
+  const size_t part = ((sizeof(double) * 16 * 2 * (size_t)tp::sm_count()) + 255) & ~(size_t)255;
+  return 5 * vec + part + ((sizeof(tp::MfState) + 255) & ~(size_t)255);
+}
+
+extern "C" int tp_mfcg_solve(const tp_mesh* m, int S, int ld, const double* De_cell,
+                             const double* alpha_cell, const double* diff_scale,
+                             const double* shift, double inv_dt, int lumped, int legacy,
+                             const uint8_t* bc_mask, const double* b, double* x,
+                             const double* rtol, int max_it, void* workspace,
+                             size_t workspace_bytes, tp_mfcg_result* res, void* stream) {
+  TP_REQUIRE(m && m->cells && m->coords4 && De_cell && b && x && rtol && workspace && res,
+             "null pointer");
+  TP_REQUIRE(S >= 1 && S <= TP_MAX_COLS && (ld == 1 || ld == 2 || ld == 4) && ld >= S,
+             "bad S/ld");
+  TP_REQUIRE(max_it >= 0, "max_it < 0");
+  TP_REQUIRE(((uintptr_t)workspace & 255) == 0, "workspace must be 256-byte aligned");
+  TP_REQUIRE(workspace_bytes >= tp_mfcg_workspace_bytes(m->n_verts, ld), "workspace too small");
+  *res = tp_mfcg_result{};
+  if (m->n_verts == 0) return TP_OK;
+  double rt[4] = {0, 0, 0, 0};
+  for (int s = 0; s < S; s++) rt[s] = rtol[s];
+  const double4 r4 = make_double4(rt[0], rt[1], rt[2], rt[3]);
+  char* ws = static_cast<char*>(workspace);
+  cudaStream_t st = as_stream(stream);
+  if (ld == 1)
+    return mf_solve<1>(m, S, De_cell, alpha_cell, diff_scale, shift, inv_dt, lumped, legacy,
+                       bc_mask, b, x, r4, max_it, ws, res, st);
+  if (ld == 2)
+    return mf_solve<2>(m, S, De_cell, alpha_cell, diff_scale, shift, inv_dt, lumped, legacy,
+                       bc_mask, b, x, r4, max_it, ws, res, st);
+  return mf_solve<4>(m, S, De_cell, alpha_cell, diff_scale, shift, inv_dt, lumped, legacy,
+                     bc_mask, b, x, r4, max_it, ws, res, st);
+}

@@ -75,6 +75,11 @@ class TpMlpInputs(ctypes.Structure):
                 ("istd", _c_dbl * 10), ("base", _c_i32), ("tc_status", _vp)]
 
 
+class TpMfcgResult(ctypes.Structure):
+    _fields_ = [("status", _c_i32), ("iterations", _c_i32), ("lane_status", _c_i32 * 4),
+                ("lane_iters", _c_i32 * 4), ("lane_rnorm", _c_dbl * 4), ("lane_bnorm", _c_dbl * 4)]
+
+
 class TpCgResult(ctypes.Structure):
     _fields_ = [("status", _c_i32), ("iterations", _c_i32), ("n_reliable", _c_i32),
                 ("n_lanes", _c_i32)]
@@ -167,6 +172,10 @@ SIGNATURES = {
     "tp_tiles_info": (ctypes.c_int, [_vp, _P(_c_i32), _P(_c_i32), _P(_c_i32), _P(_c_i64),
                                      _P(ctypes.c_size_t)]),
     "tp_tiles_destroy": (ctypes.c_int, [_vp]),
+    "tp_mfcg_workspace_bytes": (ctypes.c_size_t, [_c_i64, ctypes.c_int]),
+    "tp_mfcg_solve": (ctypes.c_int, [_P(TpMesh), ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp,
+                                     _c_dbl, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp,
+                                     ctypes.c_int, _vp, ctypes.c_size_t, _P(TpMfcgResult), _vp]),
     "tp_pcg_set_wait_limit": (ctypes.c_int, [_vp, ctypes.c_ulonglong, ctypes.c_uint]),
     "tp_pcg_destroy": (ctypes.c_int, [_vp]),
     "tp_mlp_param_count": (ctypes.c_int, []),

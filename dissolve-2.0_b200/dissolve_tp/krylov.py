@@ -290,3 +290,48 @@ class PersistentCG:
             self.close()
         except Exception:
             pass
+
+
+class MatrixFreeCG:
+    """Jacobi-PCG whose product is the matrix-free apply (tp_mfcg_solve): the operator of
+    tp_matfree_apply -- per column s, sum_e [dscale_s De_e K_e + (inv_dt + alpha_e +
+    shift_s) M_e] -- is never assembled; every product recomputes the P1 gradients from the
+    coordinates.  The solve of the reference's MatShell branch (numerics/solvers.py:172-203,
+    375-404) on the GPU.  b, x: (n_verts, ld) FP64 device arrays; x is the initial guess
+    and receives the solution."""
+
+    def __init__(self, dm, S: int = 1, ld: int = 1, rtol=1e-8, max_it: int = 1000,
+                 lumped: int = 0, legacy: int = 0):
+        from .device import empty_aligned
+        self.dm, self.S, self.ld = dm, int(S), int(ld)
+        self.max_it, self.lumped, self.legacy = int(max_it), int(lumped), int(legacy)
+        self.rtol = np.broadcast_to(np.asarray(rtol, dtype=np.float64), (self.S,)).copy()
+        dev = dm.device
+        self.b = torch.zeros((dm.n_verts, self.ld), dtype=torch.float64, device=dev)
+        self.x = torch.zeros((dm.n_verts, self.ld), dtype=torch.float64, device=dev)
+        nb = int(_lib.lib.tp_mfcg_workspace_bytes(dm.n_verts, self.ld))
+        self._ws_buf, self._ws = empty_aligned(nb, dev)
+        self._nb = nb
+
+    def solve(self, De_cell, inv_dt: float, alpha_cell=None, dscale=None, shift=None,
+              bc_mask=None) -> dict:
+        from ._lib import TpMfcgResult
+        c = ctypes
+        res = TpMfcgResult()
+        ds = None if dscale is None else (c.c_double * 4)(*(list(dscale) + [0.0] * 4)[:4])
+        sh = None if shift is None else (c.c_double * 4)(*(list(shift) + [0.0] * 4)[:4])
+        rt = (c.c_double * 4)(*(list(self.rtol) + [0.0] * 4)[:4])
+        call("tp_mfcg_solve", c.byref(self.dm.tpm), self.S, self.ld, ptr(De_cell),
+             ptr(alpha_cell), ds, sh, float(inv_dt), self.lumped, self.legacy, ptr(bc_mask),
+             ptr(self.b), ptr(self.x), rt, self.max_it, self._ws, self._nb, c.byref(res),
+             stream_handle())
+        S = self.S
+        return {"status": int(res.status), "converged": int(res.status) == 0,
+                "iterations": int(res.iterations),
+                "lane_iterations": np.array(res.lane_iters[:S]),
+                "lane_status": np.array(res.lane_status[:S]),
+                "rnorm": np.array(res.lane_rnorm[:S]), "bnorm": np.array(res.lane_bnorm[:S])}
+
+    def close(self):
+        """Nothing to release beyond the tensors (no handle)."""
+

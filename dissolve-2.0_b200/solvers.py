@@ -18,9 +18,15 @@ Differences, stated:
     cooperative kernel; ksp_type "gmres"/"cg" and pc_type "bjacobi"/"jacobi"/None are
     accepted and all run it.  The stopping rule is ||b - A x||_2 <= rtol ||b||_2 in FP64
     (PETSc's default test is relative to the preconditioned initial residual).
-  * The DOLFINx/UFL branches (_solve_ceed with a PETSc MatShell, _solve_standard) need
-    DOLFINx and PETSc, which are not part of this build: they raise NotImplementedError
-    instead of silently falling back to the CPU.
+  * The matrix-free branch (ceed_op given, _solve_ceed, solvers.py:375-404) runs on the
+    GPU as tp_mfcg_solve: Jacobi-PCG whose every product is the fused matrix-free apply
+    (the operator of CeedDiffusionMassOp, never assembled).  Its right-hand side is
+    assembled on the GPU from u_old (consistent mass, as the operator's) instead of from
+    the UFL L_form, and it is preconditioned by the operator's diagonal (computed from the
+    same geometry) where the reference's MatShell runs unpreconditioned (pc "none").
+  * The DOLFINx/UFL branches without u_old (_solve_ceed with an L_form, _solve_standard)
+    need DOLFINx and PETSc, which are not part of this build: they raise
+    NotImplementedError instead of silently falling back to the CPU.
 """
 from __future__ import annotations
 
@@ -32,7 +38,7 @@ import torch
 from dissolve_tp import _lib
 from dissolve_tp.assembler import GPUSparseAssembler
 from dissolve_tp.device import ptr, stream_handle, to_device
-from dissolve_tp.krylov import CsrOperator, PersistentCG
+from dissolve_tp.krylov import CsrOperator, MatrixFreeCG, PersistentCG
 
 _SHARED_GEOM = None
 _GPU_ASM_CACHE: dict = {}
@@ -82,9 +88,19 @@ def solve_transport(name, a_form=None, L_form=None, u=None, bcs=None, ksp_type="
         ua = _array(u)
         u_old = ua.clone() if isinstance(ua, torch.Tensor) else np.array(ua, copy=True)
     if ceed_op is not None:
-        raise NotImplementedError(
-            "the MatShell branch assembles its right-hand side from UFL forms (DOLFINx); "
-            "use the GPU-assembled branch (use_gpu=True, de_field=..., u_old=...)")
+        if u_old is None:
+            raise NotImplementedError(
+                "the MatShell branch without u_old assembles its right-hand side from UFL "
+                "forms (DOLFINx); pass u_old (and de_field carrying _solver_bc_dofs) to run "
+                "it on the GPU")
+        bc_dofs = getattr(de_field, "_solver_bc_dofs", None) if de_field is not None else None
+        converged, iterations = _solve_ceed_gpu(name, ceed_op, u, rtol, max_it, u_old=u_old,
+                                                source_field=source_field, bc_dofs=bc_dofs,
+                                                bc_value=bc_value, under_relax=under_relax)
+        if hasattr(u, "x") and hasattr(u.x, "scatter_forward"):
+            u.x.scatter_forward()
+        return {"converged": bool(converged), "iterations": int(iterations),
+                "time_s": time.time() - t0}
     if not (use_gpu and de_field is not None and pc_type in (None, "bjacobi", "jacobi")):
         raise NotImplementedError(
             "only the GPU-assembled transport branch is part of this build "
@@ -100,6 +116,49 @@ def solve_transport(name, a_form=None, L_form=None, u=None, bcs=None, ksp_type="
         u.x.scatter_forward()
     return {"converged": bool(converged), "iterations": int(iterations),
             "time_s": time.time() - t0}
+
+
+def _solve_ceed_gpu(name, ceed_op, u, rtol, max_it, u_old, source_field=None, bc_dofs=None,
+                    bc_value=0.0, under_relax=None):
+    """The matrix-free solve (solvers.py:375-404) on the GPU: b = M (u_old/dt + f) with the
+    consistent mass and Dirichlet values, then tp_mfcg_solve with the CeedDiffusionMassOp's
+    coefficients, warm-started from u."""
+    import ctypes
+
+    op = getattr(ceed_op, "ceed_op", ceed_op)  # MatrixFreeOperator or the operator itself
+    dm = op._dm
+    if bc_dofs is not None and len(bc_dofs) == 0:
+        bc_dofs = None
+    key = ("ceed", name, id(op))
+    cache = _GPU_ASM_CACHE.get(key)
+    if cache is None or cache["solver"].max_it != int(max_it):
+        cache = {"solver": MatrixFreeCG(dm, 1, 1, rtol=rtol, max_it=max_it, lumped=0,
+                                        legacy=int(op.legacy))}
+        _GPU_ASM_CACHE[key] = cache
+    sol = cache["solver"]
+    sol.rtol[:] = rtol
+    d_u = to_device(_array(u_old), torch.float64, dm.device)
+    d_f = to_device(_array(source_field), torch.float64, dm.device) if source_field is not None \
+        else None
+    d_bc = to_device(np.asarray(bc_dofs, dtype=np.int32), torch.int32, dm.device) \
+        if bc_dofs is not None else None
+    n_bc = 0 if d_bc is None else int(d_bc.numel())
+    bcv = (ctypes.c_double * 4)(float(bc_value), 0.0, 0.0, 0.0)
+    _lib.call("tp_assemble_rhs", ctypes.byref(dm.tpm), 1, 1, ptr(d_u), ptr(d_f), op.inv_dt, 0,
+              n_bc, ptr(d_bc), bcv, ptr(sol.b), stream_handle())
+    mask = dm.bc_mask(np.asarray(bc_dofs, dtype=np.int32)) if bc_dofs is not None else None
+    u_arr = _array(u)
+    sol.x.view(-1).copy_(to_device(u_arr, torch.float64, dm.device))
+    res = sol.solve(op._De, op.inv_dt, alpha_cell=op.alpha, bc_mask=mask)
+    x = sol.x.view(-1)
+    if under_relax is not None and under_relax < 1.0:
+        _lib.call("tp_axpby", x.numel(), 1.0 - float(under_relax), ptr(d_u), float(under_relax),
+                  ptr(x), stream_handle())
+    if isinstance(u_arr, torch.Tensor):
+        u_arr.copy_(x)
+    else:
+        u_arr[...] = x.cpu().numpy()
+    return res["converged"], res["iterations"]
 
 
 def _solve_gpu_asm(name, de_field, u, rtol, max_it, alpha_field=None, u_old=None,

@@ -346,6 +346,27 @@ typedef struct tp_csr_op {
   const int64_t* sys_row_ptr;
 } tp_csr_op;
 
+/* [sync] Matrix-free Jacobi-PCG (numerics/solvers.py:172-203, 375-404: the reference's
+ * PETSc KSP around the CeedDiffusionMassOp MatShell): solves A x = b for S interleaved
+ * columns, A the operator of tp_matfree_apply (same arguments), every product recomputing
+ * the P1 gradients from coords4; nothing is assembled.  FP64.  bc_mask (or NULL): those
+ * rows are identity rows (x = b there).  rtol (host, S values): stops each lane when its
+ * recurrence residual ||r||_2 <= rtol ||b||_2, then confirms it on ||b - A x||_2 (reported
+ * per lane in res).  x: initial guess in, solution out.  workspace: 256-byte aligned,
+ * tp_mfcg_workspace_bytes(n_verts, ld) bytes. */
+typedef struct tp_mfcg_result {
+  int32_t status, iterations;
+  int32_t lane_status[4], lane_iters[4];
+  double lane_rnorm[4], lane_bnorm[4];
+} tp_mfcg_result;
+TP_API size_t tp_mfcg_workspace_bytes(int64_t n_verts, int ld);
+TP_API int tp_mfcg_solve(const tp_mesh* m, int S, int ld, const double* De_cell,
+                         const double* alpha_cell, const double* diff_scale,
+                         const double* shift, double inv_dt, int lumped, int legacy,
+                         const uint8_t* bc_mask, const double* b, double* x,
+                         const double* rtol, int max_it, void* workspace,
+                         size_t workspace_bytes, tp_mfcg_result* res, void* stream);
+
 /* y = A x with the FP64 (fp32 = 0) or FP32 (fp32 = 1) values of op */
 TP_API int tp_csr_apply(const tp_csr_op* op, int fp32, const void* x, void* y, void* stream);
 
