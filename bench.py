@@ -45,7 +45,7 @@ PARITY_STEPS = 3
 # relative residual of the oracle's Jacobi-PCG solves that stand in for exact solutions
 ORACLE_RTOL = 1e-12
 # measured with ncu on this workload (see profiles/); None until captured
-DRAM_BYTES_PER_ITERATION = 11.30e6  # 3.040 GB over a 269-iteration launch of k_cgw
+DRAM_BYTES_PER_ITERATION = {"k_cgw": 10.2e6}  # k_cgw: 2.627 GB over a 258-iteration launch
 WORKLOAD = ("3-species backward-Euler step, 64^3 Kuhn cube (1,572,864 P1 tets, 274,625 "
             "vertices), jitter 0.2h, De = D_s exp(0.3 xi), rtol 1e-8")
 
@@ -161,6 +161,16 @@ def run_ours(args, rank, world, local_rank):
     cg_extra = {"use_graph_loop": not args.host_loop}
     fast = BatchedTransport(m, coef, D_S, K_S, DT, rtol=RTOL, inner_fp32=True, guess="previous",
                             cg=cg_extra)
+    if args.roofline_only:
+        # W steps with the previous-step guess (W solves), then the roofline solve: the
+        # (W+1)-th launch of the solve kernel, a one-launch case for a profiler
+        fast.set_state(u0)
+        for _ in range(args.warmup):
+            fast.step(sync=True)
+        if rank == 0:
+            print(json.dumps({"workload": WORKLOAD, "cg_launch": fast.cg_config,
+                              "roofline": roofline_solve(fast, flush, torch)}), flush=True)
+        return
     learned = False
     if args.guess == "learned":
         from dissolve_tp import mlp as mlpmod
@@ -202,54 +212,8 @@ def run_ours(args, rank, world, local_rank):
     conv = all(r["converged"] for r in results)
     iters = [int(r["iterations"]) for r in results]
 
-    # ---- roofline of the dominant kernel: the persistent CG (one launch per solve), timed
-    # live with CUDA events around its launch on the same stream, on the last timed state
-    # started from the previous-step guess (a solve of ~230 iterations: the per-iteration
-    # rate, not the per-launch set-up and final residual that dominate the shortest
-    # learned-guess solves)
     nnz, nv = fast.dm.nnz, fast.dm.n_verts
-    fast.assemble_operator()
-    fast.solver.refresh_values()
-    fast.assemble_rhs()
-    fast.solver.x.copy_(fast.U)
-    torch.cuda.synchronize()
-    flush()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    fast.solver.run()
-    e1.record()
-    e1.synchronize()
-    solve_ms = e0.elapsed_time(e1)
-    rk = fast.solver.result()
-    its = max(int(rk["iterations"]), 1)
-    window = fast.cg_config.get("form", "").startswith("window")
-    if window:
-        # window engine, per iteration: FP32 value per nonzero (columns stay in shared
-        # memory for the whole solve) and 12 passes of (V, 4) FP32: u read once into the
-        # windows; P reads p, s, xi, r, D^-1 and writes p, s, xi, r, u; the product reads
-        # the row diagonal (w = A u of the own rows stays in shared memory)
-        bytes_it = nnz * 4 + 12 * nv * 16
-        kernel = ("k_cgw<float,4> (persistent 3-column Jacobi-PCG, Chronopoulos-Gear form, "
-                  "shared-memory windows, one cooperative launch per solve)")
-    else:
-        # streaming engine: int32 column + FP32 value per nonzero and 12 passes of (V, 4)
-        # FP32: A reads z, p and writes p, q; B reads p, q, r, xi, D^-1, writes xi, r, z
-        bytes_it = nnz * 8 + 12 * nv * 16
-        kernel = ("k_pcg<float,4> (persistent 3-column Jacobi-PCG, one cooperative launch "
-                  "per solve)")
-    # DRAM bytes per iteration of the same kernel on this workload, from an ncu capture
-    # (dram__bytes_read.sum + dram__bytes_write.sum of one launch / its iterations)
-    traffic = (DRAM_BYTES_PER_ITERATION * its) if (window and DRAM_BYTES_PER_ITERATION) else None
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
-    except OSError:
-        pass
-    # the driver-measured copy bandwidth of this pool's B200s, else the recipe's fallback
-    hbm = float(peaks.get("hbm_gbs", 6650.0))
-    peak_src = "of measured" if "hbm_gbs" in peaks else "of fallback: MEASURED_PEAKS.json absent"
-    achieved = bytes_it * its / (solve_ms * 1e-3) / 1e9
+    roof = roofline_solve(fast, flush, torch)
     # ---- e2e through the host-buffer API
     e2e = None
     if args.e2e:
@@ -341,16 +305,7 @@ def run_ours(args, rank, world, local_rank):
                    "cg_launch": fast.cg_config},
         "converged": conv, "cg_iterations": iters,
         "gpu_launches": launches,
-        "roofline": {"bound": "hbm", "kernel": kernel,
-                     "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": traffic,
-                     "algorithmic_bytes": bytes_it * its, "bytes_per_iteration": bytes_it,
-                     "iterations": its, "launch_us": solve_ms * 1e3,
-                     "note": f"peak = HBM copy bandwidth ({peak_src}); one solve of "
-                             "the last timed state from the previous-step guess; the "
-                             "operator and vectors stay in the 126 MB L2 between "
-                             "iterations; traffic = ncu DRAM bytes per iteration x "
-                             "iterations of this launch"},
+        "roofline": roof,
         "clocks": clk.summary(),
         "e2e": e2e,
         "forms": forms,
@@ -379,6 +334,78 @@ def run_ours(args, rank, world, local_rank):
             gyroid=parity_inputs.get("gyroid_48"))
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def roofline_solve(fast, flush, torch):
+    """Roofline of the dominant kernel: the persistent CG (one launch per solve), timed live
+    with CUDA events around its launch on the same stream, on the current state started
+    from the previous-step guess (a solve of ~250 iterations at the last timed state: the
+    per-iteration rate, not the per-launch set-up and final residual that dominate the
+    shortest learned-guess solves)."""
+    nnz, nv = fast.dm.nnz, fast.dm.n_verts
+    fast.assemble_operator()
+    fast.solver.refresh_values()
+    fast.assemble_rhs()
+    fast.solver.x.copy_(fast.U)
+    torch.cuda.synchronize()
+    flush()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    fast.solver.run()
+    e1.record()
+    e1.synchronize()
+    solve_ms = e0.elapsed_time(e1)
+    rk = fast.solver.result()
+    its = max(int(rk["iterations"]), 1)
+    form = fast.cg_config.get("form", "")
+    window = form.startswith("window")
+    if window and "pipelined" in form:
+        # pipelined engine, per iteration, counted as for the window engine: the FP32 value
+        # per nonzero and 12 passes of (V, 4) FP32 vectors (m into the windows, the update's
+        # reads and writes of z, s, p, r, w, xi)
+        bytes_it = nnz * 4 + 12 * nv * 16
+        kernel = ("k_pcgp<4> (persistent 3-column pipelined Jacobi-PCG, one grid barrier per "
+                  "iteration, values and vectors in tensor memory, one cooperative launch "
+                  "per solve)")
+        engine = "k_pcgp"
+    elif window:
+        # window engine, per iteration: FP32 value per nonzero (columns stay in shared
+        # memory for the whole solve) and 12 passes of (V, 4) FP32: u read once into the
+        # windows; P reads p, s, xi, r, D^-1 and writes p, s, xi, r, u; the product reads
+        # the row diagonal (w = A u of the own rows stays in shared memory)
+        bytes_it = nnz * 4 + 12 * nv * 16
+        kernel = ("k_cgw<float,4> (persistent 3-column Jacobi-PCG, Chronopoulos-Gear form, "
+                  "shared-memory windows, one cooperative launch per solve)")
+        engine = "k_cgt" if "tensor memory" in form else "k_cgw"
+    else:
+        # streaming engine: int32 column + FP32 value per nonzero and 12 passes of (V, 4)
+        # FP32: A reads z, p and writes p, q; B reads p, q, r, xi, D^-1, writes xi, r, z
+        bytes_it = nnz * 8 + 12 * nv * 16
+        kernel = ("k_pcg<float,4> (persistent 3-column Jacobi-PCG, one cooperative launch "
+                  "per solve)")
+        engine = "k_pcg"
+    # DRAM bytes per iteration of the same kernel on this workload, from an ncu capture
+    # (dram__bytes_read.sum + dram__bytes_write.sum of one launch / its iterations)
+    per_it = DRAM_BYTES_PER_ITERATION.get(engine)
+    traffic = per_it * its if per_it else None
+    peaks = _peaks()
+    # the driver-measured copy bandwidth of this pool's B200s, else the recipe's fallback
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "of measured" if "hbm_gbs" in peaks else "of fallback: MEASURED_PEAKS.json absent"
+    achieved = bytes_it * its / (solve_ms * 1e-3) / 1e9
+    return {"bound": "hbm", "kernel": kernel,
+            "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "traffic": traffic,
+            "algorithmic_bytes": bytes_it * its, "bytes_per_iteration": bytes_it,
+            "iterations": its, "launch_us": solve_ms * 1e3,
+            "us_per_iteration": solve_ms * 1e3 / its,
+            "note": f"peak = HBM copy bandwidth ({peak_src}); one solve of the current "
+                    "state from the previous-step guess; the operator and vectors stay on "
+                    "chip (tensor memory, shared memory) and in the 126 MB L2 between "
+                    "iterations, so the solve is bound by its grid barrier and on-chip "
+                    "latencies, not by DRAM; traffic = ncu DRAM bytes per iteration x "
+                    "iterations of this launch"}
 
 
 def guess_ablation(fast, u0, args, flush, torch):
@@ -860,6 +887,9 @@ def main():
                     help="skip the assembly / RHS / apply bandwidth table")
     ap.add_argument("--no-configs", dest="configs", action="store_false",
                     help="skip the multi-mesh batch and gyroid coupled-step workloads")
+    ap.add_argument("--roofline-only", action="store_true",
+                    help="W steps with the previous-step guess, then only the roofline solve "
+                         "(the solve kernel's launch W + 1)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="print only the assembly / RHS / apply bandwidth table (no step)")
     args = ap.parse_args()

@@ -1682,6 +1682,1375 @@ __global__ void __launch_bounds__(512, 1) k_cgw(PArgs<VT> a) {
 #undef FOR_OWN_ROWS
 }
 
+// ----------------------------------------------------------------- tensor-memory engine
+// k_cgt: the window engine's FP32 solve (no mass matrix; slices of at most 16 entries; at
+// most 4 slices per warp, i.e. 2048 rows per CTA) with every per-row vector of the
+// recurrence on chip.  The SM's 512 tensor-memory columns hold, for warp w (lanes
+// 32 (w % 4) .., columns 128 (w / 4) ..), the FP32 values of its slices (16 columns per
+// slice) and one 16-column record per slice row, [p | s | xi | r] (4 columns each, the
+// first LD used); D^-1 of the own rows sits in shared memory where k_cgw keeps w, and u
+// in the window as before.  The only per-iteration global traffic left is the halo of u
+// (written by the P phase, copied by the other CTAs) and the row diagonals.
+//
+// Iteration: the Chronopoulos-Gear recurrences of k_cgw, with the direction update moved
+// into the product.  beta = gamma / gamma_old only needs the P-phase sums, which every CTA
+// holds right after barrier B, so the product of row i also forms p_i = u_i + beta p_i and
+// s_i = w_i + beta s_i, and w never leaves registers:
+//
+//   barrier B | halo copies in flight, gamma and r.r totals, lane decisions, beta
+//             | w = A u, p = u + beta p, s = w + beta s, w.u
+//   barrier A | delta total, alpha = gamma / (delta - beta gamma / alpha_old)
+//             | xi += alpha p, r -= alpha s, u = D^-1 r (window and global), r.u, r.r
+//   barrier B ...
+//
+// Partial slots per CTA: r.u 0-3, r.r 4-7, w.u 8-11, b.b 12-15 (written only by the FP64
+// refreshes), so no slot is rewritten while another CTA may still read it.  A lane whose
+// alpha denominator is not positive (rounding) takes no step and restarts through an FP64
+// refresh (beta = 0 after it), as does a lane that was frozen.
+constexpr int CGT_MAXS = 4;
+constexpr int CGT_WARPS = 16;
+constexpr uint32_t CGT_COLS = 512;
+
+template <int LD>
+__global__ void __launch_bounds__(512, 1) k_cgt(PArgs<float> a) {
+  using VT = float;
+  static_assert(LD == 2 || LD == 4, "FP64 residual windows hold LD / 2 doubles per entry");
+  constexpr int CP = LD / 2;  // FP64 columns per window entry in the residual passes
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  int32_t* s_sp = reinterpret_cast<int32_t*>(s_dyn);
+  int32_t* s_halo = s_sp + a.sp_cap;
+  uint16_t* s_col = reinterpret_cast<uint16_t*>(s_halo + a.halo_cap);
+  VT* s_win = reinterpret_cast<VT*>(
+      s_dyn + ((4 * (size_t)(a.sp_cap + a.halo_cap) + 2 * (size_t)a.col_cap + 15) & ~(size_t)15));
+  VT* s_dinv = s_win + (size_t)a.win_cap * LD;  // D^-1 of the own rows
+  __shared__ double sh[32 * 12];
+  __shared__ double s_buf[512];
+  __shared__ double s_tot[16];
+  __shared__ LaneState L;
+  __shared__ double s_gm[4], s_step[4];
+  __shared__ int s_restart[4];
+  __shared__ uint32_t s_taddr;
+  __shared__ unsigned long long s_clk[8];
+  unsigned int target = 0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int sb = (int)((int64_t)blockIdx.x * a.ns / gridDim.x);
+  const int se = (int)((int64_t)(blockIdx.x + 1) * a.ns / gridDim.x);
+  const int S = a.S;
+  const int r0 = sb * 32;
+  const int nown = (se > sb) ? (int)(min((int64_t)se * 32, a.n) - r0) : 0;
+  const int nhalo = a.halo_ptr[blockIdx.x + 1] - a.halo_ptr[blockIdx.x];
+  PhaseClock clk;
+  clk.start(a.prof != nullptr, s_clk);
+  for (int i = threadIdx.x; i <= se - sb; i += blockDim.x) s_sp[i] = a.slice_ptr[sb + i];
+  {
+    const int hb = a.halo_ptr[blockIdx.x];
+    for (int i = threadIdx.x; i < nhalo; i += blockDim.x) s_halo[i] = a.halo[hb + i];
+    if (se > sb) {
+      const int e0 = a.slice_ptr[sb], ne = a.slice_ptr[se] - e0;
+      const uint4* src = reinterpret_cast<const uint4*>(a.loc_col + e0);
+      uint4* dst = reinterpret_cast<uint4*>(s_col);
+      for (int i = threadIdx.x; i < ne / 8; i += blockDim.x) dst[i] = src[i];
+    }
+  }
+  if (threadIdx.x < 4) s_restart[threadIdx.x] = 0;
+  // ---- tensor memory: the whole of it; values of slice j at tw + 16 j, records at
+  // tw + 64 + 16 j
+  if (warp == 0) tm_alloc(&s_taddr, CGT_COLS);
+  tm_fence_before();
+  __syncthreads();
+  tm_fence_after();
+  const uint32_t tw = s_taddr + ((uint32_t)(32 * (warp & 3)) << 16) + 128u * (uint32_t)(warp >> 2);
+  auto rec_ld = [&](int j, float rc[16]) { tm_ld16(tw + 64u + 16u * (uint32_t)j, rc); };
+  auto rec_st = [&](int j, const float rc[16]) {
+    uint32_t v[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) v[k] = __float_as_uint(rc[k]);
+    tm_st16(tw + 64u + 16u * (uint32_t)j, v);
+  };
+#pragma unroll
+  for (int j = 0; j < CGT_MAXS; j++) {
+    const int sl = sb + warp + j * CGT_WARPS;
+    uint32_t v[16];
+    const int base = (sl < se) ? a.slice_ptr[sl] : 0;
+    const int w = (sl < se) ? (a.slice_ptr[sl + 1] - base) >> 5 : 0;
+#pragma unroll
+    for (int k = 0; k < 16; k++)
+      v[k] = (k < w) ? __float_as_uint(ld_na(a.sK + base + k * 32 + lane)) : 0u;
+    tm_st16(tw + 16u * (uint32_t)j, v);
+  }
+  tm_wait_st();
+
+  // window of u: own rows (unless the P phase wrote them) and halo, asynchronously
+  auto fill_window = [&](bool own_done) {
+    const int W = nown + nhalo;
+    for (int i = (own_done ? nown : 0) + threadIdx.x; i < W; i += blockDim.x) {
+      const int64_t g = (i < nown) ? (int64_t)(r0 + i) : (int64_t)s_halo[i - nown];
+      cp_async<LD * 4>(s_win + (size_t)i * LD, a.u + g * LD);
+    }
+  };
+
+  // ---- w = A u of the own rows; p = u + beta p, s = w + beta s; w.u into acc
+  auto product_rows = [&](const float be[LD], double acc[4]) {
+    // the row diagonals and Dirichlet flags of this warp's rows, in flight while the
+    // window copies land
+    float dg[CGT_MAXS][LD];
+    bool bcm[CGT_MAXS];
+#pragma unroll
+    for (int j = 0; j < CGT_MAXS; j++) {
+      const int64_t row = (int64_t)(sb + warp + j * CGT_WARPS) * 32 + lane;
+      const bool in = sb + warp + j * CGT_WARPS < se && row < a.n;
+#pragma unroll
+      for (int s = 0; s < LD; s++) dg[j][s] = 0.f;
+      if (in && a.diag) ldv<VT, LD>(a.diag, row, dg[j]);
+      bcm[j] = in && a.bc && a.bc[row];
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const int e0 = s_sp[0];
+#pragma unroll
+    for (int j = 0; j < CGT_MAXS; j++) {
+      const int sl = sb + warp + j * CGT_WARPS;
+      if (sl >= se) break;
+      float vals[16], rc[16];
+      tm_ld16(tw + 16u * (uint32_t)j, vals);
+      rec_ld(j, rc);
+      tm_wait_ld();
+      const int64_t row = (int64_t)sl * 32 + lane;
+      const int base = s_sp[sl - sb], w = (s_sp[sl - sb + 1] - base) >> 5;
+      const int lb = base - e0;
+      float ak[LD];
+#pragma unroll
+      for (int s = 0; s < LD; s++) ak[s] = 0.f;
+#pragma unroll
+      for (int k = 0; k < 16; k++) {
+        if (k < w) {
+          float pv[LD];
+          ld_win<VT, LD>(s_win, s_col[lb + k * 32 + lane], pv);
+#pragma unroll
+          for (int s = 0; s < LD; s++) ak[s] += vals[k] * pv[s];
+        }
+      }
+      if (row < a.n) {
+        float ur[LD];
+        ld_win<VT, LD>(s_win, (int)(row - r0), ur);
+#pragma unroll
+        for (int s = 0; s < LD; s++) {
+          const float v = (float)a.dscale[s] * ak[s] + dg[j][s] * ur[s];
+          const float wv = bcm[j] ? ur[s] : v;
+          acc[s] += (double)wv * (double)ur[s];
+          rc[s] = ur[s] + be[s] * rc[s];
+          rc[4 + s] = wv + be[s] * rc[4 + s];
+        }
+      }
+      rec_st(j, rc);
+    }
+    tm_wait_st();
+  };
+
+  // ---- xi += alpha p, r -= alpha s, u = D^-1 r (window and global); r.u, r.r into acc
+  auto p_rows = [&](const float al[LD], double acc[8]) {
+#pragma unroll
+    for (int j = 0; j < CGT_MAXS; j++) {
+      const int sl = sb + warp + j * CGT_WARPS;
+      if (sl >= se) break;
+      float rc[16];
+      rec_ld(j, rc);
+      tm_wait_ld();
+      const int64_t row = (int64_t)sl * 32 + lane;
+      if (row < a.n) {
+        const int lr = (int)(row - r0);
+        float dv[LD], uv[LD];
+        ld_win<VT, LD>(s_dinv, lr, dv);
+#pragma unroll
+        for (int s = 0; s < LD; s++) {
+          rc[8 + s] += al[s] * rc[s];
+          rc[12 + s] -= al[s] * rc[4 + s];
+          uv[s] = dv[s] * rc[12 + s];
+          acc[s] += (double)rc[12 + s] * (double)uv[s];
+          acc[4 + s] += (double)rc[12 + s] * (double)rc[12 + s];
+        }
+        st_win<VT, LD>(s_win, lr, uv);
+        stv<VT, LD>(a.u, row, uv);
+      }
+      rec_st(j, rc);
+    }
+    tm_wait_st();
+  };
+
+  // ---- x += xi for the lanes in tr (xi of those lanes back to 0)
+  auto add_xi = [&](const int tr[LD]) {
+#pragma unroll
+    for (int j = 0; j < CGT_MAXS; j++) {
+      const int sl = sb + warp + j * CGT_WARPS;
+      if (sl >= se) break;
+      float rc[16];
+      rec_ld(j, rc);
+      tm_wait_ld();
+      const int64_t row = (int64_t)sl * 32 + lane;
+      if (row < a.n) {
+#pragma unroll
+        for (int s = 0; s < LD; s++) {
+          if (tr[s]) {
+            a.x[row * LD + s] += (double)rc[8 + s];
+            rc[8 + s] = 0.f;
+          }
+        }
+      }
+      rec_st(j, rc);
+    }
+    tm_wait_st();
+  };
+
+  // ---- FP64 residual r64 = b - A64 x with x read through the window (CP columns per
+  // pass).  final = false: for the lanes in tr, r = (float) r64 into the records, u =
+  // D^-1 r into global memory (the next product refills the whole window), partials r.u
+  // 0-3, r.r 4-7, b.b 8-11 of acc; final = true: r.r of every lane into acc[0..3].
+  auto refresh = [&](const int tr[LD], double* acc, bool final) {
+    const int W = nown + nhalo;
+    const int e0 = s_sp[0];
+    double* s_x = reinterpret_cast<double*>(s_win);
+#pragma unroll
+    for (int c0 = 0; c0 < LD; c0 += CP) {
+      bool any_c = false;
+#pragma unroll
+      for (int c = 0; c < CP; c++) any_c |= final ? (c0 + c < S) : (tr[c0 + c] != 0);
+      if (!any_c) continue;
+      cp_async_wait_all();
+      __syncthreads();  // the window may still be read (previous pass or product)
+      for (int i = threadIdx.x; i < W; i += blockDim.x) {
+        const int64_t g = (i < nown) ? (int64_t)(r0 + i) : (int64_t)s_halo[i - nown];
+        cp_async<CP * 8>(s_x + (size_t)i * CP, a.x + g * LD + c0);
+      }
+      cp_async_wait_all();
+      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < CGT_MAXS; j++) {
+        const int sl = sb + warp + j * CGT_WARPS;
+        if (sl >= se) break;
+        float rc[16];
+        if (!final) {
+          rec_ld(j, rc);
+          tm_wait_ld();
+        }
+        const int64_t row = (int64_t)sl * 32 + lane;
+        if (row < a.n) {
+          const int lr = (int)(row - r0);
+          double xo[CP], ax[CP];
+#pragma unroll
+          for (int c = 0; c < CP; c++) xo[c] = s_x[lr * CP + c];
+          const bool bcr = a.bc && a.bc[row];
+          if (bcr) {
+#pragma unroll
+            for (int c = 0; c < CP; c++) ax[c] = xo[c];
+          } else {
+            double ak[CP];
+#pragma unroll
+            for (int c = 0; c < CP; c++) ak[c] = 0.0;
+            const int p0 = a.A64.indptr[row], len = a.A64.indptr[row + 1] - p0;
+            const int lb = s_sp[sl - sb] - e0;
+            // eight entries at a time: their value loads are in flight together; the sums
+            // run entry by entry in CSR order
+            for (int k0 = 0; k0 < len; k0 += 8) {
+              double kv[8];
+              int loc[8];
+#pragma unroll
+              for (int u = 0; u < 8; u++) {
+                const bool in = k0 + u < len;
+                kv[u] = in ? __ldg(a.A64.K + p0 + k0 + u) : 0.0;
+                loc[u] = in ? s_col[lb + (k0 + u) * 32 + lane] : 0;
+              }
+#pragma unroll
+              for (int u = 0; u < 8; u++) {
+                if (k0 + u < len) {
+#pragma unroll
+                  for (int c = 0; c < CP; c++) ak[c] += kv[u] * s_x[loc[u] * CP + c];
+                }
+              }
+            }
+#pragma unroll
+            for (int c = 0; c < CP; c++) {
+              const double dr = a.A64.diag ? a.A64.diag[row * LD + c0 + c] : 0.0;
+              ax[c] = a.dscale[c0 + c] * ak[c] + dr * xo[c];
+            }
+          }
+          float dv[LD];
+          ld_win<VT, LD>(s_dinv, lr, dv);
+#pragma unroll
+          for (int c = 0; c < CP; c++) {
+            const int s = c0 + c;
+            const double bv = (s < S) ? a.b[row * LD + s] : 0.0;
+            const double r64 = (s < S) ? bv - ax[c] : 0.0;
+            if (final) {
+              acc[s] += r64 * r64;
+            } else if (tr[s]) {
+              const VT rv = (VT)r64;
+              const VT uv = dv[s] * rv;
+              acc[s] += (double)rv * (double)uv;
+              acc[4 + s] += r64 * r64;
+              acc[8 + s] += bv * bv;
+              rc[12 + s] = rv;
+              a.u[row * LD + s] = uv;
+            }
+          }
+        }
+        if (!final) rec_st(j, rc);
+      }
+      if (!final) tm_wait_st();
+    }
+  };
+
+  auto release = [&]() {
+    tm_fence_before();
+    __syncthreads();
+    if (warp == 0) tm_dealloc(s_taddr, CGT_COLS);
+  };
+
+  // ---- I1: Jacobi diagonal (FP64 values) into shared memory, Dirichlet values into x,
+  // records zero
+#pragma unroll
+  for (int j = 0; j < CGT_MAXS; j++) {
+    const int sl = sb + warp + j * CGT_WARPS;
+    if (sl >= se) break;
+    const int64_t row = (int64_t)sl * 32 + lane;
+    if (row < a.n) {
+      VT dv[LD];
+      if (a.bc && a.bc[row]) {
+#pragma unroll
+        for (int s = 0; s < LD; s++) {
+          dv[s] = VT(0);
+          a.x[row * LD + s] = a.b[row * LD + s];
+        }
+      } else {
+        const int lo = a.A64.indptr[row], hi = a.A64.indptr[row + 1];
+        int l = lo, h = hi;
+        while (l < h) {
+          const int mid = (l + h) >> 1;
+          if (a.A64.indices[mid] < row)
+            l = mid + 1;
+          else
+            h = mid;
+        }
+        const bool found = l < hi && a.A64.indices[l] == row;
+        const double kd = found ? a.A64.K[l] : 0.0;
+#pragma unroll
+        for (int s = 0; s < LD; s++) {
+          double d = a.dscale[s] * kd;
+          if (a.A64.diag) d += a.A64.diag[row * LD + s];
+          dv[s] = (s < S && d != 0.0) ? VT(1.0 / d) : VT(0);
+        }
+      }
+      st_win<VT, LD>(s_dinv, (int)(row - r0), dv);
+    }
+    float z[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) z[k] = 0.f;
+    rec_st(j, z);
+  }
+  tm_wait_st();
+  bool ok = grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
+
+  // ---- I2: r = b - A x, u = D^-1 r for every lane; r.u, r.r, b.b
+  {
+    double acc[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) acc[k] = 0.0;
+    int tr[LD];
+#pragma unroll
+    for (int s = 0; s < LD; s++) tr[s] = 1;
+    if (ok) refresh(tr, acc, false);
+    block_partial<8>(acc, a.part, sh);
+    block_partial<4>(acc + 8, a.part + 12, sh);
+  }
+  ok = ok && grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
+  if (ok) {
+    fill_window(false);
+    grid_totals<8, 0>(a.part, s_tot, s_buf);
+    grid_totals<4, 12>(a.part, s_tot, s_buf);
+  }
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < 4; s++) {
+      const bool use = s < S && ok;
+      const double rz = use ? s_tot[s] : 0.0, rr = use ? s_tot[4 + s] : 0.0;
+      const double bb = use ? s_tot[12 + s] : 0.0;
+      const double rt = use ? a.rtol[s] : 0.0;
+      L.bb[s] = bb;
+      L.tol2[s] = rt * rt * bb;
+      L.rr[s] = rr;
+      L.rtrue[s] = rr;
+      L.rmax2[s] = rr;
+      L.rz[s] = 0.0;  // no previous gamma: beta = 0 in the first product
+      L.alpha[s] = 0.0;
+      L.beta[s] = 0.0;
+      L.trigger[s] = 0;
+      L.frozen[s] = 0;
+      L.iters[s] = 0;
+      s_gm[s] = rz;
+      const bool fin = isfinite(rr) && isfinite(rz);
+      const bool act = use && fin && rr > L.tol2[s];
+      L.active[s] = act;
+      L.status[s] = !use ? TP_OK : (!fin ? TP_ERR_NONFINITE : (act ? -1 : TP_OK));
+    }
+  }
+  __syncthreads();
+  clk.lap(7);  // init phases
+
+  int it = 0, n_rel = 0;
+  bool decided = true;  // the lane state is set for this pass (the init above)
+  while (ok) {
+    if (!decided) {
+      // ---- lane decisions on gamma = r.u and r.r of the last P phase or FP64 refresh.
+      // A lane whose recurrence residual reaches the tolerance freezes (its columns stand
+      // still) until the next FP64 sweep confirms it; a sweep runs for every active lane
+      // when any lane asks for one (its residual dropped by delta, or a restart) or when
+      // every lane still active is frozen.  Every CTA holds the same totals and decides
+      // the same.
+      int want = 0;
+      if (threadIdx.x < S) {
+        const int s = threadIdx.x;
+        if (L.active[s]) {
+          const double gm = s_tot[s], rr = s_tot[4 + s];
+          if (L.trigger[s]) {  // refreshed in FP64 just now
+            L.trigger[s] = 0;
+            L.rtrue[s] = rr;
+            if (!isfinite(rr) || !isfinite(gm)) {
+              L.active[s] = 0;
+              L.status[s] = TP_ERR_NONFINITE;
+              L.iters[s] = it;
+            } else if (rr <= L.tol2[s]) {
+              L.active[s] = 0;
+              L.status[s] = TP_OK;
+              L.iters[s] = it;
+            } else {
+              L.rr[s] = rr;
+              L.rmax2[s] = rr;
+              s_gm[s] = gm;
+              if (L.frozen[s] || s_restart[s]) L.rz[s] = 0.0;  // restart: beta = 0
+              L.frozen[s] = 0;
+              s_restart[s] = 0;
+            }
+          } else if (!L.frozen[s]) {
+            if (!isfinite(gm) || !isfinite(rr)) {
+              L.active[s] = 0;
+              L.status[s] = TP_ERR_NONFINITE;
+              L.iters[s] = it;
+            } else {
+              L.rr[s] = rr;
+              s_gm[s] = gm;
+              if (s_restart[s])
+                want = 1;
+              else if (rr <= L.tol2[s])
+                L.frozen[s] = 1;
+              else
+                want = a.delta2 > 0.0 && rr < a.delta2 * L.rmax2[s];
+            }
+          }
+        }
+      }
+      int any = __syncthreads_or(want);
+      if (!any) {
+        int running = 0, pending = 0;
+        for (int s = 0; s < S; s++) {
+          running |= L.active[s] && !L.frozen[s];
+          pending |= L.active[s] && L.frozen[s];
+        }
+        any = pending && !running;
+      }
+      clk.lap(4);
+      if (any) {
+        // ---- RU: x += xi, then the FP64 residual replaces r and u of every active lane
+        int tr[LD];
+#pragma unroll
+        for (int s = 0; s < LD; s++) tr[s] = (s < S) ? L.active[s] : 0;
+        __syncthreads();  // every thread has read L.active
+        if (threadIdx.x < S) L.trigger[threadIdx.x] = L.active[threadIdx.x];
+        cp_async_wait_all();  // the halo copies issued after the last barrier
+        add_xi(tr);
+        ok = grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
+        if (!ok) break;
+        {
+          double acc[12];
+#pragma unroll
+          for (int k = 0; k < 12; k++) acc[k] = 0.0;
+          refresh(tr, acc, false);
+          block_partial<8>(acc, a.part, sh);
+        }
+        ok = grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
+        if (!ok) break;
+        fill_window(false);
+        grid_totals<8, 0>(a.part, s_tot, s_buf);
+        n_rel++;
+        clk.lap(5);  // reliable update
+        continue;
+      }
+    }
+    decided = false;
+    int nact = 0;
+#pragma unroll
+    for (int s = 0; s < 4; s++) nact += L.active[s];
+    if (!nact || it >= a.max_it) break;
+    // ---- beta of every running lane (0 for frozen lanes and after a restart)
+    __syncthreads();  // every thread has counted the active lanes
+    if (threadIdx.x < S) {
+      const int s = threadIdx.x;
+      const bool run = L.active[s] && !L.frozen[s];
+      L.beta[s] = (run && L.rz[s] != 0.0) ? s_gm[s] / L.rz[s] : 0.0;
+    }
+    __syncthreads();
+    clk.lap(4);
+    {
+      VT be[LD];
+#pragma unroll
+      for (int s = 0; s < LD; s++) be[s] = (s < S) ? (VT)L.beta[s] : VT(0);
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+      product_rows(be, acc);
+      block_partial<4>(acc, a.part + 8, sh);
+    }
+    clk.lap(0);
+    ok = grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
+    clk.lap(1);
+    if (!ok) break;
+    grid_totals<4, 8>(a.part, s_tot, s_buf);
+    // ---- alpha of every running lane
+    if (threadIdx.x < S) {
+      const int s = threadIdx.x;
+      double step = 0.0;
+      if (L.active[s] && !L.frozen[s]) {
+        const double dl = s_tot[8 + s], gm = s_gm[s], beta = L.beta[s];
+        if (!isfinite(dl)) {
+          L.active[s] = 0;
+          L.status[s] = TP_ERR_NONFINITE;
+          L.iters[s] = it;
+        } else if (!(dl > 0.0)) {
+          L.active[s] = 0;
+          L.status[s] = TP_ERR_BREAKDOWN;
+          L.iters[s] = it;
+        } else {
+          const double den =
+              (beta != 0.0 && L.alpha[s] != 0.0) ? dl - beta * gm / L.alpha[s] : dl;
+          if (den > 0.0) {
+            L.alpha[s] = gm / den;
+            L.rz[s] = gm;
+            step = L.alpha[s];
+          } else {
+            s_restart[s] = 1;  // no step; an FP64 refresh restarts the lane
+          }
+        }
+      }
+      s_step[s] = step;
+    }
+    __syncthreads();
+    clk.lap(4);
+    {
+      VT al[LD];
+#pragma unroll
+      for (int s = 0; s < LD; s++) al[s] = (s < S) ? (VT)s_step[s] : VT(0);
+      double acc[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) acc[k] = 0.0;
+      p_rows(al, acc);
+      block_partial<8>(acc, a.part, sh);
+    }
+    it++;
+    clk.lap(2);
+    ok = grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);  // u published
+    clk.lap(3);
+    if (!ok) break;
+    fill_window(true);
+    grid_totals<8, 0>(a.part, s_tot, s_buf);
+  }
+  cp_async_wait_all();
+
+  // ---- final: x += xi and the FP64 residual norms, unless every lane was confirmed by
+  // a sweep (then x and the residual norms are final already; the same decision in every
+  // CTA)
+  bool all_confirmed = true;
+  for (int s = 0; s < S; s++) all_confirmed &= !L.active[s] && L.status[s] == TP_OK;
+  if (ok && all_confirmed) {
+    if (clk.on) {
+      clk.lap(6);
+#pragma unroll
+      for (int k = 0; k < 8; k++) a.prof[blockIdx.x * 8 + k] = clk.acc[k];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) write_result(a, L, true, s_tot, it, n_rel, false);
+    release();
+    return;
+  }
+  if (ok) {
+    int all[LD];
+#pragma unroll
+    for (int s = 0; s < LD; s++) all[s] = s < S;
+    add_xi(all);
+  }
+  bool ok2 = ok && grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
+  {
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    if (ok2) {
+      int none[LD];
+#pragma unroll
+      for (int s = 0; s < LD; s++) none[s] = 0;
+      refresh(none, acc, true);
+    }
+    block_partial<4>(acc, a.part, sh);
+  }
+  ok2 = ok2 && grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
+  if (ok2) grid_totals<4>(a.part, s_tot, s_buf);
+  if (clk.on) {
+    clk.lap(6);
+#pragma unroll
+    for (int k = 0; k < 8; k++) a.prof[blockIdx.x * 8 + k] = clk.acc[k];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) write_result(a, L, ok2, s_tot, it, n_rel);
+  release();
+}
+
+// ----------------------------------------------------------------- pipelined engine
+// k_pcgp: Jacobi-preconditioned pipelined CG (Ghysels-Vanroose) with one grid barrier per
+// iteration.  The standard and Chronopoulos-Gear forms need two global synchronisations
+// per iteration -- the dot products that give alpha, and the exchange of the new vector the
+// product reads -- and on this problem size each costs a barrier plus an L2 round trip for
+// the partial sums.  The pipelined form carries the next product's input m = D^-1 w
+// through recurrences, so one barrier publishes m and the partial sums together, and the
+// reduction's round trip overlaps the product n = A m:
+//
+//   barrier | halo copies of m and the partial-sum loads in flight; n = A m (registers)
+//           | gamma = r.u, delta = w.u, r.r totals; lane decisions; alpha, beta
+//           | z = n + beta z, s = w + beta s, p = u + beta p, xi += alpha p,
+//           | r -= alpha s, w -= alpha z, u = D^-1 r, m = D^-1 w (window and global);
+//           | partials of the next gamma, delta, r.r
+//   barrier | ...
+//
+// With a diagonal preconditioner q = D^-1 s and u = D^-1 r exactly, so the state per row
+// and column is r, w, z, s, p (in tensor memory: one 16-column record per slice row next
+// to the 16 value columns, CW = 3 (LD 4) or LD columns each) and xi (global memory, read
+// ahead of its update).  m is double-buffered in global memory and the partial sums in
+// the partial rows (a single barrier per iteration: a CTA may write the next ones while
+// another still reads the last).
+//
+// FP32 recurrences of the pipelined form drift faster than the two-barrier forms, so the
+// FP64 refresh (x += xi, r = b - A64 x) restarts every refreshed lane (beta = 0); a lane
+// whose recurrence residual grows by 1e4 over its last refresh is refreshed too, and a
+// lane whose sums turn non-finite drops its increment since the last refresh and is
+// refreshed (a second time in a row it fails with TP_ERR_NONFINITE).  Convergence is
+// only ever declared on the FP64 residual.
+constexpr int PGP_MAXS = 4;
+constexpr int PGP_WARPS = 16;
+constexpr uint32_t PGP_COLS = 512;
+
+struct PgpLanes {
+  int poisoned[4];  // the lane's sums were not finite: its xi is dropped at the refresh
+  int fails[4];     // refreshes in a row forced by non-finite sums
+};
+
+template <int LD>
+__global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
+  using VT = float;
+  static_assert(LD == 2 || LD == 4, "FP64 residual windows hold LD / 2 doubles per entry");
+  constexpr int CP = LD / 2;
+  constexpr int CW = (LD == 4) ? 3 : LD;  // record columns per vector (S <= CW)
+  // record layout: z 0, s CW, p 2 CW, r 3 CW, w 4 CW
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  int32_t* s_sp = reinterpret_cast<int32_t*>(s_dyn);
+  int32_t* s_halo = s_sp + a.sp_cap;
+  uint16_t* s_col = reinterpret_cast<uint16_t*>(s_halo + a.halo_cap);
+  VT* s_win = reinterpret_cast<VT*>(
+      s_dyn + ((4 * (size_t)(a.sp_cap + a.halo_cap) + 2 * (size_t)a.col_cap + 15) & ~(size_t)15));
+  VT* s_dinv = s_win + (size_t)a.win_cap * LD;
+  __shared__ double sh[32 * 12];
+  __shared__ double s_buf[512];
+  __shared__ double s_tot[16];
+  __shared__ LaneState L;
+  __shared__ PgpLanes P;
+  __shared__ float s_al[4], s_be[4];
+  __shared__ uint32_t s_taddr;
+  __shared__ unsigned long long s_clk[8];
+  unsigned int target = 0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int sb = (int)((int64_t)blockIdx.x * a.ns / gridDim.x);
+  const int se = (int)((int64_t)(blockIdx.x + 1) * a.ns / gridDim.x);
+  const int S = a.S;
+  const int r0 = sb * 32;
+  const int nown = (se > sb) ? (int)(min((int64_t)se * 32, a.n) - r0) : 0;
+  const int nhalo = a.halo_ptr[blockIdx.x + 1] - a.halo_ptr[blockIdx.x];
+  // double buffers: m (and u in the refresh) alternate between a.u and a.w, the partial
+  // rows between a.part and a.part + 16 gridDim.x
+  auto mbuf = [&](int k) { return k ? a.w : a.u; };
+  int vp = 0;  // buffer of the last published vector
+  int pp = 0;  // partial rows of the last published sums
+  auto part_of = [&](int k) { return a.part + (size_t)k * 16 * gridDim.x; };
+  PhaseClock clk;
+  clk.start(a.prof != nullptr, s_clk);
+  for (int i = threadIdx.x; i <= se - sb; i += blockDim.x) s_sp[i] = a.slice_ptr[sb + i];
+  {
+    const int hb = a.halo_ptr[blockIdx.x];
+    for (int i = threadIdx.x; i < nhalo; i += blockDim.x) s_halo[i] = a.halo[hb + i];
+    if (se > sb) {
+      const int e0 = a.slice_ptr[sb], ne = a.slice_ptr[se] - e0;
+      const uint4* src = reinterpret_cast<const uint4*>(a.loc_col + e0);
+      uint4* dst = reinterpret_cast<uint4*>(s_col);
+      for (int i = threadIdx.x; i < ne / 8; i += blockDim.x) dst[i] = src[i];
+    }
+  }
+  if (threadIdx.x < 4) {
+    P.poisoned[threadIdx.x] = 0;
+    P.fails[threadIdx.x] = 0;
+  }
+  // ---- tensor memory: slice j of warp w: values at tw + 32 j, record at tw + 32 j + 16
+  if (warp == 0) tm_alloc(&s_taddr, PGP_COLS);
+  tm_fence_before();
+  __syncthreads();
+  tm_fence_after();
+  const uint32_t tw = s_taddr + ((uint32_t)(32 * (warp & 3)) << 16) + 128u * (uint32_t)(warp >> 2);
+  auto rec_ld = [&](int j, float rc[16]) { tm_ld16(tw + 32u * (uint32_t)j + 16u, rc); };
+  auto rec_st = [&](int j, const float rc[16]) {
+    uint32_t v[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) v[k] = __float_as_uint(rc[k]);
+    tm_st16(tw + 32u * (uint32_t)j + 16u, v);
+  };
+#pragma unroll
+  for (int j = 0; j < PGP_MAXS; j++) {
+    const int sl = sb + warp + j * PGP_WARPS;
+    uint32_t v[16];
+    const int base = (sl < se) ? a.slice_ptr[sl] : 0;
+    const int w = (sl < se) ? (a.slice_ptr[sl + 1] - base) >> 5 : 0;
+#pragma unroll
+    for (int k = 0; k < 16; k++)
+      v[k] = (k < w) ? __float_as_uint(ld_na(a.sK + base + k * 32 + lane)) : 0u;
+    tm_st16(tw + 32u * (uint32_t)j, v);
+  }
+  tm_wait_st();
+
+  auto fill_window = [&](bool own_done, const VT* src) {
+    const int W = nown + nhalo;
+    for (int i = (own_done ? nown : 0) + threadIdx.x; i < W; i += blockDim.x) {
+      const int64_t g = (i < nown) ? (int64_t)(r0 + i) : (int64_t)s_halo[i - nown];
+      cp_async<LD * 4>(s_win + (size_t)i * LD, src + g * LD);
+    }
+  };
+
+  // partial-sum loads of slots 0..11 (gamma, delta, r.r) of every CTA, issued early;
+  // totals_finish sums them in the fixed order of grid_totals
+  auto totals_load = [&](const double* part, double x[5]) {
+    const int k = threadIdx.x % 16, g = threadIdx.x / 16;
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+      const int b = g + q * 32;
+      x[q] = (k < 12 && b < (int)gridDim.x) ? __ldcg(part + (int64_t)b * 16 + k) : 0.0;
+    }
+  };
+  auto totals_finish = [&](const double* part, double x[5]) {
+    const int k = threadIdx.x % 16, g = threadIdx.x / 16;
+    double v = 0.0;
+#pragma unroll
+    for (int q = 0; q < 5; q++)
+      if (g + q * 32 < (int)gridDim.x) v += x[q];
+    for (int b = g + 5 * 32; b < (int)gridDim.x; b += 32)
+      if (k < 12) v += __ldcg(part + (int64_t)b * 16 + k);
+    s_buf[threadIdx.x] = v;
+    __syncthreads();
+    const int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
+    if (w < 12) {
+      double t = (ln < 32) ? s_buf[ln * 16 + w] : 0.0;
+      t = warp_sum(t);
+      if (ln == 0) s_tot[w] = t;
+    }
+    __syncthreads();
+  };
+
+  // ---- n = A src (the window) of this warp's rows into nr (registers).  The row
+  // diagonals are loaded while the copies into the window land; a Dirichlet row (identity,
+  // D^-1 = 0 in every column) is recognised by its D^-1.
+  auto product_rows = [&](float nr[PGP_MAXS][CW]) {
+    float dgs[PGP_MAXS][CW];
+#pragma unroll
+    for (int j = 0; j < PGP_MAXS; j++) {
+      const int64_t row = (int64_t)(sb + warp + j * PGP_WARPS) * 32 + lane;
+      float dg[LD];
+#pragma unroll
+      for (int s = 0; s < LD; s++) dg[s] = 0.f;
+      if (sb + warp + j * PGP_WARPS < se && row < a.n && a.diag) ldv<VT, LD>(a.diag, row, dg);
+#pragma unroll
+      for (int c = 0; c < CW; c++) dgs[j][c] = dg[c];
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    clk.lap(3);
+    const int e0 = s_sp[0];
+#pragma unroll
+    for (int j = 0; j < PGP_MAXS; j++) {
+      const int sl = sb + warp + j * PGP_WARPS;
+#pragma unroll
+      for (int c = 0; c < CW; c++) nr[j][c] = 0.f;
+      if (sl >= se) continue;
+      const int64_t row = (int64_t)sl * 32 + lane;
+      const bool in = row < a.n;
+      const bool bcr = in && a.bc && s_dinv[(row - r0) * LD] == 0.f;
+      float vals[16];
+      tm_ld16(tw + 32u * (uint32_t)j, vals);
+      tm_wait_ld();
+      const int base = s_sp[sl - sb], w = (s_sp[sl - sb + 1] - base) >> 5;
+      const int lb = base - e0;
+      float ak[LD];
+#pragma unroll
+      for (int s = 0; s < LD; s++) ak[s] = 0.f;
+#pragma unroll
+      for (int k = 0; k < 16; k++) {
+        if (k < w) {
+          float pv[LD];
+          ld_win<VT, LD>(s_win, s_col[lb + k * 32 + lane], pv);
+#pragma unroll
+          for (int s = 0; s < LD; s++) ak[s] += vals[k] * pv[s];
+        }
+      }
+      if (in) {
+        float mr[LD];
+        ld_win<VT, LD>(s_win, (int)(row - r0), mr);
+#pragma unroll
+        for (int c = 0; c < CW; c++) {
+          const float v = (float)a.dscale[c] * ak[c] + dgs[j][c] * mr[c];
+          nr[j][c] = bcr ? mr[c] : v;
+        }
+      }
+    }
+  };
+
+  // ---- the update pass (see the header); partials gamma 0-3, delta 4-7, r.r 8-11.  The
+  // records of two slices are read per tensor-memory round.
+  auto update_rows = [&](const float nr[PGP_MAXS][CW], const float xr[PGP_MAXS][LD],
+                         double acc[12], VT* mdst) {
+    float al[CW], be[CW];
+#pragma unroll
+    for (int c = 0; c < CW; c++) {
+      al[c] = s_al[c];
+      be[c] = s_be[c];
+    }
+    auto one = [&](int j, float rc[16]) {
+      const int64_t row = (int64_t)(sb + warp + j * PGP_WARPS) * 32 + lane;
+      if (row >= a.n) return;
+      const int lr = (int)(row - r0);
+      float dv[LD], mv[LD], xv[LD];
+      ld_win<VT, LD>(s_dinv, lr, dv);
+#pragma unroll
+      for (int s = 0; s < LD; s++) {
+        mv[s] = 0.f;
+        xv[s] = xr[j][s];
+      }
+#pragma unroll
+      for (int c = 0; c < CW; c++) {
+        float& z = rc[c];
+        float& sv = rc[CW + c];
+        float& p = rc[2 * CW + c];
+        float& r = rc[3 * CW + c];
+        float& w = rc[4 * CW + c];
+        z = nr[j][c] + be[c] * z;
+        sv = w + be[c] * sv;
+        p = dv[c] * r + be[c] * p;
+        xv[c] += al[c] * p;
+        r -= al[c] * sv;
+        w -= al[c] * z;
+        const float u = dv[c] * r;
+        mv[c] = dv[c] * w;
+        acc[c] += (double)r * (double)u;
+        acc[4 + c] += (double)w * (double)u;
+        acc[8 + c] += (double)r * (double)r;
+      }
+      st_win<VT, LD>(s_win, lr, mv);
+      stv<VT, LD>(mdst, row, mv);
+      stv<VT, LD>(a.xi, row, xv);
+    };
+#pragma unroll
+    for (int j = 0; j < PGP_MAXS; j += 2) {
+      const bool h0 = sb + warp + j * PGP_WARPS < se;
+      const bool h1 = sb + warp + (j + 1) * PGP_WARPS < se;
+      if (!h0) break;
+      float rc0[16], rc1[16];
+      rec_ld(j, rc0);
+      if (h1) rec_ld(j + 1, rc1);
+      tm_wait_ld();
+      one(j, rc0);
+      rec_st(j, rc0);
+      if (h1) {
+        one(j + 1, rc1);
+        rec_st(j + 1, rc1);
+      }
+    }
+    tm_wait_st();
+  };
+
+  // ---- x += xi for the lanes in tr (dropped for poisoned lanes), xi = 0 for them
+  auto add_xi = [&](const int tr[LD], const int drop[LD]) {
+#pragma unroll
+    for (int j = 0; j < PGP_MAXS; j++) {
+      const int sl = sb + warp + j * PGP_WARPS;
+      if (sl >= se) break;
+      const int64_t row = (int64_t)sl * 32 + lane;
+      if (row < a.n) {
+        VT xv[LD];
+        ldv_cg<VT, LD>(a.xi, row, xv);
+#pragma unroll
+        for (int s = 0; s < LD; s++) {
+          if (tr[s]) {
+            if (!drop[s]) a.x[row * LD + s] += (double)xv[s];
+            xv[s] = VT(0);
+          }
+        }
+        stv<VT, LD>(a.xi, row, xv);
+      }
+    }
+  };
+
+  // ---- FP64 residual through the window (as k_cgt): final = false: for the lanes in tr
+  // r = (float) r64 into the records and u = D^-1 r into udst; partials r.u 0-3, r.r 8-11,
+  // b.b 12-15 (r.r in the slot the decisions read); final = true: r.r of every lane in
+  // acc[0..3]
+  auto refresh = [&](const int tr[LD], double* acc, bool final, VT* udst) {
+    const int W = nown + nhalo;
+    const int e0 = s_sp[0];
+    double* s_x = reinterpret_cast<double*>(s_win);
+#pragma unroll
+    for (int c0 = 0; c0 < LD; c0 += CP) {
+      bool any_c = false;
+#pragma unroll
+      for (int c = 0; c < CP; c++) any_c |= final ? (c0 + c < S) : (tr[c0 + c] != 0);
+      if (!any_c) continue;
+      cp_async_wait_all();
+      __syncthreads();
+      for (int i = threadIdx.x; i < W; i += blockDim.x) {
+        const int64_t g = (i < nown) ? (int64_t)(r0 + i) : (int64_t)s_halo[i - nown];
+        cp_async<CP * 8>(s_x + (size_t)i * CP, a.x + g * LD + c0);
+      }
+      cp_async_wait_all();
+      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < PGP_MAXS; j++) {
+        const int sl = sb + warp + j * PGP_WARPS;
+        if (sl >= se) break;
+        float rc[16];
+        if (!final) {
+          rec_ld(j, rc);
+          tm_wait_ld();
+        }
+        const int64_t row = (int64_t)sl * 32 + lane;
+        if (row < a.n) {
+          const int lr = (int)(row - r0);
+          double xo[CP], ax[CP];
+#pragma unroll
+          for (int c = 0; c < CP; c++) xo[c] = s_x[lr * CP + c];
+          const bool bcr = a.bc && a.bc[row];
+          if (bcr) {
+#pragma unroll
+            for (int c = 0; c < CP; c++) ax[c] = xo[c];
+          } else {
+            double ak[CP];
+#pragma unroll
+            for (int c = 0; c < CP; c++) ak[c] = 0.0;
+            const int p0 = a.A64.indptr[row], len = a.A64.indptr[row + 1] - p0;
+            const int lb = s_sp[sl - sb] - e0;
+            for (int k0 = 0; k0 < len; k0 += 8) {
+              double kv[8];
+              int loc[8];
+#pragma unroll
+              for (int u = 0; u < 8; u++) {
+                const bool in = k0 + u < len;
+                kv[u] = in ? __ldg(a.A64.K + p0 + k0 + u) : 0.0;
+                loc[u] = in ? s_col[lb + (k0 + u) * 32 + lane] : 0;
+              }
+#pragma unroll
+              for (int u = 0; u < 8; u++) {
+                if (k0 + u < len) {
+#pragma unroll
+                  for (int c = 0; c < CP; c++) ak[c] += kv[u] * s_x[loc[u] * CP + c];
+                }
+              }
+            }
+#pragma unroll
+            for (int c = 0; c < CP; c++) {
+              const double dr = a.A64.diag ? a.A64.diag[row * LD + c0 + c] : 0.0;
+              ax[c] = a.dscale[c0 + c] * ak[c] + dr * xo[c];
+            }
+          }
+          float dv[LD];
+          ld_win<VT, LD>(s_dinv, lr, dv);
+#pragma unroll
+          for (int c = 0; c < CP; c++) {
+            const int s = c0 + c;
+            const double bv = (s < S) ? a.b[row * LD + s] : 0.0;
+            const double r64 = (s < S) ? bv - ax[c] : 0.0;
+            if (final) {
+              acc[s] += r64 * r64;
+            } else if (tr[s]) {
+              const VT rv = (VT)r64;
+              const VT uv = dv[s] * rv;
+              acc[s] += (double)rv * (double)uv;
+              acc[8 + s] += r64 * r64;
+              acc[12 + s] += bv * bv;
+              if (s < CW) rc[3 * CW + s] = rv;
+              udst[row * LD + s] = uv;
+            }
+          }
+        }
+        if (!final) rec_st(j, rc);
+      }
+      if (!final) tm_wait_st();
+    }
+  };
+
+  // ---- w = A u after a refresh (u in the window): w into the records of the lanes in tr,
+  // m = D^-1 w into the window and mdst, partials gamma, delta, r.r of the new state
+  auto restart_rows = [&](const int tr[LD], double acc[12], VT* mdst) {
+    float nr[PGP_MAXS][CW];
+    product_rows(nr);
+    __syncthreads();  // every warp has read the window: m may replace u in it
+#pragma unroll
+    for (int j = 0; j < PGP_MAXS; j++) {
+      const int sl = sb + warp + j * PGP_WARPS;
+      if (sl >= se) break;
+      float rc[16];
+      rec_ld(j, rc);
+      tm_wait_ld();
+      const int64_t row = (int64_t)sl * 32 + lane;
+      if (row < a.n) {
+        const int lr = (int)(row - r0);
+        float dv[LD], mv[LD];
+        ld_win<VT, LD>(s_dinv, lr, dv);
+#pragma unroll
+        for (int s = 0; s < LD; s++) mv[s] = 0.f;
+#pragma unroll
+        for (int c = 0; c < CW; c++) {
+          float& r = rc[3 * CW + c];
+          float& w = rc[4 * CW + c];
+          if (tr[c]) w = nr[j][c];
+          const float u = dv[c] * r;
+          mv[c] = dv[c] * w;
+          acc[c] += (double)r * (double)u;
+          acc[4 + c] += (double)w * (double)u;
+          acc[8 + c] += (double)r * (double)r;
+        }
+        st_win<VT, LD>(s_win, lr, mv);
+        stv<VT, LD>(mdst, row, mv);
+      }
+      rec_st(j, rc);
+    }
+    tm_wait_st();
+  };
+
+  auto release = [&]() {
+    tm_fence_before();
+    __syncthreads();
+    if (warp == 0) tm_dealloc(s_taddr, PGP_COLS);
+  };
+
+  auto publish12 = [&](double acc[12], double* part) {
+    block_partial<12>(acc, part, sh);
+  };
+
+  // ---- I1: Jacobi diagonal into shared memory, Dirichlet values into x, records and xi 0
+#pragma unroll
+  for (int j = 0; j < PGP_MAXS; j++) {
+    const int sl = sb + warp + j * PGP_WARPS;
+    if (sl >= se) break;
+    const int64_t row = (int64_t)sl * 32 + lane;
+    if (row < a.n) {
+      VT dv[LD], zero[LD];
+#pragma unroll
+      for (int s = 0; s < LD; s++) zero[s] = VT(0);
+      if (a.bc && a.bc[row]) {
+#pragma unroll
+        for (int s = 0; s < LD; s++) {
+          dv[s] = VT(0);
+          a.x[row * LD + s] = a.b[row * LD + s];
+        }
+      } else {
+        const int lo = a.A64.indptr[row], hi = a.A64.indptr[row + 1];
+        int l = lo, h = hi;
+        while (l < h) {
+          const int mid = (l + h) >> 1;
+          if (a.A64.indices[mid] < row)
+            l = mid + 1;
+          else
+            h = mid;
+        }
+        const bool found = l < hi && a.A64.indices[l] == row;
+        const double kd = found ? a.A64.K[l] : 0.0;
+#pragma unroll
+        for (int s = 0; s < LD; s++) {
+          double d = a.dscale[s] * kd;
+          if (a.A64.diag) d += a.A64.diag[row * LD + s];
+          dv[s] = (s < S && d != 0.0) ? VT(1.0 / d) : VT(0);
+        }
+      }
+      st_win<VT, LD>(s_dinv, (int)(row - r0), dv);
+      stv<VT, LD>(a.xi, row, zero);
+    }
+    float z[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) z[k] = 0.f;
+    rec_st(j, z);
+  }
+  tm_wait_st();
+  bool ok = grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
+
+  // ---- the lane state from an FP64 refresh of the lanes in tr (all lanes at the start):
+  // the residuals were published in partial rows pp and u in buffer vp.  Lanes below the
+  // tolerance are done; the others restart (beta = 0) from w = A u.  Returns false when
+  // no lane goes on.
+  int tr_all[LD];
+#pragma unroll
+  for (int s = 0; s < LD; s++) tr_all[s] = 1;
+  int it = 0, n_rel = 0;
+  bool first = true;
+  auto after_refresh = [&](const int tr[LD]) -> bool {
+    fill_window(false, mbuf(vp));
+    grid_totals<8, 0>(part_of(pp), s_tot, s_buf);
+    grid_totals<8, 8>(part_of(pp), s_tot, s_buf);
+    if (threadIdx.x < 4) {
+      const int s = threadIdx.x;
+      const double gm = s_tot[s], rr = s_tot[8 + s], bb = s_tot[12 + s];
+      if (first) {
+        const bool use = s < S;
+        const double rt = use ? a.rtol[s] : 0.0;
+        L.bb[s] = use ? bb : 0.0;
+        L.tol2[s] = rt * rt * L.bb[s];
+        L.rr[s] = L.rtrue[s] = L.rmax2[s] = use ? rr : 0.0;
+        L.rz[s] = L.alpha[s] = L.beta[s] = 0.0;
+        L.trigger[s] = L.frozen[s] = L.iters[s] = 0;
+        const bool fin = isfinite(rr) && isfinite(gm) && isfinite(bb);
+        const bool act = use && fin && rr > L.tol2[s];
+        L.active[s] = act;
+        L.status[s] = !use ? TP_OK : (!fin ? TP_ERR_NONFINITE : (act ? -1 : TP_OK));
+      } else if (s < S && tr[s] && L.active[s]) {
+        L.rtrue[s] = rr;
+        L.frozen[s] = 0;
+        L.rz[s] = 0.0;  // restart: beta = 0
+        if (!isfinite(rr) || !isfinite(gm)) {
+          L.active[s] = 0;
+          L.status[s] = TP_ERR_NONFINITE;
+          L.iters[s] = it;
+        } else if (rr <= L.tol2[s]) {
+          L.active[s] = 0;
+          L.status[s] = TP_OK;
+          L.iters[s] = it;
+        } else {
+          L.rr[s] = rr;
+          L.rmax2[s] = rr;
+          if (!P.poisoned[s]) P.fails[s] = 0;
+        }
+        P.poisoned[s] = 0;
+      }
+    }
+    first = false;
+    __syncthreads();
+    int nact = 0;
+    for (int s = 0; s < S; s++) nact += L.active[s];
+    if (!nact) return false;
+    double acc[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) acc[k] = 0.0;
+    restart_rows(tr, acc, mbuf(vp ^ 1));
+    vp ^= 1;
+    pp ^= 1;
+    publish12(acc, part_of(pp));
+    return true;
+  };
+
+  // ---- I2: r = b - A x, u = D^-1 r for every lane, then w = A u
+  if (ok) {
+    double acc[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) acc[k] = 0.0;
+    refresh(tr_all, acc, false, mbuf(vp));
+    block_partial<8>(acc, part_of(pp), sh);
+    block_partial<8>(acc + 8, part_of(pp) + 8, sh);
+  }
+  ok = ok && grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
+  bool going = ok && after_refresh(tr_all);
+  ok = ok && grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
+  clk.lap(7);
+
+  while (ok && going) {
+    // ---- after the barrier: m of the halo and the partial sums in flight
+    fill_window(true, mbuf(vp));
+    double tx[5];
+    totals_load(part_of(pp), tx);
+    float nr[PGP_MAXS][CW];
+    product_rows(nr);
+    clk.lap(0);
+    // xi of the own rows, read ahead of the update
+    float xr[PGP_MAXS][LD];
+#pragma unroll
+    for (int j = 0; j < PGP_MAXS; j++) {
+      const int64_t row = (int64_t)(sb + warp + j * PGP_WARPS) * 32 + lane;
+#pragma unroll
+      for (int s = 0; s < LD; s++) xr[j][s] = 0.f;
+      if (sb + warp + j * PGP_WARPS < se && row < a.n) ldv_cg<VT, LD>(a.xi, row, xr[j]);
+    }
+    totals_finish(part_of(pp), tx);
+    // ---- lane decisions (thread s: lane s), the same in every CTA
+    int want = 0;
+    if (threadIdx.x < S) {
+      const int s = threadIdx.x;
+      if (L.active[s] && !L.frozen[s]) {
+        const double gm = s_tot[s], dl = s_tot[4 + s], rr = s_tot[8 + s];
+        if (!isfinite(gm) || !isfinite(dl) || !isfinite(rr)) {
+          if (++P.fails[s] >= 2) {
+            L.active[s] = 0;
+            L.status[s] = TP_ERR_NONFINITE;
+            L.iters[s] = it;
+          } else {
+            P.poisoned[s] = 1;
+            want = 1;
+          }
+        } else if (!(dl > 0.0)) {
+          // w.u = u.Au is exact right after a restart: not positive there means the
+          // operator is not positive definite; later it is recurrence drift
+          if (L.rz[s] == 0.0) {
+            L.active[s] = 0;
+            L.status[s] = TP_ERR_BREAKDOWN;
+            L.iters[s] = it;
+          } else {
+            want = 1;
+          }
+        } else {
+          L.rr[s] = rr;
+          if (rr <= L.tol2[s])
+            L.frozen[s] = 1;
+          else if (rr > 1e4 * L.rmax2[s])
+            want = 1;  // the recurrences drifted off: refresh and restart
+          else
+            want = a.delta2 > 0.0 && rr < a.delta2 * L.rmax2[s];
+        }
+      }
+    }
+    int any = __syncthreads_or(want);
+    if (!any) {
+      int running = 0, pending = 0;
+      for (int s = 0; s < S; s++) {
+        running |= L.active[s] && !L.frozen[s];
+        pending |= L.active[s] && L.frozen[s];
+      }
+      any = pending && !running;
+    }
+    if (!any && it >= a.max_it) break;
+    if (any) {
+      // ---- RU: x += xi, FP64 residual, restart from w = A u
+      clk.lap(4);
+      int tr[LD], drop[LD];
+#pragma unroll
+      for (int s = 0; s < LD; s++) {
+        tr[s] = (s < S) ? L.active[s] : 0;
+        drop[s] = (s < S) ? P.poisoned[s] : 0;
+      }
+      __syncthreads();
+      add_xi(tr, drop);
+      ok = grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
+      if (!ok) break;
+      {
+        double acc[16];
+#pragma unroll
+        for (int k = 0; k < 16; k++) acc[k] = 0.0;
+        refresh(tr, acc, false, mbuf(vp ^ 1));
+        pp ^= 1;
+        block_partial<8>(acc, part_of(pp), sh);
+        block_partial<8>(acc + 8, part_of(pp) + 8, sh);
+      }
+      vp ^= 1;
+      ok = grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
+      if (!ok) break;
+      n_rel++;
+      going = after_refresh(tr);
+      ok = grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
+      clk.lap(5);
+      continue;
+    }
+    // ---- alpha, beta of every running lane (0 for frozen and finished lanes)
+    if (threadIdx.x < 4) {
+      const int s = threadIdx.x;
+      float al = 0.f, be = 0.f;
+      if (s < S && L.active[s] && !L.frozen[s]) {
+        const double gm = s_tot[s], dl = s_tot[4 + s];
+        if (!(dl > 0.0)) {
+          L.active[s] = 0;
+          L.status[s] = TP_ERR_BREAKDOWN;
+          L.iters[s] = it;
+        } else {
+          double beta = (L.rz[s] != 0.0) ? gm / L.rz[s] : 0.0;
+          double den = (beta != 0.0 && L.alpha[s] != 0.0) ? dl - beta * gm / L.alpha[s] : dl;
+          if (!(den > 0.0)) {  // rounding: restart the direction
+            beta = 0.0;
+            den = dl;
+          }
+          L.beta[s] = beta;
+          L.alpha[s] = gm / den;
+          L.rz[s] = gm;
+          al = (float)L.alpha[s];
+          be = (float)beta;
+        }
+      }
+      s_al[s] = al;
+      s_be[s] = be;
+    }
+    __syncthreads();
+    clk.lap(4);
+    {
+      double acc[12];
+#pragma unroll
+      for (int k = 0; k < 12; k++) acc[k] = 0.0;
+      update_rows(nr, xr, acc, mbuf(vp ^ 1));
+      vp ^= 1;
+      pp ^= 1;
+      publish12(acc, part_of(pp));
+    }
+    it++;
+    clk.lap(2);
+    ok = grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
+    clk.lap(1);
+  }
+  cp_async_wait_all();
+
+  bool all_confirmed = true;
+  for (int s = 0; s < S; s++) all_confirmed &= !L.active[s] && L.status[s] == TP_OK;
+  if (ok && all_confirmed) {
+    if (clk.on) {
+      clk.lap(6);
+#pragma unroll
+      for (int k = 0; k < 8; k++) a.prof[blockIdx.x * 8 + k] = clk.acc[k];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) write_result(a, L, true, s_tot, it, n_rel, false);
+    release();
+    return;
+  }
+  if (ok) {
+    int all[LD], none[LD];
+#pragma unroll
+    for (int s = 0; s < LD; s++) {
+      all[s] = s < S;
+      none[s] = 0;
+    }
+    add_xi(all, none);
+  }
+  bool ok2 = ok && grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
+  pp ^= 1;
+  {
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    if (ok2) {
+      int none[LD];
+#pragma unroll
+      for (int s = 0; s < LD; s++) none[s] = 0;
+      refresh(none, acc, true, nullptr);
+    }
+    block_partial<4>(acc, part_of(pp), sh);
+  }
+  ok2 = ok2 && grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
+  if (ok2) grid_totals<4>(part_of(pp), s_tot, s_buf);
+  if (clk.on) {
+    clk.lap(6);
+#pragma unroll
+    for (int k = 0; k < 8; k++) a.prof[blockIdx.x * 8 + k] = clk.acc[k];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) write_result(a, L, ok2, s_tot, it, n_rel);
+  release();
+}
+
 // ----------------------------------------------------------------- SELL-32 build
 __global__ void k_slice_width(int64_t n, const int32_t* __restrict__ indptr, int ns,
                               int32_t* __restrict__ width) {
@@ -1888,8 +3257,9 @@ static void fill_pargs(PArgs<VT>& a, const tp_csr_op* op, const tp_sell* sl, con
   a.tmem_values = 0;
   a.wait_limit_ns = WAIT_LIMIT_NS;
   a.wait_missing = 0;
+  // two rows of 16 partial sums per CTA: the pipelined engine alternates between them
   a.part = reinterpret_cast<double*>(p);
-  p += a256(sizeof(double) * 16 * grid);
+  p += a256(sizeof(double) * 2 * 16 * grid);
   a.bar = reinterpret_cast<PBar*>(p);
   p += a256(sizeof(PBar));
   a.out = reinterpret_cast<POut*>(p);
@@ -2013,7 +3383,7 @@ extern "C" size_t tp_pcg_workspace_bytes(const tp_csr_op* op, int inner_fp32) {
   // partial rows for the largest grid (2 CTAs per SM)
   const int grid = 2 * sm_count();
   const size_t vt = inner_fp32 ? 4 : 8;
-  return 8 * a256(vt * op->ld * (size_t)op->n_rows) + a256(sizeof(double) * 16 * grid) +
+  return 8 * a256(vt * op->ld * (size_t)op->n_rows) + a256(sizeof(double) * 2 * 16 * grid) +
          a256(sizeof(PBar)) + a256(sizeof(POut));
 }
 
@@ -2037,7 +3407,21 @@ static int try_window(tp_pcg_handle* h, const tp_sell* sell, bool hasM, cudaStre
   const size_t head = (4 * (size_t)(w.sp_cap + w.halo_cap) + 2 * (size_t)w.col_cap + 15) & ~(size_t)15;
   // window (own rows + halo), then w of the own rows (at most 32 per slice)
   const size_t d = head + ((size_t)w.win_cap + 32 * (size_t)w.sp_cap) * h->ld * vt;
-  void* fn = pcg_kernel(h->fp32, h->ld, 1, hasM, true);
+  // tensor-memory engine (k_cgt): FP32 without a mass matrix, 16 warps with at most 4
+  // slices each, slices of at most 16 entries, 2 or 4 columns; DISSOLVE_PCG_CGT=0 keeps
+  // k_cgw
+  const int ns = (int)((sell->n_rows + 31) / 32);
+  const int max_sl = (ns + h->grid - 1) / h->grid;
+  const bool tm_fit = h->fp32 && !hasM && h->block == 512 && w.max_width <= 16 && max_sl <= 64;
+  const bool cgt = tm_fit && (h->ld == 2 || h->ld == 4) && h->af.A64.M == nullptr &&
+                   getenv_flag("DISSOLVE_PCG_CGT", 1) != 0;
+  // pipelined form (k_pcgp): the same conditions, at most 3 columns (5 record vectors of
+  // 3 columns next to the 16 value columns); DISSOLVE_PCG_PIPE=0 keeps k_cgt
+  const int S = h->af.S;
+  const bool pipe = cgt && S <= (h->ld == 4 ? 3 : h->ld) && getenv_flag("DISSOLVE_PCG_PIPE", 1) != 0;
+  void* fn = pipe  ? (h->ld == 4 ? (void*)k_pcgp<4> : (void*)k_pcgp<2>)
+             : cgt ? (h->ld == 4 ? (void*)k_cgt<4> : (void*)k_cgt<2>)
+                   : pcg_kernel(h->fp32, h->ld, 1, hasM, true);
   cudaFuncAttributes fa;
   TP_CUDA_TRY(cudaFuncGetAttributes(&fa, fn));
   int optin = 0, dev = 0;
@@ -2071,12 +3455,7 @@ static int try_window(tp_pcg_handle* h, const tp_sell* sell, bool hasM, cudaStre
     a.reg_values = w.max_width <= 16 ? 1 : 0;  // the kernel's register-staging width
     // FP32 values in tensor memory: 16 warps, one round of at most 4 slices per warp
     // (k_cgw's MAXS for FP32 without a mass matrix), slices of at most 16 entries
-    const int ns = (int)((sell->n_rows + 31) / 32);
-    const int max_sl = (ns + h->grid - 1) / h->grid;
-    a.tmem_values = (h->fp32 && !hasM && h->block == 512 && a.reg_values && max_sl <= 64 &&
-                     getenv_flag("DISSOLVE_PCG_TMEM", 1))
-                        ? 1
-                        : 0;
+    a.tmem_values = (tm_fit && getenv_flag("DISSOLVE_PCG_TMEM", 1)) ? 1 : 0;
   };
   if (h->fp32)
     set(h->af);
@@ -2084,7 +3463,7 @@ static int try_window(tp_pcg_handle* h, const tp_sell* sell, bool hasM, cudaStre
     set(h->ad);
   h->fn = fn;
   h->dyn_smem = d;
-  h->window = 1;
+  h->window = pipe ? 3 : (cgt ? 2 : 1);
   return TP_OK;
 }
 

@@ -255,10 +255,13 @@ class PersistentCG:
         return int(g.value), int(b.value)
 
     def engine(self) -> dict:
-        """Engine of the handle: shared-memory window (Chronopoulos-Gear) or streaming."""
+        """Engine of the handle: shared-memory window (Chronopoulos-Gear; `tmem`: with the
+        recurrence vectors in tensor memory; `pipelined`: the one-barrier pipelined form,
+        vectors in tensor memory) or streaming."""
         w, sm = ctypes.c_int(0), ctypes.c_size_t(0)
         call("tp_pcg_engine", self._h, ctypes.byref(w), ctypes.byref(sm))
-        return {"window": bool(w.value), "smem_bytes": int(sm.value)}
+        return {"window": bool(w.value), "tmem": w.value >= 2, "pipelined": w.value == 3,
+                "smem_bytes": int(sm.value)}
 
     def run(self):
         call("tp_pcg_run", self._h, stream_handle())

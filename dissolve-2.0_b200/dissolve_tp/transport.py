@@ -159,8 +159,11 @@ class BatchedTransport:
             self.solver = PersistentCG(self.op, rtol=rtol, max_it=max_it, inner_fp32=inner_fp32,
                                        delta=delta, ctas_per_sm=int(cg.get("ctas_per_sm", 0)))
             self.cg_config["grid"], self.cg_config["block"] = self.solver.grid()
-            self.cg_config["form"] = ("window (Chronopoulos-Gear)" if self.solver.engine()["window"]
-                                      else "streaming")
+            eng = self.solver.engine()
+            self.cg_config["form"] = (
+                "window (pipelined, vectors in tensor memory)" if eng["pipelined"] else
+                "window (Chronopoulos-Gear, vectors in tensor memory)" if eng["tmem"] else
+                "window (Chronopoulos-Gear)" if eng["window"] else "streaming")
         else:
             if autotune and not {"group", "block", "rows_per_tile"} & set(cg):
                 self.assemble_operator()

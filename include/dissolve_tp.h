@@ -505,10 +505,17 @@ TP_API int tp_pcg_grid(tp_pcg_handle* h, int* grid, int* block);
  * CTAs is u = D^-1 r; every CTA keeps u of its rows plus its halo (the columns outside its
  * row range that its rows reference) and 16-bit window-local column indices in shared
  * memory (one CTA per SM, at most 65535 window entries per CTA, the tables within the
- * per-block shared-memory limit).  *window = 0: the streaming engine (standard
- * recurrences, columns and gathers from global memory).  *smem_bytes: dynamic shared
- * memory per CTA.  The environment variable DISSOLVE_PCG_ENGINE=stream at create forces
- * the streaming engine. */
+ * per-block shared-memory limit).  *window = 2: the window engine with the operator
+ * values and every per-row vector of the recurrence (p, s, xi, r) in tensor memory and
+ * D^-1 in shared memory (FP32 inner iterations, no mass matrix, 2 or 4 columns, at most
+ * 2048 rows per CTA, rows of at most 16 entries; DISSOLVE_PCG_CGT=0 at create keeps
+ * engine 1).  *window = 3: the pipelined form of the same Jacobi-PCG (Ghysels-Vanroose,
+ * one grid barrier per iteration; its FP64 refreshes restart the refreshed lanes) with
+ * the same tensor-memory layout, for at most 3 columns (DISSOLVE_PCG_PIPE=0 at create keeps
+ * engine 2).  *window = 0: the streaming engine (standard recurrences, columns and
+ * gathers from global memory).  *smem_bytes: dynamic shared memory per CTA.  The
+ * environment variable DISSOLVE_PCG_ENGINE=stream at create forces the streaming
+ * engine. */
 TP_API int tp_pcg_engine(tp_pcg_handle* h, int* window, size_t* smem_bytes);
 /* per-CTA phase times of the next runs: prof (grid * 8 device u64, ns) receives per CTA
  * [A work, A barrier wait, B work, B barrier wait, scalar updates, reliable updates,

@@ -1,0 +1,128 @@
+"""The tensor-memory engines of the persistent solver -- the Chronopoulos-Gear form with
+the operator values and the recurrence vectors of every row in tensor memory ("cgt"), and
+the one-barrier pipelined form with the same layout ("pipe") -- against the window engine
+("cgw"), the FP64 oracle, themselves (bit reproducibility) and their failure path (a grid
+barrier that runs out).
+
+Bars: every engine iterates in FP32 and declares convergence on the FP64 residual
+(||b - A x|| <= rtol ||b||); solutions agree with the oracle's FP64 direct solves within
+1e-7 relative L2 after every step, and with the window engine's within 1e-9 for the
+Chronopoulos-Gear form (the same recurrences) and 1e-7 for the pipelined form (other
+recurrences: two solutions that each meet the residual bound).
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+def _problem(S, n=12, bc=False):
+    from dissolve_tp.mesh import face_dofs, kuhn_cube
+    m = kuhn_cube(n, 0.2, seed=0)
+    rng = np.random.default_rng(1)
+    coef = np.exp(0.3 * rng.standard_normal(m.n_cells))
+    D, kk = (1.0, 1.0, 2.6, 0.7)[:S], (0.5, 0.0, 0.2, 1.0)[:S]
+    u0 = rng.uniform(0, 1, (m.n_verts, S))
+    bcd = face_dofs(m, 0, "min") if bc else None
+    return m, coef, D, kk, 0.02, u0, bcd
+
+
+def _transport(T, monkeypatch, engine, S, m, coef, D, kk, dt, bcd, rtol=1e-8):
+    monkeypatch.setenv("DISSOLVE_PCG_CGT", "0" if engine == "cgw" else "1")
+    monkeypatch.setenv("DISSOLVE_PCG_PIPE", "1" if engine == "pipe" else "0")
+    tr = T.BatchedTransport(m, coef, D, kk, dt, rtol=rtol, inner_fp32=True,
+                            bc_dofs=bcd, bc_values=[1.0] * S if bcd is not None else None)
+    eng = tr.solver.engine()
+    assert eng["tmem"] == (engine != "cgw") and eng["pipelined"] == (engine == "pipe"), eng
+    return tr
+
+
+@pytest.mark.parametrize("engine,S,bc", [("cgt", 3, False), ("cgt", 2, True), ("cgt", 4, False),
+                                         ("pipe", 3, False), ("pipe", 2, True)])
+def test_tensor_memory_engine_matches_window_engine_and_oracle(cuda_device, monkeypatch, engine,
+                                                               S, bc):
+    """(the pipelined form holds at most 3 columns: 4 species run the "cgt" form)"""
+    from dissolve_tp import transport as T
+    m, coef, D, kk, dt, u0, bcd = _problem(S, bc=bc)
+    fast = _transport(T, monkeypatch, engine, S, m, coef, D, kk, dt, bcd)
+    ref = _transport(T, monkeypatch, "cgw", S, m, coef, D, kk, dt, bcd)
+    detJ, G, JT = orc.geometry(m.coords, m.cells)
+    ip, ix, sm = orc.csr_pattern(m.cells, m.n_verts)
+    As = [orc.assemble(detJ, G, D[s] * coef, np.full(m.n_cells, kk[s]), 1 / dt, 1, sm, ix.size,
+                       bc_dofs=bcd, indptr=ip, indices=ix) for s in range(S)]
+    fast.set_state(u0)
+    ref.set_state(u0)
+    U = u0.copy()
+    for _ in range(3):
+        rf, rr = fast.step(), ref.step()
+        assert rf["converged"] and rr["converged"], (rf, rr)
+        if engine == "cgt":
+            assert abs(rf["iterations"] - rr["iterations"]) <= 3, (rf, rr)
+        else:  # restarts at the FP64 refreshes cost some iterations
+            assert rf["iterations"] <= 1.5 * rr["iterations"] + 10, (rf, rr)
+        for s in range(S):
+            bs = orc.assemble_rhs(m.cells, detJ, U[:, s], None, 1 / dt, 1, bc_dofs=bcd,
+                                  bc_value=1.0)
+            U[:, s] = orc.direct_solve(ip, ix, As[s], bs)
+        uf, ur = fast.state(), ref.state()
+        assert np.linalg.norm(uf - ur) / np.linalg.norm(ur) < (1e-9 if engine == "cgt" else 1e-7)
+        assert np.linalg.norm(uf - U) / np.linalg.norm(U) < 1e-7
+        for s in range(S):
+            assert rf["rnorm"][s] <= 1e-8 * rf["bnorm"][s], rf
+        if bcd is not None:
+            assert np.all(uf[bcd] == 1.0)
+
+
+@pytest.mark.parametrize("engine", ["cgt", "pipe"])
+def test_tensor_memory_engine_is_bit_reproducible(cuda_device, monkeypatch, engine):
+    import torch
+    from dissolve_tp import transport as T
+    m, coef, D, kk, dt, u0, bcd = _problem(3, n=16)
+    tr = _transport(T, monkeypatch, engine, 3, m, coef, D, kk, dt, bcd, rtol=1e-10)
+    tr.set_state(u0)
+    tr.assemble_operator()
+    tr.assemble_rhs()
+    sol = tr.solver
+    outs = []
+    for _ in range(2):
+        sol.x.copy_(tr.U)
+        res = sol.solve()
+        assert res["converged"], res
+        outs.append((sol.x.clone(), res["iterations"], res["n_reliable"]))
+    assert torch.equal(outs[0][0], outs[1][0]) and outs[0][1:] == outs[1][1:]
+
+
+@pytest.mark.parametrize("engine", ["cgt", "pipe"])
+def test_tensor_memory_engine_wait_runs_out_then_recovers(cuda_device, monkeypatch, engine):
+    """Every barrier waits for one CTA that does not exist: the solve ends with
+    TP_ERR_TIMEOUT after the 1 ms limit, releases its tensor memory, and the handle then
+    solves normally with the same bits as before."""
+    import time
+
+    import torch
+    from dissolve_tp import transport as T
+    m, coef, D, kk, dt, u0, bcd = _problem(3, n=16)
+    tr = _transport(T, monkeypatch, engine, 3, m, coef, D, kk, dt, bcd)
+    tr.set_state(u0)
+    tr.assemble_operator()
+    tr.assemble_rhs()
+    sol = tr.solver
+    sol.x.copy_(tr.U)
+    ref = sol.solve()
+    assert ref["converged"], ref
+    x_ref = sol.x.clone()
+    sol.set_wait_limit(1e-3, missing_arrivals=1)
+    sol.x.copy_(tr.U)
+    t0 = time.perf_counter()
+    res = sol.solve()
+    took = time.perf_counter() - t0
+    assert res["status"] == 9 and not res["converged"], res
+    assert list(res["lane_status"]) == [9, 9, 9]
+    assert took < 1.0
+    sol.set_wait_limit(0.0, 0)
+    sol.x.copy_(tr.U)
+    res2 = sol.solve()
+    assert res2["converged"] and res2["iterations"] == ref["iterations"], res2
+    assert torch.equal(sol.x, x_ref)

@@ -303,16 +303,22 @@ def test_inference_wait_runs_out_then_recovers(cuda_device):
 
 
 @pytest.mark.gpu
-def test_network_adds_to_the_projection_in_the_early_steps(cuda_device):
+@pytest.mark.parametrize("engine", ["cgt", "pipe"])
+def test_network_adds_to_the_projection_in_the_early_steps(cuda_device, monkeypatch, engine):
     """Ablation of the learned guess on the 32^3 version of the benchmarked workload: the
     energy-norm projection over past step increments with the trained network's correction
     as one more direction needs fewer CG iterations over steps 2-6 than the same projection
-    without the network (the network's own gain, measured at 6 % on this trajectory), and
-    both beat the previous-step guess of the reference (numerics/solvers.py:367).  Every
-    solve runs to the same tolerance, so the guess changes the iteration count only."""
+    without the network (the network's own gain), and than the previous-step guess of the
+    reference (numerics/solvers.py:367).  Every solve runs to the same tolerance, so the
+    guess changes the iteration count only.  With the Chronopoulos-Gear engine ("cgt"),
+    which keeps its direction across the FP64 refreshes, the projection alone also beats
+    the previous-step guess; the pipelined engine ("pipe") restarts at every refresh, so
+    its iteration count moves in whole refresh cycles (a factor 1e3 of the residual each)
+    and a modestly better start often saves none: only the network's direction moves it."""
     from dissolve_tp import mlp
     from dissolve_tp.mesh import kuhn_cube
     from dissolve_tp.transport import BatchedTransport
+    monkeypatch.setenv("DISSOLVE_PCG_PIPE", "1" if engine == "pipe" else "0")
     m = kuhn_cube(32, 0.2, seed=0)
     coef = np.exp(0.3 * np.random.default_rng(1).standard_normal(m.n_cells))
     u0 = np.random.default_rng(2).uniform(0, 1, (m.n_verts, 3))
@@ -328,8 +334,11 @@ def test_network_adds_to_the_projection_in_the_early_steps(cuda_device):
         assert all(r["converged"] for r in res)
         its[name] = sum(int(r["iterations"]) for r in res[1:])
         states[name] = tr.state()
+    assert tr.solver.engine()["pipelined"] == (engine == "pipe")
     assert its["projection_and_network"] <= 0.98 * its["projection"], its
-    assert its["projection"] < its["previous"], its
+    assert its["projection_and_network"] < its["previous"], its
+    if engine == "cgt":
+        assert its["projection"] < its["previous"], its
     ref = states["previous"]
     for name in ("projection", "projection_and_network"):
         assert np.linalg.norm(states[name] - ref) / np.linalg.norm(ref) < 1e-7
