@@ -93,7 +93,15 @@ struct PArgs {
   int win_cap;                    // window entries (own rows + halo) of the largest CTA
   int reg_values;                 // every slice at most 16 wide: values via registers
   int tmem_values;                // FP32 values resident in tensor memory for the solve
-  double* part;  // gridDim.x * 16
+  // pipelined engine: the halo of each CTA as bulk-copy runs (int4 {global row, window
+  // slot past the own rows, entries, 0}) and the entries left to single copies (halo
+  // positions), per CTA ranges in run_ptr / single_ptr
+  const int4* runs;
+  const int32_t* run_ptr;
+  const uint16_t* single;
+  const int32_t* single_ptr;
+  int single_cap;                 // shared-memory capacity of the single list (entries)
+  double* part;  // gridDim.x * 32: two rows of 16 partial sums per CTA
   PBar* bar;
   POut* out;
   unsigned long long* prof;  // optional: gridDim.x * 8 phase times (ns)
@@ -2335,6 +2343,51 @@ __global__ void __launch_bounds__(512, 1) k_cgt(PArgs<float> a) {
 constexpr int PGP_MAXS = 4;
 constexpr int PGP_WARPS = 16;
 constexpr uint32_t PGP_COLS = 512;
+constexpr int PGP_RUNS_SMEM = 32;  // = PGP_RUNCAP of the host tables
+
+// bulk copy global -> shared (no multicast) completing on an mbarrier; both addresses on
+// 16-byte boundaries, bytes a multiple of 16
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
+                                         uint64_t* bar) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(d), "l"(__cvta_generic_to_global(src)), "r"(bytes), "r"(b)
+      : "memory");
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+  const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes)
+               : "memory");
+}
+// bounded wait for the completion of phase `parity`; false when limit_ns ran out
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          unsigned long long limit_ns) {
+  const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
+  unsigned long long t0 = 0;
+  for (uint32_t spins = 1;; spins++) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}"
+        : "=r"(done)
+        : "r"(b), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if ((spins & 63u) == 0u) {
+      const unsigned long long t = gtime();
+      if (t0 == 0)
+        t0 = t;
+      else if (t - t0 > limit_ns)
+        return false;
+    }
+  }
+}
 
 struct PgpLanes {
   int poisoned[4];  // the lane's sums were not finite: its xi is dropped at the refresh
@@ -2355,6 +2408,14 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
   VT* s_win = reinterpret_cast<VT*>(
       s_dyn + ((4 * (size_t)(a.sp_cap + a.halo_cap) + 2 * (size_t)a.col_cap + 15) & ~(size_t)15));
   VT* s_dinv = s_win + (size_t)a.win_cap * LD;
+  // halo runs and single entries after D^-1
+  int4* s_runs = reinterpret_cast<int4*>(
+      s_dyn + ((((4 * (size_t)(a.sp_cap + a.halo_cap) + 2 * (size_t)a.col_cap + 15) & ~(size_t)15) +
+                ((size_t)a.win_cap + 32 * (size_t)a.sp_cap) * LD * sizeof(VT) + 15) &
+               ~(size_t)15));
+  uint16_t* s_single = reinterpret_cast<uint16_t*>(s_runs + PGP_RUNS_SMEM);
+  __shared__ __align__(8) uint64_t s_mbar;
+  __shared__ uint32_t s_halo_bytes;
   __shared__ double sh[32 * 12];
   __shared__ double s_buf[512];
   __shared__ double s_tot[16];
@@ -2394,6 +2455,20 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
     P.poisoned[threadIdx.x] = 0;
     P.fails[threadIdx.x] = 0;
   }
+  constexpr int EB = LD * (int)sizeof(VT);  // bytes of one window entry
+  const int run0 = a.run_ptr[blockIdx.x], nrun = a.run_ptr[blockIdx.x + 1] - run0;
+  const int sg0 = a.single_ptr[blockIdx.x], nsingle = a.single_ptr[blockIdx.x + 1] - sg0;
+  for (int i = threadIdx.x; i < nrun; i += blockDim.x) s_runs[i] = a.runs[run0 + i];
+  for (int i = threadIdx.x; i < nsingle; i += blockDim.x) s_single[i] = a.single[sg0 + i];
+  if (threadIdx.x == 0) {
+    uint32_t hb = 0;
+    for (int q = 0; q < nrun; q++) hb += (uint32_t)a.runs[run0 + q].z * EB;
+    s_halo_bytes = hb;
+    mbar_init(&s_mbar);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  const int own_bulk_rows = (int)(((int64_t)nown * EB & ~(int64_t)15) / EB);
+  uint32_t mphase = 0;
   // ---- tensor memory: slice j of warp w: values at tw + 32 j, record at tw + 32 j + 16
   if (warp == 0) tm_alloc(&s_taddr, PGP_COLS);
   tm_fence_before();
@@ -2420,12 +2495,47 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
   }
   tm_wait_st();
 
-  auto fill_window = [&](bool own_done, const VT* src) {
-    const int W = nown + nhalo;
-    for (int i = (own_done ? nown : 0) + threadIdx.x; i < W; i += blockDim.x) {
-      const int64_t g = (i < nown) ? (int64_t)(r0 + i) : (int64_t)s_halo[i - nown];
-      cp_async<LD * 4>(s_win + (size_t)i * LD, src + g * LD);
+  // window fill: the halo runs (and the own rows unless the update wrote them) as bulk
+  // copies issued by thread 0 on the mbarrier, the rest as single asynchronous copies;
+  // returns whether bulk copies were issued (the same in every thread)
+  auto fill_window = [&](bool own_done, const VT* src) -> bool {
+    const bool own_bulk = !own_done && own_bulk_rows > 0;
+    const bool bulk = nrun > 0 || own_bulk;
+    if (threadIdx.x == 0 && bulk) {
+      const uint32_t bytes = s_halo_bytes + (own_bulk ? (uint32_t)own_bulk_rows * EB : 0u);
+      asm volatile("fence.proxy.async;" ::: "memory");
+      mbar_expect_tx(&s_mbar, bytes);
+      if (own_bulk) bulk_g2s(s_win, src + (int64_t)r0 * LD, (uint32_t)own_bulk_rows * EB, &s_mbar);
+      for (int q = 0; q < nrun; q++) {
+        const int4 r = s_runs[q];
+        bulk_g2s(s_win + (size_t)(nown + r.y) * LD, src + (int64_t)r.x * LD, (uint32_t)r.z * EB,
+                 &s_mbar);
+      }
     }
+    if (!own_done)
+      for (int i = own_bulk_rows + threadIdx.x; i < nown; i += blockDim.x)
+        cp_async<EB>(s_win + (size_t)i * LD, src + (int64_t)(r0 + i) * LD);
+    for (int i = threadIdx.x; i < nsingle; i += blockDim.x) {
+      const int k = s_single[i];
+      cp_async<EB>(s_win + (size_t)(nown + k) * LD, src + (int64_t)s_halo[k] * LD);
+    }
+    return bulk;
+  };
+  // every copy of the last fill landed (false in every thread when the bulk copies did
+  // not complete within the wait bound: the grid aborts)
+  auto wait_window = [&](bool bulk) -> bool {
+    cp_async_wait_all();
+    bool ok_w = true;
+    if (bulk) {
+      // a second bounded wait after a first that ran out: the copies in flight land before
+      // the CTA gives up
+      ok_w = mbar_wait(&s_mbar, mphase, a.wait_limit_ns);
+      if (!ok_w) mbar_wait(&s_mbar, mphase, a.wait_limit_ns);
+      mphase ^= 1u;
+    }
+    const int bad = __syncthreads_or(!ok_w);
+    if (bad && threadIdx.x == 0) atomicExch(&a.bar->abort, 1u);
+    return !bad;
   };
 
   // partial-sum loads of slots 0..11 (gamma, delta, r.r) of every CTA, issued early;
@@ -2460,7 +2570,12 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
   // ---- n = A src (the window) of this warp's rows into nr (registers).  The row
   // diagonals are loaded while the copies into the window land; a Dirichlet row (identity,
   // D^-1 = 0 in every column) is recognised by its D^-1.
-  auto product_rows = [&](float nr[PGP_MAXS][CW]) {
+  // ---- n = A src (the window) of this warp's rows into nr (registers).  The row
+  // diagonals of all four slices are loaded while the copies into the window land; a
+  // Dirichlet row (identity, D^-1 = 0 in every column) is recognised by its D^-1.  (A
+  // split into the own-column terms, summed while the halo copies land, and the halo
+  // terms after them was measured slower: 10.4 against 3.2 us per product.)
+  auto product_rows = [&](float nr[PGP_MAXS][CW], bool bulk) -> bool {
     float dgs[PGP_MAXS][CW];
 #pragma unroll
     for (int j = 0; j < PGP_MAXS; j++) {
@@ -2472,8 +2587,7 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
 #pragma unroll
       for (int c = 0; c < CW; c++) dgs[j][c] = dg[c];
     }
-    cp_async_wait_all();
-    __syncthreads();
+    if (!wait_window(bulk)) return false;
     clk.lap(3);
     const int e0 = s_sp[0];
 #pragma unroll
@@ -2512,6 +2626,7 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
         }
       }
     }
+    return true;
   };
 
   // ---- the update pass (see the header); partials gamma 0-3, delta 4-7, r.r 8-11.  The
@@ -2697,9 +2812,9 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
 
   // ---- w = A u after a refresh (u in the window): w into the records of the lanes in tr,
   // m = D^-1 w into the window and mdst, partials gamma, delta, r.r of the new state
-  auto restart_rows = [&](const int tr[LD], double acc[12], VT* mdst) {
+  auto restart_rows = [&](const int tr[LD], double acc[12], VT* mdst, bool bulk) -> bool {
     float nr[PGP_MAXS][CW];
-    product_rows(nr);
+    if (!product_rows(nr, bulk)) return false;
     __syncthreads();  // every warp has read the window: m may replace u in it
 #pragma unroll
     for (int j = 0; j < PGP_MAXS; j++) {
@@ -2732,6 +2847,7 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
       rec_st(j, rc);
     }
     tm_wait_st();
+    return true;
   };
 
   auto release = [&]() {
@@ -2799,8 +2915,9 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
   for (int s = 0; s < LD; s++) tr_all[s] = 1;
   int it = 0, n_rel = 0;
   bool first = true;
+  bool wfail = false;  // a window fill did not land within the wait bound
   auto after_refresh = [&](const int tr[LD]) -> bool {
-    fill_window(false, mbuf(vp));
+    const bool bulk = fill_window(false, mbuf(vp));
     grid_totals<8, 0>(part_of(pp), s_tot, s_buf);
     grid_totals<8, 8>(part_of(pp), s_tot, s_buf);
     if (threadIdx.x < 4) {
@@ -2846,7 +2963,10 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
     double acc[12];
 #pragma unroll
     for (int k = 0; k < 12; k++) acc[k] = 0.0;
-    restart_rows(tr, acc, mbuf(vp ^ 1));
+    if (!restart_rows(tr, acc, mbuf(vp ^ 1), bulk)) {
+      wfail = true;
+      return false;
+    }
     vp ^= 1;
     pp ^= 1;
     publish12(acc, part_of(pp));
@@ -2864,16 +2984,19 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
   }
   ok = ok && grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
   bool going = ok && after_refresh(tr_all);
-  ok = ok && grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
+  ok = ok && !wfail && grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
   clk.lap(7);
 
   while (ok && going) {
     // ---- after the barrier: m of the halo and the partial sums in flight
-    fill_window(true, mbuf(vp));
+    const bool bulk = fill_window(true, mbuf(vp));
     double tx[5];
     totals_load(part_of(pp), tx);
     float nr[PGP_MAXS][CW];
-    product_rows(nr);
+    if (!product_rows(nr, bulk)) {
+      ok = false;
+      break;
+    }
     clk.lap(0);
     // xi of the own rows, read ahead of the update
     float xr[PGP_MAXS][LD];
@@ -2958,7 +3081,7 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
       if (!ok) break;
       n_rel++;
       going = after_refresh(tr);
-      ok = grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
+      ok = !wfail && grid_sync(a.bar, target, a.wait_limit_ns, a.wait_missing);
       clk.lap(5);
       continue;
     }
@@ -3160,10 +3283,13 @@ struct tp_pcg_handle {
   int32_t* d_halo_ptr = nullptr;
   int32_t* d_halo = nullptr;
   uint16_t* d_loc_col = nullptr;
+  // pipelined engine: bulk-copy runs and single entries of the halo
+  void* d_runs = nullptr;
   ~tp_pcg_handle() {
     if (d_halo_ptr) cudaFree(d_halo_ptr);
     if (d_halo) cudaFree(d_halo);
     if (d_loc_col) cudaFree(d_loc_col);
+    if (d_runs) cudaFree(d_runs);
   }
 };
 
@@ -3199,6 +3325,7 @@ static void* pcg_kernel(int fp32, int ld, int minb, bool hasM, bool win = false)
 }
 
 static size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
+static size_t a16(size_t x) { return (x + 15) & ~(size_t)15; }
 
 template <typename VT>
 static void fill_pargs(PArgs<VT>& a, const tp_csr_op* op, const tp_sell* sl, const double* b,
@@ -3255,6 +3382,11 @@ static void fill_pargs(PArgs<VT>& a, const tp_csr_op* op, const tp_sell* sl, con
   a.sp_cap = a.halo_cap = a.col_cap = a.win_cap = 0;
   a.reg_values = 0;
   a.tmem_values = 0;
+  a.runs = nullptr;
+  a.run_ptr = nullptr;
+  a.single = nullptr;
+  a.single_ptr = nullptr;
+  a.single_cap = 0;
   a.wait_limit_ns = WAIT_LIMIT_NS;
   a.wait_missing = 0;
   // two rows of 16 partial sums per CTA: the pipelined engine alternates between them
@@ -3274,7 +3406,64 @@ struct WinTables {
   std::vector<int32_t> halo_ptr, halo;
   std::vector<uint16_t> loc_col;
   int sp_cap = 0, halo_cap = 0, col_cap = 0, win_cap = 0, max_width = 0;
+  // bulk-copy runs of the halo and the entries left to single copies (build_runs)
+  std::vector<int4> runs;
+  std::vector<int32_t> run_ptr, single_ptr;
+  std::vector<uint16_t> single;
+  int single_cap = 0;
 };
+
+constexpr int PGP_RUNCAP = 32;  // bulk runs per CTA (shared-memory list)
+constexpr int PGP_MINRUN = 8;   // shortest run copied in bulk (entries)
+
+// The halo of every CTA (sorted global rows, window slots nown + k) split into runs of
+// consecutive rows.  A run of at least PGP_MINRUN entries whose source and destination
+// start on 16-byte boundaries and whose length is a multiple of 16 bytes is one bulk copy
+// (entry bytes eb = 16: always; eb = 8: the even-aligned middle of the run), at most
+// PGP_RUNCAP per CTA; every other entry is a single copy.
+static void build_runs(WinTables& w, int grid, int64_t n, int ns, int eb) {
+  w.runs.clear();
+  w.single.clear();
+  w.run_ptr.assign(grid + 1, 0);
+  w.single_ptr.assign(grid + 1, 0);
+  int max_single = 0;
+  for (int c = 0; c < grid; c++) {
+    const int sb = (int)((int64_t)c * ns / grid), se = (int)((int64_t)(c + 1) * ns / grid);
+    const int64_t r0 = (int64_t)sb * 32, r1 = std::min<int64_t>((int64_t)se * 32, n);
+    const int64_t nown = se > sb ? r1 - r0 : 0;
+    const int h0 = w.halo_ptr[c], h1 = w.halo_ptr[c + 1];
+    int nr = 0;
+    const size_t s0 = w.single.size();
+    for (int k = h0; k < h1;) {
+      int e = k + 1;
+      while (e < h1 && w.halo[e] == w.halo[e - 1] + 1) e++;
+      // run of halo positions [k, e): rows halo[k] .., window slots nown + (k - h0) ..
+      int a = k, b = e;
+      if (eb == 8) {
+        const int64_t g = w.halo[k], slot = nown + (k - h0);
+        if (((g ^ slot) & 1) != 0) {
+          a = b = k;  // source and destination parities differ: no bulk part
+        } else {
+          if (g & 1) a++;
+          if ((b - a) & 1) b--;
+        }
+      }
+      if (b - a >= PGP_MINRUN && nr < PGP_RUNCAP) {
+        w.runs.push_back(make_int4(w.halo[a], (int)(a - h0), b - a, 0));
+        nr++;
+      } else {
+        a = b = k;
+      }
+      for (int q = k; q < e; q++)
+        if (q < a || q >= b) w.single.push_back((uint16_t)(q - h0));
+      k = e;
+    }
+    w.run_ptr[c + 1] = (int32_t)w.runs.size();
+    w.single_ptr[c + 1] = (int32_t)w.single.size();
+    max_single = std::max(max_single, (int)(w.single.size() - s0));
+  }
+  w.single_cap = (max_single + 7) & ~7;
+}
 
 static int build_window(const tp_sell* sell, int grid, cudaStream_t st, WinTables& w, bool* ok) {
   *ok = false;
@@ -3422,15 +3611,21 @@ static int try_window(tp_pcg_handle* h, const tp_sell* sell, bool hasM, cudaStre
   void* fn = pipe  ? (h->ld == 4 ? (void*)k_pcgp<4> : (void*)k_pcgp<2>)
              : cgt ? (h->ld == 4 ? (void*)k_cgt<4> : (void*)k_cgt<2>)
                    : pcg_kernel(h->fp32, h->ld, 1, hasM, true);
+  // the pipelined engine's halo runs and single entries, after D^-1 in shared memory
+  size_t d_pipe = d;
+  if (pipe) {
+    build_runs(w, h->grid, sell->n_rows, ns, h->ld * 4);
+    d_pipe = a16(d) + 16 * (size_t)PGP_RUNCAP + 2 * (size_t)w.single_cap;
+  }
   cudaFuncAttributes fa;
   TP_CUDA_TRY(cudaFuncGetAttributes(&fa, fn));
   int optin = 0, dev = 0;
   TP_CUDA_TRY(cudaGetDevice(&dev));
   TP_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  if (fa.sharedSizeBytes + d + 1024 > (size_t)optin) return TP_OK;  // does not fit
-  TP_CUDA_TRY(raise_smem_limits(fn, d, 1));
+  if (fa.sharedSizeBytes + d_pipe + 1024 > (size_t)optin) return TP_OK;  // does not fit
+  TP_CUDA_TRY(raise_smem_limits(fn, d_pipe, 1));
   int occ = 0;
-  TP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, h->block, d));
+  TP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, h->block, d_pipe));
   if (occ < 1) return TP_OK;
   TP_CUDA_TRY(cudaMalloc(&h->d_halo_ptr, sizeof(int32_t) * w.halo_ptr.size()));
   TP_CUDA_TRY(cudaMalloc(&h->d_halo, sizeof(int32_t) * std::max<size_t>(w.halo.size(), 1)));
@@ -3443,6 +3638,31 @@ static int try_window(tp_pcg_handle* h, const tp_sell* sell, bool hasM, cudaStre
   if (!w.loc_col.empty())
     TP_CUDA_TRY(cudaMemcpyAsync(h->d_loc_col, w.loc_col.data(),
                                 sizeof(uint16_t) * w.loc_col.size(), cudaMemcpyHostToDevice, st));
+  if (pipe) {
+    // one allocation: runs (int4), run_ptr, single_ptr (int32), single (uint16)
+    const size_t b_runs = a256(sizeof(int4) * std::max<size_t>(w.runs.size(), 1));
+    const size_t b_ptr = a256(sizeof(int32_t) * w.run_ptr.size());
+    const size_t b_single = a256(sizeof(uint16_t) * std::max<size_t>(w.single.size(), 8));
+    TP_CUDA_TRY(cudaMalloc(&h->d_runs, b_runs + 2 * b_ptr + b_single));
+    char* base = static_cast<char*>(h->d_runs);
+    if (!w.runs.empty())
+      TP_CUDA_TRY(cudaMemcpyAsync(base, w.runs.data(), sizeof(int4) * w.runs.size(),
+                                  cudaMemcpyHostToDevice, st));
+    TP_CUDA_TRY(cudaMemcpyAsync(base + b_runs, w.run_ptr.data(),
+                                sizeof(int32_t) * w.run_ptr.size(), cudaMemcpyHostToDevice, st));
+    TP_CUDA_TRY(cudaMemcpyAsync(base + b_runs + b_ptr, w.single_ptr.data(),
+                                sizeof(int32_t) * w.single_ptr.size(), cudaMemcpyHostToDevice,
+                                st));
+    if (!w.single.empty())
+      TP_CUDA_TRY(cudaMemcpyAsync(base + b_runs + 2 * b_ptr, w.single.data(),
+                                  sizeof(uint16_t) * w.single.size(), cudaMemcpyHostToDevice,
+                                  st));
+    h->af.runs = reinterpret_cast<const int4*>(base);
+    h->af.run_ptr = reinterpret_cast<const int32_t*>(base + b_runs);
+    h->af.single_ptr = reinterpret_cast<const int32_t*>(base + b_runs + b_ptr);
+    h->af.single = reinterpret_cast<const uint16_t*>(base + b_runs + 2 * b_ptr);
+    h->af.single_cap = w.single_cap;
+  }
   TP_CUDA_TRY(cudaStreamSynchronize(st));
   auto set = [&](auto& a) {
     a.halo_ptr = h->d_halo_ptr;
@@ -3462,7 +3682,7 @@ static int try_window(tp_pcg_handle* h, const tp_sell* sell, bool hasM, cudaStre
   else
     set(h->ad);
   h->fn = fn;
-  h->dyn_smem = d;
+  h->dyn_smem = d_pipe;
   h->window = pipe ? 3 : (cgt ? 2 : 1);
   return TP_OK;
 }

@@ -33,12 +33,17 @@ def build_oracle(verbose: bool = False) -> str:
     return out
 
 
+# where the reference checkout is mounted when it is (this build recipe reads its kernel
+# sources there); DISSOLVE_REFERENCE_ROOT names another checkout
+REFERENCE_MOUNT = os.environ.get("DISSOLVE_REFERENCE_ROOT", "/root/reference")
+
+
 def build_all(verbose: bool = False):
     build_oracle(verbose)
     from oracle import ref_recipe
 
-    if ref_recipe.reference_present():
-        ref_recipe.build(verbose=verbose)
+    if ref_recipe.reference_present(REFERENCE_MOUNT):
+        ref_recipe.build(REFERENCE_MOUNT, verbose=verbose)
 
 
 if __name__ == "__main__":

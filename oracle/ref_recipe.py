@@ -26,18 +26,27 @@ import shutil
 import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_ROOT = os.environ.get("DISSOLVE_REFERENCE_ROOT", "/root/reference")
-REF_FILE = os.path.join(REF_ROOT, "gpu", "gpu_assembler.py")
+# the reference checkout: an argument of build() / the command line, else this variable
+REF_ROOT = os.environ.get("DISSOLVE_REFERENCE_ROOT")
 OUT = os.path.join(HERE, "_ref")
 KERNEL_VARS = ("_ASSEMBLE_KERNEL", "_BC_KERNEL_SRC", "_RHS_KERNEL_SRC",
                "_RHS_BC_KERNEL_SRC", "_GRAD_KERNEL_SRC")
 
 
-def reference_present() -> bool:
-    return os.path.exists(REF_FILE)
+def ref_file(ref_root: str | None = None) -> str:
+    root = ref_root or REF_ROOT
+    if not root:
+        raise RuntimeError("the reference checkout is not given: pass its root or set "
+                           "DISSOLVE_REFERENCE_ROOT")
+    return os.path.join(root, "gpu", "gpu_assembler.py")
 
 
-def extract_sources(path: str = REF_FILE) -> dict[str, str]:
+def reference_present(ref_root: str | None = None) -> bool:
+    root = ref_root or REF_ROOT
+    return bool(root) and os.path.exists(ref_file(root))
+
+
+def extract_sources(path: str) -> dict[str, str]:
     tree = ast.parse(open(path).read())
     found = {}
     for node in tree.body:
@@ -87,8 +96,8 @@ def _wrapper(name, params, gpu: bool) -> str:
             f"    }}\n}}\n")
 
 
-def write_sources(workdir: str) -> tuple[str, str, list]:
-    srcs = extract_sources()
+def write_sources(workdir: str, ref_root: str | None = None) -> tuple[str, str, list]:
+    srcs = extract_sources(ref_file(ref_root))
     body = "\n".join(srcs[k] for k in KERNEL_VARS)
     kernels = parse_kernels(body)
     cpu = os.path.join(workdir, "ref_kernels_cpu.cpp")
@@ -108,17 +117,19 @@ def write_sources(workdir: str) -> tuple[str, str, list]:
     return cpu, gpu, kernels
 
 
-def build(verbose: bool = False, gpu: bool = True) -> dict:
-    """Compile in a temporary directory; only the two libraries land in oracle/_ref/."""
+def build(ref_root: str | None = None, verbose: bool = False, gpu: bool = True) -> dict:
+    """Compile the kernels of the reference checkout at ref_root (else
+    DISSOLVE_REFERENCE_ROOT) in a temporary directory; only the two libraries land in
+    oracle/_ref/."""
     import tempfile
 
     os.makedirs(OUT, exist_ok=True)
     with tempfile.TemporaryDirectory(prefix="ref_recipe_") as work:
-        return _build_in(work, verbose, gpu)
+        return _build_in(work, ref_root, verbose, gpu)
 
 
-def _build_in(work: str, verbose: bool, gpu: bool) -> dict:
-    cpu_src, gpu_src, kernels = write_sources(work)
+def _build_in(work: str, ref_root: str | None, verbose: bool, gpu: bool) -> dict:
+    cpu_src, gpu_src, kernels = write_sources(work, ref_root)
     outs = {}
     cpu_so = os.path.join(OUT, "libref_kernels_cpu.so")
     cmd = ["g++", "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-I", HERE,
@@ -140,7 +151,10 @@ def _build_in(work: str, verbose: bool, gpu: bool) -> dict:
 
 
 if __name__ == "__main__":
-    r = build(verbose=True)
+    import sys
+
+    # python -m oracle.ref_recipe <reference checkout>   (or DISSOLVE_REFERENCE_ROOT)
+    r = build(sys.argv[1] if len(sys.argv) > 1 else None, verbose=True)
     print({k: v for k, v in r.items() if k != "kernels"})
     for name, params in r["kernels"]:
         print(name, [n for _, n in params])

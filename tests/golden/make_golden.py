@@ -1,6 +1,7 @@
 """Generate golden vectors by running the reference's own gpu_assembler.py on the CPU.
 
-    python tests/golden/make_golden.py        # needs the reference mounted; writes *.npz here
+    python tests/golden/make_golden.py <reference checkout>    # writes *.npz here
+    (or DISSOLVE_REFERENCE_ROOT=<reference checkout> python tests/golden/make_golden.py)
 
 The reference module (gpu/gpu_assembler.py) imports cupy, petsc4py and mpi4py,
 none of which exist in this image.  This script imports the module UNMODIFIED
@@ -39,7 +40,7 @@ sys.path.insert(0, os.path.join(REPO, "dissolve-2.0_b200"))
 from oracle import ref_recipe  # noqa: E402
 from dissolve_tp.mesh import kuhn_cube, face_dofs  # noqa: E402
 
-REF_GPU_ASSEMBLER = os.path.join(ref_recipe.REF_ROOT, "gpu", "gpu_assembler.py")
+REF_GPU_ASSEMBLER = None  # set by main() from the command line or DISSOLVE_REFERENCE_ROOT
 
 
 # ----------------------------------------------------------------------------- stand-ins
@@ -231,8 +232,10 @@ def run_case(mod, name, n, jitter, seed):
 
 
 def main():
+    global REF_GPU_ASSEMBLER
+    REF_GPU_ASSEMBLER = ref_recipe.ref_file(sys.argv[1] if len(sys.argv) > 1 else None)
     if not os.path.exists(REF_GPU_ASSEMBLER):
-        raise SystemExit(f"reference not mounted at {REF_GPU_ASSEMBLER}")
+        raise SystemExit(f"no reference gpu_assembler.py at {REF_GPU_ASSEMBLER}")
     mod = load_reference_assembler()
     for case in CASES:
         o = run_case(mod, *case)
