@@ -621,8 +621,11 @@ def reference_kernel_baseline(dm, De, alpha, ours64, flush, hbm):
 
 def setup_times(m):
     """Mesh setup on the GPU at this workload: geometry, incidence, CSR pattern and the
-    element-to-nonzero slots (DeviceMesh), then the reference-layout scatter map on
-    request; host wall time around each (the setup calls synchronise)."""
+    element-to-nonzero slots (DeviceMesh), the row tiles of the tiled kernels, then the
+    reference-layout scatter map on request; host wall time around each (the setup calls
+    synchronise).  Beside it, the reference's own setup (GPUSparseAssembler.__init__ of
+    gpu/gpu_assembler.py:331-450) timed on the CPU by tests/golden/time_reference_setup.py
+    (recorded in tests/golden/ref_setup_timing.json; its Python and numpy work alone)."""
     import torch
 
     from dissolve_tp.assembler import DeviceMesh
@@ -630,16 +633,28 @@ def setup_times(m):
     for rep in range(2):  # the first run pays one-time module loading
         torch.cuda.synchronize()
         t = time.perf_counter()
-        dm = DeviceMesh(m.coords, m.cells)
+        dm = DeviceMesh(m.coords, m.cells, tile_rows=0)
         torch.cuda.synchronize()
         t1 = time.perf_counter()
-        _ = dm.scatter_map
+        dm.set_tiles(64)
         torch.cuda.synchronize()
         t2 = time.perf_counter()
-        out = {"device_mesh_s": round(t1 - t, 4), "scatter_map_s": round(t2 - t1, 4),
+        _ = dm.scatter_map
+        torch.cuda.synchronize()
+        t3 = time.perf_counter()
+        out = {"device_mesh_s": round(t1 - t, 4), "tiles_s": round(t2 - t1, 4),
+               "scatter_map_s": round(t3 - t2, 4),
                "includes": "H2D of coords and cells, geometry, incidence, pattern (two "
-                           "passes), slots; scatter map built only on request"}
+                           "passes), slots; row tiles (host-built tables); scatter map built "
+                           "only on request"}
         del dm
+    try:
+        ref = json.load(open(os.path.join(REPO, "tests", "golden", "ref_setup_timing.json")))
+        out["reference_setup_s"] = ref["setup_64cube_s"]
+        out["reference_setup_note"] = ("GPUSparseAssembler.__init__ on this mesh, timed on "
+                                       "the CPU of the build container: " + ref["what"])
+    except (OSError, KeyError, ValueError):
+        pass
     return out
 
 
