@@ -305,6 +305,7 @@ def run_ours(args, rank, world, local_rank):
                    "before every timed step", "parallelism": f"replicas x{world}",
                    "cg_launch": fast.cg_config},
         "converged": conv, "cg_iterations": iters,
+        "learned_guess_training": getattr(fast.predictor, "timings", None) if learned else None,
         "gpu_launches": launches,
         "roofline": roof,
         "clocks": clk.summary(),

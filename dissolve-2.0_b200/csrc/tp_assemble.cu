@@ -1485,6 +1485,93 @@ extern "C" int tp_redistance(const tp_mesh* m, double* phi, int iters, double h_
   return TP_OK;
 }
 
+// ----------------------------------------------------------------- level set from regions
+// domain/mesh_utils.py:367-449 (_init_phi_from_regions): a vertex of any cell with the
+// scaffold label is inside (+1), every other vertex outside (-1); the interface vertices
+// are those of at least one scaffold cell and one other cell; phi = sign * the distance to
+// the nearest interface vertex, or sign * 0.5 when there is none.  Distances are
+// sqrt((dx dx + dy dy) + dz dz) in FP64 with every operation rounded once, and the minimum
+// over all interface vertices is exact and order-free, as the reference's KD-tree query.
+__global__ void k_region_marks(int64_t n, const int4* __restrict__ cells,
+                               const int32_t* __restrict__ regions, int label,
+                               int32_t* __restrict__ marks) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    const int4 v = cells[c];
+    const int mk = (regions[c] == label) ? 1 : 2;
+    atomicOr(marks + v.x, mk);
+    atomicOr(marks + v.y, mk);
+    atomicOr(marks + v.z, mk);
+    atomicOr(marks + v.w, mk);
+  }
+}
+
+// coordinates of the interface vertices (marks 3) appended to list; count in *count
+__global__ void k_interface_list(int64_t nv, const int32_t* __restrict__ marks,
+                                 const double4* __restrict__ X, double4* __restrict__ list,
+                                 int32_t* __restrict__ count) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    if (marks[v] == 3) list[atomicAdd(count, 1)] = X[v];
+  }
+}
+
+constexpr int PHI_CHUNK = 1024;  // interface points staged per round (32 KB)
+
+__global__ void __launch_bounds__(256) k_phi_nearest(int64_t nv, const int32_t* __restrict__ marks,
+                                                     const double4* __restrict__ X,
+                                                     const double4* __restrict__ list,
+                                                     const int32_t* __restrict__ count,
+                                                     double* __restrict__ phi) {
+  __shared__ double4 s_pts[PHI_CHUNK];
+  const int ni = *count;
+  const int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const bool in = v < nv;
+  const double sign = (in && (marks[v] & 1)) ? 1.0 : -1.0;
+  const double4 x = in ? X[v] : make_double4(0.0, 0.0, 0.0, 0.0);
+  double best = INFINITY;
+  for (int b = 0; b < ni; b += PHI_CHUNK) {
+    const int m = min(PHI_CHUNK, ni - b);
+    __syncthreads();
+    for (int i = threadIdx.x; i < m; i += blockDim.x) s_pts[i] = list[b + i];
+    __syncthreads();
+    for (int i = 0; i < m; i++) {
+      const double4 p = s_pts[i];
+      const double dx = __dsub_rn(x.x, p.x), dy = __dsub_rn(x.y, p.y), dz = __dsub_rn(x.z, p.z);
+      const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+      best = fmin(best, d2);
+    }
+  }
+  if (in) phi[v] = (ni == 0) ? sign * 0.5 : sign * __dsqrt_rn(best);
+}
+
+extern "C" size_t tp_phi_from_regions_scratch_bytes(int64_t n_verts) {
+  const auto a256 = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  return a256(sizeof(int32_t) * (size_t)n_verts) + 256 + sizeof(double4) * (size_t)n_verts;
+}
+
+extern "C" int tp_phi_from_regions(const tp_mesh* m, const int32_t* regions, int scaffold_label,
+                                   double* phi, void* scratch, void* stream) {
+  TP_REQUIRE(mesh_ok(m) && m->coords4 && regions && phi && scratch, "null pointer");
+  if (m->n_verts == 0) return TP_OK;
+  cudaStream_t st = as_stream(stream);
+  const size_t mb = (sizeof(int32_t) * (size_t)m->n_verts + 255) & ~(size_t)255;
+  int32_t* marks = static_cast<int32_t*>(scratch);
+  int32_t* count = reinterpret_cast<int32_t*>(static_cast<char*>(scratch) + mb);
+  double4* list = reinterpret_cast<double4*>(static_cast<char*>(scratch) + mb + 256);
+  TP_CUDA_TRY(cudaMemsetAsync(scratch, 0, mb + 256, st));
+  if (m->n_cells > 0)
+    k_region_marks<<<grid_for(m->n_cells, 256, 65535), 256, 0, st>>>(
+        m->n_cells, reinterpret_cast<const int4*>(m->cells), regions, scaffold_label, marks);
+  const double4* X = reinterpret_cast<const double4*>(m->coords4);
+  k_interface_list<<<grid_for(m->n_verts, 256, 65535), 256, 0, st>>>(m->n_verts, marks, X, list,
+                                                                     count);
+  k_phi_nearest<<<grid_for(m->n_verts, 256), 256, 0, st>>>(m->n_verts, marks, X, list, count,
+                                                          phi);
+  TP_LAUNCH_CHECK();
+  return TP_OK;
+}
+
 extern "C" int tp_mean_cell_diameter(const tp_mesh* m, double* out_dev, void* scratch,
                                      void* stream) {
   TP_REQUIRE(mesh_ok(m) && m->coords4 && out_dev && scratch, "null pointer");

@@ -135,6 +135,8 @@ SIGNATURES = {
     "tp_redistance": (ctypes.c_int, [_P(TpMesh), _vp, ctypes.c_int, _c_dbl, _c_dbl, _c_dbl, _vp,
                                      _vp]),
     "tp_mean_cell_diameter": (ctypes.c_int, [_P(TpMesh), _vp, _vp, _vp]),
+    "tp_phi_from_regions_scratch_bytes": (ctypes.c_size_t, [_c_i64]),
+    "tp_phi_from_regions": (ctypes.c_int, [_P(TpMesh), _vp, ctypes.c_int, _vp, _vp, _vp]),
     "tp_advance_state": (ctypes.c_int, [_c_i64, _vp, _vp, _vp, _vp, _vp]),
     "tp_advance_history": (ctypes.c_int, [_c_i64, _vp, _vp, _vp, ctypes.c_int,
                                           _P(ctypes.c_void_p), _P(ctypes.c_void_p), _vp]),

@@ -14,6 +14,7 @@ from __future__ import annotations
 
 import ctypes
 import math
+import time
 
 import numpy as np
 import torch
@@ -238,11 +239,20 @@ def attach_trained_predictor(fast, mesh, coef, u_ref, D, K, DT, train_steps=12,
                            guess="previous", asm=fast.asm)
     u_train = np.random.default_rng(seed).uniform(0.0, 1.0, np.asarray(u_ref).shape)
     gen.set_state(u_train)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
     pairs, ops = trajectory_pairs(gen, train_steps + 1)
     mlp = WarmStartMLP(fast.device, seed=seed)
     mlp.fit_normalization(pairs, fast.S, D, K, ops=ops)
     mlp.add_pairs(pairs, fast.S, fast.ld, D, K, ops=ops)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
     log = mlp.train(steps=epochs, log_every=100 if verbose else 0)
+    torch.cuda.synchronize()
+    # wall time of the trajectory (FP64 solves, features) and of the training steps
+    mlp.timings = {"trajectory_s": round(t1 - t0, 4), "train_s": round(time.perf_counter() - t1, 4),
+                   "train_steps": epochs, "rows_per_step": min(65536, mlp.rows),
+                   "training_rows": int(mlp.rows)}
     if verbose:
         print("mlp training loss", log)
     fast.predictor = mlp

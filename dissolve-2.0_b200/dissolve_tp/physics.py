@@ -96,3 +96,18 @@ def redistance(dm, phi: torch.Tensor, num_iters: int = 8, h_avg: float | None = 
     call("tp_redistance", ctypes.byref(dm.tpm), ptr(phi), int(num_iters), h, float(band_factor),
          float(eps_factor), ptr(scratch), stream_handle())
     return phi
+
+
+def phi_from_regions(dm, regions, scaffold_label: int = 1) -> torch.Tensor:
+    """Level set from cell region labels (domain/mesh_utils.py:367-449): + inside the
+    scaffold cells' vertices, - elsewhere, magnitude the distance to the nearest vertex
+    shared by a scaffold cell and another cell (0.5 when there is none).  regions: one
+    int label per cell (load_mesh's cell tags)."""
+    reg = to_device(np.asarray(regions, dtype=np.int32) if not isinstance(regions, torch.Tensor)
+                    else regions, torch.int32, dm.device)
+    phi = torch.empty(dm.n_verts, dtype=torch.float64, device=dm.device)
+    nb = int(_lib.lib.tp_phi_from_regions_scratch_bytes(dm.n_verts))
+    scratch = torch.empty(max(nb, 8) // 8 + 1, dtype=torch.float64, device=dm.device)
+    call("tp_phi_from_regions", ctypes.byref(dm.tpm), ptr(reg), int(scaffold_label), ptr(phi),
+         ptr(scratch), stream_handle())
+    return phi

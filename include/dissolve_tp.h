@@ -278,6 +278,16 @@ TP_API size_t tp_redistance_scratch_bytes(int64_t n_verts);
 TP_API int tp_redistance(const tp_mesh* m, double* phi, int iters, double h_avg,
                          double band_factor, double eps_factor, void* scratch, void* stream);
 
+/* domain/mesh_utils.py:367-449 (_init_phi_from_regions): the level set from cell region
+ * labels (regions: n_cells int32; the scaffold cells carry scaffold_label).  Vertices of a
+ * scaffold cell are inside (+), the others outside (-); phi (n_verts) = sign times the
+ * distance to the nearest interface vertex (a vertex of a scaffold cell and of another
+ * cell), or sign times 0.5 when there is none.  FP64 distances, each operation rounded
+ * once; the nearest search is exhaustive.  scratch >= tp_phi_from_regions_scratch_bytes. */
+TP_API size_t tp_phi_from_regions_scratch_bytes(int64_t n_verts);
+TP_API int tp_phi_from_regions(const tp_mesh* m, const int32_t* regions, int scaffold_label,
+                               double* phi, void* scratch, void* stream);
+
 /* Sum over cells of the cell diameter (longest edge), into out_dev (1 double); divided by
  * n_cells it is the h_avg of domain/mesh_utils.py:559-575 (dolfinx mesh.h).
  * scratch >= 1024 doubles. */

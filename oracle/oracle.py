@@ -309,6 +309,28 @@ def redistance(cells, detJ, JinvT, phi, iters, h_avg, band_factor=3.0, eps_facto
         phi = phi + np.where(mask, 0.0, dtau * sign * (1.0 - gm))
     return phi
 
+def phi_from_regions(coords, cells, regions, scaffold_label=1):
+    """domain/mesh_utils.py:367-449 (_init_phi_from_regions) on a P1 mesh whose dofs are its
+    vertices: vertices of scaffold cells +1, others -1; interface vertices = in a scaffold
+    cell and in another cell; phi = sign * (distance to the nearest interface vertex by a
+    KD-tree query, as the reference), or sign * 0.5 without interface vertices."""
+    from scipy.spatial import cKDTree
+
+    nv = coords.shape[0]
+    scaf = regions == scaffold_label
+    sign = np.full(nv, -1.0)
+    sign[np.unique(cells[scaf])] = 1.0
+    in_s = np.zeros(nv, bool)
+    in_f = np.zeros(nv, bool)
+    in_s[cells[scaf].ravel()] = True
+    in_f[cells[~scaf].ravel()] = True
+    iface = np.nonzero(in_s & in_f)[0]
+    if iface.size == 0:
+        return sign * 0.5
+    dist, _ = cKDTree(coords[iface]).query(coords)
+    return sign * dist
+
+
 def under_relax(u_new, u_old, omega):
     """numerics/solvers.py:278-279."""
     return omega * u_new + (1.0 - omega) * u_old
