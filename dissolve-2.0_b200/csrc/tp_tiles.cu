@@ -12,6 +12,9 @@
 // unstructured and jittered meshes alike; the depth-first order puts neighbouring tiles
 // next to each other in the launch, so cell records shared by them stay in L2.
 #include <algorithm>
+#include <cstdio>
+#include <functional>
+#include <thread>
 #include <vector>
 
 #include "tp_tiles.cuh"
@@ -105,97 +108,151 @@ extern "C" int tp_tiles_create(const tp_mesh* m, int rows_per_tile, void* stream
   std::vector<int32_t> rows((size_t)nt * R, -1), dpos((size_t)nt * R, -1);
   std::vector<int32_t> cell_ptr(nt + 1, 0), dterm_ptr(nt + 1, 0), edge_ptr(nt + 1, 0),
       eterm_ptr(nt + 1, 0);
+  // Tiles are independent: contiguous tile ranges are built on host threads into local
+  // buffers (per-tile sizes in the *_ptr slots), then concatenated in tile order, so the
+  // tables are the same whatever the thread count.
+  struct Local {
+    std::vector<int32_t> cells;
+    std::vector<uint16_t> dterms, eterms;
+    std::vector<int2> edges, edge_rv;
+    int max_cells = 0, max_edges = 0, rc = TP_OK;
+    char msg[160] = {0};
+  };
+  auto build_range = [&](int t0, int t1, Local& L) {
+    std::vector<int32_t> tc;
+    std::vector<std::vector<uint16_t>> eterm_lists;  // per owned edge of the tile
+    std::vector<int32_t> slot_edge(256);
+    auto fail = [&](int rc, const char* msg) {
+      L.rc = rc;
+      snprintf(L.msg, sizeof(L.msg), "%s", msg);
+    };
+    for (int t = t0; t < t1; t++) {
+      const int64_t b = starts[t], e = (t + 1 < nt) ? starts[t + 1] : nv;
+      // rows of the tile ascending (writes then walk the CSR forward)
+      std::sort(idx.begin() + b, idx.begin() + e);
+      tc.clear();
+      int kmax = 0;
+      for (int64_t i = b; i < e; i++) {
+        const int32_t r = idx[i];
+        rows[(size_t)t * R + (i - b)] = r;
+        dpos[(size_t)t * R + (i - b)] = pos_in_row(r, r);
+        kmax = std::max(kmax, vptr[r + 1] - vptr[r]);
+        for (int k = vptr[r]; k < vptr[r + 1]; k++) tc.push_back(v2c[k] >> 2);
+      }
+      std::sort(tc.begin(), tc.end());
+      tc.erase(std::unique(tc.begin(), tc.end()), tc.end());
+      if (tc.size() >= (1u << TILE_LOC_BITS)) {
+        char m[160];
+        snprintf(m, sizeof(m), "tile %d touches %zu cells (at most %d)", t, tc.size(),
+                 (1 << TILE_LOC_BITS) - 1);
+        return fail(TP_ERR_CAPACITY, m);
+      }
+      L.max_cells = std::max(L.max_cells, (int)tc.size());
+      L.cells.insert(L.cells.end(), tc.begin(), tc.end());
+      cell_ptr[t + 1] = (int32_t)tc.size();
+      // diagonal terms [row][k]; owned edges and their terms
+      const int KD = (kmax + 7) & ~7;
+      const size_t dbase = L.dterms.size();
+      L.dterms.resize(dbase + (size_t)KD * R, TILE_TERM_NONE);
+      eterm_lists.clear();
+      const size_t ebase = L.edges.size();
+      for (int64_t i = b; i < e; i++) {
+        const int32_t r = idx[i];
+        const int32_t p0 = indptr[r], len = indptr[r + 1] - p0;
+        if (len > 256) {
+          char m[160];
+          snprintf(m, sizeof(m), "row %d has %d entries (tiles support 256)", r, len);
+          return fail(TP_ERR_CAPACITY, m);
+        }
+        std::fill(slot_edge.begin(), slot_edge.begin() + len, -1);
+        for (int k = vptr[r]; k < vptr[r + 1]; k++) {
+          const int32_t c = v2c[k] >> 2;
+          const int li = v2c[k] & 3;
+          const uint16_t loc = (uint16_t)(std::lower_bound(tc.begin(), tc.end(), c) - tc.begin());
+          L.dterms[dbase + (size_t)(i - b) * KD + (k - vptr[r])] =
+              (uint16_t)(loc | (li << TILE_LOC_BITS));
+          for (int j = 0; j < 4; j++) {
+            if (j == li) continue;
+            const int sl = (slots[k] >> (8 * j)) & 0xff;
+            if (sl >= len) {
+              char m[160];
+              snprintf(m, sizeof(m), "incidence slot %d outside row %d", sl, r);
+              return fail(TP_ERR_INDEX, m);
+            }
+            const int32_t v = indices[p0 + sl];
+            if (v < r) continue;  // owned by v's tile
+            if (slot_edge[sl] < 0) {
+              slot_edge[sl] = (int32_t)eterm_lists.size();
+              eterm_lists.emplace_back();
+              const int32_t q = pos_in_row(v, r);
+              if (q < 0) {
+                char m[160];
+                snprintf(m, sizeof(m), "pattern is not symmetric at (%d, %d)", r, v);
+                return fail(TP_ERR_INDEX, m);
+              }
+              L.edges.push_back(make_int2(p0 + sl, q));
+              L.edge_rv.push_back(make_int2(r, v));
+            }
+            eterm_lists[slot_edge[sl]].push_back(
+                (uint16_t)(loc | (tri_host(li, j) << TILE_LOC_BITS)));
+          }
+        }
+      }
+      dterm_ptr[t + 1] = (int32_t)(L.dterms.size() - dbase);
+      const int ne = (int)(L.edges.size() - ebase);
+      L.max_edges = std::max(L.max_edges, ne);
+      edge_ptr[t + 1] = ne;
+      size_t ke = 0;
+      for (const auto& l : eterm_lists) ke = std::max(ke, l.size());
+      const size_t KE = (ke + 7) & ~(size_t)7;
+      const size_t tbase = L.eterms.size();
+      L.eterms.resize(tbase + KE * (size_t)ne, TILE_TERM_NONE);
+      for (int q = 0; q < ne; q++)
+        for (size_t k = 0; k < eterm_lists[q].size(); k++)
+          L.eterms[tbase + (size_t)q * KE + k] = eterm_lists[q][k];
+      eterm_ptr[t + 1] = (int32_t)(KE * (size_t)ne);
+    }
+  };
+  const int nthreads =
+      (int)std::max(1u, std::min(16u, std::min((unsigned)std::max(nt / 64, 1),
+                                               std::thread::hardware_concurrency())));
+  std::vector<Local> locals(nthreads);
+  {
+    std::vector<std::thread> pool;
+    for (int k = 0; k < nthreads; k++) {
+      const int t0 = (int)((int64_t)nt * k / nthreads), t1 = (int)((int64_t)nt * (k + 1) / nthreads);
+      pool.emplace_back(build_range, t0, t1, std::ref(locals[k]));
+    }
+    for (auto& th : pool) th.join();
+  }
   std::vector<int32_t> cells;
   std::vector<uint16_t> dterms, eterms;
   std::vector<int2> edges, edge_rv;
   int max_cells = 0, max_edges = 0;
-  std::vector<int32_t> tc;
-  std::vector<std::vector<uint16_t>> eterm_lists;  // per owned edge of the tile
-  std::vector<int32_t> slot_edge(256);
+  for (auto& L : locals) {
+    if (L.rc != TP_OK) {
+      set_error("%s", L.msg);
+      return L.rc;
+    }
+    cells.insert(cells.end(), L.cells.begin(), L.cells.end());
+    dterms.insert(dterms.end(), L.dterms.begin(), L.dterms.end());
+    eterms.insert(eterms.end(), L.eterms.begin(), L.eterms.end());
+    edges.insert(edges.end(), L.edges.begin(), L.edges.end());
+    edge_rv.insert(edge_rv.end(), L.edge_rv.begin(), L.edge_rv.end());
+    max_cells = std::max(max_cells, L.max_cells);
+    max_edges = std::max(max_edges, L.max_edges);
+  }
+  if (eterms.size() > (size_t)INT32_MAX || dterms.size() > (size_t)INT32_MAX ||
+      cells.size() > (size_t)INT32_MAX) {
+    set_error("tile terms exceed int32 offsets");
+    return TP_ERR_CAPACITY;
+  }
+  // per-tile sizes -> offsets
   for (int t = 0; t < nt; t++) {
-    const int64_t b = starts[t], e = (t + 1 < nt) ? starts[t + 1] : nv;
-    // rows of the tile ascending (writes then walk the CSR forward)
-    std::sort(idx.begin() + b, idx.begin() + e);
-    tc.clear();
-    int kmax = 0;
-    for (int64_t i = b; i < e; i++) {
-      const int32_t r = idx[i];
-      rows[(size_t)t * R + (i - b)] = r;
-      dpos[(size_t)t * R + (i - b)] = pos_in_row(r, r);
-      kmax = std::max(kmax, vptr[r + 1] - vptr[r]);
-      for (int k = vptr[r]; k < vptr[r + 1]; k++) tc.push_back(v2c[k] >> 2);
-    }
-    std::sort(tc.begin(), tc.end());
-    tc.erase(std::unique(tc.begin(), tc.end()), tc.end());
-    if (tc.size() >= (1u << TILE_LOC_BITS)) {
-      set_error("tile %d touches %zu cells (at most %d)", t, tc.size(),
-                (1 << TILE_LOC_BITS) - 1);
-      return TP_ERR_CAPACITY;
-    }
-    max_cells = std::max(max_cells, (int)tc.size());
-    cells.insert(cells.end(), tc.begin(), tc.end());
-    cell_ptr[t + 1] = (int32_t)cells.size();
-    // diagonal terms [row][k]; owned edges and their terms
-    const int KD = (kmax + 7) & ~7;
-    const size_t dbase = dterms.size();
-    dterms.resize(dbase + (size_t)KD * R, TILE_TERM_NONE);
-    eterm_lists.clear();
-    const size_t ebase = edges.size();
-    for (int64_t i = b; i < e; i++) {
-      const int32_t r = idx[i];
-      const int32_t p0 = indptr[r], len = indptr[r + 1] - p0;
-      if (len > 256) {
-        set_error("row %d has %d entries (tiles support 256)", r, len);
-        return TP_ERR_CAPACITY;
-      }
-      std::fill(slot_edge.begin(), slot_edge.begin() + len, -1);
-      for (int k = vptr[r]; k < vptr[r + 1]; k++) {
-        const int32_t c = v2c[k] >> 2;
-        const int li = v2c[k] & 3;
-        const uint16_t loc = (uint16_t)(std::lower_bound(tc.begin(), tc.end(), c) - tc.begin());
-        dterms[dbase + (size_t)(i - b) * KD + (k - vptr[r])] =
-            (uint16_t)(loc | (li << TILE_LOC_BITS));
-        for (int j = 0; j < 4; j++) {
-          if (j == li) continue;
-          const int s = (slots[k] >> (8 * j)) & 0xff;
-          if (s >= len) {
-            set_error("incidence slot %d outside row %d", s, r);
-            return TP_ERR_INDEX;
-          }
-          const int32_t v = indices[p0 + s];
-          if (v < r) continue;  // owned by v's tile
-          if (slot_edge[s] < 0) {
-            slot_edge[s] = (int32_t)eterm_lists.size();
-            eterm_lists.emplace_back();
-            const int32_t q = pos_in_row(v, r);
-            if (q < 0) {
-              set_error("pattern is not symmetric at (%d, %d)", r, v);
-              return TP_ERR_INDEX;
-            }
-            edges.push_back(make_int2(p0 + s, q));
-            edge_rv.push_back(make_int2(r, v));
-          }
-          eterm_lists[slot_edge[s]].push_back((uint16_t)(loc | (tri_host(li, j) << TILE_LOC_BITS)));
-        }
-      }
-    }
-    dterm_ptr[t + 1] = (int32_t)dterms.size();
-    const int ne = (int)(edges.size() - ebase);
-    max_edges = std::max(max_edges, ne);
-    edge_ptr[t + 1] = (int32_t)edges.size();
-    size_t ke = 0;
-    for (const auto& l : eterm_lists) ke = std::max(ke, l.size());
-    const size_t KE = (ke + 7) & ~(size_t)7;
-    const size_t tbase = eterms.size();
-    eterms.resize(tbase + KE * (size_t)ne, TILE_TERM_NONE);
-    for (int q = 0; q < ne; q++)
-      for (size_t k = 0; k < eterm_lists[q].size(); k++)
-        eterms[tbase + (size_t)q * KE + k] = eterm_lists[q][k];
-    if (eterms.size() > (size_t)INT32_MAX || dterms.size() > (size_t)INT32_MAX) {
-      set_error("tile terms exceed int32 offsets");
-      return TP_ERR_CAPACITY;
-    }
-    eterm_ptr[t + 1] = (int32_t)eterms.size();
+    cell_ptr[t + 1] += cell_ptr[t];
+    dterm_ptr[t + 1] += dterm_ptr[t];
+    edge_ptr[t + 1] += edge_ptr[t];
+    eterm_ptr[t + 1] += eterm_ptr[t];
   }
 
   tp_tiles* h = new tp_tiles();

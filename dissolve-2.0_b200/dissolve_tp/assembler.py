@@ -232,14 +232,16 @@ class CsrMatrix:
 class GPUSparseAssembler:
     """P1 (1/dt + alpha) M + De K assembler on the GPU (gpu_assembler.py:311)."""
 
-    def __init__(self, domain=None, V=None, comm=None, ref_asm=None):
+    def __init__(self, domain=None, V=None, comm=None, ref_asm=None, *, tile_rows=None):
+        """tile_rows (keyword, not in the reference's signature): rows per tile of the
+        tiled kernels (None: the default, 0: none)."""
         self.comm = comm
         if ref_asm is not None:
             # shared read-only geometry and pattern (gpu_assembler.py:346-367)
             self._dm = ref_asm._dm
         else:
             coords, cells = extract_mesh(domain, V)
-            self._dm = DeviceMesh(coords, cells)
+            self._dm = DeviceMesh(coords, cells, tile_rows=tile_rows)
         dm = self._dm
         self.n_cells = dm.n_cells
         self.n_dofs = dm.n_verts

@@ -21,7 +21,7 @@ import torch
 from . import _lib
 from ._lib import call
 from .assembler import GPUSparseAssembler
-from .autotune import tune_cg
+from .autotune import tune_cg, tune_tiles
 from .device import ptr, stream_handle, to_device
 from .krylov import CGSolver, CsrOperator, PersistentCG
 from .mesh import concat_meshes, kuhn_cube
@@ -59,9 +59,12 @@ class MeshBatch:
     def __init__(self, meshes, D, k, dt, rtol=1e-8, max_it=5000, inner_fp32=True,
                  autotune=True, cg=None):
         self.n_meshes = len(meshes)
+        self.inv_dt = 1.0 / float(dt)
+        # the assembly's rows per tile, tuned on the largest mesh before the union is built
+        asm_tiles = self.tune_assembly(meshes) if autotune else None
         union, vp, cp = concat_meshes(meshes)
         self.vert_ptr, self.cell_ptr = vp, cp
-        self.asm = GPUSparseAssembler(union)
+        self.asm = GPUSparseAssembler(union, tile_rows=asm_tiles)
         dm = self.asm._dm
         self.dm = dm
         dev = dm.device
@@ -70,7 +73,6 @@ class MeshBatch:
         self.De = to_device(np.repeat(np.asarray(D, dtype=np.float64), ncell), torch.float64, dev)
         self.alpha = to_device(np.repeat(np.asarray(k, dtype=np.float64), ncell), torch.float64,
                                dev)
-        self.inv_dt = 1.0 / float(dt)
         self.K64 = torch.zeros(dm.nnz, dtype=torch.float64, device=dev)
         self.K32 = torch.zeros(dm.nnz, dtype=torch.float32, device=dev) if inner_fp32 else None
         self.op = CsrOperator(dm.indptr, dm.indices[: dm.nnz], self.K64, K32=self.K32,
@@ -80,12 +82,34 @@ class MeshBatch:
             self.assemble_operator()
             cg.update(tune_cg(self.op, inner_fp32=inner_fp32))
         self.cg_config = dict(cg, engine="graph", n_systems=self.n_meshes)
+        if asm_tiles is not None:
+            self.cg_config["assembly_rows_per_tile"] = asm_tiles
         self.solver = CGSolver(self.op, rtol=rtol, max_it=max_it, inner_fp32=inner_fp32, **cg)
         self.U = torch.zeros(dm.n_verts, dtype=torch.float64, device=dev)
 
     @property
     def n_cells(self) -> int:
         return self.dm.n_cells
+
+    def tune_assembly(self, meshes) -> int:
+        """Rows per tile of the batch's assembly, chosen by the project autotuner
+        (autotune.tune_tiles) on the batch's largest mesh: the union of hundreds of
+        meshes would need its tile tables rebuilt for every candidate."""
+        from .assembler import DeviceMesh
+        big = max(meshes, key=lambda m_: m_.n_cells)
+        sample = DeviceMesh(big.coords, big.cells, tile_rows=0)
+        dev = sample.device
+        De = torch.ones(sample.n_cells, dtype=torch.float64, device=dev)
+        out = torch.empty(sample.nnz, dtype=torch.float64, device=dev)
+        out32 = torch.empty(sample.nnz, dtype=torch.float32, device=dev)
+
+        def run():
+            call("tp_assemble_csr", ctypes.byref(sample.tpm), ptr(De), ptr(De), self.inv_dt, 1,
+                 _lib.TP_ASM_FULL, None, ptr(out), ptr(out32), stream_handle())
+
+        best = tune_tiles(sample, run, key=(big.n_verts, big.n_cells, sample.nnz))
+        del sample
+        return best["rows_per_tile"]
 
     def assemble_operator(self):
         call("tp_assemble_csr", ctypes.byref(self.dm.tpm), ptr(self.De), ptr(self.alpha),

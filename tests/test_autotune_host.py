@@ -53,3 +53,53 @@ def test_tune_picks_fastest_and_caches(monkeypatch):
     at.tune_cg(_op(), inner_fp32=False)
     at.tune_cg(_op(n_systems=5), inner_fp32=True)
     assert len(_FakeSolver.made) == 3 * n_timed
+
+
+class _FakeMesh:
+    def __init__(self):
+        self.n_verts, self.n_cells, self.nnz = 100, 500, 1400
+        self.tile_rows = 64
+        self.installed = []
+
+    def set_tiles(self, rows):
+        self.tile_rows = rows
+        self.installed.append(rows)
+
+
+def test_tune_tiles_picks_fastest_installs_and_caches(monkeypatch):
+    """Every tile size is installed and timed; the fastest (median of the timed runs) stays
+    installed and is cached per mesh shape."""
+    import torch
+
+    dm = _FakeMesh()
+    cost = {0: 150.0, 32: 120.0, 64: 100.0, 128: 90.0}   # us per launch
+
+    class _Ev:
+        def __init__(self, enable_timing=True):
+            self.t = 0.0
+
+        def record(self):
+            self.t = _Ev.clock
+            _Ev.clock += cost[dm.tile_rows] * 1e-3 / 2   # half before, half after the launch
+
+        def synchronize(self):
+            pass
+
+        def elapsed_time(self, other):
+            return other.t - self.t
+
+    _Ev.clock = 0.0
+    monkeypatch.setattr(torch.cuda, "Event", _Ev)
+    monkeypatch.setattr(at, "_CACHE", {})
+    runs = []
+    best = at.tune_tiles(dm, lambda: runs.append(dm.tile_rows), reps=5)
+    assert best["rows_per_tile"] == 128 and dm.tile_rows == 128
+    assert dm.installed[:len(at.TILE_ROWS)] == list(at.TILE_ROWS)
+    assert len(runs) == len(at.TILE_ROWS) * 7          # 2 warm-up + 5 timed each
+    table = at.last_tiles_table((dm.n_verts, dm.n_cells, dm.nnz))
+    assert sorted(r for _, r in table) == sorted(at.TILE_ROWS)
+    # cached: installed again without timing
+    dm.set_tiles(0)
+    n = len(runs)
+    assert at.tune_tiles(dm, lambda: runs.append(dm.tile_rows))["rows_per_tile"] == 128
+    assert dm.tile_rows == 128 and len(runs) == n
