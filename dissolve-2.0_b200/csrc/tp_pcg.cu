@@ -2422,6 +2422,8 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
   __shared__ LaneState L;
   __shared__ PgpLanes P;
   __shared__ float s_al[4], s_be[4];
+  __shared__ double s_nalpha[4], s_nbeta[4], s_ngm[4];
+  __shared__ int s_commit[4];
   __shared__ uint32_t s_taddr;
   __shared__ unsigned long long s_clk[8];
   unsigned int target = 0;
@@ -2538,8 +2540,8 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
     return !bad;
   };
 
-  // partial-sum loads of slots 0..11 (gamma, delta, r.r) of every CTA, issued early;
-  // totals_finish sums them in the fixed order of grid_totals
+  // partial-sum loads of slots 0..11 (gamma, delta, r.r) of every CTA, issued early and
+  // summed after the product in the fixed order of grid_totals
   auto totals_load = [&](const double* part, double x[5]) {
     const int k = threadIdx.x % 16, g = threadIdx.x / 16;
 #pragma unroll
@@ -2548,25 +2550,6 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
       x[q] = (k < 12 && b < (int)gridDim.x) ? __ldcg(part + (int64_t)b * 16 + k) : 0.0;
     }
   };
-  auto totals_finish = [&](const double* part, double x[5]) {
-    const int k = threadIdx.x % 16, g = threadIdx.x / 16;
-    double v = 0.0;
-#pragma unroll
-    for (int q = 0; q < 5; q++)
-      if (g + q * 32 < (int)gridDim.x) v += x[q];
-    for (int b = g + 5 * 32; b < (int)gridDim.x; b += 32)
-      if (k < 12) v += __ldcg(part + (int64_t)b * 16 + k);
-    s_buf[threadIdx.x] = v;
-    __syncthreads();
-    const int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
-    if (w < 12) {
-      double t = (ln < 32) ? s_buf[ln * 16 + w] : 0.0;
-      t = warp_sum(t);
-      if (ln == 0) s_tot[w] = t;
-    }
-    __syncthreads();
-  };
-
   // ---- n = A src (the window) of this warp's rows into nr (registers).  The row
   // diagonals are loaded while the copies into the window land; a Dirichlet row (identity,
   // D^-1 = 0 in every column) is recognised by its D^-1.
@@ -3007,41 +2990,80 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
       for (int s = 0; s < LD; s++) xr[j][s] = 0.f;
       if (sb + warp + j * PGP_WARPS < se && row < a.n) ldv_cg<VT, LD>(a.xi, row, xr[j]);
     }
-    totals_finish(part_of(pp), tx);
-    // ---- lane decisions (thread s: lane s), the same in every CTA
+    // ---- totals and lane decisions with two CTA barriers: warp s sums lane s's partial
+    // sums (gamma, delta, r.r; the fixed order of grid_totals) and its lane 0 decides for
+    // the lane and forms alpha and beta tentatively; the lane state of alpha, beta and
+    // gamma_old is committed only when no lane asks for a refresh.  Every CTA holds the
+    // same totals and decides the same.
+    {
+      const int k = threadIdx.x % 16, g = threadIdx.x / 16;
+      double v = 0.0;
+#pragma unroll
+      for (int q = 0; q < 5; q++)
+        if (g + q * 32 < (int)gridDim.x) v += tx[q];
+      for (int bb = g + 5 * 32; bb < (int)gridDim.x; bb += 32)
+        if (k < 12) v += __ldcg(part_of(pp) + (int64_t)bb * 16 + k);
+      s_buf[threadIdx.x] = v;
+    }
+    __syncthreads();
     int want = 0;
-    if (threadIdx.x < S) {
-      const int s = threadIdx.x;
-      if (L.active[s] && !L.frozen[s]) {
-        const double gm = s_tot[s], dl = s_tot[4 + s], rr = s_tot[8 + s];
-        if (!isfinite(gm) || !isfinite(dl) || !isfinite(rr)) {
-          if (++P.fails[s] >= 2) {
-            L.active[s] = 0;
-            L.status[s] = TP_ERR_NONFINITE;
-            L.iters[s] = it;
+    if (warp < 4) {
+      const int s = warp;
+      double gm = 0.0, dl = 0.0, rr = 0.0;
+      if (s < S) {
+        gm = warp_sum(s_buf[lane * 16 + s]);
+        dl = warp_sum(s_buf[lane * 16 + 4 + s]);
+        rr = warp_sum(s_buf[lane * 16 + 8 + s]);
+      }
+      if (lane == 0) {
+        float al = 0.f, be = 0.f;
+        s_commit[s] = 0;
+        if (s < S && L.active[s] && !L.frozen[s]) {
+          if (!isfinite(gm) || !isfinite(dl) || !isfinite(rr)) {
+            if (++P.fails[s] >= 2) {
+              L.active[s] = 0;
+              L.status[s] = TP_ERR_NONFINITE;
+              L.iters[s] = it;
+            } else {
+              P.poisoned[s] = 1;
+              want = 1;
+            }
+          } else if (!(dl > 0.0)) {
+            // w.u = u.Au is exact right after a restart: not positive there means the
+            // operator is not positive definite; later it is recurrence drift
+            if (L.rz[s] == 0.0) {
+              L.active[s] = 0;
+              L.status[s] = TP_ERR_BREAKDOWN;
+              L.iters[s] = it;
+            } else {
+              want = 1;
+            }
           } else {
-            P.poisoned[s] = 1;
-            want = 1;
+            L.rr[s] = rr;
+            if (rr <= L.tol2[s])
+              L.frozen[s] = 1;
+            else if (rr > 1e4 * L.rmax2[s])
+              want = 1;  // the recurrences drifted off: refresh and restart
+            else
+              want = a.delta2 > 0.0 && rr < a.delta2 * L.rmax2[s];
+            if (!L.frozen[s] && !want) {
+              double beta = (L.rz[s] != 0.0) ? gm / L.rz[s] : 0.0;
+              double den = (beta != 0.0 && L.alpha[s] != 0.0) ? dl - beta * gm / L.alpha[s] : dl;
+              if (!(den > 0.0)) {  // rounding: restart the direction
+                beta = 0.0;
+                den = dl;
+              }
+              s_nbeta[s] = beta;
+              s_nalpha[s] = gm / den;
+              s_ngm[s] = gm;
+              s_commit[s] = 1;
+              al = (float)s_nalpha[s];
+              be = (float)beta;
+            }
           }
-        } else if (!(dl > 0.0)) {
-          // w.u = u.Au is exact right after a restart: not positive there means the
-          // operator is not positive definite; later it is recurrence drift
-          if (L.rz[s] == 0.0) {
-            L.active[s] = 0;
-            L.status[s] = TP_ERR_BREAKDOWN;
-            L.iters[s] = it;
-          } else {
-            want = 1;
-          }
-        } else {
-          L.rr[s] = rr;
-          if (rr <= L.tol2[s])
-            L.frozen[s] = 1;
-          else if (rr > 1e4 * L.rmax2[s])
-            want = 1;  // the recurrences drifted off: refresh and restart
-          else
-            want = a.delta2 > 0.0 && rr < a.delta2 * L.rmax2[s];
         }
+        s_al[s] = al;
+        s_be[s] = be;
       }
     }
     int any = __syncthreads_or(want);
@@ -3085,34 +3107,14 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
       clk.lap(5);
       continue;
     }
-    // ---- alpha, beta of every running lane (0 for frozen and finished lanes)
-    if (threadIdx.x < 4) {
+    // ---- commit alpha, beta, gamma_old of the lanes that step (read again only after
+    // the barriers of the update)
+    if (threadIdx.x < S && s_commit[threadIdx.x]) {
       const int s = threadIdx.x;
-      float al = 0.f, be = 0.f;
-      if (s < S && L.active[s] && !L.frozen[s]) {
-        const double gm = s_tot[s], dl = s_tot[4 + s];
-        if (!(dl > 0.0)) {
-          L.active[s] = 0;
-          L.status[s] = TP_ERR_BREAKDOWN;
-          L.iters[s] = it;
-        } else {
-          double beta = (L.rz[s] != 0.0) ? gm / L.rz[s] : 0.0;
-          double den = (beta != 0.0 && L.alpha[s] != 0.0) ? dl - beta * gm / L.alpha[s] : dl;
-          if (!(den > 0.0)) {  // rounding: restart the direction
-            beta = 0.0;
-            den = dl;
-          }
-          L.beta[s] = beta;
-          L.alpha[s] = gm / den;
-          L.rz[s] = gm;
-          al = (float)L.alpha[s];
-          be = (float)beta;
-        }
-      }
-      s_al[s] = al;
-      s_be[s] = be;
+      L.beta[s] = s_nbeta[s];
+      L.alpha[s] = s_nalpha[s];
+      L.rz[s] = s_ngm[s];
     }
-    __syncthreads();
     clk.lap(4);
     {
       double acc[12];
@@ -3414,6 +3416,7 @@ struct WinTables {
 };
 
 constexpr int PGP_RUNCAP = 32;  // bulk runs per CTA (shared-memory list)
+constexpr double PGP_MIN_DELTA = 1e-3;  // the pipelined engine's largest refresh interval
 constexpr int PGP_MINRUN = 8;   // shortest run copied in bulk (entries)
 
 // The halo of every CTA (sorted global rows, window slots nown + k) split into runs of
@@ -3684,6 +3687,9 @@ static int try_window(tp_pcg_handle* h, const tp_sell* sell, bool hasM, cudaStre
   h->fn = fn;
   h->dyn_smem = d_pipe;
   h->window = pipe ? 3 : (cgt ? 2 : 1);
+  // the pipelined recurrences run at most three decades between FP64 refreshes: at 1e-4
+  // a refresh threshold let their FP32 drift stall a solve on the benchmark mesh
+  if (pipe) h->af.delta2 = std::max(h->af.delta2, PGP_MIN_DELTA * PGP_MIN_DELTA);
   return TP_OK;
 }
 

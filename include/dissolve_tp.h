@@ -522,7 +522,8 @@ TP_API int tp_pcg_grid(tp_pcg_handle* h, int* grid, int* block);
  * engine 1).  *window = 3: the pipelined form of the same Jacobi-PCG (Ghysels-Vanroose,
  * one grid barrier per iteration; its FP64 refreshes restart the refreshed lanes) with
  * the same tensor-memory layout, for at most 3 columns (DISSOLVE_PCG_PIPE=0 at create keeps
- * engine 2).  *window = 0: the streaming engine (standard recurrences, columns and
+ * engine 2); it refreshes at least every factor 1e3 of residual reduction whatever
+ * `delta` asks for.  *window = 0: the streaming engine (standard recurrences, columns and
  * gathers from global memory).  *smem_bytes: dynamic shared memory per CTA.  The
  * environment variable DISSOLVE_PCG_ENGINE=stream at create forces the streaming
  * engine. */
