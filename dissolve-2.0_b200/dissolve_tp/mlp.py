@@ -230,7 +230,7 @@ def trajectory_pairs(tr, steps):
 
 
 def attach_trained_predictor(fast, mesh, coef, u_ref, D, K, DT, train_steps=12,
-                             epochs=400, seed=3, verbose=False):
+                             epochs=1600, seed=3, verbose=False):
     """Train a WarmStartMLP on a trajectory of the FP64 batched solver started from a
     different random state (seed `seed`) and attach it to `fast` as its guess."""
     from .transport import BatchedTransport
