@@ -748,7 +748,9 @@ __global__ void __launch_bounds__(256) k_mf_diag(int64_t n, const int4* __restri
   }
 }
 
-// per-block partial sums of NQ quantities, then the last block sums them in block order
+// per-block partial sums of NQ quantities, then the last block sums them: thread t adds
+// the partials of blocks t, t + blockDim, ... and a fixed block tree sums the threads (the
+// same order on every run; one round trip for the partials instead of one per block)
 template <int NQ>
 __device__ __forceinline__ bool mf_reduce(double v[NQ], double* part, uint32_t* ticket,
                                           double out[NQ]) {
@@ -764,15 +766,16 @@ __device__ __forceinline__ bool mf_reduce(double v[NQ], double* part, uint32_t* 
   __syncthreads();
   if (!s_last) return false;
   __threadfence();
-  if (threadIdx.x == 0) {
+  double acc[NQ];
 #pragma unroll
-    for (int q = 0; q < NQ; q++) out[q] = 0.0;
-    for (unsigned b = 0; b < gridDim.x; b++) {
+  for (int q = 0; q < NQ; q++) acc[q] = 0.0;
+  for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
 #pragma unroll
-      for (int q = 0; q < NQ; q++) out[q] += __ldcg(part + b * 16 + q);
-    }
-    *ticket = 0;
+    for (int q = 0; q < NQ; q++) acc[q] += __ldcg(part + b * 16 + q);
   }
+#pragma unroll
+  for (int q = 0; q < NQ; q++) out[q] = block_sum(acc[q], sh);
+  if (threadIdx.x == 0) *ticket = 0;
   return true;
 }
 
