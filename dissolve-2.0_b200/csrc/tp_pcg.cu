@@ -2320,8 +2320,9 @@ __global__ void __launch_bounds__(512, 1) k_cgt(PArgs<float> a) {
 // through recurrences, so one barrier publishes m and the partial sums together, and the
 // reduction's round trip overlaps the product n = A m:
 //
-//   barrier | halo copies of m and the partial-sum loads in flight; n = A m (registers)
-//           | gamma = r.u, delta = w.u, r.r totals; lane decisions; alpha, beta
+//   barrier | halo copies of m and the partial-sum loads in flight;
+//           | gamma = r.u, delta = w.u, r.r totals; lane decisions; alpha, beta (while
+//           | the halo copies land); n = A m (registers)
 //           | z = n + beta z, s = w + beta s, p = u + beta p, xi += alpha p,
 //           | r -= alpha s, w -= alpha z, u = D^-1 r, m = D^-1 w (window and global);
 //           | partials of the next gamma, delta, r.r
@@ -2540,8 +2541,8 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
     return !bad;
   };
 
-  // partial-sum loads of slots 0..11 (gamma, delta, r.r) of every CTA, issued early and
-  // summed after the product in the fixed order of grid_totals
+  // partial-sum loads of slots 0..11 (gamma, delta, r.r) of every CTA, issued right after
+  // the barrier and summed in the fixed order of grid_totals
   auto totals_load = [&](const double* part, double x[5]) {
     const int k = threadIdx.x % 16, g = threadIdx.x / 16;
 #pragma unroll
@@ -2551,15 +2552,11 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
     }
   };
   // ---- n = A src (the window) of this warp's rows into nr (registers).  The row
-  // diagonals are loaded while the copies into the window land; a Dirichlet row (identity,
-  // D^-1 = 0 in every column) is recognised by its D^-1.
-  // ---- n = A src (the window) of this warp's rows into nr (registers).  The row
-  // diagonals of all four slices are loaded while the copies into the window land; a
-  // Dirichlet row (identity, D^-1 = 0 in every column) is recognised by its D^-1.  (A
+  // diagonals of all four slices (diag_load) are loaded while the copies into the window
+  // land; a Dirichlet row (identity, D^-1 = 0 in every column) is recognised by its D^-1.  (A
   // split into the own-column terms, summed while the halo copies land, and the halo
   // terms after them was measured slower: 10.4 against 3.2 us per product.)
-  auto product_rows = [&](float nr[PGP_MAXS][CW], bool bulk) -> bool {
-    float dgs[PGP_MAXS][CW];
+  auto diag_load = [&](float dgs[PGP_MAXS][CW]) {
 #pragma unroll
     for (int j = 0; j < PGP_MAXS; j++) {
       const int64_t row = (int64_t)(sb + warp + j * PGP_WARPS) * 32 + lane;
@@ -2570,6 +2567,9 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
 #pragma unroll
       for (int c = 0; c < CW; c++) dgs[j][c] = dg[c];
     }
+  };
+  auto product_rows = [&](float nr[PGP_MAXS][CW], const float dgs[PGP_MAXS][CW],
+                          bool bulk) -> bool {
     if (!wait_window(bulk)) return false;
     clk.lap(3);
     const int e0 = s_sp[0];
@@ -2796,8 +2796,9 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
   // ---- w = A u after a refresh (u in the window): w into the records of the lanes in tr,
   // m = D^-1 w into the window and mdst, partials gamma, delta, r.r of the new state
   auto restart_rows = [&](const int tr[LD], double acc[12], VT* mdst, bool bulk) -> bool {
-    float nr[PGP_MAXS][CW];
-    if (!product_rows(nr, bulk)) return false;
+    float nr[PGP_MAXS][CW], dgs[PGP_MAXS][CW];
+    diag_load(dgs);
+    if (!product_rows(nr, dgs, bulk)) return false;
     __syncthreads();  // every warp has read the window: m may replace u in it
 #pragma unroll
     for (int j = 0; j < PGP_MAXS; j++) {
@@ -2839,8 +2840,21 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
     if (warp == 0) tm_dealloc(s_taddr, PGP_COLS);
   };
 
+  // this CTA's partial row of gamma, delta, r.r: a shuffle tree per warp, then warp k
+  // sums slot k over the 16 warps with a second fixed tree.  Every caller comes after a
+  // CTA barrier that follows the last reads of sh.
   auto publish12 = [&](double acc[12], double* part) {
-    block_partial<12>(acc, part, sh);
+#pragma unroll
+    for (int k = 0; k < 12; k++) acc[k] = warp_sum(acc[k]);
+    if (lane == 0) {
+#pragma unroll
+      for (int k = 0; k < 12; k++) sh[k * 32 + warp] = acc[k];
+    }
+    __syncthreads();
+    if (warp < 12) {
+      const double t = warp_sum(lane < PGP_WARPS ? sh[warp * 32 + lane] : 0.0);
+      if (lane == 0) part[(int64_t)blockIdx.x * 16 + warp] = t;
+    }
   };
 
   // ---- I1: Jacobi diagonal into shared memory, Dirichlet values into x, records and xi 0
@@ -2971,25 +2985,14 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
   clk.lap(7);
 
   while (ok && going) {
-    // ---- after the barrier: m of the halo and the partial sums in flight
+    // ---- after the barrier: m of the halo and the partial sums in flight.  The totals
+    // and lane decisions need only the partial sums, so they run while the halo copies
+    // land; the product waits for the window after them.
     const bool bulk = fill_window(true, mbuf(vp));
     double tx[5];
     totals_load(part_of(pp), tx);
-    float nr[PGP_MAXS][CW];
-    if (!product_rows(nr, bulk)) {
-      ok = false;
-      break;
-    }
-    clk.lap(0);
-    // xi of the own rows, read ahead of the update
-    float xr[PGP_MAXS][LD];
-#pragma unroll
-    for (int j = 0; j < PGP_MAXS; j++) {
-      const int64_t row = (int64_t)(sb + warp + j * PGP_WARPS) * 32 + lane;
-#pragma unroll
-      for (int s = 0; s < LD; s++) xr[j][s] = 0.f;
-      if (sb + warp + j * PGP_WARPS < se && row < a.n) ldv_cg<VT, LD>(a.xi, row, xr[j]);
-    }
+    float dgs[PGP_MAXS][CW];
+    diag_load(dgs);
     // ---- totals and lane decisions with two CTA barriers: warp s sums lane s's partial
     // sums (gamma, delta, r.r; the fixed order of grid_totals) and its lane 0 decides for
     // the lane and forms alpha and beta tentatively; the lane state of alpha, beta and
@@ -3075,10 +3078,19 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
       }
       any = pending && !running;
     }
-    if (!any && it >= a.max_it) break;
+    if (!any && it >= a.max_it) {
+      // the window's copies land before the final refresh reuses the window
+      if (!wait_window(bulk)) ok = false;
+      break;
+    }
     if (any) {
-      // ---- RU: x += xi, FP64 residual, restart from w = A u
+      // ---- RU: x += xi, FP64 residual, restart from w = A u (after the window's copies
+      // landed: the refresh reuses the window)
       clk.lap(4);
+      if (!wait_window(bulk)) {
+        ok = false;
+        break;
+      }
       int tr[LD], drop[LD];
 #pragma unroll
       for (int s = 0; s < LD; s++) {
@@ -3116,6 +3128,22 @@ __global__ void __launch_bounds__(512, 1) k_pcgp(PArgs<float> a) {
       L.rz[s] = s_ngm[s];
     }
     clk.lap(4);
+    float nr[PGP_MAXS][CW];
+    if (!product_rows(nr, dgs, bulk)) {
+      ok = false;
+      break;
+    }
+    clk.lap(0);
+    // xi of the own rows, read ahead of the update
+    float xr[PGP_MAXS][LD];
+#pragma unroll
+    for (int j = 0; j < PGP_MAXS; j++) {
+      const int64_t row = (int64_t)(sb + warp + j * PGP_WARPS) * 32 + lane;
+#pragma unroll
+      for (int s = 0; s < LD; s++) xr[j][s] = 0.f;
+      if (sb + warp + j * PGP_WARPS < se && row < a.n) ldv_cg<VT, LD>(a.xi, row, xr[j]);
+    }
+    __syncthreads();  // every warp has read the window: the update may replace m in it
     {
       double acc[12];
 #pragma unroll
