@@ -173,23 +173,35 @@ __global__ void __launch_bounds__(256) k_csr_images(int64_t n, const int32_t* __
 #pragma unroll
     for (int s = 0; s < LD; s++) a1[s] = a2[s] = 0.0;
     const int beg = indptr[rr], end = indptr[rr + 1];
-    for (int p = beg + gl; p < end; p += G) {
-      const int j = __ldg(indices + p);
-      const double kv = __ldg(K + p);
-      double u[LD], up[LD];
-      if constexpr (W256 && LD == 4) {
-        const double4 a = ldg_d4(reinterpret_cast<const double4*>(x1) + j);
-        const double4 c = ldg_d4(reinterpret_cast<const double4*>(x2) + j);
-        u[0] = a.x, u[1] = a.y, u[2] = a.z, u[3] = a.w;
-        up[0] = c.x, up[1] = c.y, up[2] = c.z, up[3] = c.w;
-      } else {
-        ldv<double, LD>(x1, j, u);
-        ldv<double, LD>(x2, j, up);
+    // the index and value loads of up to RP entries per lane in flight before their gathers
+    constexpr int RP = 4;
+    for (int p0 = beg + gl; p0 < end; p0 += G * RP) {
+      int jj[RP];
+      double kv[RP];
+#pragma unroll
+      for (int v = 0; v < RP; v++) {
+        const int p = p0 + v * G;
+        jj[v] = p < end ? __ldg(indices + p) : 0;
+        kv[v] = p < end ? __ldg(K + p) : 0.0;
       }
 #pragma unroll
-      for (int s = 0; s < LD; s++) {
-        a1[s] += kv * u[s];
-        a2[s] += kv * (u[s] - up[s]);
+      for (int v = 0; v < RP; v++) {
+        if (p0 + v * G >= end) break;
+        double u[LD], up[LD];
+        if constexpr (W256 && LD == 4) {
+          const double4 a = ldg_d4(reinterpret_cast<const double4*>(x1) + jj[v]);
+          const double4 c = ldg_d4(reinterpret_cast<const double4*>(x2) + jj[v]);
+          u[0] = a.x, u[1] = a.y, u[2] = a.z, u[3] = a.w;
+          up[0] = c.x, up[1] = c.y, up[2] = c.z, up[3] = c.w;
+        } else {
+          ldv<double, LD>(x1, jj[v], u);
+          ldv<double, LD>(x2, jj[v], up);
+        }
+#pragma unroll
+        for (int s = 0; s < LD; s++) {
+          a1[s] += kv[v] * u[s];
+          a2[s] += kv[v] * (u[s] - up[s]);
+        }
       }
     }
 #pragma unroll
@@ -236,10 +248,12 @@ __host__ __device__ constexpr int gp_nq() {
 constexpr int GP_SLOTS = gp_nq<GP_MAXD>() * 4;
 
 // A d_k for the first NG directions by one CSR walk per row (the others come with their
-// images d.img[k]): a group of LD lanes per row, lane s reads column s of every gathered
-// row (the group's loads are one contiguous run).  The sums of lane s feed column s; one
-// row of GP_SLOTS partials per block (slot q * 4 + s), summed over the warps in a fixed
-// order.
+// images d.img[k]).  A group of LD lanes per row; lane s feeds column s.  With NG <= 2 the
+// group walks the row together: lane s takes entries s, s + LD, ... and gathers whole
+// LD-column rows of the directions, the index and value loads of up to 4 LD entries in
+// flight before their gathers, and a shuffle tree over the group gives every column's sum.
+// With more gathered directions each lane walks the whole row for its own column.  One row
+// of GP_SLOTS partials per block (slot q * 4 + s), summed over the warps in a fixed order.
 template <int LD, int M, int NG>
 __global__ void __launch_bounds__(256) k_guess_dots(
     int64_t n, int S, const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
@@ -247,6 +261,8 @@ __global__ void __launch_bounds__(256) k_guess_dots(
     const uint8_t* __restrict__ bc, const double* __restrict__ b, const double* __restrict__ U,
     const double* __restrict__ opU, GuessDirs dirs, double* __restrict__ part) {
   constexpr int NQ = gp_nq<M>();
+  constexpr bool COOP = NG >= 1 && NG <= 2;
+  constexpr int NGA = NG > 0 ? NG : 1;
   __shared__ double red[8][NQ * 4];  // blockDim 256: 8 warps
   const double dscale[4] = {dsc.x, dsc.y, dsc.z, dsc.w};
   const int s = threadIdx.x % LD;
@@ -260,43 +276,97 @@ __global__ void __launch_bounds__(256) k_guess_dots(
   for (int q = 0; q < NQ; q++) acc[q] = 0.0;
   for (int64_t base = blockIdx.x * rpb; base < n; base += (int64_t)gridDim.x * rpb) {
     const int64_t row = base + threadIdx.x / LD;
-    if (row >= n || s >= S || (bc && bc[row])) continue;
+    // the same in every lane of the row's group (the group's shuffles need all of it)
+    const bool live = row < n && !(bc && bc[row]);
+    const bool act = live && s < S;
+    if (!COOP && !act) continue;
     // the row's vector entries first: they do not depend on the CSR walk, so their loads
     // are in flight during it
-    const int64_t i = row * LD + s;
-    const double u = U[i], dg = diag[i], bi = b[i], ou = opU[i];
-    double dv[M], im[M];
+    const int64_t i = (live ? row : 0) * LD + s;
+    double u = 0.0, dg = 0.0, bi = 0.0, ou = 0.0, dv[M], im[M];
 #pragma unroll
-    for (int k = 0; k < M; k++) {
-      dv[k] = dirs.d[k][i];
-      im[k] = k < NG ? 0.0 : dirs.img[k][i];
+    for (int k = 0; k < M; k++) dv[k] = im[k] = 0.0;
+    if (act) {
+      u = U[i], dg = diag[i], bi = b[i], ou = opU[i];
+#pragma unroll
+      for (int k = 0; k < M; k++) {
+        dv[k] = dirs.d[k][i];
+        im[k] = k < NG ? 0.0 : dirs.img[k][i];
+      }
     }
-    double kd[NG > 0 ? NG : 1];
+    double kd[NGA];
 #pragma unroll
-    for (int k = 0; k < NG; k++) kd[k] = 0.0;
-    const int beg = indptr[row], end = indptr[row + 1];
-    // four entries at a time: their index, value and gathers in flight together; the
-    // sums still run entry by entry in CSR order
-    constexpr int RP = 4;
-    for (int p0 = beg; p0 < end; p0 += RP) {
-      int64_t jj[RP];
-      double kv[RP], dvv[RP][NG > 0 ? NG : 1];
+    for (int k = 0; k < NGA; k++) kd[k] = 0.0;
+    if constexpr (COOP) {
+      double kg[NGA][LD];
 #pragma unroll
-      for (int u = 0; u < RP; u++) {
-        const bool in = p0 + u < end;
-        const int j = in ? __ldg(indices + p0 + u) : 0;
-        kv[u] = (in && !(bc && bc[j])) ? __ldg(K + p0 + u) : 0.0;
-        jj[u] = (int64_t)j * LD + s;
+      for (int k = 0; k < NGA; k++)
+#pragma unroll
+        for (int c = 0; c < LD; c++) kg[k][c] = 0.0;
+      if (live) {
+        const int beg = indptr[row], end = indptr[row + 1];
+        constexpr int RP = 4;
+        for (int p0 = beg; p0 < end; p0 += LD * RP) {
+          int jj[RP];
+          double kv[RP];
+#pragma unroll
+          for (int v = 0; v < RP; v++) {
+            const int p = p0 + s + v * LD;
+            const bool in = p < end;
+            jj[v] = in ? __ldg(indices + p) : 0;
+            kv[v] = (in && !(bc && bc[jj[v]])) ? __ldg(K + p) : 0.0;
+          }
+#pragma unroll
+          for (int v = 0; v < RP; v++) {
+            if (p0 + s + v * LD < end) {
+#pragma unroll
+              for (int k = 0; k < NGA; k++) {
+                double g[LD];
+                ldv<double, LD>(dirs.d[k], jj[v], g);
+#pragma unroll
+                for (int c = 0; c < LD; c++) kg[k][c] += kv[v] * g[c];
+              }
+            }
+          }
+        }
       }
 #pragma unroll
-      for (int u = 0; u < RP; u++)
+      for (int o = 1; o < LD; o <<= 1)
 #pragma unroll
-        for (int k = 0; k < NG; k++) dvv[u][k] = __ldg(dirs.d[k] + jj[u]);
+        for (int k = 0; k < NGA; k++)
 #pragma unroll
-      for (int u = 0; u < RP; u++) {
-        if (p0 + u >= end) break;
+          for (int c = 0; c < LD; c++) kg[k][c] += __shfl_xor_sync(0xffffffffu, kg[k][c], o);
+      if (!act) continue;
 #pragma unroll
-        for (int k = 0; k < NG; k++) kd[k] += kv[u] * dvv[u][k];
+      for (int k = 0; k < NGA; k++)
+#pragma unroll
+        for (int c = 0; c < LD; c++)
+          if (c == s) kd[k] = kg[k][c];
+    } else {
+      const int beg = indptr[row], end = indptr[row + 1];
+      // four entries at a time: their index, value and gathers in flight together; the
+      // sums still run entry by entry in CSR order
+      constexpr int RP = 4;
+      for (int p0 = beg; p0 < end; p0 += RP) {
+        int64_t jj[RP];
+        double kv[RP], dvv[RP][NGA];
+#pragma unroll
+        for (int v = 0; v < RP; v++) {
+          const bool in = p0 + v < end;
+          const int j = in ? __ldg(indices + p0 + v) : 0;
+          kv[v] = (in && !(bc && bc[j])) ? __ldg(K + p0 + v) : 0.0;
+          jj[v] = (int64_t)j * LD + s;
+        }
+#pragma unroll
+        for (int v = 0; v < RP; v++)
+#pragma unroll
+          for (int k = 0; k < NG; k++) dvv[v][k] = __ldg(dirs.d[k] + jj[v]);
+#pragma unroll
+        for (int v = 0; v < RP; v++) {
+          if (p0 + v >= end) break;
+#pragma unroll
+          for (int k = 0; k < NG; k++) kd[k] += kv[v] * dvv[v][k];
+        }
       }
     }
     const double r0 = bi - (ou + dg * u);
