@@ -72,23 +72,44 @@ __device__ __forceinline__ void mma_bf16(float c[4], uint32_t a0, uint32_t a1, u
       : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-// all NFEAT normalised features of row r = v * S + s (r < number of rows), branch-free
-__device__ __forceinline__ void row_features(const MlpFeat& F, int64_t v, int s,
-                                             float f[NFEAT]) {
+// the fields row r = v * S + s reads (r < number of rows)
+struct RowFields {
+  double u, up, phi, ngphi, opu, opdu;
+};
+
+__device__ __forceinline__ RowFields row_fields(const MlpFeat& F, int64_t v, int s) {
   const int64_t i = v * F.ld + s;
-  const double u = F.U[i], up = F.Up[i];
+  RowFields x;
+  x.u = F.U[i];
+  x.up = F.Up[i];
+  x.phi = F.phi ? F.phi[v] : 0.0;
+  x.ngphi = F.ngphi ? F.ngphi[v] : 0.0;
+  x.opu = F.opU ? F.opU[i] : 0.0;
+  x.opdu = F.opDU ? F.opDU[i] : 0.0;
+  return x;
+}
+
+// all NFEAT normalised features of a row from its fields, branch-free
+__device__ __forceinline__ void fields_features(const MlpFeat& F, const RowFields& r, int s,
+                                                float f[NFEAT]) {
   float x[NFEAT];
-  x[0] = F.phi ? (float)F.phi[v] : 0.0f;
-  x[1] = F.ngphi ? (float)F.ngphi[v] : 0.0f;
-  x[2] = (float)u;
-  x[3] = (float)up;
-  x[4] = (float)(u - up);
+  x[0] = (float)r.phi;
+  x[1] = (float)r.ngphi;
+  x[2] = (float)r.u;
+  x[3] = (float)r.up;
+  x[4] = (float)(r.u - r.up);
   x[5] = F.logD[s];
   x[6] = F.k[s];
-  x[8] = F.opU ? (float)F.opU[i] : 0.0f;
-  x[9] = F.opDU ? (float)F.opDU[i] : 0.0f;
+  x[7] = 0.0f;
+  x[8] = (float)r.opu;
+  x[9] = (float)r.opdu;
 #pragma unroll
   for (int k = 0; k < NFEAT; k++) f[k] = (k == 7) ? 1.0f : (x[k] - F.mean[k]) * F.istd[k];
+}
+
+__device__ __forceinline__ void row_features(const MlpFeat& F, int64_t v, int s,
+                                             float f[NFEAT]) {
+  fields_features(F, row_fields(F, v, s), s, f);
 }
 
 // shared-memory copy of the BF16 weights
@@ -338,17 +359,31 @@ __global__ void __launch_bounds__(TC_M) k_mlp_predict(MlpFeat F, int64_t nrows,
   const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
   uint32_t phase = 0;
   const int64_t ntiles = (nrows + TC_M - 1) / TC_M;
+  // (vertex, species) of this thread's row of a tile (vertex 0 past the last row)
+  auto row_of = [&](int64_t tile, int64_t& v, int& s) {
+    const int64_t r = tile * TC_M + tid;
+    // 32-bit division while the row index fits
+    v = r >= nrows ? 0
+                   : (r < (int64_t)UINT32_MAX ? (int64_t)((uint32_t)r / (uint32_t)F.S) : r / F.S);
+    s = r >= nrows ? 0 : (int)(r - v * F.S);
+  };
+  // the fields of the CTA's first tile; every tile's MMAs overlap the next tile's loads
+  RowFields cur{};
+  if (blockIdx.x < ntiles) {
+    int64_t v0;
+    int s0;
+    row_of(blockIdx.x, v0, s0);
+    cur = row_fields(F, v0, s0);
+  }
   for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int64_t r = tile * TC_M + tid;
     const bool in = r < nrows;
-    // 32-bit division while the row index fits
-    const int64_t v = !in ? 0
-                          : (r < (int64_t)UINT32_MAX ? (int64_t)((uint32_t)r / (uint32_t)F.S)
-                                                     : r / F.S);
-    const int s = in ? (int)(r - v * F.S) : 0;
+    int64_t v;
+    int s;
+    row_of(tile, v, s);
     {
       float f[NFEAT];
-      row_features(F, v, s, f);
+      fields_features(F, cur, s, f);
       uint32_t w[8];
 #pragma unroll
       for (int k = 0; k < 8; k++) {
@@ -366,6 +401,13 @@ __global__ void __launch_bounds__(TC_M) k_mlp_predict(MlpFeat F, int64_t nrows,
     if (tid == 0 && !tw.skip_issue) {
       tc_mma(taddr, tc_desc(sm.A1), tc_desc(sm.W1), 0);
       tc_commit(&sm.bar);
+    }
+    RowFields nxt{};
+    if (tile + gridDim.x < ntiles) {
+      int64_t vn;
+      int sn;
+      row_of(tile + gridDim.x, vn, sn);
+      nxt = row_fields(F, vn, sn);
     }
     bool ok = tc_wait(&sm.bar, phase, tw.polls);
     phase ^= 1u;
@@ -413,7 +455,7 @@ __global__ void __launch_bounds__(TC_M) k_mlp_predict(MlpFeat F, int64_t nrows,
     if (in && ok) {
       if (x_out) {
         const int64_t i = v * F.ld + s;
-        const double b = F.base == 1 ? 2.0 * F.U[i] - F.Up[i] : (F.base == 0 ? F.U[i] : 0.0);
+        const double b = F.base == 1 ? 2.0 * cur.u - cur.up : (F.base == 0 ? cur.u : 0.0);
         x_out[i] = b + (double)sigma * (double)y;
       } else {
         y_out[r] = y;
@@ -425,6 +467,7 @@ __global__ void __launch_bounds__(TC_M) k_mlp_predict(MlpFeat F, int64_t nrows,
       if (tid == 0) tc_timed_out(tw);
       break;
     }
+    cur = nxt;
   }
   tc_fence_before();
   __syncthreads();
