@@ -45,8 +45,8 @@ PARITY_STEPS = 3
 # relative residual of the oracle's Jacobi-PCG solves that stand in for exact solutions
 ORACLE_RTOL = 1e-12
 # measured with ncu on this workload (see profiles/); None until captured
-# (k_cgw: 2.627 GB over a 258-iteration launch; k_pcgp: 130.6 MB over a 334-iteration launch)
-DRAM_BYTES_PER_ITERATION = {"k_cgw": 10.2e6, "k_pcgp": 0.391e6}
+# (k_cgw: 2.627 GB over a 258-iteration launch; k_pcgp: 133.5 MB over a 334-iteration launch)
+DRAM_BYTES_PER_ITERATION = {"k_cgw": 10.2e6, "k_pcgp": 0.400e6}
 WORKLOAD = ("3-species backward-Euler step, 64^3 Kuhn cube (1,572,864 P1 tets, 274,625 "
             "vertices), jitter 0.2h, De = D_s exp(0.3 xi), rtol 1e-8")
 
@@ -507,6 +507,9 @@ def kernel_table(m, coef, u0, flush):
                                          n * (16 + 64 + 8) + V * 24 + nnz * 12),
         "rhs_3col": (lambda: _lib.call("tp_assemble_rhs", tpm, 3, 4, ptr(U), None, 50.0, 1, 0,
                                        None, None, ptr(b), st), n * 24 + V * 64),
+        # consistent mass: cell vertices (16 B) and |detJ| (8 B) per cell, u and b per vertex
+        "rhs_3col_consistent": (lambda: _lib.call("tp_assemble_rhs", tpm, 3, 4, ptr(U), None, 50.0,
+                                                  0, 0, None, None, ptr(b), st), n * 24 + V * 64),
         "matfree_3col_fp64": (lambda: _lib.call("tp_matfree_apply", tpm, 3, 4, 0, ptr(De), None,
                                                 ds, sh, 50.0, 0, 0, ptr(x64), ptr(y64), st),
                               n * 40 + V * 72),
@@ -517,7 +520,8 @@ def kernel_table(m, coef, u0, flush):
     out = {}
     # the row walk the tiled kernels replaced (same results), for comparison
     rows_walk = {"assemble_full_fp64_row_walk": rows["assemble_full_fp64"],
-                 "assemble_stiffness_fp64_fp32_row_walk": rows["assemble_stiffness_fp64_fp32"]}
+                 "assemble_stiffness_fp64_fp32_row_walk": rows["assemble_stiffness_fp64_fp32"],
+                 "rhs_3col_consistent_row_walk": rows["rhs_3col_consistent"]}
     tile_rows = dm.tile_rows
     dm.set_tiles(0)
     for name, (fn, nbytes) in rows_walk.items():

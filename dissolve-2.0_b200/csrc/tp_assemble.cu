@@ -592,10 +592,15 @@ __global__ void k_rhs_rows(int64_t nv, int S, int ld, const int32_t* __restrict_
   }
 }
 
-// Lumped right-hand side on row tiles: the tile's cells' lumped-mass factors
-// Ld = (|detJ| / 120) 5 in shared memory, then each tile row sums Ld (inv_dt u + f) over its
-// cells in ascending order -- the same ordered sums as k_rhs_rows (lumped branch).
+// Right-hand side on row tiles: the tile's cells' factors in shared memory, then each
+// tile row sums its cells in ascending order -- the same ordered sums, with the same
+// rounding, as k_rhs_rows.  Lumped: one slot per cell, Ld = (|detJ| / 120) 5, and the row
+// adds Ld (inv_dt u + f).  Consistent: a slot of CW = 6 (10 with f) doubles per cell,
+// [base dt^-1, base, sum of u over the cell's vertices (4 columns), the same for f], base =
+// |detJ| / 120, and the row adds base dt^-1 (su + u_r) + base (sf + f_r).
+template <bool LUMPED>
 __global__ void __launch_bounds__(256) k_rhs_tiles(TileView tv, int S, int ld,
+                                                   const int32_t* __restrict__ cells,
                                                    const double* __restrict__ geo,
                                                    const double* __restrict__ u,
                                                    const double* __restrict__ f, double inv_dt,
@@ -603,27 +608,60 @@ __global__ void __launch_bounds__(256) k_rhs_tiles(TileView tv, int S, int ld,
   extern __shared__ double sm_ld[];
   const int R = tv.R, T = blockDim.x, t = blockIdx.x, tid = threadIdx.x;
   const int c0 = __ldg(tv.cell_ptr + t), m = __ldg(tv.cell_ptr + t + 1) - c0;
+  const int CW = LUMPED ? 1 : (f ? 10 : 6);
   {
     constexpr int MAXC = 4;
     int64_t cid[MAXC];
     double dj[MAXC];
+    int4 cv[MAXC];
 #pragma unroll
     for (int k = 0; k < MAXC; k++) {
       const int i = tid + k * T;
       cid[k] = (i < m) ? (int64_t)__ldg(tv.cells + c0 + i) : -1;
     }
 #pragma unroll
-    for (int k = 0; k < MAXC; k++) dj[k] = (cid[k] >= 0) ? __ldg(geo + 8 * cid[k] + 6) : 0.0;
+    for (int k = 0; k < MAXC; k++) {
+      dj[k] = (cid[k] >= 0) ? __ldg(geo + 8 * cid[k] + 6) : 0.0;
+      if constexpr (!LUMPED)
+        cv[k] = (cid[k] >= 0) ? __ldg(reinterpret_cast<const int4*>(cells) + cid[k])
+                              : make_int4(0, 0, 0, 0);
+    }
+    auto put = [&](int i, double djv, const int4& c4) {
+      double* slot = sm_ld + (size_t)i * CW;
+      if constexpr (LUMPED) {
+        slot[0] = __dmul_rn(__ddiv_rn(djv, 120.0), 5.0);
+      } else {
+        const double base = __ddiv_rn(djv, 120.0);
+        slot[0] = __dmul_rn(base, inv_dt);
+        slot[1] = base;
+#pragma unroll
+        for (int s = 0; s < 4; s++) {
+          if (s >= S) break;
+          slot[2 + s] = __dadd_rn(
+              __dadd_rn(__dadd_rn(__ldg(u + (int64_t)c4.x * ld + s), __ldg(u + (int64_t)c4.y * ld + s)),
+                        __ldg(u + (int64_t)c4.z * ld + s)),
+              __ldg(u + (int64_t)c4.w * ld + s));
+          if (f)
+            slot[6 + s] = __dadd_rn(
+                __dadd_rn(__dadd_rn(__ldg(f + (int64_t)c4.x * ld + s), __ldg(f + (int64_t)c4.y * ld + s)),
+                          __ldg(f + (int64_t)c4.z * ld + s)),
+                __ldg(f + (int64_t)c4.w * ld + s));
+        }
+      }
+    };
 #pragma unroll
     for (int k = 0; k < MAXC; k++)
-      if (cid[k] >= 0) sm_ld[tid + k * T] = __dmul_rn(__ddiv_rn(dj[k], 120.0), 5.0);
-    for (int i = tid + MAXC * T; i < m; i += T)
-      sm_ld[i] = __dmul_rn(__ddiv_rn(__ldg(geo + 8 * (int64_t)__ldg(tv.cells + c0 + i) + 6), 120.0), 5.0);
+      if (cid[k] >= 0) put(tid + k * T, dj[k], cv[k]);
+    for (int i = tid + MAXC * T; i < m; i += T) {
+      const int64_t c = __ldg(tv.cells + c0 + i);
+      put(i, __ldg(geo + 8 * c + 6),
+          LUMPED ? make_int4(0, 0, 0, 0) : __ldg(reinterpret_cast<const int4*>(cells) + c));
+    }
   }
   // the row's first 24 terms and its u, f are loaded before the barrier (in flight with
   // the loads above)
   int64_t r = -1;
-  double w[4] = {0.0, 0.0, 0.0, 0.0};
+  double w[4] = {0.0, 0.0, 0.0, 0.0}, fr[4] = {0.0, 0.0, 0.0, 0.0};
   const uint4* dv = nullptr;
   int KD = 0;
   const uint4 none4 = make_uint4(0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu);
@@ -638,9 +676,15 @@ __global__ void __launch_bounds__(256) k_rhs_tiles(TileView tv, int S, int ld,
       if (8 * g < KD) dq[g] = __ldg(dv + g);
     if (r >= 0) {
 #pragma unroll
-      for (int s = 0; s < 4; s++)
-        if (s < S)
+      for (int s = 0; s < 4; s++) {
+        if (s >= S) continue;
+        if constexpr (LUMPED) {
           w[s] = __dadd_rn(__dmul_rn(inv_dt, u[r * ld + s]), f ? f[r * ld + s] : 0.0);
+        } else {
+          w[s] = u[r * ld + s];  // u_r
+          fr[s] = f ? f[r * ld + s] : 0.0;
+        }
+      }
     }
   }
   __syncthreads();
@@ -651,10 +695,22 @@ __global__ void __launch_bounds__(256) k_rhs_tiles(TileView tv, int S, int ld,
     for (int k = 0; k < 8; k++) {
       const uint32_t tm = term_of(g8, k);
       if (tm == TILE_TERM_NONE) return false;
-      const double Ld = sm_ld[tm & ((1 << TILE_LOC_BITS) - 1)];
+      const double* slot = sm_ld + (size_t)(tm & ((1 << TILE_LOC_BITS) - 1)) * CW;
+      if constexpr (LUMPED) {
+        const double Ld = slot[0];
 #pragma unroll
-      for (int s = 0; s < 4; s++)
-        if (s < S) acc[s] = __dadd_rn(acc[s], __dmul_rn(Ld, w[s]));
+        for (int s = 0; s < 4; s++)
+          if (s < S) acc[s] = __dadd_rn(acc[s], __dmul_rn(Ld, w[s]));
+      } else {
+        const double mdt = slot[0], base = slot[1];
+#pragma unroll
+        for (int s = 0; s < 4; s++) {
+          if (s >= S) continue;
+          const double sf = f ? slot[6 + s] : 0.0;
+          acc[s] = __dadd_rn(acc[s], __dadd_rn(__dmul_rn(mdt, __dadd_rn(slot[2 + s], w[s])),
+                                               __dmul_rn(base, __dadd_rn(sf, fr[s]))));
+        }
+      }
     }
     return true;
   };
@@ -1233,14 +1289,21 @@ extern "C" int tp_assemble_rhs(const tp_mesh* m, int S, int ld, const double* u_
   TP_REQUIRE(mesh_ok(m) && u_old && b, "null pointer");
   TP_REQUIRE(S >= 1 && S <= TP_MAX_COLS && ld >= S && ld <= TP_MAX_COLS, "bad S/ld");
   cudaStream_t st = as_stream(stream);
-  if (m->n_verts > 0 && lumped && m->tiles && m->tiles->v.n_tiles > 0 &&
-      m->tiles->v.R <= 256) {
+  int optin = 0;
+  if (m->n_verts > 0 && m->tiles && m->tiles->v.n_tiles > 0 && m->tiles->v.R <= 256) {
+    int dev = 0;
+    TP_CUDA_TRY(cudaGetDevice(&dev));
+    TP_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  }
+  const size_t cw = lumped ? 1 : (f ? 10 : 6);  // k_rhs_tiles' slot width
+  const size_t smem_t = m->tiles ? sizeof(double) * cw * (size_t)std::max(m->tiles->v.max_cells, 1) : 0;
+  if (m->n_verts > 0 && m->tiles && m->tiles->v.n_tiles > 0 && m->tiles->v.R <= 256 &&
+      smem_t <= (size_t)optin) {
     const TileView& tv = m->tiles->v;
-    const size_t smem = sizeof(double) * (size_t)std::max(tv.max_cells, 1);
-    if (smem > 48 * 1024)
-      TP_CUDA_TRY(cudaFuncSetAttribute(k_rhs_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem));
-    k_rhs_tiles<<<tv.n_tiles, 256, smem, st>>>(tv, S, ld, m->geo, u_old, f, inv_dt, b);
+    auto fn = lumped ? k_rhs_tiles<true> : k_rhs_tiles<false>;
+    if (smem_t > 48 * 1024)
+      TP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_t));
+    fn<<<tv.n_tiles, 256, smem_t, st>>>(tv, S, ld, m->cells, m->geo, u_old, f, inv_dt, b);
     TP_LAUNCH_CHECK();
   } else if (m->n_verts > 0) {
     k_rhs_rows<<<grid_for(m->n_verts, 128, 65535), 128, 0, st>>>(

@@ -3,7 +3,8 @@ through the C ABI.
 
 Bar: bit-identical outputs -- both sum every row's cells in ascending cell order with the
 same rounding -- for every assembly mode, lumped and consistent mass, Dirichlet rows, the
-FP32 copies, the SELL-32 values and lumped diagonals of the batched step, on a jittered
+FP32 copies, the SELL-32 values and lumped diagonals of the batched step, the lumped and
+consistent right-hand sides, on a jittered
 Kuhn cube and on the same mesh with its vertices and cells renumbered at random, for
 tiles of 32, 64 and 128 rows."""
 import ctypes
@@ -103,8 +104,10 @@ def test_tiled_stiffness_diag_equals_row_walk(mesh, S):
         assert np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("S,ld,with_f", [(1, 1, False), (3, 4, True), (2, 2, True)])
-def test_tiled_lumped_rhs_equals_row_walk(mesh, S, ld, with_f):
+@pytest.mark.parametrize("lumped", [1, 0])
+@pytest.mark.parametrize("S,ld,with_f", [(1, 1, False), (3, 4, True), (2, 2, True),
+                                         (3, 4, False)])
+def test_tiled_rhs_equals_row_walk(mesh, S, ld, with_f, lumped):
     import torch
 
     from dissolve_tp import _lib
@@ -122,7 +125,7 @@ def test_tiled_lumped_rhs_equals_row_walk(mesh, S, ld, with_f):
     for tiles in (0, 64):
         dm.set_tiles(tiles)
         b = torch.full((dm.n_verts, ld), -7.0, dtype=torch.float64, device=dev)
-        _lib.call("tp_assemble_rhs", ctypes.byref(dm.tpm), S, ld, ptr(u), ptr(f), 50.0, 1,
+        _lib.call("tp_assemble_rhs", ctypes.byref(dm.tpm), S, ld, ptr(u), ptr(f), 50.0, lumped,
                   bc.size, ptr(bcd), vals, ptr(b), stream_handle())
         outs.append(b.cpu().numpy())
     assert np.array_equal(outs[0], outs[1])
