@@ -194,16 +194,25 @@ __device__ __forceinline__ void sts2(double* p, double a, double b) {
   *reinterpret_cast<double2*>(p) = make_double2(a, b);
 }
 
-template <int MODE, bool DIAG>
+// CMP (compact, DIAG without per-cell alpha): ew = 11, the slot keeps only the cell's
+// lumped-mass factor Ld at 10 (each column's term shift_s Ld is formed where it is summed,
+// with the same rounding); the odd stride leaves slots 8-byte aligned only, so every
+// access is a single double.
+template <int MODE, bool DIAG, bool CMP = false>
 __device__ __forceinline__ void tile_cell_entries(double* slot, bool has_alpha, double inv_dt,
                                                   int lumped, const RowExtras& ex,
                                                   const double dsh[4]) {
   // the whole raw record first (the entries overwrite it)
   double r[10];
+  if constexpr (CMP) {
 #pragma unroll
-  for (int k = 0; k < 5; k++) lds2(slot + 2 * k, r[2 * k], r[2 * k + 1]);
+    for (int k = 0; k < 10; k++) r[k] = slot[k];
+  } else {
+#pragma unroll
+    for (int k = 0; k < 5; k++) lds2(slot + 2 * k, r[2 * k], r[2 * k + 1]);
+  }
   double alc[4] = {0.0, 0.0, 0.0, 0.0};
-  if constexpr (DIAG) {
+  if constexpr (DIAG && !CMP) {
     if (ex.alpha) {
       alc[0] = r[9];
 #pragma unroll
@@ -225,9 +234,16 @@ __device__ __forceinline__ void tile_cell_entries(double* slot, bool has_alpha, 
     for (int j = li; j < 4; j++)
       e[tri_index(li, j)] = elem_entry<MODE>(kr, li, j, g.dJ, ks, react, lumped);
   }
+  if constexpr (CMP) {
 #pragma unroll
-  for (int k = 0; k < 5; k++) sts2(slot + 2 * k, e[2 * k], e[2 * k + 1]);
-  if constexpr (DIAG) {
+    for (int k = 0; k < 10; k++) slot[k] = e[k];
+  } else {
+#pragma unroll
+    for (int k = 0; k < 5; k++) sts2(slot + 2 * k, e[2 * k], e[2 * k + 1]);
+  }
+  if constexpr (DIAG && CMP) {
+    slot[10] = __dmul_rn(__ddiv_rn(g.dJ, 120.0), 5.0);
+  } else if constexpr (DIAG) {
     const double Ld = __dmul_rn(__ddiv_rn(g.dJ, 120.0), 5.0);
     double dt[4];
 #pragma unroll
@@ -249,7 +265,7 @@ __device__ __forceinline__ uint32_t term_of(const uint4& v, int k) {
   return (k & 1) ? (w >> 16) : (w & 0xffffu);
 }
 
-template <int MODE, bool DIAG>
+template <int MODE, bool DIAG, bool CMP = false>
 __global__ void __launch_bounds__(TILE_BLOCK, 3) k_assemble_tiles(
     TileView tv, const double* __restrict__ geo, const double* __restrict__ De,
     const double* __restrict__ alpha, double inv_dt, int lumped,
@@ -284,14 +300,21 @@ __global__ void __launch_bounds__(TILE_BLOCK, 3) k_assemble_tiles(
       for (int k = 0; k < 4; k++) {
         const int j = (lane >> 2) + 8 * k;
         const int64_t c = __shfl_sync(0xffffffffu, cid[u], j);
-        if (ib + j < m) cp_async<16>(E + (size_t)(ib + j) * ew + 2 * h, geo + 8 * c + 2 * h);
+        if (ib + j < m) {
+          if constexpr (CMP) {
+            cp_async<8>(E + (size_t)(ib + j) * ew + 2 * h, geo + 8 * c + 2 * h);
+            cp_async<8>(E + (size_t)(ib + j) * ew + 2 * h + 1, geo + 8 * c + 2 * h + 1);
+          } else {
+            cp_async<16>(E + (size_t)(ib + j) * ew + 2 * h, geo + 8 * c + 2 * h);
+          }
+        }
       }
       if (cid[u] >= 0) {
         double* slot = E + (size_t)(ib + lane) * ew;
         const int64_t c = cid[u];
         if (MODE != TP_ASM_MASS) cp_async<8>(slot + 8, De + c);
         if (MODE == TP_ASM_FULL && alpha) cp_async<8>(slot + 9, alpha + c);
-        if constexpr (DIAG) {
+        if constexpr (DIAG && !CMP) {
           if (ex.alpha)
             for (int s = 0; s < ex.ld; s++) cp_async<8>(slot + 9 + s, ex.alpha + c * ex.ld + s);
         }
@@ -300,11 +323,16 @@ __global__ void __launch_bounds__(TILE_BLOCK, 3) k_assemble_tiles(
     for (int i = tid + MAXC * T; i < m; i += T) {  // tiles of more than MAXC * T cells
       const int64_t c = __ldg(tv.cells + c0 + i);
       double* slot = E + (size_t)i * ew;
+      if constexpr (CMP) {
 #pragma unroll
-      for (int h = 0; h < 4; h++) cp_async<16>(slot + 2 * h, geo + 8 * c + 2 * h);
+        for (int h = 0; h < 8; h++) cp_async<8>(slot + h, geo + 8 * c + h);
+      } else {
+#pragma unroll
+        for (int h = 0; h < 4; h++) cp_async<16>(slot + 2 * h, geo + 8 * c + 2 * h);
+      }
       if (MODE != TP_ASM_MASS) cp_async<8>(slot + 8, De + c);
       if (MODE == TP_ASM_FULL && alpha) cp_async<8>(slot + 9, alpha + c);
-      if constexpr (DIAG) {
+      if constexpr (DIAG && !CMP) {
         if (ex.alpha)
           for (int s = 0; s < ex.ld; s++) cp_async<8>(slot + 9 + s, ex.alpha + c * ex.ld + s);
       }
@@ -344,7 +372,8 @@ __global__ void __launch_bounds__(TILE_BLOCK, 3) k_assemble_tiles(
   // ... and each thread turns the records it copied into element entries in place
   cp_async_wait_all();
   for (int i = tid; i < m; i += T)
-    tile_cell_entries<MODE, DIAG>(E + (size_t)i * ew, alpha != nullptr, inv_dt, lumped, ex, dsh);
+    tile_cell_entries<MODE, DIAG, CMP>(E + (size_t)i * ew, alpha != nullptr, inv_dt, lumped, ex,
+                                       dsh);
   __syncthreads();
 
   // ---- phase B1: the diagonal of each tile row
@@ -360,7 +389,12 @@ __global__ void __launch_bounds__(TILE_BLOCK, 3) k_assemble_tiles(
           const int loc = tm & ((1 << TILE_LOC_BITS) - 1), li = tm >> TILE_LOC_BITS;
           const double* e = E + (size_t)loc * ew;
           dacc = __dadd_rn(dacc, e[tri_index(li, li)]);
-          if constexpr (DIAG) {
+          if constexpr (DIAG && CMP) {
+            // the term tile_cell_entries forms without per-cell alpha, (shift_s + 0) Ld
+#pragma unroll
+            for (int s = 0; s < 4; s++)
+              if (s < ex.S) dg[s] = __dadd_rn(dg[s], __dmul_rn(__dadd_rn(dsh[s], 0.0), e[10]));
+          } else if constexpr (DIAG) {
 #pragma unroll
             for (int s = 0; s < 4; s++)
               if (s < ex.S) dg[s] = __dadd_rn(dg[s], e[10 + s]);
@@ -1148,16 +1182,24 @@ static int launch_tiles(const tp_mesh* m, const double* De, const double* alpha,
   *used = false;
   if (!m->tiles) return TP_OK;
   const TileView& tv = m->tiles->v;
-  // slot of 5 or 7 sixteen-byte units (tile_cell_entries)
-  const int ew = DIAG ? 14 : 10;
+  // slot of 5 or 7 sixteen-byte units (tile_cell_entries), or 11 doubles for DIAG without
+  // per-cell alpha (three CTAs of the largest tiles per SM instead of two)
+  const bool cmp = DIAG && ex.alpha == nullptr;
+  const int ew = DIAG ? (cmp ? 11 : 14) : 10;
   const size_t smem = sizeof(double) * (size_t)tv.max_cells * ew;
   int dev = 0, optin = 0;
   TP_CUDA_TRY(cudaGetDevice(&dev));
   TP_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   if (smem > (size_t)optin || tv.R > TILE_BLOCK || tv.n_tiles == 0) return TP_OK;
-  auto fn = k_assemble_tiles<MODE, DIAG>;
+  auto fn = k_assemble_tiles<MODE, DIAG, false>;
+  if constexpr (DIAG) {
+    if (cmp) fn = k_assemble_tiles<MODE, DIAG, true>;
+  }
   if (smem > 48 * 1024)
     TP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (cmp)
+    TP_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared));
   fn<<<tv.n_tiles, TILE_BLOCK, smem, st>>>(tv, m->geo, De, alpha, inv_dt, lumped, bc_mask,
                                            m->indptr, out64, out32, ex, ew, m->n_verts);
   TP_LAUNCH_CHECK();
