@@ -7,7 +7,7 @@ correction to a base guess (u^n by default, or the linear extrapolation 2 u^n - 
 and the transport guess is the energy-norm projection onto span{u^n - u^{n-1}, that
 correction} around u^n (tp_guess_project).  The Krylov solve always
 runs to the same tolerance, so the guess only changes how many iterations it takes: the
-plain method is both the fallback (no predictor -> previous step) and the judge of the
+plain method is both the fallback (no predictor -> previous step) and the measure of the
 prediction's error.
 """
 from __future__ import annotations
