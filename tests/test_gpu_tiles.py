@@ -71,8 +71,10 @@ def test_tiled_assembly_equals_row_walk(mesh, tiles):
     assert info["rows_per_tile"] == tiles and info["n_tiles"] == -(-dm.n_verts // tiles)
 
 
+@pytest.mark.parametrize("with_alpha", [True, False])
 @pytest.mark.parametrize("S", [1, 3])
-def test_tiled_stiffness_diag_equals_row_walk(mesh, S):
+def test_tiled_stiffness_diag_equals_row_walk(mesh, S, with_alpha):
+    """Without per-cell alpha the tiles keep 88-byte cell slots (the lumped factor alone)."""
     import torch
 
     from dissolve_tp.assembler import DeviceMesh
@@ -96,7 +98,8 @@ def test_tiled_stiffness_diag_equals_row_walk(mesh, S):
         s32 = torch.full((sell.n_entries,), -7.0, dtype=torch.float32, device=dev)
         d64 = torch.full((dm.n_verts, ld), -7.0, dtype=torch.float64, device=dev)
         d32 = torch.full((dm.n_verts, ld), -7.0, dtype=torch.float32, device=dev)
-        _lib.call("tp_assemble_stiffness_diag", ctypes.byref(dm.tpm), ptr(De), S, ld, ptr(alpha),
+        _lib.call("tp_assemble_stiffness_diag", ctypes.byref(dm.tpm), ptr(De), S, ld,
+                  ptr(alpha) if with_alpha else None,
                   shift, ptr(bc), ptr(o64), ptr(o32), ptr(sell.slice_ptr), ptr(s32), ptr(d64),
                   ptr(d32), stream_handle())
         outs.append([t.cpu().numpy() for t in (o64, o32, s32, d64, d32)])
