@@ -303,19 +303,22 @@ __device__ __forceinline__ void proxy_fence() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-// 16 consecutive FP32 columns of this thread's TMEM lane
-__device__ __forceinline__ void tc_ld16(uint32_t taddr, float v[16]) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
-      "%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
+// 64 consecutive FP32 columns of this thread's TMEM lane: four loads in flight, one wait
+__device__ __forceinline__ void tc_ld64(uint32_t taddr, float v[64]) {
+  uint32_t r[64];
+#pragma unroll
+  for (int j = 0; j < 4; j++)
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+        "%14,%15}, [%16];"
+        : "=r"(r[16 * j + 0]), "=r"(r[16 * j + 1]), "=r"(r[16 * j + 2]), "=r"(r[16 * j + 3]),
+          "=r"(r[16 * j + 4]), "=r"(r[16 * j + 5]), "=r"(r[16 * j + 6]), "=r"(r[16 * j + 7]),
+          "=r"(r[16 * j + 8]), "=r"(r[16 * j + 9]), "=r"(r[16 * j + 10]), "=r"(r[16 * j + 11]),
+          "=r"(r[16 * j + 12]), "=r"(r[16 * j + 13]), "=r"(r[16 * j + 14]), "=r"(r[16 * j + 15])
+        : "r"(taddr + 16u * (uint32_t)j));
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-  for (int k = 0; k < 16; k++) v[k] = __uint_as_float(r[k]);
+  for (int k = 0; k < 64; k++) v[k] = __uint_as_float(r[k]);
 }
 
 // x_out[v, s] = B[v, s] + sigma * y(v, s)  (or y_out[r] = y when x_out is NULL).
@@ -413,10 +416,11 @@ __global__ void __launch_bounds__(TC_M) k_mlp_predict(MlpFeat F, int64_t nrows,
     phase ^= 1u;
     tc_fence_after();
     // h1 = relu(z1 + b1), BF16, into the layer-2 operand
+    float z1[64];
+    tc_ld64(taddr + lane_base, z1);
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-      float z[16];
-      tc_ld16(taddr + lane_base + 16 * j, z);
+      const float* z = z1 + 16 * j;
       uint32_t w[8];
 #pragma unroll
       for (int k = 0; k < 8; k++)
@@ -442,14 +446,12 @@ __global__ void __launch_bounds__(TC_M) k_mlp_predict(MlpFeat F, int64_t nrows,
     tc_fence_after();
     // layer 3 on the CUDA cores: BF16-rounded h2 . w3 + b3
     float y = 0.f;
+    {
+      float z2[64];
+      tc_ld64(taddr + lane_base + MLP_H, z2);
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-      float z[16];
-      tc_ld16(taddr + lane_base + MLP_H + 16 * j, z);
-#pragma unroll
-      for (int k = 0; k < 16; k++)
-        y += __bfloat162float(__float2bfloat16_rn(fmaxf(z[k] + sm.b2[16 * j + k], 0.f))) *
-             sm.w3[16 * j + k];
+      for (int k = 0; k < 64; k++)
+        y += __bfloat162float(__float2bfloat16_rn(fmaxf(z2[k] + sm.b2[k], 0.f))) * sm.w3[k];
     }
     y += sm.b3;
     if (in && ok) {
