@@ -45,8 +45,8 @@ PARITY_STEPS = 3
 # relative residual of the oracle's Jacobi-PCG solves that stand in for exact solutions
 ORACLE_RTOL = 1e-12
 # measured with ncu on this workload (see profiles/); None until captured
-# (k_cgw: 2.627 GB over a 258-iteration launch; k_pcgp: 130.7 MB over a 334-iteration launch)
-DRAM_BYTES_PER_ITERATION = {"k_cgw": 10.2e6, "k_pcgp": 0.391e6}
+# (k_cgw: 2.627 GB over a 258-iteration launch; k_pcgp: 131.4 MB over a 334-iteration launch)
+DRAM_BYTES_PER_ITERATION = {"k_cgw": 10.2e6, "k_pcgp": 0.393e6}
 WORKLOAD = ("3-species backward-Euler step, 64^3 Kuhn cube (1,572,864 P1 tets, 274,625 "
             "vertices), jitter 0.2h, De = D_s exp(0.3 xi), rtol 1e-8")
 
