@@ -2318,7 +2318,8 @@ __global__ void __launch_bounds__(512, 1) k_cgt(PArgs<float> a) {
 // product reads -- and on this problem size each costs a barrier plus an L2 round trip for
 // the partial sums.  The pipelined form carries the next product's input m = D^-1 w
 // through recurrences, so one barrier publishes m and the partial sums together, and the
-// reduction's round trip overlaps the product n = A m:
+// reduction's round trip and the lane decisions overlap the halo copies that the product
+// n = A m waits for:
 //
 //   barrier | halo copies of m and the partial-sum loads in flight;
 //           | gamma = r.u, delta = w.u, r.r totals; lane decisions; alpha, beta (while
