@@ -43,16 +43,20 @@ def _transport(T, monkeypatch, engine, S, m, coef, D, kk, dt, bcd, rtol=1e-8):
 @pytest.mark.parametrize("engine,S,bc,n", [("cgt", 3, False, 12), ("cgt", 2, True, 12),
                                            ("cgt", 4, False, 12), ("pipe", 3, False, 12),
                                            ("pipe", 2, True, 12), ("pipe", 3, False, 32),
-                                           ("cgt", 3, False, 32)])
+                                           ("pipe", 3, True, 32), ("cgt", 3, False, 32)])
 def test_tensor_memory_engine_matches_window_engine_and_oracle(cuda_device, monkeypatch, engine,
                                                                S, bc, n):
     """(the pipelined form holds at most 3 columns: 4 species run the "cgt" form).  At
     n = 32 every CTA holds several warps of rows, so a warp that updates the window while
-    another still reads it in the product would show."""
+    another still reads it in the product would show.  The n = 32 cases solve to rtol
+    1e-10: with Dirichlet rows a 1e-8 residual leaves 2-5e-7 relative error against the
+    exact solution in every engine (measured), so 1e-8 would test the stopping rule's
+    conditioning, not the engine."""
     from dissolve_tp import transport as T
     m, coef, D, kk, dt, u0, bcd = _problem(S, n=n, bc=bc)
-    fast = _transport(T, monkeypatch, engine, S, m, coef, D, kk, dt, bcd)
-    ref = _transport(T, monkeypatch, "cgw", S, m, coef, D, kk, dt, bcd)
+    rtol = 1e-10 if n > 16 else 1e-8
+    fast = _transport(T, monkeypatch, engine, S, m, coef, D, kk, dt, bcd, rtol=rtol)
+    ref = _transport(T, monkeypatch, "cgw", S, m, coef, D, kk, dt, bcd, rtol=rtol)
     detJ, G, JT = orc.geometry(m.coords, m.cells)
     ip, ix, sm = orc.csr_pattern(m.cells, m.n_verts)
     As = [orc.assemble(detJ, G, D[s] * coef, np.full(m.n_cells, kk[s]), 1 / dt, 1, sm, ix.size,
@@ -72,14 +76,18 @@ def test_tensor_memory_engine_matches_window_engine_and_oracle(cuda_device, monk
                                   bc_value=1.0)
             if n <= 16:
                 U[:, s] = orc.direct_solve(ip, ix, As[s], bs)
-            else:  # the oracle's FP64 Jacobi-PCG to 1e-12 (direct LU takes ~7 s a solve here)
-                U[:, s], _, st, _ = orc.pcg_jacobi(ip, ix, As[s], bs, U[:, s], 1e-12, bc_dofs=bcd)
+            else:  # the oracle's FP64 Jacobi-PCG to 1e-12 (direct LU takes ~7 s a solve here),
+                # started from a guess that holds the Dirichlet values (it never updates them)
+                x0 = U[:, s].copy()
+                if bcd is not None:
+                    x0[bcd] = 1.0
+                U[:, s], _, st, _ = orc.pcg_jacobi(ip, ix, As[s], bs, x0, 1e-12, bc_dofs=bcd)
                 assert st == 0
         uf, ur = fast.state(), ref.state()
         assert np.linalg.norm(uf - ur) / np.linalg.norm(ur) < (1e-9 if engine == "cgt" else 1e-7)
         assert np.linalg.norm(uf - U) / np.linalg.norm(U) < 1e-7
         for s in range(S):
-            assert rf["rnorm"][s] <= 1e-8 * rf["bnorm"][s], rf
+            assert rf["rnorm"][s] <= rtol * rf["bnorm"][s], rf
         if bcd is not None:
             assert np.all(uf[bcd] == 1.0)
 
